@@ -1,0 +1,153 @@
+"""Generate the golden fixtures in this folder from the reference's own sources.
+
+Runs only where the reference tree is mounted (it builds and loads
+oracle/_ref/libscp3ref.so, compiled from the reference's unmodified sources by
+oracle/Makefile).  The committed .npz files are what the tests read; nothing
+here runs on a GPU box.
+
+    python tests/golden/make_golden.py            # writes tests/golden/*.npz
+
+Fixtures:
+  sobol_ref.npz   i8_sobol uniforms (sobol.cpp:14198-27868) and std_normal draws
+                  (sobol.cpp:28706-28713), from index 0 and from the default skip 2^30
+                  (SCP3.cpp:48), 66 dimensions.
+  pes_ref.npz     qTIP4P/f and TTM3-F energies (qtip4pf.cpp:190-286, ttm3f.cpp:92-321)
+                  on the test-potentials.cpp:14-33 prism, relaxed dimer/prism, random
+                  3- and 4-water clusters and seeded perturbations of each.
+  hbuild_ref.npz  the -G sample loop (SCP3.cpp:187-232 with get_bra + dsyr2k,
+                  ScaledMatrixElements.cpp:870-971) for small dimer/hexamer bases,
+                  with the normal-mode inputs it used.
+"""
+import os
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from scp3_b200 import clusters, constants as C, modes  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("SCP3_REFERENCE", "/root/reference")
+
+# test-potentials.cpp:14-33, O H H order, Angstrom
+PRISM_TP = np.array([
+    -1.501133590, -0.197346710, 1.441262950, -2.000985830, -0.388094000, 2.232286820,
+    -0.613018210, -0.604501640, 1.565741520, -1.738921070, -0.356671650, -1.311647220,
+    -2.485655290, -0.756663570, -1.757003500, -1.883593590, -0.495826200, -0.359467970,
+    -0.590049110, 2.045369740, -0.113997110, -1.009913650, 1.627267800, -0.873288670,
+    -0.961441910, 1.549440890, 0.629166980, 0.999999910, -1.179514770, 1.454043080,
+    1.550433810, -0.395916830, 1.334139300, 1.004009200, -1.558530670, 0.559262460,
+    0.982946210, -1.411538550, -1.350690300, 1.478885410, -0.585694520, -1.278498130,
+    0.076249970, -1.127406420, -1.530339410, 1.967206930, 1.048112740, -0.137872390,
+    2.659992820, 1.698771500, -0.239214400, 1.124990980, 1.547180090, -0.146635510])
+
+
+def ref_energy(L, fn):
+    def f(X):
+        X = np.atleast_2d(X)
+        return np.array([getattr(L, fn)(x.size // 9, oracle._dp(np.ascontiguousarray(x))) for x in X])
+    return f
+
+
+def gen_sobol(L):
+    import ctypes
+    dims = 66
+    seed = ctypes.c_longlong(0)
+    u0 = np.zeros((64, dims))
+    for k in range(64):
+        L.ref_i8_sobol(dims, ctypes.byref(seed), oracle._dp(u0[k]))
+    seed = ctypes.c_longlong(1 << 30)
+    t = time.time()
+    u30 = np.zeros((8, dims))
+    for k in range(8):
+        L.ref_i8_sobol(dims, ctypes.byref(seed), oracle._dp(u30[k]))
+    print("skip walk %.1fs" % (time.time() - t))
+    seed = ctypes.c_longlong(1 << 30)
+    n30 = np.zeros((16, 48))
+    for k in range(16):
+        L.ref_std_normal(48, ctypes.byref(seed), oracle._dp(n30[k]))
+    np.savez_compressed(os.path.join(OUT, "sobol_ref.npz"), u_from0=u0, u_from2_30=u30, std_normal48_from2_30=n30)
+
+
+def gen_pes(L):
+    rng = np.random.default_rng(2024)
+    eq = ref_energy(L, "ref_qtip4pf_energy")
+    dimer, _, _, _ = clusters.relax(eq, clusters.dimer(), maxiter=400)
+    prism, _, _, _ = clusters.relax(eq, clusters.prism(), maxiter=400)
+    bases = [PRISM_TP, dimer, prism, clusters.random_cluster(3, 7), clusters.random_cluster(4, 11),
+             clusters.water().ravel()]
+    geoms = []
+    for b in bases:
+        geoms.append(b)
+        for _ in range(6):
+            geoms.append(b + rng.normal(scale=0.05, size=b.size))
+    names = []
+    eq_out, et_out = [], []
+    et = ref_energy(L, "ref_ttm3f_energy")
+    for g in geoms:
+        eq_out.append(eq(g)[0])
+        et_out.append(et(g)[0])
+        names.append(g.size // 9)
+    obj = np.empty(len(geoms), dtype=object)
+    obj[:] = geoms
+    np.savez_compressed(os.path.join(OUT, "pes_ref.npz"), geoms=obj, nw=np.array(names),
+                        e_qtip4pf=np.array(eq_out), e_ttm3f=np.array(et_out), allow_pickle=True)
+    return dimer, prism
+
+
+def setup_modes(L, x):
+    eq = ref_energy(L, "ref_qtip4pf_energy")
+    nw = x.size // 9
+    mass = np.tile(np.repeat([C.Omass, C.Hmass, C.Hmass], 3), nw)
+    H, x0 = clusters.hessian(eq, x, mass)
+    omega, MUa, _ = modes.normal_modes(H, mass)
+    return x0, MUa, omega
+
+
+def gen_hbuild(L, dimer, prism):
+    cases = {}
+    specs = [
+        # name, geometry, pes, modes, N2, N3, nsamples, block, scramble seed (None = reference Sobol from 2^30)
+        ("dimer_qtip4pf", dimer, 0, None, 12, 4, 2048, 256, 0x5C3),
+        ("dimer_qtip4pf_unscrambled", dimer, 0, None, 12, 0, 1024, 256, None),
+        ("hexamer_qtip4pf", prism, 0, None, 10, 6, 512, 256, 0x5C3),
+        ("hexamer_qtip4pf_modesel", prism, 0, np.r_[0:8, 20:30, 40:48], 8, 3, 256, 128, 77),
+        ("dimer_ttm3f", dimer, 1, None, 12, 3, 512, 256, 0x5C3),
+        ("hexamer_ttm3f", prism, 1, None, 6, 4, 256, 128, 0x5C3),
+    ]
+    for name, x, pes, sel, n2, n3, ns, block, sseed in specs:
+        x0, MUa, omega = setup_modes(L, x)
+        nw = x.size // 9
+        nm0 = omega.size
+        sel = np.arange(nm0, dtype=np.int32) if sel is None else np.asarray(sel, dtype=np.int32)
+        if sseed is None:
+            normals = oracle.std_normals(nm0, 1 << 30, ns)
+        else:
+            normals = oracle.std_normals(nm0, 0, ns, scramble_seed=sseed)
+        M, _, _ = oracle.ref_hbuild(pes, nw, x0, MUa, omega, sel, n2, n3, ns, block, normals=normals)
+        iu = np.triu_indices(M.shape[0])
+        cases[name] = dict(x0=x0, MUa=MUa, omega=omega, modes=sel, pes=pes, nw=nw, n2=n2, n3=n3,
+                           nsamples=ns, block=block, scramble_seed=-1 if sseed is None else sseed,
+                           index0=(1 << 30) if sseed is None else 0, M_upper=M.T[iu[1], iu[0]])
+        print(name, M.shape, "done")
+    flat = {}
+    for name, d in cases.items():
+        for k, v in d.items():
+            flat[name + "__" + k] = np.asarray(v)
+    np.savez_compressed(os.path.join(OUT, "hbuild_ref.npz"), **flat)
+
+
+def main():
+    oracle.build(REF)
+    L = oracle.ref_lib()
+    gen_sobol(L)
+    dimer, prism = gen_pes(L)
+    gen_hbuild(L, dimer, prism)
+
+
+if __name__ == "__main__":
+    main()
