@@ -1,0 +1,278 @@
+"""Benchmark of the B200 Hamiltonian build (one JSON line on rank 0).
+
+Workload (one step): the hexamer-prism doubles build -- six waters relaxed on
+qTIP4P/f, 48 modes, N2 = 48 (1225 basis functions), 2^20 scrambled Sobol points
+per step and per GPU (weak scaling), each point through BSM, the back-transform,
+the potential and the accumulation of <i|V|j>.  Inputs are synthetic: the
+geometry is built and relaxed by scp3_b200.inputs, the Sobol points are
+generated on the device.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3|fp64]
+  python bench.py --impl reference ...   # the reference's CPU build, timed on this host
+
+value   samples/s over all ranks, device-timed (CUDA events on the build's stream,
+        max over ranks), L2 flushed between steps (256 MB write)
+e2e     samples/s through the C ABI with host buffers: the -r path (SCP3.cpp:188-194)
+        with 2^20 x 48 FP64 normals copied in from pinned memory and Mout read back
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SAMPLES = 1 << 20
+INPUT = "prism_qtip4pf"
+SCRAMBLE_SEED = 0x5C3
+WORKLOAD = "hexamer prism qTIP4P/f, 48 modes, doubles basis Nb=1225, 2^20 scrambled Sobol points per GPU per step"
+METRIC = "Sobol samples/s (hexamer H-build) at <=0.1 cm^-1 on 10 lowest levels vs FP64"
+FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (vector and tensor) nominal; no measured FP64 peak on this pool
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "of measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "of fallback"
+
+
+class Clocks:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+
+    def __init__(self, gpu):
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%d.csv" % os.getpid())
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=None)
+    return world, rank, local
+
+
+def cpu_reference(nw, x0, MUa, omega, modes, n2, n3, normals, target_s=12.0, max_samples=None):
+    """The reference's own build (oracle/_ref, release flags) on this host: samples/s."""
+    import oracle
+    fast = oracle.ref_available(fast=True)
+    if not (fast or oracle.ref_available()):
+        return None
+    block = 1024
+    n = block * 4
+    M, t, _ = oracle.ref_hbuild(0, nw, x0, MUa, omega, modes, n2, n3, n, block, normals=normals[:n], fast=fast)
+    per = max(t.sum(), 1e-6) / n
+    n = int(min(max(block * 4, target_s / per), normals.shape[0] if max_samples is None else max_samples))
+    n -= n % block
+    t0 = time.perf_counter()
+    M, t, _ = oracle.ref_hbuild(0, nw, x0, MUa, omega, modes, n2, n3, n, block, normals=normals[:n], fast=fast, M=M)
+    wall = time.perf_counter() - t0
+    return {"value": n / wall, "unit": "samples/s", "cores": os.cpu_count(), "kind": "reference" if fast else "port",
+            "sample": "%d of the %d samples (blocks of %d, -r normals path: PES + get_bra + dsyr2k, OpenMP/OpenBLAS on "
+                      "all host threads); Sobol skip walk excluded" % (n, SAMPLES, block),
+            "split_s": {"pes": float(t[0]), "bra": float(t[1]), "dsyr2k": float(t[2])}}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from scp3_b200 import inputs, std_normals
+    nw, x0, MUa, omega = inputs.load(INPUT)
+    modes = np.arange(omega.size, dtype=np.int32)
+    import oracle
+    if not (oracle.ref_available(fast=True) or oracle.ref_available()):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference built from its sources) "
+                                                              "is not present on this host"}))
+        return
+    per_step = 1 << 14
+    normals = oracle.std_normals(omega.size, 0, per_step, scramble_seed=SCRAMBLE_SEED)
+    fast = oracle.ref_available(fast=True)
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.ref_hbuild(0, nw, x0, MUa, omega, modes, 48, 0, per_step, 1024, normals=normals, fast=fast)
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    v = per_step * len(times) / sum(times)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "samples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD + " (each reference step: a bounded 2^14-sample slice)",
+                       "samples_per_step": per_step},
+            "cpu_baseline": {"value": v, "unit": "samples/s", "cores": os.cpu_count(),
+                             "kind": "reference" if fast else "port",
+                             "sample": "2^14 samples per step of the same workload, -r normals path"},
+            "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "bf16x3"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    import scp3_b200
+    from scp3_b200 import inputs
+    nw, x0, MUa, omega = inputs.load(INPUT)
+    nm0 = omega.size
+    hb = scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=0, pes="qtip4pf", precision=args.precision,
+                          scramble_seed=SCRAMBLE_SEED, device=local)
+    nb = hb.nb
+    stream = torch.cuda.ExternalStream(hb.stream, device=local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=local)
+    Mdev = torch.zeros((nb, nb), dtype=torch.float64, device=local)
+    base = rank * (1 << 40)            # disjoint Sobol index ranges per rank
+
+    def step(k):
+        hb.accumulate(base + k * SAMPLES, SAMPLES)
+        if world > 1:
+            import torch.distributed as dist
+            hb.read_dev(Mdev.data_ptr(), nb, 0)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            torch.cuda.current_stream().wait_event(ev)
+            dist.all_reduce(Mdev)
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    hb.reset()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    hb.profile(True)
+    total_ms = 0.0
+    for k in range(args.steps):
+        flush.fill_(k & 0xff)          # L2 flush between steps, outside the timed events
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step(args.warmup + k)
+        e1.record(torch.cuda.current_stream() if world > 1 else stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    ms, launches = hb.profile(False)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], dtype=torch.float64, device=local)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = world * SAMPLES * args.steps / (total_ms / 1e3)
+    rc, nonfinite, notconv = hb.status()
+
+    # dominant kernel: the contraction; algorithmic work Nb(Nb+1) flops per sample
+    peaks, peak_src = load_peaks()
+    flops_per_sample = nb * (nb + 1)
+    cont_launches = int(launches[2])
+    avg_ms = ms[2] / max(cont_launches, 1)
+    samples_per_launch = SAMPLES * args.steps / max(cont_launches, 1)
+    achieved = flops_per_sample * samples_per_launch / (avg_ms / 1e3) / 1e12
+    if args.precision == "fp64":
+        roof = {"bound": "fp64", "achieved": achieved, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                "frac": achieved / FP64_NOMINAL_TFLOPS, "traffic": None,
+                "note": "FP64 DFMA contraction; peak is B200 nominal FP64 (no measured FP64 peak)"}
+    else:
+        pk = peaks["bf16_tflops"]
+        roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
+                "traffic": None, "note": "algorithmic Nb(Nb+1) flops/sample; BF16x3 issues 3 tensor products each "
+                                         "(ceiling 1/3); peak " + peak_src}
+
+    line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3/f32/f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": args.precision, "nb": nb, "samples_per_step": SAMPLES,
+                       "l2": "flushed between steps (256 MB write)", "parallelism": "dp%d (sample ranges)" % world},
+            "roofline": roof, "gpu_launches": int(launches.sum()) // max(args.steps, 1) * args.steps,
+            "kernel_ms": {"per_sample": ms[0], "expand": ms[1], "contract": ms[2], "readout": ms[3]},
+            "clocks": clk, "status": {"rc": rc, "nonfinite": nonfinite, "not_converged": notconv}}
+
+    if rank == 0 and not args.no_e2e:
+        # the -r path with host buffers: normals in from pinned memory, Mout back to host
+        normals = torch.from_numpy(scp3_b200.std_normals(nm0, 1 << 41, SAMPLES, scramble_seed=SCRAMBLE_SEED))
+        normals = normals.pin_memory().numpy()
+        Mh = np.asfortranarray(torch.empty((nb, nb), dtype=torch.float64).pin_memory().numpy().T)
+        hb.reset()
+        hb.accumulate_normals(normals)
+        hb.read(1, out=Mh)
+        t0 = time.perf_counter()
+        ne = max(2, min(args.steps, 5))
+        for k in range(ne):
+            hb.accumulate_normals(normals)
+            hb.read(1, out=Mh)
+        e2e_s = (time.perf_counter() - t0) / ne
+        line["e2e"] = {"value": SAMPLES / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": int(normals.nbytes),
+                       "d2h_bytes_per_step": int(nb * nb * 8),
+                       "path": "scp3gpu_hbuild_accumulate_normals + scp3gpu_hbuild_read(mode 1), host buffers"}
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        normals = scp3_b200.std_normals(nm0, 0, 1 << 17, scramble_seed=SCRAMBLE_SEED)
+        line["cpu_baseline"] = cpu_reference(nw, x0, MUa, omega, np.arange(nm0, dtype=np.int32), 48, 0, normals)
+    if rank == 0:
+        print(json.dumps(line))
+    hb.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

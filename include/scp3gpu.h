@@ -1,0 +1,167 @@
+/*
+ * scp3gpu.h -- C ABI of the B200 Hamiltonian build (libscp3gpu.so).
+ *
+ * Plain C types only: host pointers unless a name says "_dev".  Every function
+ * returns an int status (SCP3GPU_OK == 0) and never exits or traps; the last
+ * error's text is available from scp3gpu_last_error().  One handle belongs to
+ * one host thread; all of a handle's device work is ordered on its own stream.
+ *
+ * The reference (SCP3) has no plugin API; the hot path sits behind three C++
+ * seams, each of which an entry point below replaces (citations are
+ * file:line in the reference tree):
+ *
+ *   h2o::PES::operator()(nw, crd)              PES.h:14-22, qtip4pf.cpp:190-286,
+ *                                              ttm3f.cpp:92-321
+ *   sobol::std_normal(dims, &seed, u)          sobol.hpp:31, sobol.cpp:28706-28713
+ *   ScaledMatrixElements(omega, N2, N3),       ScaledMatrixElements.h:75-96,
+ *     getBasisSize, getSubBasisSize,           ScaledMatrixElements.cpp:73-99,
+ *     addEpot(q, V, M)  (-G path),             ScaledMatrixElements.cpp:951-971,
+ *     addHODiagonal(M)                         ScaledMatrixElements.cpp:735-784
+ *
+ * and the fused sample loop of SCP3_a (SCP3.cpp:154-272) that drives them.
+ */
+#ifndef SCP3GPU_H
+#define SCP3GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference calls exit(EXIT_FAILURE) instead,
+ *      e.g. SCP3.cpp:156-160, ScaledMatrixElements.cpp:202-205) ---- */
+#define SCP3GPU_OK 0
+#define SCP3GPU_ERR_ARG 1           /* bad shape, option or pointer            */
+#define SCP3GPU_ERR_CUDA 2          /* a CUDA runtime/driver call failed       */
+#define SCP3GPU_ERR_NOMEM 3         /* device allocation failed                */
+#define SCP3GPU_ERR_NOT_CONVERGED 4 /* TTM3-F dipoles hit the iteration cap    */
+#define SCP3GPU_ERR_NONFINITE 5     /* a sample produced a non-finite V        */
+#define SCP3GPU_ERR_TIMEOUT 6       /* a bounded device-side wait gave up      */
+#define SCP3GPU_ERR_UNSUPPORTED 7   /* no sm_100 device / feature missing      */
+
+/* potentials (h2o.h:20-47 knows "qtip4pf"; TTM3-F added, ttm3f.cpp) */
+#define SCP3GPU_PES_QTIP4PF 0
+#define SCP3GPU_PES_TTM3F 1
+
+/* arithmetic of the build */
+#define SCP3GPU_PREC_FP64 0   /* plain: everything FP64 (parity form)                  */
+#define SCP3GPU_PREC_BF16X3 1 /* split: potential FP32, contraction BF16x3 on tcgen05,
+                                 FP32 accumulation flushed to FP64 every 4096 samples */
+
+/* sampling */
+#define SCP3GPU_SOBOL_REFERENCE 0 /* i8_sobol points, unscrambled (sobol.cpp:14198-27868) */
+#define SCP3GPU_SOBOL_SCRAMBLED 1 /* seeded linear matrix scramble + digital shift         */
+
+const char* scp3gpu_last_error(void);
+int scp3gpu_version(void);
+
+/* ------------------------------------------------------------------ PES
+ * Energies of n geometries, each 9*nw doubles in Angstrom, O H H per water;
+ * E[k] in kcal/mol.  Replaces h2o::PES::operator()(nw, crd) (PES.h:14-22).
+ * Host buffers; `iters` (may be NULL) receives the TTM3-F Jacobi sweep count
+ * per geometry (0 for qTIP4P/f).  Returns SCP3GPU_ERR_NOT_CONVERGED if any
+ * TTM3-F geometry hit the 500-sweep cap (its energy is still written). */
+int scp3gpu_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters);
+
+/* Device-buffer variant (crd_dev, E_dev on `device`), ordered on the legacy
+ * default stream of that device. */
+int scp3gpu_pes_energy_dev(int pes, int nw, int64_t n, const double* crd_dev, double* E_dev, int device);
+
+/* ------------------------------------------------------------------ sampling
+ * n x dims standard normals of points index0 .. index0+n-1, sample-major,
+ * into host memory.  SCP3GPU_SOBOL_REFERENCE reproduces the reference's
+ * sobol::std_normal stream: call k of std_normal(dims, &seed) with seed
+ * starting at S returns row (S + k) - index0 when index0 = S (sobol.hpp:31).
+ * Uniform bit patterns are exact; BSM uses the device log (<= 2 ulp). */
+int scp3gpu_sobol_std_normal(int dims, int64_t index0, int64_t n, int scramble, uint64_t scramble_seed,
+                             double* out);
+
+/* ------------------------------------------------------------------ basis
+ * getBasisSize / getSubBasisSize (ScaledMatrixElements.cpp:73-99). */
+int64_t scp3gpu_basis_size(int nmodes, int n2, int n3);
+int64_t scp3gpu_sub_basis_size(int nmodes, int n2, int n3, int level);
+
+/* ------------------------------------------------------------------ the build
+ * One handle = one ScaledMatrixElements + the SCP3_a sample loop around it. */
+typedef struct scp3gpu_hbuild scp3gpu_hbuild;
+
+typedef struct scp3gpu_config {
+    int nw;                 /* waters; coordinates = 9*nw                              */
+    int nmodes0;            /* internal modes 9*nw-6 (rows of `by`, SCP3.cpp:183)      */
+    const double* x0;       /* [9*nw] reference geometry, bohr, O H H (SCP3.cpp:292)   */
+    const double* MUa;      /* [9*nw x nmodes0] column-major (SCP3.cpp:309-314)        */
+    const double* omega;    /* [nmodes0] harmonic frequencies, hartree (SCP3.cpp:307)  */
+    int nmodes;             /* selected modes (-m, SCP3.cpp:316-318)                   */
+    const int* modes;       /* [nmodes] indices into 0..nmodes0-1                      */
+    int n2;                 /* modes with double excitations (-2)                      */
+    int n3;                 /* modes with triple excitations (-3)                      */
+    int pes;                /* SCP3GPU_PES_*  (-p)                                     */
+    int precision;          /* SCP3GPU_PREC_*                                          */
+    int scramble;           /* SCP3GPU_SOBOL_*                                         */
+    uint64_t scramble_seed;
+    int chunk;              /* samples per device pass; multiple of 4096, 0 = auto     */
+    int device;             /* CUDA device ordinal                                     */
+} scp3gpu_config;
+
+/* Replaces ScaledMatrixElements(omega(modes), N2, N3) + M.zeros (SCP3.cpp:164-169). */
+int scp3gpu_hbuild_create(const scp3gpu_config* cfg, scp3gpu_hbuild** out);
+int scp3gpu_hbuild_destroy(scp3gpu_hbuild* h);
+/* Zero the accumulated sums and the sample count. */
+int scp3gpu_hbuild_reset(scp3gpu_hbuild* h);
+int64_t scp3gpu_hbuild_basis_size(const scp3gpu_hbuild* h);
+/* The cudaStream_t all of the handle's work is ordered on. */
+void* scp3gpu_hbuild_stream(const scp3gpu_hbuild* h);
+
+/* Samples index0 .. index0+n-1 of the handle's Sobol stream, generated on the
+ * device: Sobol -> BSM -> q = y/sqrt(2) -> r = bohr(x0 + MUa q) -> V/autokcal
+ * -> V_anh = V - q.(omega%q)/2 -> M += sum Phi V_anh Phi^T (upper).  The
+ * fused form of SCP3.cpp:187-232 with use_gradient = false (-G).  Asynchronous
+ * on the handle's stream. */
+int scp3gpu_hbuild_accumulate(scp3gpu_hbuild* h, int64_t index0, int64_t n);
+
+/* The -r path (SCP3.cpp:188-194): n x nmodes0 standard normals, sample-major,
+ * in host memory (copied in, overlapped with compute).  Blocks until the host
+ * buffer may be reused. */
+int scp3gpu_hbuild_accumulate_normals(scp3gpu_hbuild* h, const double* normals, int64_t n);
+
+/* addEpot(q, V, M) of the -G path on caller data (ScaledMatrixElements.cpp:951-971):
+ * q is n x nmodes (selected modes, sample-major), V is n; both host buffers. */
+int scp3gpu_hbuild_add_epot(scp3gpu_hbuild* h, const double* q, const double* V, int64_t n);
+
+/* Samples accumulated so far. */
+int64_t scp3gpu_hbuild_sample_count(const scp3gpu_hbuild* h);
+
+/* Synchronise, then write the accumulated matrix into host memory M
+ * (column-major, leading dimension ld >= Nb), upper triangle plus the mirrored
+ * lower triangle.  mode 0: the raw FP64 sum (M of SCP3_a before dividing);
+ * mode 1: Mout = sum/count + HO diagonal + inactive-mode zero-point energy
+ * (SCP3.cpp:237-239 with addHODiagonal, ScaledMatrixElements.cpp:735-784). */
+int scp3gpu_hbuild_read(scp3gpu_hbuild* h, double* M, int64_t ld, int mode);
+
+/* As scp3gpu_hbuild_read, into device memory M_dev (on the handle's device),
+ * ordered on the handle's stream without a host synchronisation. */
+int scp3gpu_hbuild_read_dev(scp3gpu_hbuild* h, double* M_dev, int64_t ld, int mode);
+
+/* The k lowest eigenvalues (hartree, ascending) of the leading `nsub` x `nsub`
+ * block of Mout (nsub = Nb for the whole basis; getSubBasisSize for the
+ * singles/doubles readouts of SCP3.cpp:241-247), FP64 on the device. */
+int scp3gpu_hbuild_eigvals(scp3gpu_hbuild* h, int64_t nsub, int k, double* evals);
+
+/* Per-sample status counters since create/reset: samples with a non-finite
+ * V, TTM3-F samples that hit the sweep cap. */
+int scp3gpu_hbuild_status(scp3gpu_hbuild* h, int64_t* nonfinite, int64_t* not_converged);
+
+/* Kernel timing (no counterpart in the reference, which has no in-code timing;
+ * only a VTune build profile, config/vtune.mk:1-4).  enable = 1 clears and starts
+ * recording CUDA events around every kernel the handle launches on its stream;
+ * enable = 0 stops, synchronises and returns, per kernel kind (0 per-sample,
+ * 1 basis expansion / sign partition, 2 contraction, 3 read-out), the summed
+ * device milliseconds and the launch counts (arrays of 4; may be NULL). */
+int scp3gpu_hbuild_profile(scp3gpu_hbuild* h, int enable, double* ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCP3GPU_H */

@@ -1,0 +1,654 @@
+// The C ABI of libscp3gpu.so (include/scp3gpu.h): handle lifecycle, the chunked
+// sample loop of SCP3_a (SCP3.cpp:154-272) on the device, the -r normals path,
+// read-out, eigenvalues and status.
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "internal.h"
+#include "tc.h"
+
+namespace scp3 {
+
+static thread_local std::string g_err;
+void set_error(const std::string& m) { g_err = m; }
+int fail(int code, const std::string& m)
+{
+    g_err = m;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char* what)
+{
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? SCP3GPU_ERR_NOMEM : SCP3GPU_ERR_CUDA;
+}
+
+namespace {
+
+template <typename T>
+int dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) return SCP3GPU_OK;
+    SCP3_CUDA(cudaMalloc((void**)p, count * sizeof(T)));
+    return SCP3GPU_OK;
+}
+
+template <typename T>
+int upload(T** p, const T* host, size_t count)
+{
+    int rc = dalloc(p, count);
+    if (rc) return rc;
+    if (count) SCP3_CUDA(cudaMemcpy(*p, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    return SCP3GPU_OK;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+int check_device(int dev)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(SCP3GPU_ERR_UNSUPPORTED, "no CUDA device");
+    if (dev < 0 || dev >= n) return fail(SCP3GPU_ERR_ARG, "device ordinal out of range");
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) return fail(SCP3GPU_ERR_UNSUPPORTED, "libscp3gpu is built for sm_100a (B200) only");
+    return SCP3GPU_OK;
+}
+
+}  // namespace
+}  // namespace scp3
+
+using namespace scp3;
+
+struct scp3gpu_hbuild {
+    scp3gpu_config cfg{};
+    std::vector<double> omega_sel;
+    double zpe_inactive = 0.0;
+    int dev = 0;
+    cudaStream_t stream = nullptr, copy_stream = nullptr;
+    cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
+    int nb = 0, nb_pad = 0, ntasks = 0, nsplit = 1;
+    int64_t chunk = 0;
+    TileMap tm{};
+    bool split_form = false;
+    // tables
+    int64_t* vdir = nullptr;
+    uint64_t* shift = nullptr;
+    double *x0 = nullptr, *MUa = nullptr, *omega = nullptr;
+    int* modes = nullptr;
+    uint32_t *tasks = nullptr, *desc = nullptr;
+    // per chunk
+    double* q64 = nullptr;
+    float* q32 = nullptr;
+    double* v = nullptr;
+    double* normals[2] = {nullptr, nullptr};
+    double *phi = nullptr, *w = nullptr;
+    double* partial = nullptr;
+    tc::Plan tcp{};
+    // read-out
+    double* dense = nullptr;
+    double* hodiag = nullptr;
+    unsigned long long* counters = nullptr;
+    int64_t count = 0;
+    // kernel timing
+    bool prof = false;
+    std::vector<cudaEvent_t> pev;
+    std::vector<int> pkind;
+};
+
+namespace {
+
+int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+
+// Records an event on the handle's stream before (open) and after (close) a
+// launch when timing is on.
+struct Timed {
+    scp3gpu_hbuild* h;
+    int kind;
+    Timed(scp3gpu_hbuild* h_, int kind_) : h(h_), kind(kind_) { mark(); }
+    ~Timed() { mark(); }
+    void mark()
+    {
+        if (!h->prof) return;
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        cudaEventRecord(e, h->stream);
+        h->pev.push_back(e);
+        h->pkind.push_back(kind);
+    }
+};
+
+// Samples per device pass and the split of each pass over CTAs of a tile.
+void plan_fp64(scp3gpu_hbuild* h, int sms)
+{
+    h->tm.tile = 64;
+    h->tm.nt = (h->nb + 63) / 64;
+    h->tm.ntiles = h->tm.nt * (h->tm.nt + 1) / 2;
+    h->nb_pad = h->tm.nt * 64;
+    int64_t chunk = h->cfg.chunk > 0 ? h->cfg.chunk : 4096;
+    // keep Phi and W of one pass under ~4 GB
+    while (chunk > 4096 && (int64_t)h->nb_pad * chunk * 16 > (4ll << 30)) chunk /= 2;
+    h->chunk = chunk;
+    int nsplit = 1;
+    while ((int64_t)h->tm.ntiles * nsplit < 2ll * sms && chunk / (nsplit * 2) >= 64) nsplit *= 2;
+    h->nsplit = nsplit;
+}
+
+int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double* normals_dev)
+{
+    const bool fp32 = h->split_form;
+    SampleArgs a{};
+    a.nw = h->cfg.nw;
+    a.nm0 = h->cfg.nmodes0;
+    a.nm = h->cfg.nmodes;
+    a.x0 = h->x0;
+    a.MUa = h->MUa;
+    a.omega = h->omega;
+    a.modes = h->modes;
+    a.vdir = h->vdir;
+    a.shift = h->shift;
+    a.tasks = h->tasks;
+    a.ntasks = h->ntasks;
+    a.normals = normals_dev;
+    a.index0 = index0;
+    a.n = h->split_form ? tc::pass_samples(h->tcp, nvalid) : round_up(nvalid, 16ll * h->nsplit);
+    a.nvalid = nvalid;
+    a.q64 = fp32 ? nullptr : h->q64;
+    a.q32 = fp32 ? h->q32 : nullptr;
+    a.v = h->v;
+    a.counters = h->counters;
+    int rc;
+    {
+        Timed t(h, 0);
+        rc = launch_samples(h->cfg.pes, fp32, a, h->stream);
+    }
+    if (rc) return rc;
+    if (h->split_form) {
+        return tc::accumulate_pass(h->tcp, h->desc, h->nb, h->cfg.nmodes, h->q32, h->v, a.n, h->stream,
+                                   h->prof ? &h->pev : nullptr, h->prof ? &h->pkind : nullptr);
+    }
+    {
+        Timed t(h, 1);
+        rc = launch_expand_fp64(h->desc, h->nb, h->nb_pad, h->cfg.nmodes, h->q64, h->v, a.n, h->chunk, h->phi, h->w,
+                                h->stream);
+    }
+    if (rc) return rc;
+    Timed t(h, 2);
+    return launch_contract_fp64(h->phi, h->w, h->chunk, a.n, h->nb_pad, h->tm, h->nsplit, h->partial, h->stream);
+}
+
+int zero_sums(scp3gpu_hbuild* h)
+{
+    if (h->split_form) return tc::zero(h->tcp, h->stream);
+    SCP3_CUDA(cudaMemsetAsync(h->partial, 0, sizeof(double) * (size_t)h->nsplit * h->tm.ntiles * 64 * 64, h->stream));
+    return SCP3GPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* scp3gpu_last_error(void) { return g_err.c_str(); }
+int scp3gpu_version(void) { return 100; }
+
+int64_t scp3gpu_basis_size(int nm, int n2, int n3)
+{
+    if (nm < 0 || n2 < 0 || n3 < 0 || n2 > nm || n3 > nm) return -1;
+    return 1 + (int64_t)nm + (int64_t)n2 * (n2 + 1) / 2 + (int64_t)n3 * (1 + n3) * (2 + n3) / 6;
+}
+
+int64_t scp3gpu_sub_basis_size(int nm, int n2, int n3, int level)
+{
+    if (scp3gpu_basis_size(nm, n2, n3) < 0) return -1;
+    int64_t s = 0;
+    if (level >= 3) s += (int64_t)n3 * (1 + n3) * (2 + n3) / 6;
+    if (level >= 2) s += (int64_t)n2 * (n2 + 1) / 2;
+    if (level >= 1) s += nm;
+    if (level >= 0) s += 1;
+    return s;
+}
+
+int scp3gpu_pes_energy_dev(int pes, int nw, int64_t n, const double* crd_dev, double* E_dev, int device)
+{
+    if (pes != SCP3GPU_PES_QTIP4PF && pes != SCP3GPU_PES_TTM3F) return fail(SCP3GPU_ERR_ARG, "unknown potential");
+    if (nw < 1 || nw > kMaxWaters || n < 0 || (n > 0 && (!crd_dev || !E_dev)))
+        return fail(SCP3GPU_ERR_ARG, "pes_energy: bad nw, n or pointer");
+    int rc = check_device(device);
+    if (rc) return rc;
+    DeviceGuard g(device);
+    if (pes == SCP3GPU_PES_TTM3F && (rc = ttm_init_device())) return rc;
+    std::vector<uint32_t> t = pair_tasks(nw);
+    uint32_t* td = nullptr;
+    if ((rc = upload(&td, t.data(), t.size()))) return rc;
+    rc = launch_pes_energy(pes, nw, n, crd_dev, E_dev, nullptr, td, (int)t.size(), 0);
+    cudaError_t e = cudaStreamSynchronize(0);
+    cudaFree(td);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "pes_energy");
+    return SCP3GPU_OK;
+}
+
+int scp3gpu_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters)
+{
+    if (pes != SCP3GPU_PES_QTIP4PF && pes != SCP3GPU_PES_TTM3F) return fail(SCP3GPU_ERR_ARG, "unknown potential");
+    if (nw < 1 || nw > kMaxWaters || n < 0 || (n > 0 && (!crd || !E)))
+        return fail(SCP3GPU_ERR_ARG, "pes_energy: bad nw, n or pointer");
+    if (n == 0) return SCP3GPU_OK;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int rc = check_device(dev);
+    if (rc) return rc;
+    if (pes == SCP3GPU_PES_TTM3F && (rc = ttm_init_device())) return rc;
+    std::vector<uint32_t> t = pair_tasks(nw);
+    uint32_t* td = nullptr;
+    double *cd = nullptr, *ed = nullptr;
+    int* id = nullptr;
+    if ((rc = upload(&td, t.data(), t.size())) || (rc = upload(&cd, crd, (size_t)n * 9 * nw)) ||
+        (rc = dalloc(&ed, (size_t)n)) || (rc = dalloc(&id, (size_t)n))) {
+        cudaFree(td), cudaFree(cd), cudaFree(ed), cudaFree(id);
+        return rc;
+    }
+    rc = launch_pes_energy(pes, nw, n, cd, ed, id, td, (int)t.size(), 0);
+    std::vector<int> it(n);
+    if (!rc) {
+        cudaError_t e = cudaMemcpy(E, ed, sizeof(double) * n, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(it.data(), id, sizeof(int) * n, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = cuda_fail(e, "pes_energy copy-out");
+    }
+    cudaFree(td), cudaFree(cd), cudaFree(ed), cudaFree(id);
+    if (rc) return rc;
+    bool capped = false;
+    for (int64_t k = 0; k < n; k++) {
+        if (iters) iters[k] = it[k];
+        capped |= it[k] > kTtmMaxIter;
+    }
+    return capped ? fail(SCP3GPU_ERR_NOT_CONVERGED, "TTM3-F dipoles hit the iteration cap") : SCP3GPU_OK;
+}
+
+int scp3gpu_sobol_std_normal(int dims, int64_t index0, int64_t n, int scramble, uint64_t seed, double* out)
+{
+    if (dims < 1 || dims > 1111 || index0 < 0 || n < 0 || (n > 0 && !out))
+        return fail(SCP3GPU_ERR_ARG, "sobol_std_normal: bad dims, index or pointer");
+    if (n == 0) return SCP3GPU_OK;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int rc = check_device(dev);
+    if (rc) return rc;
+    std::vector<int64_t> v;
+    std::vector<uint64_t> sh;
+    if ((rc = sobol_tables(dims, scramble, seed, v, sh))) return rc;
+    int64_t* vd = nullptr;
+    uint64_t* sd = nullptr;
+    double* od = nullptr;
+    if ((rc = upload(&vd, v.data(), v.size())) || (rc = upload(&sd, sh.data(), sh.size())) ||
+        (rc = dalloc(&od, (size_t)n * dims))) {
+        cudaFree(vd), cudaFree(sd), cudaFree(od);
+        return rc;
+    }
+    rc = launch_std_normal(dims, index0, n, vd, scramble ? sd : nullptr, od, 0);
+    if (!rc) {
+        cudaError_t e = cudaMemcpy(out, od, sizeof(double) * n * dims, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = cuda_fail(e, "sobol copy-out");
+    }
+    cudaFree(vd), cudaFree(sd), cudaFree(od);
+    return rc;
+}
+
+int scp3gpu_hbuild_destroy(scp3gpu_hbuild* h)
+{
+    if (!h) return SCP3GPU_OK;
+    DeviceGuard g(h->dev);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+    void* ptrs[] = {h->vdir, h->shift, h->x0, h->MUa, h->omega, h->modes, h->tasks, h->desc, h->q64, h->q32,
+                    h->v, h->normals[0], h->normals[1], h->phi, h->w, h->partial, h->dense, h->hodiag,
+                    h->counters};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    tc::destroy(h->tcp);
+    for (int b = 0; b < 2; b++) {
+        if (h->copied[b]) cudaEventDestroy(h->copied[b]);
+        if (h->consumed[b]) cudaEventDestroy(h->consumed[b]);
+    }
+    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+    delete h;
+    return SCP3GPU_OK;
+}
+
+int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
+{
+    if (!c || !out) return fail(SCP3GPU_ERR_ARG, "null config or output");
+    *out = nullptr;
+    if (c->nw < 1 || c->nw > kMaxWaters) return fail(SCP3GPU_ERR_ARG, "nw must be 1..16");
+    if (c->nmodes0 != 9 * c->nw - 6) return fail(SCP3GPU_ERR_ARG, "nmodes0 must be 9*nw-6");
+    if (c->nmodes < 1 || c->nmodes > c->nmodes0 || c->nmodes > kMaxModes)
+        return fail(SCP3GPU_ERR_ARG, "nmodes out of range");
+    // SCP3.cpp:156-160
+    if (c->n2 < 0 || c->n3 < 0 || c->n2 > c->nmodes || c->n3 > c->nmodes)
+        return fail(SCP3GPU_ERR_ARG, "Number of double or triple excitations exceed number of modes.");
+    if (!c->x0 || !c->MUa || !c->omega || !c->modes) return fail(SCP3GPU_ERR_ARG, "null geometry or mode arrays");
+    if (c->pes != SCP3GPU_PES_QTIP4PF && c->pes != SCP3GPU_PES_TTM3F) return fail(SCP3GPU_ERR_ARG, "unknown potential");
+    if (c->precision != SCP3GPU_PREC_FP64 && c->precision != SCP3GPU_PREC_BF16X3)
+        return fail(SCP3GPU_ERR_ARG, "unknown precision");
+    if (c->pes == SCP3GPU_PES_TTM3F && c->nw > 8) return fail(SCP3GPU_ERR_ARG, "TTM3-F kernel supports nw <= 8");
+    if (c->chunk < 0 || c->chunk % 4096 != 0) return fail(SCP3GPU_ERR_ARG, "chunk must be a multiple of 4096");
+    for (int m = 0; m < c->nmodes; m++)
+        if (c->modes[m] < 0 || c->modes[m] >= c->nmodes0) return fail(SCP3GPU_ERR_ARG, "mode index out of range");
+    int rc = check_device(c->device);
+    if (rc) return rc;
+    DeviceGuard g(c->device);
+    if (c->pes == SCP3GPU_PES_TTM3F && (rc = ttm_init_device())) return rc;
+
+    scp3gpu_hbuild* h = new scp3gpu_hbuild();
+    h->cfg = *c;
+    h->cfg.x0 = h->cfg.MUa = h->cfg.omega = nullptr;
+    h->cfg.modes = nullptr;
+    h->dev = c->device;
+    h->split_form = c->precision == SCP3GPU_PREC_BF16X3;
+    const int nm0 = c->nmodes0, N3 = 9 * c->nw;
+    h->nb = (int)scp3gpu_basis_size(c->nmodes, c->n2, c->n3);
+    // HO diagonal of the selected modes and the inactive-mode zero point (SCP3.cpp:239)
+    double sum_all = 0, sum_sel = 0;
+    for (int k = 0; k < nm0; k++) sum_all += c->omega[k];
+    for (int m = 0; m < c->nmodes; m++) {
+        h->omega_sel.push_back(c->omega[c->modes[m]]);
+        sum_sel += c->omega[c->modes[m]];
+    }
+    h->zpe_inactive = 0.5 * (sum_all - sum_sel);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+
+    auto bail = [&](int code) {
+        scp3gpu_hbuild_destroy(h);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(SCP3GPU_ERR_CUDA, "stream creation failed"));
+    for (int b = 0; b < 2; b++)
+        if (cudaEventCreateWithFlags(&h->copied[b], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->consumed[b], cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(SCP3GPU_ERR_CUDA, "event creation failed"));
+
+    std::vector<int64_t> vd;
+    std::vector<uint64_t> sh;
+    if ((rc = sobol_tables(nm0, c->scramble, c->scramble_seed, vd, sh))) return bail(rc);
+    std::vector<uint32_t> tasks = pair_tasks(c->nw), desc = basis_descriptors(c->nmodes, c->n2, c->n3);
+    h->ntasks = (int)tasks.size();
+    if ((rc = upload(&h->vdir, vd.data(), vd.size())) ||
+        (c->scramble && (rc = upload(&h->shift, sh.data(), sh.size()))) ||
+        (rc = upload(&h->x0, c->x0, (size_t)N3)) || (rc = upload(&h->MUa, c->MUa, (size_t)N3 * nm0)) ||
+        (rc = upload(&h->omega, c->omega, (size_t)nm0)) || (rc = upload(&h->modes, c->modes, (size_t)c->nmodes)) ||
+        (rc = upload(&h->tasks, tasks.data(), tasks.size())) || (rc = upload(&h->desc, desc.data(), desc.size())) ||
+        (rc = dalloc(&h->counters, 2)))
+        return bail(rc);
+    SCP3_CUDA(cudaMemset(h->counters, 0, 2 * sizeof(unsigned long long)));
+
+    if (h->split_form) {
+        if ((rc = tc::create(h->tcp, h->nb, c->nmodes, c->chunk, sms))) return bail(rc);
+        h->chunk = h->tcp.chunk;
+        h->nb_pad = h->tcp.nb_pad;
+        if ((rc = dalloc(&h->q32, (size_t)h->chunk * c->nmodes)) || (rc = dalloc(&h->v, (size_t)h->chunk)))
+            return bail(rc);
+    } else {
+        plan_fp64(h, sms);
+        if ((rc = dalloc(&h->q64, (size_t)h->chunk * c->nmodes)) || (rc = dalloc(&h->v, (size_t)h->chunk)) ||
+            (rc = dalloc(&h->phi, (size_t)h->nb_pad * h->chunk)) || (rc = dalloc(&h->w, (size_t)h->nb_pad * h->chunk)) ||
+            (rc = dalloc(&h->partial, (size_t)h->nsplit * h->tm.ntiles * 64 * 64)))
+            return bail(rc);
+    }
+    if ((rc = zero_sums(h))) return bail(rc);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(fail(SCP3GPU_ERR_CUDA, "create sync failed"));
+    *out = h;
+    return SCP3GPU_OK;
+}
+
+int scp3gpu_hbuild_reset(scp3gpu_hbuild* h)
+{
+    if (!h) return fail(SCP3GPU_ERR_ARG, "null handle");
+    DeviceGuard g(h->dev);
+    int rc = zero_sums(h);
+    if (rc) return rc;
+    SCP3_CUDA(cudaMemsetAsync(h->counters, 0, 2 * sizeof(unsigned long long), h->stream));
+    h->count = 0;
+    return SCP3GPU_OK;
+}
+
+int64_t scp3gpu_hbuild_basis_size(const scp3gpu_hbuild* h) { return h ? h->nb : -1; }
+void* scp3gpu_hbuild_stream(const scp3gpu_hbuild* h) { return h ? (void*)h->stream : nullptr; }
+int64_t scp3gpu_hbuild_sample_count(const scp3gpu_hbuild* h) { return h ? h->count : -1; }
+
+int scp3gpu_hbuild_accumulate(scp3gpu_hbuild* h, int64_t index0, int64_t n)
+{
+    if (!h || index0 < 0 || n < 0) return fail(SCP3GPU_ERR_ARG, "accumulate: bad handle or range");
+    if (index0 + n > (1ll << 62)) return fail(SCP3GPU_ERR_ARG, "accumulate: Sobol index beyond 2^62");
+    DeviceGuard g(h->dev);
+    for (int64_t off = 0; off < n; off += h->chunk) {
+        const int64_t c = std::min(h->chunk, n - off);
+        int rc = launch_chunk(h, index0 + off, c, nullptr);
+        if (rc) return rc;
+        h->count += c;
+    }
+    return SCP3GPU_OK;
+}
+
+int scp3gpu_hbuild_accumulate_normals(scp3gpu_hbuild* h, const double* normals, int64_t n)
+{
+    if (!h || n < 0 || (n > 0 && !normals)) return fail(SCP3GPU_ERR_ARG, "accumulate_normals: bad arguments");
+    DeviceGuard g(h->dev);
+    const int nm0 = h->cfg.nmodes0;
+    int rc = SCP3GPU_OK;
+    for (int b = 0; b < 2 && !h->normals[b]; b++)
+        if ((rc = dalloc(&h->normals[b], (size_t)h->chunk * nm0))) return rc;
+    int k = 0;
+    for (int64_t off = 0; off < n; off += h->chunk, k++) {
+        const int b = k & 1;
+        const int64_t c = std::min(h->chunk, n - off);
+        // the copy into buffer b may start once the pass that last read it is done
+        SCP3_CUDA(cudaStreamWaitEvent(h->copy_stream, h->consumed[b], 0));
+        SCP3_CUDA(cudaMemcpyAsync(h->normals[b], normals + off * nm0, sizeof(double) * c * nm0,
+                                  cudaMemcpyHostToDevice, h->copy_stream));
+        SCP3_CUDA(cudaEventRecord(h->copied[b], h->copy_stream));
+        SCP3_CUDA(cudaStreamWaitEvent(h->stream, h->copied[b], 0));
+        if ((rc = launch_chunk(h, 0, c, h->normals[b]))) return rc;
+        SCP3_CUDA(cudaEventRecord(h->consumed[b], h->stream));
+        h->count += c;
+    }
+    SCP3_CUDA(cudaStreamSynchronize(h->copy_stream));
+    return SCP3GPU_OK;
+}
+
+int scp3gpu_hbuild_add_epot(scp3gpu_hbuild* h, const double* q, const double* V, int64_t n)
+{
+    if (!h || n < 0 || (n > 0 && (!q || !V))) return fail(SCP3GPU_ERR_ARG, "add_epot: bad arguments");
+    DeviceGuard g(h->dev);
+    const int nm = h->cfg.nmodes;
+    for (int64_t off = 0; off < n; off += h->chunk) {
+        const int64_t c = std::min(h->chunk, n - off);
+        const int64_t kn = h->split_form ? tc::pass_samples(h->tcp, c) : round_up(c, 16ll * h->nsplit);
+        SCP3_CUDA(cudaMemsetAsync(h->v, 0, sizeof(double) * kn, h->stream));
+        SCP3_CUDA(cudaMemcpyAsync(h->v, V + off, sizeof(double) * c, cudaMemcpyHostToDevice, h->stream));
+        int rc;
+        if (h->split_form) {
+            std::vector<float> qf((size_t)kn * nm, 0.0f);
+            for (int64_t i = 0; i < c * nm; i++) qf[i] = (float)q[off * nm + i];
+            SCP3_CUDA(cudaMemcpyAsync(h->q32, qf.data(), sizeof(float) * qf.size(), cudaMemcpyHostToDevice, h->stream));
+            rc = tc::accumulate_pass(h->tcp, h->desc, h->nb, nm, h->q32, h->v, kn, h->stream, nullptr, nullptr);
+            SCP3_CUDA(cudaStreamSynchronize(h->stream));
+        } else {
+            SCP3_CUDA(cudaMemsetAsync(h->q64, 0, sizeof(double) * kn * nm, h->stream));
+            SCP3_CUDA(cudaMemcpyAsync(h->q64, q + off * nm, sizeof(double) * c * nm, cudaMemcpyHostToDevice, h->stream));
+            rc = launch_expand_fp64(h->desc, h->nb, h->nb_pad, nm, h->q64, h->v, kn, h->chunk, h->phi, h->w, h->stream);
+            if (!rc) rc = launch_contract_fp64(h->phi, h->w, h->chunk, kn, h->nb_pad, h->tm, h->nsplit, h->partial,
+                                               h->stream);
+            SCP3_CUDA(cudaStreamSynchronize(h->stream));
+        }
+        if (rc) return rc;
+        h->count += c;
+    }
+    return SCP3GPU_OK;
+}
+
+static int build_dense(scp3gpu_hbuild* h, int mode)
+{
+    int rc;
+    if (!h->dense && (rc = dalloc(&h->dense, (size_t)h->nb * h->nb))) return rc;
+    const double* diag = nullptr;
+    double divisor = 1.0, zpe = 0.0;
+    if (mode == 1) {
+        if (h->count <= 0) return fail(SCP3GPU_ERR_ARG, "read: no samples accumulated");
+        if (!h->hodiag) {
+            // addHODiagonal (ScaledMatrixElements.cpp:735-784)
+            const int nm = h->cfg.nmodes, n2 = h->cfg.n2, n3 = h->cfg.n3;
+            const std::vector<double>& w = h->omega_sel;
+            std::vector<double> d;
+            double e0 = 0;
+            for (double x : w) e0 += x;
+            e0 *= 0.5;
+            d.push_back(e0);
+            for (int k = 0; k < nm; k++) d.push_back(e0 + w[k]);
+            for (int k = 0; k < n2; k++) d.push_back(e0 + 2 * w[k]);
+            for (int k = 0; k < n2; k++)
+                for (int l = k + 1; l < n2; l++) d.push_back(e0 + w[k] + w[l]);
+            for (int k = 0; k < n3; k++) d.push_back(e0 + 3.0 * w[k]);
+            for (int k = 0; k < n3; k++)
+                for (int l = k + 1; l < n3; l++) {
+                    d.push_back(e0 + 2.0 * w[k] + w[l]);
+                    d.push_back(e0 + w[k] + 2.0 * w[l]);
+                }
+            for (int k = 0; k < n3; k++)
+                for (int l = k + 1; l < n3; l++)
+                    for (int j = l + 1; j < n3; j++) d.push_back(e0 + w[k] + w[l] + w[j]);
+            if ((rc = upload(&h->hodiag, d.data(), d.size()))) return rc;
+        }
+        diag = h->hodiag;
+        divisor = (double)h->count;
+        zpe = h->zpe_inactive;
+    }
+    Timed t(h, 3);
+    if (h->split_form) return tc::unpack(h->tcp, h->nb, divisor, diag, zpe, h->dense, h->nb, h->stream);
+    return launch_unpack(h->partial, h->tm, h->nsplit, h->nb, divisor, diag, zpe, h->dense, h->nb, h->stream);
+}
+
+int scp3gpu_hbuild_read(scp3gpu_hbuild* h, double* M, int64_t ld, int mode)
+{
+    if (!h || !M || ld < h->nb || (mode != 0 && mode != 1)) return fail(SCP3GPU_ERR_ARG, "read: bad arguments");
+    DeviceGuard g(h->dev);
+    int rc = build_dense(h, mode);
+    if (rc) return rc;
+    SCP3_CUDA(cudaMemcpy2DAsync(M, sizeof(double) * ld, h->dense, sizeof(double) * h->nb, sizeof(double) * h->nb,
+                                h->nb, cudaMemcpyDeviceToHost, h->stream));
+    SCP3_CUDA(cudaStreamSynchronize(h->stream));
+    return SCP3GPU_OK;
+}
+
+int scp3gpu_hbuild_read_dev(scp3gpu_hbuild* h, double* M_dev, int64_t ld, int mode)
+{
+    if (!h || !M_dev || ld < h->nb || (mode != 0 && mode != 1)) return fail(SCP3GPU_ERR_ARG, "read_dev: bad arguments");
+    DeviceGuard g(h->dev);
+    int rc = build_dense(h, mode);
+    if (rc) return rc;
+    SCP3_CUDA(cudaMemcpy2DAsync(M_dev, sizeof(double) * ld, h->dense, sizeof(double) * h->nb, sizeof(double) * h->nb,
+                                h->nb, cudaMemcpyDeviceToDevice, h->stream));
+    return SCP3GPU_OK;
+}
+
+int scp3gpu_hbuild_eigvals(scp3gpu_hbuild* h, int64_t nsub, int k, double* evals)
+{
+    if (!h || nsub < 1 || nsub > h->nb || k < 1 || k > nsub || !evals)
+        return fail(SCP3GPU_ERR_ARG, "eigvals: bad arguments");
+    DeviceGuard g(h->dev);
+    int rc = build_dense(h, 1);
+    if (rc) return rc;
+    const int n = (int)nsub;
+    double *A = nullptr, *W = nullptr, *work = nullptr;
+    int* info = nullptr;
+    if ((rc = dalloc(&A, (size_t)n * n)) || (rc = dalloc(&W, (size_t)n)) || (rc = dalloc(&info, 1))) {
+        cudaFree(A), cudaFree(W), cudaFree(info);
+        return rc;
+    }
+    cudaMemcpy2DAsync(A, sizeof(double) * n, h->dense, sizeof(double) * h->nb, sizeof(double) * n, n,
+                      cudaMemcpyDeviceToDevice, h->stream);
+    cusolverDnHandle_t sol = nullptr;
+    int lwork = 0, meig = 0, hinfo = 0;
+    rc = SCP3GPU_OK;
+    if (cusolverDnCreate(&sol) != CUSOLVER_STATUS_SUCCESS) rc = fail(SCP3GPU_ERR_CUDA, "cusolverDnCreate failed");
+    if (!rc) cusolverDnSetStream(sol, h->stream);
+    if (!rc && cusolverDnDsyevdx_bufferSize(sol, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_RANGE_I,
+                                            CUBLAS_FILL_MODE_UPPER, n, A, n, 0.0, 0.0, 1, k, &meig, W,
+                                            &lwork) != CUSOLVER_STATUS_SUCCESS)
+        rc = fail(SCP3GPU_ERR_CUDA, "syevdx buffer query failed");
+    if (!rc && (rc = dalloc(&work, (size_t)std::max(lwork, 1)))) {}
+    if (!rc && cusolverDnDsyevdx(sol, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_UPPER, n, A,
+                                 n, 0.0, 0.0, 1, k, &meig, W, work, lwork, info) != CUSOLVER_STATUS_SUCCESS)
+        rc = fail(SCP3GPU_ERR_CUDA, "syevdx failed");
+    if (!rc) {
+        cudaMemcpyAsync(evals, W, sizeof(double) * k, cudaMemcpyDeviceToHost, h->stream);
+        cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "eigvals");
+        else if (hinfo != 0) rc = fail(SCP3GPU_ERR_CUDA, "syevdx did not converge");
+    }
+    if (sol) cusolverDnDestroy(sol);
+    cudaFree(A), cudaFree(W), cudaFree(work), cudaFree(info);
+    return rc;
+}
+
+int scp3gpu_hbuild_profile(scp3gpu_hbuild* h, int enable, double* ms, int64_t* launches)
+{
+    if (!h) return fail(SCP3GPU_ERR_ARG, "null handle");
+    DeviceGuard g(h->dev);
+    double tot[4] = {0, 0, 0, 0};
+    int64_t cnt[4] = {0, 0, 0, 0};
+    int rc = SCP3GPU_OK;
+    if (!enable) {
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "profile sync");
+        for (size_t k = 0; !rc && k + 1 < h->pev.size(); k += 2) {
+            float t = 0;
+            cudaEventElapsedTime(&t, h->pev[k], h->pev[k + 1]);
+            const int kind = h->pkind[k] & 3;
+            tot[kind] += t;
+            cnt[kind]++;
+        }
+    }
+    for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
+    h->pev.clear();
+    h->pkind.clear();
+    h->prof = enable != 0;
+    if (ms) std::copy(tot, tot + 4, ms);
+    if (launches) std::copy(cnt, cnt + 4, launches);
+    return rc;
+}
+
+int scp3gpu_hbuild_status(scp3gpu_hbuild* h, int64_t* nonfinite, int64_t* not_converged)
+{
+    if (!h) return fail(SCP3GPU_ERR_ARG, "null handle");
+    DeviceGuard g(h->dev);
+    unsigned long long c[2] = {0, 0};
+    SCP3_CUDA(cudaMemcpyAsync(c, h->counters, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+    SCP3_CUDA(cudaStreamSynchronize(h->stream));
+    if (nonfinite) *nonfinite = (int64_t)c[0];
+    if (not_converged) *not_converged = (int64_t)c[1];
+    if (c[0]) return fail(SCP3GPU_ERR_NONFINITE, "samples with non-finite V were accumulated");
+    if (c[1]) return fail(SCP3GPU_ERR_NOT_CONVERGED, "TTM3-F samples hit the iteration cap");
+    return SCP3GPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+// Internal declarations shared by the translation units of libscp3gpu.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/scp3gpu.h"
+
+namespace scp3 {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define SCP3_CUDA(call)                                                  \
+    do {                                                                 \
+        cudaError_t e_ = (call);                                         \
+        if (e_ != cudaSuccess) return ::scp3::cuda_fail(e_, #call);      \
+    } while (0)
+
+constexpr int kLogMax = 62;           // bits of the Sobol state (sobol.cpp:27700)
+constexpr int kMaxModes = 255;        // modes fit the 8-bit fields of a basis descriptor
+constexpr int kMaxWaters = 16;        // per-sample kernels keep one geometry per warp in smem
+constexpr int kTtmMaxIter = 500;      // ttm3f.cpp:31
+constexpr double kBohr = 0.52917721092;              // Constants.cpp:12
+constexpr double kAuToKcalPerMol = 627.509474277194; // Constants.h:21
+
+// ---------------------------------------------------------------- host tables
+// Sobol direction numbers, [bit][dim] layout (bit-major, dims contiguous), each
+// scaled by 2^(61-bit) as i8_sobol does (sobol.cpp:27684-27752).  With a
+// scramble seed, every direction number is pushed through the dimension's
+// linear scramble matrix (scrambling commutes with the Gray-code XOR) and the
+// digital shifts are returned separately.
+int sobol_tables(int dims, int scramble, uint64_t seed, std::vector<int64_t>& v_bit_major,
+                 std::vector<uint64_t>& shift);
+
+// Basis descriptors in getBasisSize order (ScaledMatrixElements.cpp:870-930):
+// kind in bits 0..2, modes m, n, p in bits 3..10, 11..18, 19..26.
+enum BasisKind : uint32_t {
+    kGround = 0, kHo1 = 1, kHo2 = 2, kHo1Ho1 = 3, kHo3 = 4, kHo2Ho1 = 5, kHo1Ho2 = 6, kHo1Ho1Ho1 = 7
+};
+std::vector<uint32_t> basis_descriptors(int nm, int n2, int n3);
+
+// Pair tasks of the water potentials, in one list per cluster size: type in
+// bits 0..1 (0: M-site(i)/H(j), 1: H/H, 2: O/O, 3: M/M) and the two atom or
+// site indices in bits 2..16 and 17..31 (atoms index 3*water+{0,1,2}; M sites
+// index the water).
+std::vector<uint32_t> pair_tasks(int nw);
+
+// ---------------------------------------------------------------- launches
+struct SampleArgs {
+    int nw, nm0, nm;              // waters, all modes, selected modes
+    const double* x0;             // [9nw] bohr
+    const double* MUa;            // [9nw x nm0] column-major
+    const double* omega;          // [nm0]
+    const int* modes;             // [nm]
+    const int64_t* vdir;          // [62 x nm0] bit-major direction numbers
+    const uint64_t* shift;        // [nm0] or nullptr
+    const uint32_t* tasks;        // pair tasks
+    int ntasks;
+    const double* normals;        // [n x nm0] sample-major, or nullptr to draw Sobol points
+    int64_t index0;               // first Sobol index
+    int64_t n;                    // samples this launch
+    int64_t nvalid;               // samples beyond this are padding (q = 0, V = 0)
+    double* q64;                  // [n x nm] selected q, FP64 (may be nullptr)
+    float* q32;                   // [n x nm] selected q, FP32 (may be nullptr)
+    double* v;                    // [n] V_anh (hartree)
+    unsigned long long* counters; // [2] non-finite, not converged
+};
+// pes: SCP3GPU_PES_*, fp32: run the potential in FP32.
+int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s);
+
+int launch_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters,
+                      const uint32_t* tasks, int ntasks, cudaStream_t s);
+
+int launch_std_normal(int dims, int64_t index0, int64_t n, const int64_t* vdir, const uint64_t* shift,
+                      double* out, cudaStream_t s);
+
+// FP64 plain form: Phi[i][s] and W[i][s] = V_s Phi[i][s], rows i < nb_pad, K = ldk.
+int launch_expand_fp64(const uint32_t* desc, int nb, int nb_pad, int nm, const double* q, const double* v,
+                       int64_t n, int64_t ldk, double* phi, double* w, cudaStream_t s);
+
+struct TileMap {
+    int tile;          // tile edge (64 FP64, 128 tensor-core)
+    int nt;            // tiles per side
+    int ntiles;        // upper tiles nt(nt+1)/2
+};
+// P[split][tile][tile*tile] += sum over this split's sample range of Phi_i W_j.
+int launch_contract_fp64(const double* phi, const double* w, int64_t ldk, int64_t k, int nb_pad,
+                         const TileMap& tm, int nsplit, double* partial, cudaStream_t s);
+
+// Sum the splits of P into a dense column-major nb x nb matrix (upper triangle
+// mirrored to the lower), divided by `divisor`; with `diag` (length nb) the
+// diagonal becomes (v + diag[i]) + zpe, the order of SCP3.cpp:237-239.
+int launch_unpack(const double* partial, const TileMap& tm, int nsplit, int nb, double divisor, const double* diag,
+                  double zpe, double* M, int64_t ld, cudaStream_t s);
+
+// Upload the TTM3-F constants (combined monomer coefficients, damping widths)
+// to the current device once.
+int ttm_init_device();
+
+}  // namespace scp3

@@ -1,0 +1,253 @@
+// Per-sample kernels: Sobol point (optionally scrambled) -> BSM -> q = y/sqrt(2)
+// -> Cartesian back-transform -> water potential -> anharmonic residual.
+// One warp per sample; the sample's q and geometry live in the warp's slice of
+// shared memory, lanes split the dimensions, the coordinates and the potential's
+// pair terms.  The FP64 form follows SCP3.cpp:196-223 operation for operation
+// where that is cheap (division by sqrt(2), x0 + MUa q then times bohr).
+#include "common.cuh"
+#include "internal.h"
+#include "pes_qtip4pf.cuh"
+#include "pes_ttm3f.cuh"
+#include "ps_coeffs.h"
+
+#include <cmath>
+#include <mutex>
+
+namespace scp3 {
+
+namespace {
+
+constexpr int kWarpsPerBlock = 8;
+
+template <typename T>
+struct WarpSlot {
+    double* q;      // nm0
+    T* crd;         // 9nw
+    T* ms;          // 3nw
+    T* ttm;         // TTM3-F scratch
+};
+
+template <typename T>
+__host__ __device__ inline size_t slot_bytes(int pes, int nm0, int nw)
+{
+    size_t b = sizeof(double) * (size_t)((nm0 + 1) & ~1) + sizeof(T) * (size_t)(12 * nw);
+    if (pes == SCP3GPU_PES_TTM3F) b += sizeof(T) * ttm::scratch_elems(nw);
+    return (b + 15) & ~(size_t)15;
+}
+
+template <typename T>
+__device__ inline WarpSlot<T> warp_slot(char* base, int pes, int nm0, int nw)
+{
+    WarpSlot<T> s;
+    s.q = reinterpret_cast<double*>(base);
+    s.crd = reinterpret_cast<T*>(s.q + ((nm0 + 1) & ~1));
+    s.ms = s.crd + 9 * nw;
+    s.ttm = s.ms + 3 * nw;
+    return s;
+}
+
+template <int PES, typename T>
+__device__ inline double potential(const WarpSlot<T>& w, int nw, const uint32_t* tasks, int ntasks, int lane,
+                                   int* iters)
+{
+    if (PES == SCP3GPU_PES_QTIP4PF) {
+        *iters = 0;
+        return qt::energy_warp<T>(w.crd, w.ms, nw, tasks, ntasks, lane);
+    }
+    return ttm::energy_warp<T>(w.crd, w.ms, w.ttm, nw, tasks, ntasks, lane, iters);
+}
+
+template <int PES, typename T>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs a)
+{
+    extern __shared__ __align__(16) char smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int nw = a.nw, nm0 = a.nm0, N3 = 9 * nw;
+    WarpSlot<T> w = warp_slot<T>(smem + wib * slot_bytes<T>(PES, nm0, nw), PES, nm0, nw);
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    for (int64_t s = (int64_t)blockIdx.x * kWarpsPerBlock + wib; s < a.n; s += nwarps) {
+        if (s >= a.nvalid) {        // padding sample: contributes nothing
+            if (lane == 0) a.v[s] = 0.0;
+            for (int m = lane; m < a.nm; m += 32) {
+                if (a.q64) a.q64[s * a.nm + m] = 0.0;
+                if (a.q32) a.q32[s * a.nm + m] = 0.0f;
+            }
+            continue;
+        }
+        // 1. standard normals -> q   (SCP3.cpp:196-201)
+        for (int d = lane; d < nm0; d += 32) {
+            double y;
+            if (a.normals) {
+                y = a.normals[s * nm0 + d];
+            } else {
+                uint64_t x = sobol_state(a.vdir, nm0, d, (uint64_t)(a.index0 + s));
+                if (a.shift) x ^= __ldg(a.shift + d);
+                y = bsm(sobol_uniform(x));
+            }
+            w.q[d] = y / 1.4142135623730951;   // by /= sqrt(2.0)
+        }
+        __syncwarp();
+        // 2. r = bohr * (x0 + MUa q)   (SCP3.cpp:208), FP64
+        for (int c = lane; c < N3; c += 32) {
+            double acc = 0.0;
+            for (int k = 0; k < nm0; k++) acc += __ldg(a.MUa + (size_t)k * N3 + c) * w.q[k];
+            w.crd[c] = (T)(kBohr * (__ldg(a.x0 + c) + acc));
+        }
+        __syncwarp();
+        // 3. V in hartree, anharmonic residual   (SCP3.cpp:219-223)
+        int iters = 0;
+        const double e = potential<PES, T>(w, nw, a.tasks, a.ntasks, lane, &iters);
+        double h = 0.0;
+        for (int d = lane; d < nm0; d += 32) h += w.q[d] * (__ldg(a.omega + d) * w.q[d]);
+        h = warp_sum(h);
+        const double V = e / kAuToKcalPerMol - 0.5 * h;
+        if (lane == 0) {
+            a.v[s] = V;
+            if (!isfinite(V)) atomicAdd(a.counters + 0, 1ull);
+            if (iters > kTtmMaxIter) atomicAdd(a.counters + 1, 1ull);
+        }
+        // 4. selected modes, coalesced per sample
+        for (int m = lane; m < a.nm; m += 32) {
+            const double qm = w.q[__ldg(a.modes + m)];
+            if (a.q64) a.q64[s * a.nm + m] = qm;
+            if (a.q32) a.q32[s * a.nm + m] = (float)qm;
+        }
+        __syncwarp();
+    }
+}
+
+template <int PES>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    pes_energy_kernel(int nw, int64_t n, const double* __restrict__ crd, double* __restrict__ E,
+                      int* __restrict__ iters_out, const uint32_t* __restrict__ tasks, int ntasks)
+{
+    extern __shared__ __align__(16) char smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    WarpSlot<double> w = warp_slot<double>(smem + wib * slot_bytes<double>(PES, 0, nw), PES, 0, nw);
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    for (int64_t g = (int64_t)blockIdx.x * kWarpsPerBlock + wib; g < n; g += nwarps) {
+        for (int c = lane; c < 9 * nw; c += 32) w.crd[c] = crd[g * 9 * nw + c];
+        __syncwarp();
+        int iters = 0;
+        const double e = potential<PES, double>(w, nw, tasks, ntasks, lane, &iters);
+        if (lane == 0) {
+            E[g] = e;
+            if (iters_out) iters_out[g] = iters;
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void std_normal_kernel(int dims, int64_t index0, int64_t n, const int64_t* __restrict__ vdir,
+                                  const uint64_t* __restrict__ shift, double* __restrict__ out)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * dims) return;
+    const int64_t s = t / dims;
+    const int d = (int)(t - s * dims);
+    uint64_t x = sobol_state(vdir, dims, d, (uint64_t)(index0 + s));
+    if (shift) x ^= shift[d];
+    out[t] = bsm(sobol_uniform(x));
+}
+
+int grid_for(int64_t nwarps_needed)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int64_t blocks = (nwarps_needed + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int64_t cap = (int64_t)sms * 16;
+    return (int)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
+}
+
+template <int PES, typename T>
+int launch_samples_t(const SampleArgs& a, cudaStream_t s)
+{
+    const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw);
+    if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_kernel<PES, T>,
+                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    samples_kernel<PES, T><<<grid_for(a.n), kWarpsPerBlock * 32, sm, s>>>(a);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
+}  // namespace
+
+int ttm_init_device()
+{
+    static std::mutex mu;
+    static bool done[128] = {false};
+    int dev = 0;
+    SCP3_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= 128) return fail(SCP3GPU_ERR_ARG, "device ordinal out of range");
+    if (done[dev]) return SCP3GPU_OK;
+    ttm::Consts c;
+    c.AA_HH = std::pow(0.496 * 0.496, 1.0 / 6.0);
+    c.AA_HM = std::pow(0.496 * 0.837, 1.0 / 6.0);
+    c.AA_MM = std::pow(0.837 * 0.837, 1.0 / 6.0);
+    c.aXX13 = std::pow(0.175, 1.0 / 3.0);
+    for (int i = 0; i < 245; i++)   // ps.cpp:508-511: f5z, fbasis, fcore, frest
+        c.c5z[i] = 0.999677885 * scp3_ps_c5zA[i] + 0.15860145369897 * scp3_ps_cbasis[i] +
+                   -1.6351695982132 * scp3_ps_ccore[i] + 1.0 * scp3_ps_crest[i];
+    c.phh1 = 0.999677885 * 16.94879431193463 * std::exp(12.66426998162947);
+    for (int i = 0; i < 84; i++) c.coefD[i] = scp3_ps_coefD[i];
+    for (int i = 0; i < 245; i++) {
+        c.idx1[i] = scp3_ps_idx1[i];
+        c.idx2[i] = scp3_ps_idx2[i];
+        c.idx3[i] = scp3_ps_idx3[i];
+    }
+    for (int i = 0; i < 84; i++) {
+        c.idxD0[i] = scp3_ps_idxD0[i];
+        c.idxD1[i] = scp3_ps_idxD1[i];
+        c.idxD2[i] = scp3_ps_idxD2[i];
+    }
+    SCP3_CUDA(cudaMemcpyToSymbol(ttm::kC, &c, sizeof(c)));
+    done[dev] = true;
+    return SCP3GPU_OK;
+}
+
+int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s)
+{
+    if (a.n <= 0) return SCP3GPU_OK;
+    if (pes == SCP3GPU_PES_QTIP4PF)
+        return fp32 ? launch_samples_t<SCP3GPU_PES_QTIP4PF, float>(a, s)
+                    : launch_samples_t<SCP3GPU_PES_QTIP4PF, double>(a, s);
+    if (pes == SCP3GPU_PES_TTM3F)
+        return fp32 ? launch_samples_t<SCP3GPU_PES_TTM3F, float>(a, s)
+                    : launch_samples_t<SCP3GPU_PES_TTM3F, double>(a, s);
+    return fail(SCP3GPU_ERR_ARG, "unknown potential id");
+}
+
+int launch_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters, const uint32_t* tasks,
+                      int ntasks, cudaStream_t s)
+{
+    if (n <= 0) return SCP3GPU_OK;
+    const size_t sm = kWarpsPerBlock * slot_bytes<double>(pes, 0, nw);
+    if (pes == SCP3GPU_PES_QTIP4PF) {
+        pes_energy_kernel<SCP3GPU_PES_QTIP4PF><<<grid_for(n), kWarpsPerBlock * 32, sm, s>>>(nw, n, crd, E, iters,
+                                                                                          tasks, ntasks);
+    } else if (pes == SCP3GPU_PES_TTM3F) {
+        if (sm > 48 * 1024)
+            SCP3_CUDA(cudaFuncSetAttribute(pes_energy_kernel<SCP3GPU_PES_TTM3F>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        pes_energy_kernel<SCP3GPU_PES_TTM3F><<<grid_for(n), kWarpsPerBlock * 32, sm, s>>>(nw, n, crd, E, iters,
+                                                                                        tasks, ntasks);
+    } else {
+        return fail(SCP3GPU_ERR_ARG, "unknown potential id");
+    }
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
+int launch_std_normal(int dims, int64_t index0, int64_t n, const int64_t* vdir, const uint64_t* shift, double* out,
+                      cudaStream_t s)
+{
+    const int64_t total = n * dims;
+    if (total <= 0) return SCP3GPU_OK;
+    std_normal_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(dims, index0, n, vdir, shift, out);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
+}  // namespace scp3

@@ -1,0 +1,42 @@
+// Split-precision (BF16x3) contraction on the tcgen05 tensor cores.
+#pragma once
+#include "internal.h"
+
+namespace scp3 {
+namespace tc {
+
+struct Plan {
+    int nb = 0, nb_pad = 0, nm = 0;
+    int nt = 0, ntiles = 0;       // 128-row tiles per side, upper tiles
+    int nsplit = 1;               // sample ranges per pass (each owns an FP64 partial per tile)
+    int64_t chunk = 0;            // samples per pass (multiple of kFlush)
+    int64_t slots = 0;            // K slots per pass after sign partition and padding
+    // device buffers
+    uint16_t* xhi = nullptr;      // [nb_pad][slots] bf16: sqrt|V| Phi, high part
+    uint16_t* xlo = nullptr;      // [nb_pad][slots] bf16: low part
+    int* slot_of = nullptr;       // [chunk] sample -> K slot
+    uint32_t* sign_groups = nullptr;  // [slots/16] bit per 16-sample group: 1 = negative V
+    int* group_meta = nullptr;    // per flush block: first negative 16-group
+    int2* tiles = nullptr;        // [ntiles] (ti, tj)
+    double* partial = nullptr;    // [nsplit][ntiles][128*128] FP64
+    void* tmap_hi = nullptr;      // CUtensorMap (host copy) for xhi / xlo
+    void* tmap_lo = nullptr;
+    int* err_flag = nullptr;      // bounded-wait failures
+};
+
+constexpr int kTile = 128;        // UMMA M = N = 128
+constexpr int kFlush = 4096;      // samples accumulated in FP32 (TMEM) before the FP64 flush
+constexpr int kSlotsPerFlush = kFlush + 64;  // sign partition pads each sign group to 16
+
+int create(Plan& p, int nb, int nm, int chunk_req, int sms);
+void destroy(Plan& p);
+int64_t pass_samples(const Plan& p, int64_t nvalid);
+int zero(Plan& p, cudaStream_t s);
+// pev/pkind (may be null): when given, an event pair is recorded around every
+// launch with its kind (1 preparation, 2 contraction) for the handle's timing.
+int accumulate_pass(Plan& p, const uint32_t* desc, int nb, int nm, const float* q32, const double* v, int64_t n,
+                    cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind);
+int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s);
+
+}  // namespace tc
+}  // namespace scp3

@@ -1,0 +1,72 @@
+"""CPU-side checks of the product: the C-ABI library loads and exports every
+symbol include/scp3gpu.h declares, its host-only entry points, and the host
+setup code (input reader, O H H reorder, normal modes)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "scp3gpu.h")).read()
+    return sorted(set(re.findall(r"\b(scp3gpu_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    from scp3_b200 import _lib
+    L = _lib.lib()
+    decl = declared_symbols()
+    assert decl, "no declarations found"
+    for name in decl:
+        assert hasattr(L, name), name
+    assert sorted(_lib.EXPORTS) == decl
+
+
+def test_basis_sizes_through_abi():
+    from scp3_b200 import _lib, modes
+    L = _lib.lib()
+    for nm, n2, n3, nb in ((12, 12, 0, 91), (48, 48, 0, 1225), (48, 48, 48, 20825)):
+        assert L.scp3gpu_basis_size(nm, n2, n3) == nb == modes.basis_size(nm, n2, n3)
+        for level in range(4):
+            assert L.scp3gpu_sub_basis_size(nm, n2, n3, level) == modes.sub_basis_size(nm, n2, n3, level)
+    assert L.scp3gpu_basis_size(4, 5, 0) == -1
+
+
+def test_no_device_is_an_error_status_not_a_crash():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from scp3_b200 import _lib
+    out = np.zeros(12)
+    rc = _lib.lib().scp3gpu_sobol_std_normal(12, 0, 1, 0, 0, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert rc == _lib.ERR_UNSUPPORTED
+
+
+def test_input_roundtrip_and_modes(tmp_path):
+    from scp3_b200 import clusters, constants as C, modes
+    import oracle
+    def en(X):
+        return np.array([oracle.qtip4pf(x) for x in np.atleast_2d(X)])
+    x, e, g, it = clusters.relax(en, clusters.dimer(), maxiter=300)
+    mass = np.tile(np.repeat([C.Omass, C.Hmass, C.Hmass], 3), 2)
+    H, x0 = clusters.hessian(en, x, mass)
+    # write H-first order to exercise the O H H reorder
+    orig = ["O", "H", "H", "O", "H", "H"]
+    perm = [1, 0, 2, 4, 3, 5]             # file order: H O H H O H
+    p3 = np.concatenate([[3 * a, 3 * a + 1, 3 * a + 2] for a in perm])
+    path = str(tmp_path / "d.dat")
+    modes.write_input(path, [orig[a] for a in perm], x0[p3], H[np.ix_(p3, p3)])
+    sp, m2, x2, H2 = modes.read_input(path)
+    _, m3, x3, H3 = modes.ohhohh(m2, x2, H2)
+    assert np.allclose(x3, x0, atol=1e-14) and np.allclose(H3, H, atol=1e-14)
+    omega, MUa, w2 = modes.normal_modes(H3, m3)
+    assert omega.size == 12 and np.all(omega > 0)
+    assert np.all(np.abs(w2[:6]) < 1e-10)
+    # mass-weighted orthonormality: MUa^T M MUa = diag(1/omega)
+    G = MUa.T @ (m3[:, None] * MUa)
+    assert np.allclose(G, np.diag(1 / omega), rtol=1e-10)
+    assert list(modes.parse_modes("0-3,7,9-10")) == [0, 1, 2, 3, 7, 9, 10]
