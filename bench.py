@@ -154,7 +154,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "bf16x3"])
+    ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -246,6 +246,20 @@ def main():
             "kernel_ms": {"per_sample": ms[0], "expand": ms[1], "contract": ms[2], "readout": ms[3]},
             "clocks": clk, "status": {"rc": rc, "nonfinite": nonfinite, "not_converged": notconv}}
 
+    if rank == 0 and args.precision != "fp64":
+        # quality gate of the metric: the same 2^20 points through the FP64 plain form
+        hb.reset()
+        hb.accumulate(base, SAMPLES)
+        e_split = hb.eigvals(10)
+        hb64 = scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=0, pes="qtip4pf", precision="fp64",
+                                scramble_seed=SCRAMBLE_SEED, device=local)
+        hb64.accumulate(base, SAMPLES)
+        e64 = hb64.eigvals(10)
+        hb64.close()
+        autocm = scp3_b200.constants.autocm
+        line["levels"] = {"max_abs_err_cm1_vs_fp64": float(np.abs(e_split - e64).max() * autocm),
+                          "lowest10_cm1_fp64": [float(x * autocm) for x in e64],
+                          "samples": SAMPLES}
     if rank == 0 and not args.no_e2e:
         # the -r path with host buffers: normals in from pinned memory, Mout back to host
         normals = torch.from_numpy(scp3_b200.std_normals(nm0, 1 << 41, SAMPLES, scramble_seed=SCRAMBLE_SEED))

@@ -1,25 +1,592 @@
-// Split-precision contraction (placeholder until the tcgen05 kernel lands).
+// Split-precision contraction on the 5th-generation tensor cores (tcgen05).
+//
+//   M_ij += sum_s Phi_i(s) V_s Phi_j(s)       (the -G accumulation,
+//                                              ScaledMatrixElements.cpp:951-971)
+//
+// Operand.  X_i(s) = sqrt|V_s| Phi_i(s), so that X_i X_j = |V_s| Phi_i Phi_j and
+// one operand array serves as both A (rows of tile ti) and B (rows of tile tj).
+// Within every 4096-sample flush block the samples are stably partitioned by the
+// sign of V (positive first), each sign group padded to a multiple of 16, so a
+// whole K=16 MMA step has one sign; negative steps set the negate-A bit of the
+// instruction descriptor.  X is stored split, X = hi + lo in BF16 (hi = bf16(x),
+// lo = bf16(x - hi)), and every product is formed as hi*hi + hi*lo + lo*hi
+// (three kind::f16 MMAs into one FP32 TMEM accumulator).
+//
+// Accumulation.  Each CTA owns one 128x128 upper tile (ti <= tj) and one range
+// of flush blocks of the pass.  The FP32 accumulator lives in TMEM and is
+// flushed into the CTA's FP64 partial tile in global memory every 4096 samples;
+// two TMEM accumulators alternate so the flush of one block overlaps the MMAs of
+// the next.  Partials of different sample ranges are summed at read-out.
+//
+// Warp roles (192 threads): warp 0 lane 0 issues the TMA loads (SWIZZLE_128B,
+// 64 K-slots x 128 rows per box), warp 1 owns TMEM and lane 0 issues the MMAs
+// and commits, warps 2..5 drain the accumulators.  Every mbarrier wait is
+// bounded (4 s of %globaltimer); on expiry the CTA records an error, stops
+// issuing, waits (bounded) for its own loads and MMAs, frees TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "common.cuh"
 #include "tc.h"
 
 namespace scp3 {
 namespace tc {
 
+namespace {
+
+constexpr int kBK = 64;                      // K slots per stage (128 B of bf16: one swizzle atom)
+constexpr int kStages = 3;
+constexpr int kTileBytes = kTile * kBK * 2;  // 16 KB per operand box
+constexpr int kStageBytes = 4 * kTileBytes;  // A_hi A_lo B_hi B_lo
+constexpr int kKBlocks = kSlotsPerFlush / kBK;   // 65 k-blocks per flush block
+constexpr int kGroups = kSlotsPerFlush / 16;     // 260 sign groups per flush block
+constexpr int kThreads = 192;
+constexpr int kSmemBytes = kStages * kStageBytes + 1024 /* align */ + 256 /* barriers */;
+constexpr unsigned long long kWaitNs = 4000000000ull;
+
+// instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A/B BF16 (bits 7-9,
+// 10-12 = 1), both K-major (bits 15/16 = 0), N>>3 at bits 17-22, M>>4 at 24-28.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTile >> 3) << 17) |
+                            ((uint32_t)(kTile >> 4) << 24);
+constexpr uint32_t kIdescNegA = kIdesc | (1u << 13);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; false (and the CTA's abort flag set) if the phase did not complete in time.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort)
+{
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    for (uint32_t it = 1;; it++) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 255u) == 0) {
+            if (*abort) return false;
+            if (globaltimer() - t0 > kWaitNs) {
+                *abort = 1;
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// K-major, SWIZZLE_128B shared-memory matrix descriptor: start address >> 4,
+// LBO 16 B (unused for swizzled K-major), SBO 1024 B (8 rows x 128 B), version 1
+// (bits 46-47), layout type 2 = SWIZZLE_128B (bits 61-63).
+__device__ __forceinline__ uint64_t smem_desc(const void* p)
+{
+    const uint64_t addr = smem_u32(p);
+    return ((addr >> 4) & 0x3FFFull) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
+        "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[j]);
+}
+
+// grid: (ntiles, nsplit).  Split s takes flush blocks [s*nflush/nsplit, (s+1)*nflush/nsplit).
+__global__ void __launch_bounds__(kThreads, 1)
+    contract_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
+                           const int2* __restrict__ tiles, const int* __restrict__ neg_group, int nflush, int ntiles,
+                           double* __restrict__ partial, int* __restrict__ err_flag)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+    uint64_t* full = bars;                    // [kStages]
+    uint64_t* empty = bars + kStages;         // [kStages]
+    uint64_t* acc_full = bars + 2 * kStages;  // [2]
+    uint64_t* acc_empty = acc_full + 2;       // [2]
+    uint64_t* drain = acc_empty + 2;          // [1]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int2 tt = tiles[blockIdx.x];
+    const bool diag = tt.x == tt.y;
+    const int split = blockIdx.y, nsplit = gridDim.y;
+    const int f0 = (int)((int64_t)split * nflush / nsplit), f1 = (int)((int64_t)(split + 1) * nflush / nsplit);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(acc_full + a, 1);
+            mbar_init(acc_empty + a, 4);
+        }
+        mbar_init(drain, 1);
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            const uint32_t bytes = diag ? 2 * kTileBytes : 4 * kTileBytes;
+            int stage = 0;
+            uint32_t phase = 0;
+            int issued[kStages] = {0, 0, 0};
+            uint32_t issued_phase[kStages] = {0, 0, 0};
+            for (int f = f0; f < f1 && !*abort; f++) {
+                for (int kb = 0; kb < kKBlocks; kb++) {
+                    if (!mbar_wait(empty + stage, phase ^ 1, abort)) break;
+                    uint8_t* st = smem + stage * kStageBytes;
+                    mbar_expect_tx(full + stage, bytes);
+                    const int x = f * kSlotsPerFlush + kb * kBK;
+                    tma_load_2d(&map_hi, full + stage, st, x, tt.x * kTile);
+                    tma_load_2d(&map_lo, full + stage, st + kTileBytes, x, tt.x * kTile);
+                    if (!diag) {
+                        tma_load_2d(&map_hi, full + stage, st + 2 * kTileBytes, x, tt.y * kTile);
+                        tma_load_2d(&map_lo, full + stage, st + 3 * kTileBytes, x, tt.y * kTile);
+                    }
+                    issued[stage] = 1;
+                    issued_phase[stage] = phase;
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            if (*abort) {   // let our own loads land before the CTA leaves
+                for (int s = 0; s < kStages; s++)
+                    if (issued[s]) {
+                        volatile int never = 0;
+                        mbar_wait(full + s, issued_phase[s], &never);
+                    }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int stage = 0, use = 0;
+            uint32_t phase = 0;
+            for (int f = f0; f < f1 && !*abort; f++, use++) {
+                const int a = use & 1;
+                const uint32_t acc_parity = ((use >> 1) & 1) ^ 1;
+                if (!mbar_wait(acc_empty + a, acc_parity, abort)) break;
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(a * kTile);
+                const int neg0 = neg_group[f];
+                bool ok = true;
+                for (int kb = 0; kb < kKBlocks; kb++) {
+                    if (!mbar_wait(full + stage, phase, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    uint8_t* st = smem + stage * kStageBytes;
+                    const uint64_t ahi = smem_desc(st), alo = smem_desc(st + kTileBytes);
+                    const uint64_t bhi = diag ? ahi : smem_desc(st + 2 * kTileBytes);
+                    const uint64_t blo = diag ? alo : smem_desc(st + 3 * kTileBytes);
+#pragma unroll
+                    for (int kk = 0; kk < kBK / 16; kk++) {
+                        const uint32_t idesc = (kb * 4 + kk >= neg0) ? kIdescNegA : kIdesc;
+                        const uint64_t adv = (uint64_t)(kk * 2);    // 32 B along K inside the swizzle atom
+                        mma_bf16(d, ahi + adv, bhi + adv, idesc, (kb | kk) != 0);
+                        mma_bf16(d, ahi + adv, blo + adv, idesc, 1);
+                        mma_bf16(d, alo + adv, bhi + adv, idesc, 1);
+                    }
+                    mma_commit(empty + stage);      // frees the stage once these MMAs have read it
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+                if (!ok) break;
+                mma_commit(acc_full + a);
+            }
+            mma_commit(drain);                     // completes when every MMA above has
+            volatile int never = 0;
+            mbar_wait(drain, 0, &never);
+        }
+    } else {
+        // epilogue: warps 2..5 own TMEM lane quadrants warp%4
+        const int quad = warp & 3;
+        const int row = quad * 32 + lane;
+        int use = 0;
+        for (int f = f0; f < f1; f++, use++) {
+            const int a = use & 1;
+            if (!mbar_wait(acc_full + a, (use >> 1) & 1, abort)) break;
+            tc_fence_after();
+            double* P = partial + ((size_t)split * ntiles + blockIdx.x) * (kTile * kTile);
+            const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * kTile);
+#pragma unroll 1
+            for (int c0 = 0; c0 < kTile; c0 += 32) {
+                float v[32];
+                tmem_ld32(base + c0, v);
+#pragma unroll
+                for (int j = 0; j < 32; j++) P[(size_t)(c0 + j) * kTile + row] += (double)v[j];
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acc_empty + a);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort) atomicExch(err_flag, 1);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem));
+    }
+}
+
+// One CTA of 1024 threads per flush block: stable partition of its 4096 samples
+// by the sign of V into K slots; writes slot -> sample (-1 = zero padding) and the
+// first negative 16-group of the block.
+__global__ void __launch_bounds__(1024) partition_kernel(const double* __restrict__ v, int* __restrict__ sample_of_slot,
+                                                         int* __restrict__ neg_group)
+{
+    __shared__ int wpos[32], wneg[32], tot[2];
+    const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int64_t s0 = (int64_t)b * kFlush + 4 * t;
+    int flags = 0, np = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const bool pos = !(v[s0 + k] < 0.0);
+        flags |= (int)pos << k;
+        np += pos;
+    }
+    int nn = 4 - np;
+    // inclusive warp scans
+    int ip = np, in = nn;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int a = __shfl_up_sync(0xffffffffu, ip, o), c = __shfl_up_sync(0xffffffffu, in, o);
+        if (lane >= o) {
+            ip += a;
+            in += c;
+        }
+    }
+    if (lane == 31) {
+        wpos[w] = ip;
+        wneg[w] = in;
+    }
+    __syncthreads();
+    if (w == 0) {
+        int p = wpos[lane], n = wneg[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int a = __shfl_up_sync(0xffffffffu, p, o), c = __shfl_up_sync(0xffffffffu, n, o);
+            if (lane >= o) {
+                p += a;
+                n += c;
+            }
+        }
+        wpos[lane] = p - wpos[lane];   // exclusive
+        wneg[lane] = n - wneg[lane];
+        if (lane == 31) {
+            tot[0] = p;
+            tot[1] = n;
+        }
+    }
+    __syncthreads();
+    const int P = tot[0], N = tot[1], P16 = (P + 15) & ~15;
+    int op = wpos[w] + ip - np, on = wneg[w] + in - nn;
+    int* out = sample_of_slot + (size_t)b * kSlotsPerFlush;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if ((flags >> k) & 1) out[op++] = (int)(s0 + k);
+        else out[P16 + on++] = (int)(s0 + k);
+    }
+    for (int sl = t; sl < kSlotsPerFlush; sl += 1024)
+        if ((sl >= P && sl < P16) || sl >= P16 + N) out[sl] = -1;
+    if (t == 0) neg_group[b] = P16 / 16;
+}
+
+// Expansion into the split operand: thread per K slot, rows in blocks of 64.
+constexpr int kExpSlots = 64, kExpRows = 64;   // 4160 slots per flush block = 65 x 64
+
+__device__ __forceinline__ float h1(float y) { return 1.41421356f * y; }
+__device__ __forceinline__ float h2(float y) { return (2.0f * y * y - 1.0f) * 0.70710678f; }
+__device__ __forceinline__ float h3(float y) { return (2.0f * y * y - 3.0f) * y * 0.57735027f; }
+
+__global__ void __launch_bounds__(kExpSlots) expand_split_kernel(const uint32_t* __restrict__ desc, int nb, int nb_pad,
+                                                                  int nm, const float* __restrict__ q,
+                                                                  const double* __restrict__ v,
+                                                                  const int* __restrict__ sample_of_slot, int64_t ldk,
+                                                                  __nv_bfloat16* __restrict__ xhi,
+                                                                  __nv_bfloat16* __restrict__ xlo)
+{
+    extern __shared__ float qs[];   // [nm][kExpSlots]
+    const int t = threadIdx.x;
+    const int64_t slot = (int64_t)blockIdx.x * kExpSlots + t;
+    const int s = sample_of_slot[slot];
+    for (int m = 0; m < nm; m++) qs[m * kExpSlots + t] = (s >= 0) ? q[(int64_t)s * nm + m] : 0.0f;
+    const float sv = (s >= 0) ? (float)sqrt(fabs(v[s])) : 0.0f;
+    __syncthreads();
+    const int r0 = blockIdx.y * kExpRows, r1 = min(r0 + kExpRows, nb_pad);
+    for (int i = r0; i < r1; i++) {
+        float x = 0.0f;
+        if (i < nb && s >= 0) {
+            const uint32_t d = __ldg(desc + i);
+            const int m = (d >> 3) & 255, n = (d >> 11) & 255, p = (d >> 19) & 255;
+            const float qm = qs[m * kExpSlots + t];
+            float ph;
+            switch (d & 7u) {
+                case kGround: ph = 1.0f; break;
+                case kHo1: ph = h1(qm); break;
+                case kHo2: ph = h2(qm); break;
+                case kHo1Ho1: ph = h1(qm) * h1(qs[n * kExpSlots + t]); break;
+                case kHo3: ph = h3(qm); break;
+                case kHo2Ho1: ph = h2(qm) * h1(qs[n * kExpSlots + t]); break;
+                case kHo1Ho2: ph = h1(qm) * h2(qs[n * kExpSlots + t]); break;
+                default: ph = h1(qm) * h1(qs[n * kExpSlots + t]) * h1(qs[p * kExpSlots + t]); break;
+            }
+            x = sv * ph;
+        }
+        const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+        xhi[(size_t)i * ldk + slot] = hi;
+        xlo[(size_t)i * ldk + slot] = lo;
+    }
+}
+
+// Dense column-major nb x nb from the tile partials (tile-local column-major).
+__global__ void unpack_tc_kernel(const double* __restrict__ partial, int nt, int ntiles, int nsplit, int nb,
+                                 double divisor, const double* __restrict__ diag, double zpe, double* __restrict__ M,
+                                 int64_t ld)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)nb * nb) return;
+    const int j = (int)(e / nb), i = (int)(e - (int64_t)j * nb);
+    const int r = min(i, j), c = max(i, j);
+    const int ti = r / kTile, tj = c / kTile;
+    const int t = ti * nt - ti * (ti - 1) / 2 + (tj - ti);
+    const size_t off = (size_t)t * kTile * kTile + (size_t)(c - tj * kTile) * kTile + (r - ti * kTile);
+    double val = 0.0;
+    for (int s = 0; s < nsplit; s++) val += partial[(size_t)s * ntiles * kTile * kTile + off];
+    val = val / divisor;
+    if (diag && i == j) val = (val + diag[i]) + zpe;
+    M[(size_t)j * ld + i] = val;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode()
+{
+    static std::mutex mu;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+int encode_map(void** out, void* base, int64_t slots, int rows)
+{
+    auto enc = get_encode();
+    if (!enc) return fail(SCP3GPU_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+    CUtensorMap* m = new CUtensorMap;
+    cuuint64_t dims[2] = {(cuuint64_t)slots, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)slots * 2};
+    cuuint32_t box[2] = {kBK, kTile};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        delete m;
+        return fail(SCP3GPU_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    }
+    *out = m;
+    return SCP3GPU_OK;
+}
+
+void record(std::vector<cudaEvent_t>* pev, std::vector<int>* pkind, int kind, cudaStream_t s)
+{
+    if (!pev) return;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, s);
+    pev->push_back(e);
+    pkind->push_back(kind);
+}
+
+}  // namespace
+
 int create(Plan& p, int nb, int nm, int chunk_req, int sms)
 {
-    (void)p, (void)nb, (void)nm, (void)chunk_req, (void)sms;
-    return fail(SCP3GPU_ERR_UNSUPPORTED, "BF16x3 contraction not built yet");
+    p.nb = nb;
+    p.nm = nm;
+    p.nt = (nb + kTile - 1) / kTile;
+    p.nb_pad = p.nt * kTile;
+    p.ntiles = p.nt * (p.nt + 1) / 2;
+    int64_t chunk = chunk_req > 0 ? chunk_req : (int64_t)kFlush * 32;
+    // the split operand of one pass stays under ~6 GB
+    while (chunk > kFlush && (int64_t)p.nb_pad * (chunk / kFlush) * kSlotsPerFlush * 4 > (6ll << 30)) chunk /= 2;
+    chunk = chunk / kFlush * kFlush;
+    p.chunk = chunk;
+    const int nflush = (int)(chunk / kFlush);
+    p.slots = (int64_t)nflush * kSlotsPerFlush;
+    int nsplit = 1;
+    while (nsplit < nflush && (int64_t)p.ntiles * nsplit < 2ll * sms) nsplit *= 2;
+    p.nsplit = nsplit;
+    std::vector<int2> t;
+    for (int i = 0; i < p.nt; i++)
+        for (int j = i; j < p.nt; j++) t.push_back(make_int2(i, j));
+    SCP3_CUDA(cudaMalloc(&p.xhi, sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
+    SCP3_CUDA(cudaMalloc(&p.xlo, sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
+    SCP3_CUDA(cudaMalloc(&p.slot_of, sizeof(int) * (size_t)p.slots));
+    SCP3_CUDA(cudaMalloc(&p.group_meta, sizeof(int) * nflush));
+    SCP3_CUDA(cudaMalloc(&p.tiles, sizeof(int2) * t.size()));
+    SCP3_CUDA(cudaMemcpy(p.tiles, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice));
+    SCP3_CUDA(cudaMalloc(&p.partial, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kTile));
+    SCP3_CUDA(cudaMalloc(&p.err_flag, sizeof(int)));
+    SCP3_CUDA(cudaMemset(p.err_flag, 0, sizeof(int)));
+    int rc = encode_map(&p.tmap_hi, p.xhi, p.slots, p.nb_pad);
+    if (!rc) rc = encode_map(&p.tmap_lo, p.xlo, p.slots, p.nb_pad);
+    if (rc) return rc;
+    SCP3_CUDA(cudaFuncSetAttribute(contract_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    return SCP3GPU_OK;
 }
-void destroy(Plan& p) { (void)p; }
-int64_t pass_samples(const Plan& p, int64_t nvalid) { return (void)p, nvalid; }
-int zero(Plan& p, cudaStream_t s) { return (void)p, (void)s, SCP3GPU_OK; }
-int accumulate_pass(Plan&, const uint32_t*, int, int, const float*, const double*, int64_t, cudaStream_t,
-                    std::vector<cudaEvent_t>*, std::vector<int>*)
+
+void destroy(Plan& p)
 {
-    return fail(SCP3GPU_ERR_UNSUPPORTED, "BF16x3 contraction not built yet");
+    void* ptrs[] = {p.xhi, p.xlo, p.slot_of, p.sign_groups, p.group_meta, p.tiles, p.partial, p.err_flag};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    delete static_cast<CUtensorMap*>(p.tmap_hi);
+    delete static_cast<CUtensorMap*>(p.tmap_lo);
+    p = Plan{};
 }
-int unpack(Plan&, int, double, const double*, double, double*, int64_t, cudaStream_t)
+
+int64_t pass_samples(const Plan& p, int64_t nvalid)
 {
-    return fail(SCP3GPU_ERR_UNSUPPORTED, "BF16x3 contraction not built yet");
+    (void)p;
+    return (nvalid + kFlush - 1) / kFlush * kFlush;
+}
+
+int zero(Plan& p, cudaStream_t s)
+{
+    SCP3_CUDA(cudaMemsetAsync(p.partial, 0, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kTile, s));
+    SCP3_CUDA(cudaMemsetAsync(p.err_flag, 0, sizeof(int), s));
+    return SCP3GPU_OK;
+}
+
+int accumulate_pass(Plan& p, const uint32_t* desc, int nb, int nm, const float* q32, const double* v, int64_t n,
+                    cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind)
+{
+    if (n % kFlush != 0 || n > p.chunk) return fail(SCP3GPU_ERR_ARG, "tc pass: sample count not in flush blocks");
+    const int nflush = (int)(n / kFlush);
+    const int64_t slots = (int64_t)nflush * kSlotsPerFlush;
+    record(pev, pkind, 1, s);
+    partition_kernel<<<nflush, 1024, 0, s>>>(v, p.slot_of, p.group_meta);
+    SCP3_CUDA(cudaGetLastError());
+    const size_t sm = sizeof(float) * nm * kExpSlots;
+    if (sm > 48 * 1024)
+        SCP3_CUDA(cudaFuncSetAttribute(expand_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    dim3 eg((unsigned)(slots / kExpSlots), (unsigned)((p.nb_pad + kExpRows - 1) / kExpRows));
+    expand_split_kernel<<<eg, kExpSlots, sm, s>>>(desc, nb, p.nb_pad, nm, q32, v, p.slot_of, p.slots,
+                                                   reinterpret_cast<__nv_bfloat16*>(p.xhi),
+                                                   reinterpret_cast<__nv_bfloat16*>(p.xlo));
+    SCP3_CUDA(cudaGetLastError());
+    record(pev, pkind, 1, s);
+    record(pev, pkind, 2, s);
+    const int nsplit = p.nsplit < nflush ? p.nsplit : nflush;
+    dim3 grid(p.ntiles, nsplit);
+    contract_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(*static_cast<CUtensorMap*>(p.tmap_hi),
+                                                              *static_cast<CUtensorMap*>(p.tmap_lo), p.tiles,
+                                                              p.group_meta, nflush, p.ntiles, p.partial, p.err_flag);
+    SCP3_CUDA(cudaGetLastError());
+    record(pev, pkind, 2, s);
+    return SCP3GPU_OK;
+}
+
+int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s)
+{
+    int err = 0;
+    SCP3_CUDA(cudaMemcpyAsync(&err, p.err_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SCP3_CUDA(cudaStreamSynchronize(s));
+    if (err) return fail(SCP3GPU_ERR_TIMEOUT, "tensor-core contraction: a bounded pipeline wait expired");
+    const int64_t total = (int64_t)nb * nb;
+    unpack_tc_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p.partial, p.nt, p.ntiles, p.nsplit, nb, divisor,
+                                                                      diag, zpe, M, ld);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
 }
 
 }  // namespace tc

@@ -1,0 +1,71 @@
+"""GPU parity of the split-precision form (BF16x3 tcgen05 contraction, FP32
+potential, FP32 accumulation flushed to FP64 every 4096 samples) against the
+reference's golden matrices and against the FP64 plain form.
+
+Tolerance per element: 5e-4 of sum_s |Phi_i||V||Phi_j| -- the FP32 running sum
+of one 4096-sample flush block is bounded by 4096 * 2^-24 = 2.4e-4 of that
+scale, BF16x3 products add ~1e-5 and the FP32 potential ~1e-5.  Eigenvalues of
+Mout: within 0.1 cm^-1 of the FP64 form."""
+import numpy as np
+import pytest
+
+from conftest import load_hbuild_case, upper_to_full
+
+pytestmark = pytest.mark.gpu
+AUTOCM = 2.194746313e5
+
+
+@pytest.fixture(scope="module")
+def scp3():
+    import torch
+    assert torch.cuda.is_available()
+    import scp3_b200
+    return scp3_b200
+
+
+def _build(scp3, c, precision):
+    sseed = int(c["scramble_seed"])
+    return scp3.HBuild(int(c["nw"]), c["x0"], c["MUa"], c["omega"], modes=c["modes"], n2=int(c["n2"]),
+                       n3=int(c["n3"]), pes=int(c["pes"]), precision=precision,
+                       scramble_seed=None if sseed < 0 else sseed)
+
+
+@pytest.mark.parametrize("name", ["dimer_qtip4pf", "hexamer_qtip4pf", "dimer_ttm3f", "hexamer_qtip4pf_modesel"])
+def test_bf16x3_matches_reference(scp3, oracle_mod, name):
+    c = load_hbuild_case(name)
+    ns = int(c["nsamples"])
+    hb = _build(scp3, c, "bf16x3")
+    hb.accumulate(int(c["index0"]), ns)
+    M = hb.read(0)
+    assert hb.status()[0] == 0
+    nb = M.shape[0]
+    ref = upper_to_full(c["M_upper"], nb)
+    sseed = int(c["scramble_seed"])
+    normals = oracle_mod.std_normals(c["omega"].size, int(c["index0"]), ns, scramble_seed=None if sseed < 0 else sseed)
+    q, v = oracle_mod.samples(int(c["pes"]), int(c["nw"]), c["x0"], c["MUa"], c["omega"], normals)
+    A = oracle_mod.accumulate(q[:, c["modes"]], v, int(c["n2"]), int(c["n3"]), absolute=True)
+    A = A + np.triu(A, 1).T
+    rel = np.abs(M - ref) / np.maximum(A, 1e-300)
+    assert rel.max() <= 5e-4, rel.max()
+    assert np.median(rel) <= 2e-5, np.median(rel)
+    # levels of Mout within 0.1 cm^-1 of the FP64 reference matrix
+    hb64 = _build(scp3, c, "fp64")
+    hb64.accumulate(int(c["index0"]), ns)
+    e32 = hb.eigvals(min(10, nb))
+    e64 = hb64.eigvals(min(10, nb))
+    assert np.abs(e32 - e64).max() * AUTOCM <= 0.1, (e32 - e64) * AUTOCM
+
+
+def test_bf16x3_hexamer_doubles_levels(scp3):
+    from scp3_b200 import inputs
+    nw, x0, MUa, omega = inputs.load("prism_qtip4pf", build_if_missing=False)
+    ns = 1 << 16
+    out = {}
+    for prec in ("bf16x3", "fp64"):
+        hb = scp3.HBuild(nw, x0, MUa, omega, n2=48, n3=0, precision=prec, scramble_seed=0x5C3)
+        hb.accumulate(0, ns)
+        assert hb.sample_count() == ns and hb.status()[0] == 0
+        out[prec] = (hb.read(1), hb.eigvals(10))
+    (M32, e32), (M64, e64) = out["bf16x3"], out["fp64"]
+    assert np.abs(e32 - e64).max() * AUTOCM <= 0.1, (e32 - e64) * AUTOCM
+    assert np.linalg.norm(M32 - M64) <= 1e-4 * np.linalg.norm(M64)
