@@ -49,6 +49,7 @@ extern "C" {
 #define SCP3GPU_PREC_FP64 0   /* plain: everything FP64 (parity form)                  */
 #define SCP3GPU_PREC_BF16X3 1 /* split: potential FP32, contraction BF16x3 on tcgen05,
                                  FP32 accumulation flushed to FP64 every 4096 samples */
+#define SCP3GPU_PREC_BF16X3_PES64 2 /* split contraction as above, potential in FP64       */
 
 /* sampling */
 #define SCP3GPU_SOBOL_REFERENCE 0 /* i8_sobol points, unscrambled (sobol.cpp:14198-27868) */

@@ -86,6 +86,7 @@ struct scp3gpu_hbuild {
     int64_t chunk = 0;
     TileMap tm{};
     bool split_form = false;
+    bool pes_fp32 = false;
     // tables
     int64_t* vdir = nullptr;
     uint64_t* shift = nullptr;
@@ -151,7 +152,7 @@ void plan_fp64(scp3gpu_hbuild* h, int sms)
 
 int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double* normals_dev)
 {
-    const bool fp32 = h->split_form;
+    const bool fp32 = h->pes_fp32;
     SampleArgs a{};
     a.nw = h->cfg.nw;
     a.nm0 = h->cfg.nmodes0;
@@ -168,8 +169,8 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     a.index0 = index0;
     a.n = h->split_form ? tc::pass_samples(h->tcp, nvalid) : round_up(nvalid, 16ll * h->nsplit);
     a.nvalid = nvalid;
-    a.q64 = fp32 ? nullptr : h->q64;
-    a.q32 = fp32 ? h->q32 : nullptr;
+    a.q64 = h->split_form ? nullptr : h->q64;
+    a.q32 = h->split_form ? h->q32 : nullptr;
     a.v = h->v;
     a.counters = h->counters;
     int rc;
@@ -344,7 +345,8 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
         return fail(SCP3GPU_ERR_ARG, "Number of double or triple excitations exceed number of modes.");
     if (!c->x0 || !c->MUa || !c->omega || !c->modes) return fail(SCP3GPU_ERR_ARG, "null geometry or mode arrays");
     if (c->pes != SCP3GPU_PES_QTIP4PF && c->pes != SCP3GPU_PES_TTM3F) return fail(SCP3GPU_ERR_ARG, "unknown potential");
-    if (c->precision != SCP3GPU_PREC_FP64 && c->precision != SCP3GPU_PREC_BF16X3)
+    if (c->precision != SCP3GPU_PREC_FP64 && c->precision != SCP3GPU_PREC_BF16X3 &&
+        c->precision != SCP3GPU_PREC_BF16X3_PES64)
         return fail(SCP3GPU_ERR_ARG, "unknown precision");
     if (c->pes == SCP3GPU_PES_TTM3F && c->nw > 8) return fail(SCP3GPU_ERR_ARG, "TTM3-F kernel supports nw <= 8");
     if (c->chunk < 0 || c->chunk % 4096 != 0) return fail(SCP3GPU_ERR_ARG, "chunk must be a multiple of 4096");
@@ -360,7 +362,8 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     h->cfg.x0 = h->cfg.MUa = h->cfg.omega = nullptr;
     h->cfg.modes = nullptr;
     h->dev = c->device;
-    h->split_form = c->precision == SCP3GPU_PREC_BF16X3;
+    h->split_form = c->precision != SCP3GPU_PREC_FP64;
+    h->pes_fp32 = c->precision == SCP3GPU_PREC_BF16X3;
     const int nm0 = c->nmodes0, N3 = 9 * c->nw;
     h->nb = (int)scp3gpu_basis_size(c->nmodes, c->n2, c->n3);
     // HO diagonal of the selected modes and the inactive-mode zero point (SCP3.cpp:239)

@@ -65,16 +65,16 @@ template <typename T>
 __device__ double energy_warp(const T* crd, T* ms, int nw, const uint32_t* __restrict__ tasks, int ntasks,
                               int lane)
 {
-    T part = 0;
+    double part = 0;     // terms in T, their sums in FP64
     for (int i = lane; i < nw; i += 32) {
         const T* w = crd + 9 * i;
 #pragma unroll
         for (int k = 0; k < 3; k++) ms[3 * i + k] = T(kGammaM) * w[k] + T(kGamma1) * (w[3 + k] + w[6 + k]);
-        part += monomer(w);
+        part += (double)monomer(w);
     }
     __syncwarp();
-    for (int t = lane; t < ntasks; t += 32) part += pair(__ldg(tasks + t), crd, ms);
-    return warp_sum((double)part);
+    for (int t = lane; t < ntasks; t += 32) part += (double)pair(__ldg(tasks + t), crd, ms);
+    return warp_sum(part);
 }
 
 }  // namespace qt

@@ -177,13 +177,13 @@ __device__ double energy_warp(const T* crd, T* ms, T* sc, int nw, const uint32_t
       *ddt = efd + n3, *fpow = ddt + n3 * n3;
     for (int i = lane; i < n3 * n3; i += 32) ddt[i] = T(0);
     for (int i = lane; i < n3; i += 32) phi[i] = efq[i] = efd[i] = T(0);
-    T part = 0;
+    double part = 0;
     for (int i = lane; i < nw; i += 32) {
         const T* w = crd + 9 * i;
         for (int k = 0; k < 3; k++) ms[3 * i + k] = T(kGamma1) * w[k] + T(kGamma2) * (w[3 + k] + w[6 + k]);
         T e, q3[3];
         monomer(w, fpow + 48 * i, e, q3);
-        part += e;
+        part += (double)e;
         const T t = T(kGamma2 / kGamma1);
         chg[3 * i + 0] = T(kChargeCon) * q3[0] / T(kGamma1);
         chg[3 * i + 1] = T(kChargeCon) * (q3[1] + t * (q3[1] + q3[2]));
@@ -209,7 +209,7 @@ __device__ double energy_warp(const T* crd, T* ms, T* sc, int nw, const uint32_t
             atomicAdd(phi + b, chg[a] * ts0);
         } else if (type == 2) {     // O/O van der Waals  (ttm3f.cpp:204-219)
             const T r2 = dist2(crd + 3 * a, crd + 3 * b);
-            part += T(kVdwC) / (r2 * r2 * r2) + T(kVdwD) * exp(-T(kVdwE) * sqrt(r2));
+            part += (double)(T(kVdwC) / (r2 * r2 * r2) + T(kVdwD) * exp(-T(kVdwE) * sqrt(r2)));
         } else {                    // M/M  (ttm3f.cpp:222-256)
             const int i3 = 3 * a, j3 = 3 * b;
             T R[3];
@@ -269,7 +269,7 @@ __device__ double energy_warp(const T* crd, T* ms, T* sc, int nw, const uint32_t
         el = (double)phi[lane] * (double)chg[lane];
         ind = -dcur * efqk;
     }
-    const double tot = warp_sum((double)part) + warp_sum(el) / 2 + warp_sum(ind) / 2;
+    const double tot = warp_sum(part) + warp_sum(el) / 2 + warp_sum(ind) / 2;
     __syncwarp();
     return tot;
 }
