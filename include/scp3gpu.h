@@ -154,6 +154,21 @@ int scp3gpu_hbuild_eigvals(scp3gpu_hbuild* h, int64_t nsub, int k, double* evals
  * V, TTM3-F samples that hit the sweep cap. */
 int scp3gpu_hbuild_status(scp3gpu_hbuild* h, int64_t* nonfinite, int64_t* not_converged);
 
+/* addEpot of the -G path without any device allocation, for callers that
+ * cannot call cudaMalloc (a host framework that owns all device memory and hands
+ * out only its own buffers, a locked-down allocator, an allocation-free hot
+ * loop).  No counterpart in the reference: it exists for those callers.
+ * q_dev (n x nmodes, sample-major), V_dev (n) and M_dev (column-major, leading
+ * dimension ld >= Nb) are device buffers of the current device; adds
+ * sum_s Phi(q_s) V_s Phi(q_s)^T into M_dev (both triangles), FP64, ordered on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream).  Working space
+ * comes from one static 64 MiB device array; bases over 4032 functions are
+ * rejected with SCP3GPU_ERR_ARG.  The first call on a device looks up that
+ * array's address (make it before any stream capture); all calls share the
+ * array, so calls that overlap on the GPU race -- order them on one stream. */
+int scp3gpu_add_epot_static(int nmodes, int n2, int n3, const double* q_dev, const double* V_dev, int64_t n,
+                            double* M_dev, int64_t ld, void* stream);
+
 /* Kernel timing (no counterpart in the reference, which has no in-code timing;
  * only a VTune build profile, config/vtune.mk:1-4).  enable = 1 clears and starts
  * recording CUDA events around every kernel the handle launches on its stream;

@@ -21,7 +21,7 @@ EXPORTS = [
     "scp3gpu_hbuild_destroy", "scp3gpu_hbuild_reset", "scp3gpu_hbuild_basis_size", "scp3gpu_hbuild_stream",
     "scp3gpu_hbuild_accumulate", "scp3gpu_hbuild_accumulate_normals", "scp3gpu_hbuild_add_epot",
     "scp3gpu_hbuild_sample_count", "scp3gpu_hbuild_read", "scp3gpu_hbuild_read_dev", "scp3gpu_hbuild_eigvals", "scp3gpu_hbuild_status",
-    "scp3gpu_hbuild_profile",
+    "scp3gpu_hbuild_profile", "scp3gpu_add_epot_static",
 ]
 
 
@@ -87,6 +87,7 @@ def lib():
     L.scp3gpu_hbuild_read_dev.argtypes = [vp, vp, i64, ctypes.c_int]
     L.scp3gpu_hbuild_eigvals.argtypes = [vp, i64, ctypes.c_int, dp]
     L.scp3gpu_hbuild_profile.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(i64)]
+    L.scp3gpu_add_epot_static.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, i64, vp, i64, vp]
     L.scp3gpu_hbuild_status.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64)]
     _lib = L
     return L
