@@ -157,7 +157,11 @@ def main():
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--samples", type=int, default=SAMPLES,
+                    help="samples per step (the benchmark is 2^20; smaller only for profiler captures)")
     args = ap.parse_args()
+    global SAMPLES
+    SAMPLES = args.samples
     world, rank, local = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, world, rank)

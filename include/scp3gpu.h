@@ -50,6 +50,8 @@ extern "C" {
 #define SCP3GPU_PREC_BF16X3 1 /* split: potential FP32, contraction BF16x3 on tcgen05,
                                  FP32 accumulation flushed to FP64 every 4096 samples */
 #define SCP3GPU_PREC_BF16X3_PES64 2 /* split contraction as above, potential in FP64       */
+#define SCP3GPU_PREC_F16X3 3  /* as BF16X3 with FP16 halves (11-bit significands, operand
+                                 scaled by 2^6): same tensor rate, ~2^-22 products      */
 
 /* sampling */
 #define SCP3GPU_SOBOL_REFERENCE 0 /* i8_sobol points, unscrambled (sobol.cpp:14198-27868) */
@@ -168,6 +170,12 @@ int scp3gpu_hbuild_status(scp3gpu_hbuild* h, int64_t* nonfinite, int64_t* not_co
  * array, so calls that overlap on the GPU race -- order them on one stream. */
 int scp3gpu_add_epot_static(int nmodes, int n2, int n3, const double* q_dev, const double* V_dev, int64_t n,
                             double* M_dev, int64_t ld, void* stream);
+
+/* Write M (n_rows x n_cols, column-major, host memory) as an sM_*.h5 file:
+ * dataset "M", dims {n_cols, n_rows}, float32 -- replaces save_hdf5(mat&, char*)
+ * (DiskIO.cpp:201-227), which SCP3 calls every 2^17 samples (SCP3.cpp:252-255).
+ * Stored contiguous rather than chunked + deflate. */
+int scp3gpu_save_h5(const char* path, const double* M, int64_t n_rows, int64_t n_cols);
 
 /* Kernel timing (no counterpart in the reference, which has no in-code timing;
  * only a VTune build profile, config/vtune.mk:1-4).  enable = 1 clears and starts

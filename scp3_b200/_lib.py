@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libscp3gpu.so")
 
 OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_NOT_CONVERGED, ERR_NONFINITE, ERR_TIMEOUT, ERR_UNSUPPORTED = range(8)
-PREC_FP64, PREC_BF16X3, PREC_BF16X3_PES64 = 0, 1, 2
+PREC_FP64, PREC_BF16X3, PREC_BF16X3_PES64, PREC_F16X3 = 0, 1, 2, 3
 SOBOL_REFERENCE, SOBOL_SCRAMBLED = 0, 1
 
 # every symbol include/scp3gpu.h declares (checked by the CPU tests)
@@ -21,7 +21,7 @@ EXPORTS = [
     "scp3gpu_hbuild_destroy", "scp3gpu_hbuild_reset", "scp3gpu_hbuild_basis_size", "scp3gpu_hbuild_stream",
     "scp3gpu_hbuild_accumulate", "scp3gpu_hbuild_accumulate_normals", "scp3gpu_hbuild_add_epot",
     "scp3gpu_hbuild_sample_count", "scp3gpu_hbuild_read", "scp3gpu_hbuild_read_dev", "scp3gpu_hbuild_eigvals", "scp3gpu_hbuild_status",
-    "scp3gpu_hbuild_profile", "scp3gpu_add_epot_static",
+    "scp3gpu_hbuild_profile", "scp3gpu_add_epot_static", "scp3gpu_save_h5",
 ]
 
 
@@ -88,6 +88,7 @@ def lib():
     L.scp3gpu_hbuild_eigvals.argtypes = [vp, i64, ctypes.c_int, dp]
     L.scp3gpu_hbuild_profile.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(i64)]
     L.scp3gpu_add_epot_static.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, i64, vp, i64, vp]
+    L.scp3gpu_save_h5.argtypes = [ctypes.c_char_p, dp, i64, i64]
     L.scp3gpu_hbuild_status.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64)]
     _lib = L
     return L

@@ -5,7 +5,7 @@
 //
 // Operand.  X_i(s) = sqrt|V_s| Phi_i(s), so that X_i X_j = |V_s| Phi_i Phi_j and
 // one operand array serves as both A (rows of tile ti) and B (rows of tile tj).
-// Within every 4096-sample flush block the samples are stably partitioned by the
+// Within every 4096-sample block the samples are stably partitioned by the
 // sign of V (positive first), each sign group padded to a multiple of 16, so a
 // whole K=16 MMA step has one sign; negative steps set the negate-A bit of the
 // instruction descriptor.  X is stored split, X = hi + lo in BF16 (hi = bf16(x),
@@ -13,18 +13,27 @@
 // (three kind::f16 MMAs into one FP32 TMEM accumulator).
 //
 // Accumulation.  Each CTA owns one 128x128 upper tile (ti <= tj) and one range
-// of flush blocks of the pass.  The FP32 accumulator lives in TMEM and is
-// flushed into the CTA's FP64 partial tile in global memory every 4096 samples;
-// two TMEM accumulators alternate so the flush of one block overlaps the MMAs of
-// the next.  Partials of different sample ranges are summed at read-out.
+// of 4096-sample blocks of the pass.  FP32 accumulators live in TMEM: one for
+// the hi*hi products and one for the (2^8 times smaller) cross products, so the
+// large accumulator takes a third of the additions.  After every 4 k-blocks
+// (256 K slots) the epilogue warps drain both into FP64 accumulators held in
+// their registers (one row and 64 columns per thread); the FP64 tile is added
+// into the CTA's partial in global memory once, at the end of its range.  Two
+// TMEM buffers alternate so a drain overlaps the next segment's MMAs.  Why so
+// often: the tensor core's FP32 accumulation error grows with the number of
+// additions into one accumulator, and V carries the cluster's binding energy
+// (~ -0.07 Eh) into every element; on the hexamer, 4096-sample FP32 runs in one
+// accumulator put ~0.45 cm^-1 into the levels, 1024-slot runs in split
+// accumulators ~0.08, 512-slot runs ~0.06 (BF16) / 0.04 (FP16 halves).
 //
-// Warp roles (192 threads): warp 0 lane 0 issues the TMA loads (SWIZZLE_128B,
-// 64 K-slots x 128 rows per box), warp 1 owns TMEM and lane 0 issues the MMAs
-// and commits, warps 2..5 drain the accumulators.  Every mbarrier wait is
+// Warp roles (320 threads): warp 0 lane 0 issues the TMA loads (SWIZZLE_128B,
+// 64 K-slots x 128 rows per box), warp 1 owns TMEM (512 columns) and lane 0
+// issues the MMAs and commits, warps 2..9 drain the accumulators.  Every mbarrier wait is
 // bounded (4 s of %globaltimer); on expiry the CTA records an error, stops
 // issuing, waits (bounded) for its own loads and MMAs, frees TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cudaTypedefs.h>
 
 #include <mutex>
@@ -41,9 +50,11 @@ constexpr int kBK = 64;                      // K slots per stage (128 B of bf16
 constexpr int kStages = 3;
 constexpr int kTileBytes = kTile * kBK * 2;  // 16 KB per operand box
 constexpr int kStageBytes = 4 * kTileBytes;  // A_hi A_lo B_hi B_lo
-constexpr int kKBlocks = kSlotsPerFlush / kBK;   // 65 k-blocks per flush block
-constexpr int kGroups = kSlotsPerFlush / 16;     // 260 sign groups per flush block
-constexpr int kThreads = 192;
+constexpr int kKBlocks = kSlotsPerFlush / kBK;   // 65 k-blocks per 4096-sample block
+constexpr int kDrainKB = 4;                      // k-blocks per FP32 accumulation run (256 K slots)
+constexpr int kSegments = (kKBlocks + kDrainKB - 1) / kDrainKB;   // runs per block
+constexpr int kThreads = 320;
+constexpr int kEpiWarps = 8;
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 /* align */ + 256 /* barriers */;
 constexpr unsigned long long kWaitNs = 4000000000ull;
 
@@ -52,6 +63,12 @@ constexpr unsigned long long kWaitNs = 4000000000ull;
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTile >> 3) << 17) |
                             ((uint32_t)(kTile >> 4) << 24);
 constexpr uint32_t kIdescNegA = kIdesc | (1u << 13);
+// FP16 inputs: A/B format 0
+constexpr uint32_t kIdescF16 = kIdesc & ~((7u << 7) | (7u << 10));
+constexpr uint32_t kIdescF16NegA = kIdescF16 | (1u << 13);
+// FP16 operands are stored as 2^6 x; products carry 2^12
+constexpr float kF16Scale = 64.0f;
+constexpr double kF16Unscale = 1.0 / 4096.0;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -160,7 +177,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
 __global__ void __launch_bounds__(kThreads, 1)
     contract_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
                            const int2* __restrict__ tiles, const int* __restrict__ neg_group, int nflush, int ntiles,
-                           double* __restrict__ partial, int* __restrict__ err_flag)
+                           int products, int f16, double* __restrict__ partial, int* __restrict__ err_flag)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -186,14 +203,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         for (int a = 0; a < 2; a++) {
             mbar_init(acc_full + a, 1);
-            mbar_init(acc_empty + a, 4);
+            mbar_init(acc_empty + a, kEpiWarps);
         }
         mbar_init(drain, 1);
         *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -240,84 +257,101 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) {
             int stage = 0, use = 0;
             uint32_t phase = 0;
-            for (int f = f0; f < f1 && !*abort; f++, use++) {
-                const int a = use & 1;
-                const uint32_t acc_parity = ((use >> 1) & 1) ^ 1;
-                if (!mbar_wait(acc_empty + a, acc_parity, abort)) break;
-                tc_fence_after();
-                const uint32_t d = tmem + (uint32_t)(a * kTile);
+            bool ok = true;
+            for (int f = f0; f < f1 && ok && !*abort; f++) {
                 const int neg0 = neg_group[f];
-                bool ok = true;
-                for (int kb = 0; kb < kKBlocks; kb++) {
-                    if (!mbar_wait(full + stage, phase, abort)) {
+                for (int seg = 0; seg < kSegments && ok; seg++, use++) {
+                    const int a = use & 1;
+                    if (!mbar_wait(acc_empty + a, ((use >> 1) & 1) ^ 1, abort)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    uint8_t* st = smem + stage * kStageBytes;
-                    const uint64_t ahi = smem_desc(st), alo = smem_desc(st + kTileBytes);
-                    const uint64_t bhi = diag ? ahi : smem_desc(st + 2 * kTileBytes);
-                    const uint64_t blo = diag ? alo : smem_desc(st + 3 * kTileBytes);
+                    const uint32_t dhh = tmem + (uint32_t)(a * 2 * kTile), dx = dhh + kTile;
+                    const int kb1 = min(kKBlocks, (seg + 1) * kDrainKB);
+                    for (int kb = seg * kDrainKB; kb < kb1; kb++) {
+                        if (!mbar_wait(full + stage, phase, abort)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        uint8_t* st = smem + stage * kStageBytes;
+                        const uint64_t ahi = smem_desc(st), alo = smem_desc(st + kTileBytes);
+                        const uint64_t bhi = diag ? ahi : smem_desc(st + 2 * kTileBytes);
+                        const uint64_t blo = diag ? alo : smem_desc(st + 3 * kTileBytes);
 #pragma unroll
-                    for (int kk = 0; kk < kBK / 16; kk++) {
-                        const uint32_t idesc = (kb * 4 + kk >= neg0) ? kIdescNegA : kIdesc;
-                        const uint64_t adv = (uint64_t)(kk * 2);    // 32 B along K inside the swizzle atom
-                        mma_bf16(d, ahi + adv, bhi + adv, idesc, (kb | kk) != 0);
-                        mma_bf16(d, ahi + adv, blo + adv, idesc, 1);
-                        mma_bf16(d, alo + adv, bhi + adv, idesc, 1);
+                        for (int kk = 0; kk < kBK / 16; kk++) {
+                            const bool neg = kb * 4 + kk >= neg0;
+                            const uint32_t idesc = f16 ? (neg ? kIdescF16NegA : kIdescF16) : (neg ? kIdescNegA : kIdesc);
+                            const uint64_t adv = (uint64_t)(kk * 2);    // 32 B along K inside the swizzle atom
+                            const uint32_t acc = (kb != seg * kDrainKB) | (kk != 0);
+                            mma_bf16(dhh, ahi + adv, bhi + adv, idesc, acc);
+                            mma_bf16(dx, ahi + adv, blo + adv, idesc, acc);
+                            mma_bf16(dx, alo + adv, bhi + adv, idesc, 1);
+                            if (products == 4) mma_bf16(dx, alo + adv, blo + adv, idesc, 1);
+                        }
+                        mma_commit(empty + stage);      // frees the stage once these MMAs have read it
+                        if (++stage == kStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
                     }
-                    mma_commit(empty + stage);      // frees the stage once these MMAs have read it
-                    if (++stage == kStages) {
-                        stage = 0;
-                        phase ^= 1;
-                    }
+                    if (ok) mma_commit(acc_full + a);
                 }
-                if (!ok) break;
-                mma_commit(acc_full + a);
             }
             mma_commit(drain);                     // completes when every MMA above has
             volatile int never = 0;
             mbar_wait(drain, 0, &never);
         }
     } else {
-        // epilogue: warps 2..5 own TMEM lane quadrants warp%4
-        const int quad = warp & 3;
+        // epilogue: warps 2..9; warp w reads TMEM lane quadrant w%4 and column half (w-2)/4
+        const int quad = warp & 3, half = (warp - 2) >> 2;
         const int row = quad * 32 + lane;
-        int use = 0;
-        for (int f = f0; f < f1; f++, use++) {
+        double acc[64];
+#pragma unroll
+        for (int j = 0; j < 64; j++) acc[j] = 0.0;
+        const int nseg = (f1 - f0) * kSegments;
+        for (int use = 0; use < nseg; use++) {
             const int a = use & 1;
             if (!mbar_wait(acc_full + a, (use >> 1) & 1, abort)) break;
             tc_fence_after();
-            double* P = partial + ((size_t)split * ntiles + blockIdx.x) * (kTile * kTile);
-            const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * kTile);
-#pragma unroll 1
-            for (int c0 = 0; c0 < kTile; c0 += 32) {
-                float v[32];
-                tmem_ld32(base + c0, v);
+            const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * 2 * kTile + half * 64);
 #pragma unroll
-                for (int j = 0; j < 32; j++) P[(size_t)(c0 + j) * kTile + row] += (double)v[j];
+            for (int c0 = 0; c0 < 64; c0 += 32) {
+#pragma unroll
+                for (int part = 0; part < 2; part++) {     // hi*hi, then the cross terms
+                    float t[32];
+                    tmem_ld32(base + part * kTile + c0, t);
+#pragma unroll
+                    for (int j = 0; j < 32; j++) acc[c0 + j] += (double)t[j];
+                }
             }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(acc_empty + a);
         }
+        double* P = partial + ((size_t)split * ntiles + blockIdx.x) * (kTile * kTile);
+        const double unscale = f16 ? kF16Unscale : 1.0;
+#pragma unroll
+        for (int j = 0; j < 64; j++) P[(size_t)(half * 64 + j) * kTile + row] += acc[j] * unscale;
     }
     tc_fence_before();
     __syncthreads();
     if (threadIdx.x == 0 && *abort) atomicExch(err_flag, 1);
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
     }
 }
 
-// One CTA of 1024 threads per flush block: stable partition of its 4096 samples
-// by the sign of V into K slots; writes slot -> sample (-1 = zero padding) and the
-// first negative 16-group of the block.
+// One CTA of 1024 threads per 4096-sample block (4 samples per thread): stable
+// partition of its samples by the sign of V into K slots; writes slot -> sample
+// (-1 = zero padding) and the first negative 16-group of the block.
 __global__ void __launch_bounds__(1024) partition_kernel(const double* __restrict__ v, int* __restrict__ sample_of_slot,
                                                          int* __restrict__ neg_group)
 {
-    __shared__ int wpos[32], wneg[32], tot[2];
+    static_assert(kFlush == 4096, "four samples per thread");
+    __shared__ int wpos[32], tot;
     const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int64_t s0 = (int64_t)b * kFlush + 4 * t;
     int flags = 0, np = 0;
@@ -327,42 +361,29 @@ __global__ void __launch_bounds__(1024) partition_kernel(const double* __restric
         flags |= (int)pos << k;
         np += pos;
     }
-    int nn = 4 - np;
-    // inclusive warp scans
-    int ip = np, in = nn;
+    int incl = np;     // inclusive warp scan of positives
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const int a = __shfl_up_sync(0xffffffffu, ip, o), c = __shfl_up_sync(0xffffffffu, in, o);
-        if (lane >= o) {
-            ip += a;
-            in += c;
-        }
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
     }
-    if (lane == 31) {
-        wpos[w] = ip;
-        wneg[w] = in;
-    }
+    if (lane == 31) wpos[w] = incl;
     __syncthreads();
     if (w == 0) {
-        int p = wpos[lane], n = wneg[lane];
+        const int c = wpos[lane];
+        int x = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int a = __shfl_up_sync(0xffffffffu, p, o), c = __shfl_up_sync(0xffffffffu, n, o);
-            if (lane >= o) {
-                p += a;
-                n += c;
-            }
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
         }
-        wpos[lane] = p - wpos[lane];   // exclusive
-        wneg[lane] = n - wneg[lane];
-        if (lane == 31) {
-            tot[0] = p;
-            tot[1] = n;
-        }
+        wpos[lane] = x - c;      // exclusive
+        if (lane == 31) tot = x;
     }
     __syncthreads();
-    const int P = tot[0], N = tot[1], P16 = (P + 15) & ~15;
-    int op = wpos[w] + ip - np, on = wneg[w] + in - nn;
+    const int P = tot, P16 = (P + 15) & ~15, N = kFlush - P;
+    int op = wpos[w] + incl - np;           // positives before this thread's samples
+    int on = 4 * t - op;                    // negatives before them
     int* out = sample_of_slot + (size_t)b * kSlotsPerFlush;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -381,19 +402,19 @@ __device__ __forceinline__ float h1(float y) { return 1.41421356f * y; }
 __device__ __forceinline__ float h2(float y) { return (2.0f * y * y - 1.0f) * 0.70710678f; }
 __device__ __forceinline__ float h3(float y) { return (2.0f * y * y - 3.0f) * y * 0.57735027f; }
 
+template <bool F16>
 __global__ void __launch_bounds__(kExpSlots) expand_split_kernel(const uint32_t* __restrict__ desc, int nb, int nb_pad,
                                                                   int nm, const float* __restrict__ q,
                                                                   const double* __restrict__ v,
                                                                   const int* __restrict__ sample_of_slot, int64_t ldk,
-                                                                  __nv_bfloat16* __restrict__ xhi,
-                                                                  __nv_bfloat16* __restrict__ xlo)
+                                                                  uint16_t* __restrict__ xhi, uint16_t* __restrict__ xlo)
 {
     extern __shared__ float qs[];   // [nm][kExpSlots]
     const int t = threadIdx.x;
     const int64_t slot = (int64_t)blockIdx.x * kExpSlots + t;
     const int s = sample_of_slot[slot];
     for (int m = 0; m < nm; m++) qs[m * kExpSlots + t] = (s >= 0) ? q[(int64_t)s * nm + m] : 0.0f;
-    const float sv = (s >= 0) ? (float)sqrt(fabs(v[s])) : 0.0f;
+    const float sv = (s >= 0) ? (float)sqrt(fabs(v[s])) * (F16 ? kF16Scale : 1.0f) : 0.0f;
     __syncthreads();
     const int r0 = blockIdx.y * kExpRows, r1 = min(r0 + kExpRows, nb_pad);
     for (int i = r0; i < r1; i++) {
@@ -415,10 +436,18 @@ __global__ void __launch_bounds__(kExpSlots) expand_split_kernel(const uint32_t*
             }
             x = sv * ph;
         }
-        const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-        xhi[(size_t)i * ldk + slot] = hi;
-        xlo[(size_t)i * ldk + slot] = lo;
+        uint16_t hb, lb;
+        if (F16) {
+            const __half hi = __float2half_rn(x);
+            const __half lo = __float2half_rn(x - __half2float(hi));
+            hb = __half_as_ushort(hi), lb = __half_as_ushort(lo);
+        } else {
+            const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+            const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+            hb = __bfloat16_as_ushort(hi), lb = __bfloat16_as_ushort(lo);
+        }
+        xhi[(size_t)i * ldk + slot] = hb;
+        xlo[(size_t)i * ldk + slot] = lb;
     }
 }
 
@@ -457,6 +486,7 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode()
 }
 
 int encode_map(void** out, void* base, int64_t slots, int rows)
+// (the 16-bit element type of the map does not matter to the copy: BF16 and FP16 share size and swizzle)
 {
     auto enc = get_encode();
     if (!enc) return fail(SCP3GPU_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
@@ -488,8 +518,9 @@ void record(std::vector<cudaEvent_t>* pev, std::vector<int>* pkind, int kind, cu
 
 }  // namespace
 
-int create(Plan& p, int nb, int nm, int chunk_req, int sms)
+int create(Plan& p, int nb, int nm, int chunk_req, int sms, bool f16)
 {
+    p.f16 = f16;
     p.nb = nb;
     p.nm = nm;
     p.nt = (nb + kTile - 1) / kTile;
@@ -557,12 +588,10 @@ int accumulate_pass(Plan& p, const uint32_t* desc, int nb, int nm, const float* 
     partition_kernel<<<nflush, 1024, 0, s>>>(v, p.slot_of, p.group_meta);
     SCP3_CUDA(cudaGetLastError());
     const size_t sm = sizeof(float) * nm * kExpSlots;
-    if (sm > 48 * 1024)
-        SCP3_CUDA(cudaFuncSetAttribute(expand_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    auto kern = p.f16 ? expand_split_kernel<true> : expand_split_kernel<false>;
+    if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     dim3 eg((unsigned)(slots / kExpSlots), (unsigned)((p.nb_pad + kExpRows - 1) / kExpRows));
-    expand_split_kernel<<<eg, kExpSlots, sm, s>>>(desc, nb, p.nb_pad, nm, q32, v, p.slot_of, p.slots,
-                                                   reinterpret_cast<__nv_bfloat16*>(p.xhi),
-                                                   reinterpret_cast<__nv_bfloat16*>(p.xlo));
+    kern<<<eg, kExpSlots, sm, s>>>(desc, nb, p.nb_pad, nm, q32, v, p.slot_of, p.slots, p.xhi, p.xlo);
     SCP3_CUDA(cudaGetLastError());
     record(pev, pkind, 1, s);
     record(pev, pkind, 2, s);
@@ -570,7 +599,8 @@ int accumulate_pass(Plan& p, const uint32_t* desc, int nb, int nm, const float* 
     dim3 grid(p.ntiles, nsplit);
     contract_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(*static_cast<CUtensorMap*>(p.tmap_hi),
                                                               *static_cast<CUtensorMap*>(p.tmap_lo), p.tiles,
-                                                              p.group_meta, nflush, p.ntiles, p.partial, p.err_flag);
+                                                              p.group_meta, nflush, p.ntiles, p.products, (int)p.f16,
+                                                              p.partial, p.err_flag);
     SCP3_CUDA(cudaGetLastError());
     record(pev, pkind, 2, s);
     return SCP3GPU_OK;

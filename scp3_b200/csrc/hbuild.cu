@@ -346,7 +346,7 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     if (!c->x0 || !c->MUa || !c->omega || !c->modes) return fail(SCP3GPU_ERR_ARG, "null geometry or mode arrays");
     if (c->pes != SCP3GPU_PES_QTIP4PF && c->pes != SCP3GPU_PES_TTM3F) return fail(SCP3GPU_ERR_ARG, "unknown potential");
     if (c->precision != SCP3GPU_PREC_FP64 && c->precision != SCP3GPU_PREC_BF16X3 &&
-        c->precision != SCP3GPU_PREC_BF16X3_PES64)
+        c->precision != SCP3GPU_PREC_BF16X3_PES64 && c->precision != SCP3GPU_PREC_F16X3)
         return fail(SCP3GPU_ERR_ARG, "unknown precision");
     if (c->pes == SCP3GPU_PES_TTM3F && c->nw > 8) return fail(SCP3GPU_ERR_ARG, "TTM3-F kernel supports nw <= 8");
     if (c->chunk < 0 || c->chunk % 4096 != 0) return fail(SCP3GPU_ERR_ARG, "chunk must be a multiple of 4096");
@@ -363,7 +363,7 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     h->cfg.modes = nullptr;
     h->dev = c->device;
     h->split_form = c->precision != SCP3GPU_PREC_FP64;
-    h->pes_fp32 = c->precision == SCP3GPU_PREC_BF16X3;
+    h->pes_fp32 = c->precision == SCP3GPU_PREC_BF16X3 || c->precision == SCP3GPU_PREC_F16X3;
     const int nm0 = c->nmodes0, N3 = 9 * c->nw;
     h->nb = (int)scp3gpu_basis_size(c->nmodes, c->n2, c->n3);
     // HO diagonal of the selected modes and the inactive-mode zero point (SCP3.cpp:239)
@@ -404,7 +404,8 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     SCP3_CUDA(cudaMemset(h->counters, 0, 2 * sizeof(unsigned long long)));
 
     if (h->split_form) {
-        if ((rc = tc::create(h->tcp, h->nb, c->nmodes, c->chunk, sms))) return bail(rc);
+        if ((rc = tc::create(h->tcp, h->nb, c->nmodes, c->chunk, sms, c->precision == SCP3GPU_PREC_F16X3)))
+            return bail(rc);
         h->chunk = h->tcp.chunk;
         h->nb_pad = h->tcp.nb_pad;
         if ((rc = dalloc(&h->q32, (size_t)h->chunk * c->nmodes)) || (rc = dalloc(&h->v, (size_t)h->chunk)))

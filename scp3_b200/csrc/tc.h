@@ -10,6 +10,8 @@ struct Plan {
     int nt = 0, ntiles = 0;       // 128-row tiles per side, upper tiles
     int nsplit = 1;               // sample ranges per pass (each owns an FP64 partial per tile)
     int64_t chunk = 0;            // samples per pass (multiple of kFlush)
+    int products = 3;             // 3: hi*hi + hi*lo + lo*hi; 4: + lo*lo
+    bool f16 = false;             // halves in FP16 (operand scaled by 2^6) instead of BF16
     int64_t slots = 0;            // K slots per pass after sign partition and padding
     // device buffers
     uint16_t* xhi = nullptr;      // [nb_pad][slots] bf16: sqrt|V| Phi, high part
@@ -25,10 +27,10 @@ struct Plan {
 };
 
 constexpr int kTile = 128;        // UMMA M = N = 128
-constexpr int kFlush = 4096;      // samples accumulated in FP32 (TMEM) before the FP64 flush
+constexpr int kFlush = 4096;      // samples per sign-partition block (the FP64 flush is finer, see contract_tc.cu)
 constexpr int kSlotsPerFlush = kFlush + 64;  // sign partition pads each sign group to 16
 
-int create(Plan& p, int nb, int nm, int chunk_req, int sms);
+int create(Plan& p, int nb, int nm, int chunk_req, int sms, bool f16);
 void destroy(Plan& p);
 int64_t pass_samples(const Plan& p, int64_t nvalid);
 int zero(Plan& p, cudaStream_t s);
