@@ -179,7 +179,8 @@ def main():
     stream = torch.cuda.ExternalStream(hb.stream, device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=local)
     Mdev = torch.zeros((nb, nb), dtype=torch.float64, device=local)
-    base = rank * (1 << 40)            # disjoint Sobol index ranges per rank
+    from scp3_b200 import shard
+    base, _ = shard.sample_range(rank, world, 0, SAMPLES, "weak")   # disjoint Sobol ranges per rank
 
     def step(k):
         hb.accumulate(base + k * SAMPLES, SAMPLES)
@@ -189,7 +190,7 @@ def main():
             ev = torch.cuda.Event()
             ev.record(stream)
             torch.cuda.current_stream().wait_event(ev)
-            dist.all_reduce(Mdev)
+            shard.reduce_matrix(Mdev)
 
     for k in range(args.warmup):
         step(k)
