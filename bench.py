@@ -149,6 +149,7 @@ def run_reference(args, world, rank):
 
 
 def main():
+    global SAMPLES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -160,7 +161,6 @@ def main():
     ap.add_argument("--samples", type=int, default=SAMPLES,
                     help="samples per step (the benchmark is 2^20; smaller only for profiler captures)")
     args = ap.parse_args()
-    global SAMPLES
     SAMPLES = args.samples
     world, rank, local = dist_setup(args.gpus)
     if args.impl == "reference":

@@ -52,6 +52,7 @@ extern "C" {
 #define SCP3GPU_PREC_BF16X3_PES64 2 /* split contraction as above, potential in FP64       */
 #define SCP3GPU_PREC_F16X3 3  /* as BF16X3 with FP16 halves (11-bit significands, operand
                                  scaled by 2^6): same tensor rate, ~2^-22 products      */
+#define SCP3GPU_PREC_F16X3_PES64 4 /* FP16x3 contraction, potential in FP64             */
 
 /* sampling */
 #define SCP3GPU_SOBOL_REFERENCE 0 /* i8_sobol points, unscrambled (sobol.cpp:14198-27868) */

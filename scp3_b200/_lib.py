@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libscp3gpu.so")
 
 OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_NOT_CONVERGED, ERR_NONFINITE, ERR_TIMEOUT, ERR_UNSUPPORTED = range(8)
-PREC_FP64, PREC_BF16X3, PREC_BF16X3_PES64, PREC_F16X3 = 0, 1, 2, 3
+PREC_FP64, PREC_BF16X3, PREC_BF16X3_PES64, PREC_F16X3, PREC_F16X3_PES64 = 0, 1, 2, 3, 4
 SOBOL_REFERENCE, SOBOL_SCRAMBLED = 0, 1
 
 # every symbol include/scp3gpu.h declares (checked by the CPU tests)

@@ -110,7 +110,8 @@ class HBuild:
         cfg.n2, cfg.n3 = n2, n3
         cfg.pes = C.PES_IDS[pes] if isinstance(pes, str) else int(pes)
         cfg.precision = {"fp64": _lib.PREC_FP64, "bf16x3": _lib.PREC_BF16X3,
-                         "bf16x3_pes64": _lib.PREC_BF16X3_PES64, "f16x3": _lib.PREC_F16X3}[precision]
+                         "bf16x3_pes64": _lib.PREC_BF16X3_PES64, "f16x3": _lib.PREC_F16X3,
+                         "f16x3_pes64": _lib.PREC_F16X3_PES64}[precision]
         cfg.scramble = _lib.SOBOL_SCRAMBLED if scramble_seed is not None else _lib.SOBOL_REFERENCE
         cfg.scramble_seed = scramble_seed or 0
         cfg.chunk, cfg.device = chunk, device

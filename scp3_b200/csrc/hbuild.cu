@@ -346,7 +346,8 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     if (!c->x0 || !c->MUa || !c->omega || !c->modes) return fail(SCP3GPU_ERR_ARG, "null geometry or mode arrays");
     if (c->pes != SCP3GPU_PES_QTIP4PF && c->pes != SCP3GPU_PES_TTM3F) return fail(SCP3GPU_ERR_ARG, "unknown potential");
     if (c->precision != SCP3GPU_PREC_FP64 && c->precision != SCP3GPU_PREC_BF16X3 &&
-        c->precision != SCP3GPU_PREC_BF16X3_PES64 && c->precision != SCP3GPU_PREC_F16X3)
+        c->precision != SCP3GPU_PREC_BF16X3_PES64 && c->precision != SCP3GPU_PREC_F16X3 &&
+        c->precision != SCP3GPU_PREC_F16X3_PES64)
         return fail(SCP3GPU_ERR_ARG, "unknown precision");
     if (c->pes == SCP3GPU_PES_TTM3F && c->nw > 8) return fail(SCP3GPU_ERR_ARG, "TTM3-F kernel supports nw <= 8");
     if (c->chunk < 0 || c->chunk % 4096 != 0) return fail(SCP3GPU_ERR_ARG, "chunk must be a multiple of 4096");
@@ -404,7 +405,8 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     SCP3_CUDA(cudaMemset(h->counters, 0, 2 * sizeof(unsigned long long)));
 
     if (h->split_form) {
-        if ((rc = tc::create(h->tcp, h->nb, c->nmodes, c->chunk, sms, c->precision == SCP3GPU_PREC_F16X3)))
+        const bool f16 = c->precision == SCP3GPU_PREC_F16X3 || c->precision == SCP3GPU_PREC_F16X3_PES64;
+        if ((rc = tc::create(h->tcp, h->nb, c->nmodes, c->chunk, sms, f16)))
             return bail(rc);
         h->chunk = h->tcp.chunk;
         h->nb_pad = h->tcp.nb_pad;
