@@ -36,6 +36,7 @@
 #include <cuda_fp16.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -452,16 +453,16 @@ __global__ void __launch_bounds__(kExpSlots) expand_split_kernel(const uint32_t*
 }
 
 // Dense column-major nb x nb from the tile partials (tile-local column-major).
-__global__ void unpack_tc_kernel(const double* __restrict__ partial, int nt, int ntiles, int nsplit, int nb,
-                                 double divisor, const double* __restrict__ diag, double zpe, double* __restrict__ M,
-                                 int64_t ld)
+__global__ void unpack_tc_kernel(const double* __restrict__ partial, const int* __restrict__ tile_index, int nt,
+                                 int ntiles, int nsplit, int nb, double divisor, const double* __restrict__ diag,
+                                 double zpe, double* __restrict__ M, int64_t ld)
 {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (int64_t)nb * nb) return;
     const int j = (int)(e / nb), i = (int)(e - (int64_t)j * nb);
     const int r = min(i, j), c = max(i, j);
     const int ti = r / kTile, tj = c / kTile;
-    const int t = ti * nt - ti * (ti - 1) / 2 + (tj - ti);
+    const int t = tile_index[(size_t)ti * nt + tj];
     const size_t off = (size_t)t * kTile * kTile + (size_t)(c - tj * kTile) * kTile + (r - ti * kTile);
     double val = 0.0;
     for (int s = 0; s < nsplit; s++) val += partial[(size_t)s * ntiles * kTile * kTile + off];
@@ -536,15 +537,28 @@ int create(Plan& p, int nb, int nm, int chunk_req, int sms, bool f16)
     int nsplit = 1;
     while (nsplit < nflush && (int64_t)p.ntiles * nsplit < 2ll * sms) nsplit *= 2;
     p.nsplit = nsplit;
+    // Launch order: upper tiles grouped into G x G super-tiles, so the CTAs of one
+    // wave share a few row and column panels of the operand and read them from L2
+    // (row-major order would stream ~150 distinct panels per wave for the
+    // triples basis).
+    const int G = 12;
     std::vector<int2> t;
-    for (int i = 0; i < p.nt; i++)
-        for (int j = i; j < p.nt; j++) t.push_back(make_int2(i, j));
+    std::vector<int> tindex((size_t)p.nt * p.nt, -1);
+    for (int bi = 0; bi < p.nt; bi += G)
+        for (int bj = bi; bj < p.nt; bj += G)
+            for (int i = bi; i < std::min(bi + G, p.nt); i++)
+                for (int j = std::max(i, bj); j < std::min(bj + G, p.nt); j++) {
+                    tindex[(size_t)i * p.nt + j] = (int)t.size();
+                    t.push_back(make_int2(i, j));
+                }
     SCP3_CUDA(cudaMalloc(&p.xhi, sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
     SCP3_CUDA(cudaMalloc(&p.xlo, sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
     SCP3_CUDA(cudaMalloc(&p.slot_of, sizeof(int) * (size_t)p.slots));
     SCP3_CUDA(cudaMalloc(&p.group_meta, sizeof(int) * nflush));
     SCP3_CUDA(cudaMalloc(&p.tiles, sizeof(int2) * t.size()));
     SCP3_CUDA(cudaMemcpy(p.tiles, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice));
+    SCP3_CUDA(cudaMalloc(&p.tile_index, sizeof(int) * tindex.size()));
+    SCP3_CUDA(cudaMemcpy(p.tile_index, tindex.data(), sizeof(int) * tindex.size(), cudaMemcpyHostToDevice));
     SCP3_CUDA(cudaMalloc(&p.partial, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kTile));
     SCP3_CUDA(cudaMalloc(&p.err_flag, sizeof(int)));
     SCP3_CUDA(cudaMemset(p.err_flag, 0, sizeof(int)));
@@ -557,7 +571,7 @@ int create(Plan& p, int nb, int nm, int chunk_req, int sms, bool f16)
 
 void destroy(Plan& p)
 {
-    void* ptrs[] = {p.xhi, p.xlo, p.slot_of, p.sign_groups, p.group_meta, p.tiles, p.partial, p.err_flag};
+    void* ptrs[] = {p.xhi, p.xlo, p.slot_of, p.sign_groups, p.group_meta, p.tiles, p.tile_index, p.partial, p.err_flag};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     delete static_cast<CUtensorMap*>(p.tmap_hi);
@@ -613,8 +627,8 @@ int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, doub
     SCP3_CUDA(cudaStreamSynchronize(s));
     if (err) return fail(SCP3GPU_ERR_TIMEOUT, "tensor-core contraction: a bounded pipeline wait expired");
     const int64_t total = (int64_t)nb * nb;
-    unpack_tc_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p.partial, p.nt, p.ntiles, p.nsplit, nb, divisor,
-                                                                      diag, zpe, M, ld);
+    unpack_tc_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p.partial, p.tile_index, p.nt, p.ntiles,
+                                                                      p.nsplit, nb, divisor, diag, zpe, M, ld);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }

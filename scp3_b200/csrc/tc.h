@@ -19,7 +19,8 @@ struct Plan {
     int* slot_of = nullptr;       // [chunk] sample -> K slot
     uint32_t* sign_groups = nullptr;  // [slots/16] bit per 16-sample group: 1 = negative V
     int* group_meta = nullptr;    // per flush block: first negative 16-group
-    int2* tiles = nullptr;        // [ntiles] (ti, tj)
+    int2* tiles = nullptr;        // [ntiles] (ti, tj), in launch order
+    int* tile_index = nullptr;    // [nt*nt] position of tile (ti, tj) in `tiles`
     double* partial = nullptr;    // [nsplit][ntiles][128*128] FP64
     void* tmap_hi = nullptr;      // CUtensorMap (host copy) for xhi / xlo
     void* tmap_lo = nullptr;
