@@ -148,6 +148,57 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+def run_triples(args):
+    """The triples configuration: TTM3-F hexamer prism, N2 = N3 = 48 (20825 basis
+    functions), 2^21 scrambled points in 2^17-sample chunks with an sM_*.h5 dump
+    after each chunk, the 10 lowest levels of the split form against the FP64
+    form on the same points.  One JSON line; not the benchmark's default."""
+    import tempfile
+
+    import torch
+    import scp3_b200
+    from scp3_b200 import h5, inputs
+    torch.cuda.set_device(0)
+    nw, x0, MUa, omega = inputs.load("prism_ttm3f")
+    total, chunk = args.samples, 1 << 17
+    res = {}
+    outdir = tempfile.mkdtemp(prefix="scp3_triples_")
+    autocm = scp3_b200.constants.autocm
+    for prec in (args.precision, "fp64"):
+        hb = scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=48, pes="ttm3f", precision=prec,
+                              scramble_seed=SCRAMBLE_SEED)
+        nb = hb.nb
+        hb.accumulate(0, 4096)           # warm-up, then start clean
+        hb.reset()
+        torch.cuda.synchronize()
+        t_compute, t_dump = 0.0, 0.0
+        Mh = np.zeros((nb, nb), order="F") if prec != "fp64" else None
+        for c0 in range(0, total, chunk):
+            t0 = time.perf_counter()
+            hb.accumulate(c0, min(chunk, total - c0))
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            t_compute += t1 - t0
+            if Mh is not None and not args.no_dump:
+                hb.read(1, out=Mh)
+                h5.save(os.path.join(outdir, "sM_%07d.h5" % (c0 + chunk)), Mh)
+                t_dump += time.perf_counter() - t1
+        t0 = time.perf_counter()
+        ev = hb.eigvals(10)
+        t_eig = time.perf_counter() - t0
+        rc, nonfinite, notconv = hb.status()
+        res[prec] = dict(samples_per_s=total / t_compute, compute_s=t_compute, dump_s=t_dump, eig_s=t_eig,
+                         levels_cm1=[float(x * autocm) for x in ev], nonfinite=nonfinite, not_converged=notconv)
+        hb.close()
+    sp, dp = res[args.precision], res["fp64"]
+    err = float(np.abs(np.array(sp["levels_cm1"]) - np.array(dp["levels_cm1"])).max())
+    print(json.dumps({"config": {"workload": "hexamer prism TTM3-F, 48 modes, triples basis Nb=20825, %d scrambled "
+                                             "Sobol points in 2^17 chunks with an sM_*.h5 dump after each" % total,
+                                 "precision": args.precision, "nb": 20825},
+                      "split": sp, "fp64": dp, "speedup_vs_fp64": sp["samples_per_s"] / dp["samples_per_s"],
+                      "max_abs_err_cm1_vs_fp64": err, "h5_dir": outdir}))
+
+
 def main():
     global SAMPLES
     ap = argparse.ArgumentParser()
@@ -158,10 +209,18 @@ def main():
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--config", default="doubles", choices=["doubles", "triples"],
+                    help="doubles: the benchmark (hexamer, Nb=1225); triples: the TTM3-F triples build")
+    ap.add_argument("--no-dump", action="store_true", help="triples: skip the sM_*.h5 dumps")
     ap.add_argument("--samples", type=int, default=SAMPLES,
                     help="samples per step (the benchmark is 2^20; smaller only for profiler captures)")
     args = ap.parse_args()
     SAMPLES = args.samples
+    if args.config == "triples":
+        if args.samples == 1 << 20:
+            args.samples = 1 << 21
+        run_triples(args)
+        return
     world, rank, local = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -396,59 +396,79 @@ __global__ void __launch_bounds__(1024) partition_kernel(const double* __restric
     if (t == 0) neg_group[b] = P16 / 16;
 }
 
-// Expansion into the split operand: thread per K slot, rows in blocks of 64.
-constexpr int kExpSlots = 64, kExpRows = 64;   // 4160 slots per flush block = 65 x 64
-
-__device__ __forceinline__ float h1(float y) { return 1.41421356f * y; }
-__device__ __forceinline__ float h2(float y) { return (2.0f * y * y - 1.0f) * 0.70710678f; }
-__device__ __forceinline__ float h3(float y) { return (2.0f * y * y - 3.0f) * y * 0.57735027f; }
+// Expansion into the split operand X = sqrt|V| Phi (hi + lo halves).  A block
+// covers 64 K slots and up to 256 basis rows: it first tabulates, per slot,
+// [1, h1(q_m), h2(q_m), h3(q_m)] for all modes in shared memory, then every basis
+// value is the product of three table entries (basis_factor_table).  Thread
+// (g, r) handles slots 4g..4g+3 of rows r, r+8, ...: one 16-byte table read per
+// factor and 8-byte stores, so the 16 threads of a row write 128 contiguous
+// bytes per half.
+constexpr int kExpSlots = 64, kExpRows = 256, kExpThreads = 128;
 
 template <bool F16>
-__global__ void __launch_bounds__(kExpSlots) expand_split_kernel(const uint32_t* __restrict__ desc, int nb, int nb_pad,
-                                                                  int nm, const float* __restrict__ q,
-                                                                  const double* __restrict__ v,
-                                                                  const int* __restrict__ sample_of_slot, int64_t ldk,
-                                                                  uint16_t* __restrict__ xhi, uint16_t* __restrict__ xlo)
+__device__ __forceinline__ void split4(float4 x, uint2& hi, uint2& lo)
 {
-    extern __shared__ float qs[];   // [nm][kExpSlots]
-    const int t = threadIdx.x;
-    const int64_t slot = (int64_t)blockIdx.x * kExpSlots + t;
-    const int s = sample_of_slot[slot];
-    for (int m = 0; m < nm; m++) qs[m * kExpSlots + t] = (s >= 0) ? q[(int64_t)s * nm + m] : 0.0f;
-    const float sv = (s >= 0) ? (float)sqrt(fabs(v[s])) * (F16 ? kF16Scale : 1.0f) : 0.0f;
-    __syncthreads();
-    const int r0 = blockIdx.y * kExpRows, r1 = min(r0 + kExpRows, nb_pad);
-    for (int i = r0; i < r1; i++) {
-        float x = 0.0f;
-        if (i < nb && s >= 0) {
-            const uint32_t d = __ldg(desc + i);
-            const int m = (d >> 3) & 255, n = (d >> 11) & 255, p = (d >> 19) & 255;
-            const float qm = qs[m * kExpSlots + t];
-            float ph;
-            switch (d & 7u) {
-                case kGround: ph = 1.0f; break;
-                case kHo1: ph = h1(qm); break;
-                case kHo2: ph = h2(qm); break;
-                case kHo1Ho1: ph = h1(qm) * h1(qs[n * kExpSlots + t]); break;
-                case kHo3: ph = h3(qm); break;
-                case kHo2Ho1: ph = h2(qm) * h1(qs[n * kExpSlots + t]); break;
-                case kHo1Ho2: ph = h1(qm) * h2(qs[n * kExpSlots + t]); break;
-                default: ph = h1(qm) * h1(qs[n * kExpSlots + t]) * h1(qs[p * kExpSlots + t]); break;
-            }
-            x = sv * ph;
-        }
-        uint16_t hb, lb;
+    const float v[4] = {x.x, x.y, x.z, x.w};
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
         if (F16) {
-            const __half hi = __float2half_rn(x);
-            const __half lo = __float2half_rn(x - __half2float(hi));
-            hb = __half_as_ushort(hi), lb = __half_as_ushort(lo);
+            const __half a = __float2half_rn(v[k]);
+            h[k] = __half_as_ushort(a);
+            l[k] = __half_as_ushort(__float2half_rn(v[k] - __half2float(a)));
         } else {
-            const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-            const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-            hb = __bfloat16_as_ushort(hi), lb = __bfloat16_as_ushort(lo);
+            const __nv_bfloat16 a = __float2bfloat16_rn(v[k]);
+            h[k] = __bfloat16_as_ushort(a);
+            l[k] = __bfloat16_as_ushort(__float2bfloat16_rn(v[k] - __bfloat162float(a)));
         }
-        xhi[(size_t)i * ldk + slot] = hb;
-        xlo[(size_t)i * ldk + slot] = lb;
+    }
+    hi = make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
+    lo = make_uint2(l[0] | (l[1] << 16), l[2] | (l[3] << 16));
+}
+
+template <bool F16>
+__global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const uint32_t* __restrict__ factors, int nb,
+                                                                    int nb_pad, int nm, const float* __restrict__ q,
+                                                                    const double* __restrict__ v,
+                                                                    const int* __restrict__ sample_of_slot,
+                                                                    int64_t ldk, uint16_t* __restrict__ xhi,
+                                                                    uint16_t* __restrict__ xlo)
+{
+    extern __shared__ __align__(16) float tab[];      // [3nm+1][kExpSlots], then sqrt|V| [kExpSlots]
+    float* sv = tab + (size_t)(3 * nm + 1) * kExpSlots;
+    const int t = threadIdx.x;
+    const int64_t slot0 = (int64_t)blockIdx.x * kExpSlots;
+    for (int e = t; e < kExpSlots; e += kExpThreads) {
+        const int s = sample_of_slot[slot0 + e];
+        tab[e] = 1.0f;
+        sv[e] = (s >= 0) ? (float)sqrt(fabs(v[s])) * (F16 ? kF16Scale : 1.0f) : 0.0f;
+    }
+    for (int e = t; e < kExpSlots * nm; e += kExpThreads) {
+        const int l = e / nm, m = e - l * nm;
+        const int s = sample_of_slot[slot0 + l];
+        const float y = (s >= 0) ? q[(int64_t)s * nm + m] : 0.0f;
+        tab[(1 + m) * kExpSlots + l] = 1.41421356f * y;                                  // ho1
+        tab[(1 + nm + m) * kExpSlots + l] = (2.0f * y * y - 1.0f) * 0.70710678f;          // ho2
+        tab[(1 + 2 * nm + m) * kExpSlots + l] = (2.0f * y * y - 3.0f) * y * 0.57735027f;  // ho3
+    }
+    __syncthreads();
+    const int g = t & 15, rl = t >> 4;
+    const float4 w = reinterpret_cast<const float4*>(sv)[g];
+    const int r0 = blockIdx.y * kExpRows, r1 = min(r0 + kExpRows, nb_pad);
+    for (int r = r0 + rl; r < r1; r += kExpThreads / 16) {
+        uint2 hi = make_uint2(0, 0), lo = make_uint2(0, 0);
+        if (r < nb) {
+            const uint32_t d = __ldg(factors + r);
+            const float4 A = reinterpret_cast<const float4*>(tab + (d & 1023u) * kExpSlots)[g];
+            const float4 B = reinterpret_cast<const float4*>(tab + ((d >> 10) & 1023u) * kExpSlots)[g];
+            const float4 C = reinterpret_cast<const float4*>(tab + (d >> 20) * kExpSlots)[g];
+            const float4 x = make_float4(w.x * (A.x * B.x * C.x), w.y * (A.y * B.y * C.y), w.z * (A.z * B.z * C.z),
+                                         w.w * (A.w * B.w * C.w));
+            split4<F16>(x, hi, lo);
+        }
+        const size_t off = (size_t)r * ldk + slot0 + 4 * g;
+        *reinterpret_cast<uint2*>(xhi + off) = hi;
+        *reinterpret_cast<uint2*>(xlo + off) = lo;
     }
 }
 
@@ -519,8 +539,9 @@ void record(std::vector<cudaEvent_t>* pev, std::vector<int>* pkind, int kind, cu
 
 }  // namespace
 
-int create(Plan& p, int nb, int nm, int chunk_req, int sms, bool f16)
+int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int chunk_req, int sms, bool f16)
 {
+    const int nm_for_factors = nm;
     p.f16 = f16;
     p.nb = nb;
     p.nm = nm;
@@ -557,6 +578,9 @@ int create(Plan& p, int nb, int nm, int chunk_req, int sms, bool f16)
     SCP3_CUDA(cudaMalloc(&p.group_meta, sizeof(int) * nflush));
     SCP3_CUDA(cudaMalloc(&p.tiles, sizeof(int2) * t.size()));
     SCP3_CUDA(cudaMemcpy(p.tiles, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice));
+    const std::vector<uint32_t> fac = basis_factor_table(nm_for_factors, n2_for_factors, n3_for_factors);
+    SCP3_CUDA(cudaMalloc(&p.factors, sizeof(uint32_t) * fac.size()));
+    SCP3_CUDA(cudaMemcpy(p.factors, fac.data(), sizeof(uint32_t) * fac.size(), cudaMemcpyHostToDevice));
     SCP3_CUDA(cudaMalloc(&p.tile_index, sizeof(int) * tindex.size()));
     SCP3_CUDA(cudaMemcpy(p.tile_index, tindex.data(), sizeof(int) * tindex.size(), cudaMemcpyHostToDevice));
     SCP3_CUDA(cudaMalloc(&p.partial, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kTile));
@@ -571,7 +595,8 @@ int create(Plan& p, int nb, int nm, int chunk_req, int sms, bool f16)
 
 void destroy(Plan& p)
 {
-    void* ptrs[] = {p.xhi, p.xlo, p.slot_of, p.sign_groups, p.group_meta, p.tiles, p.tile_index, p.partial, p.err_flag};
+    void* ptrs[] = {p.xhi, p.xlo, p.slot_of, p.sign_groups, p.group_meta, p.tiles, p.tile_index, p.factors, p.partial,
+                    p.err_flag};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     delete static_cast<CUtensorMap*>(p.tmap_hi);
@@ -601,11 +626,11 @@ int accumulate_pass(Plan& p, const uint32_t* desc, int nb, int nm, const float* 
     record(pev, pkind, 1, s);
     partition_kernel<<<nflush, 1024, 0, s>>>(v, p.slot_of, p.group_meta);
     SCP3_CUDA(cudaGetLastError());
-    const size_t sm = sizeof(float) * nm * kExpSlots;
+    const size_t sm = sizeof(float) * (size_t)(3 * nm + 2) * kExpSlots;
     auto kern = p.f16 ? expand_split_kernel<true> : expand_split_kernel<false>;
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     dim3 eg((unsigned)(slots / kExpSlots), (unsigned)((p.nb_pad + kExpRows - 1) / kExpRows));
-    kern<<<eg, kExpSlots, sm, s>>>(desc, nb, p.nb_pad, nm, q32, v, p.slot_of, p.slots, p.xhi, p.xlo);
+    kern<<<eg, kExpThreads, sm, s>>>(p.factors, nb, p.nb_pad, nm, q32, v, p.slot_of, p.slots, p.xhi, p.xlo);
     SCP3_CUDA(cudaGetLastError());
     record(pev, pkind, 1, s);
     record(pev, pkind, 2, s);

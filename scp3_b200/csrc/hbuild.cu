@@ -406,7 +406,7 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
 
     if (h->split_form) {
         const bool f16 = c->precision == SCP3GPU_PREC_F16X3 || c->precision == SCP3GPU_PREC_F16X3_PES64;
-        if ((rc = tc::create(h->tcp, h->nb, c->nmodes, c->chunk, sms, f16)))
+        if ((rc = tc::create(h->tcp, h->nb, c->nmodes, c->n2, c->n3, c->chunk, sms, f16)))
             return bail(rc);
         h->chunk = h->tcp.chunk;
         h->nb_pad = h->tcp.nb_pad;

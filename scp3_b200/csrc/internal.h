@@ -44,6 +44,10 @@ enum BasisKind : uint32_t {
 };
 std::vector<uint32_t> basis_descriptors(int nm, int n2, int n3);
 
+// The same basis as products of entries of a per-sample Hermite table
+// [1, h1(q_m), h2(q_m), h3(q_m)] (indices a, b, c in 10-bit fields).
+std::vector<uint32_t> basis_factor_table(int nm, int n2, int n3);
+
 // Pair tasks of the water potentials, in one list per cluster size: type in
 // bits 0..1 (0: M-site(i)/H(j), 1: H/H, 2: O/O, 3: M/M) and the two atom or
 // site indices in bits 2..16 and 17..31 (atoms index 3*water+{0,1,2}; M sites

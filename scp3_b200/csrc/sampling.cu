@@ -57,13 +57,26 @@ __device__ inline double potential(const WarpSlot<T>& w, int nw, const uint32_t*
     return ttm::energy_warp<T>(w.crd, w.ms, w.ttm, nw, tasks, ntasks, lane, iters);
 }
 
+// MUa is staged in shared memory (FP64) when it fits this many bytes.
+constexpr size_t kMuaSmemMax = 64 * 1024;
+
 template <int PES, typename T>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs a)
 {
     extern __shared__ __align__(16) char smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int nw = a.nw, nm0 = a.nm0, N3 = 9 * nw;
-    WarpSlot<T> w = warp_slot<T>(smem + wib * slot_bytes<T>(PES, nm0, nw), PES, nm0, nw);
+    const size_t mua_b = sizeof(double) * (size_t)N3 * nm0;
+    const bool mua_in_smem = mua_b <= kMuaSmemMax;
+    const double* MUa = a.MUa;
+    if (mua_in_smem) {
+        double* m = reinterpret_cast<double*>(smem);
+        for (int e = threadIdx.x; e < N3 * nm0; e += blockDim.x) m[e] = a.MUa[e];
+        MUa = m;
+        __syncthreads();
+    }
+    char* slots = smem + (mua_in_smem ? (mua_b + 15) / 16 * 16 : 0);
+    WarpSlot<T> w = warp_slot<T>(slots + wib * slot_bytes<T>(PES, nm0, nw), PES, nm0, nw);
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
     for (int64_t s = (int64_t)blockIdx.x * kWarpsPerBlock + wib; s < a.n; s += nwarps) {
         if (s >= a.nvalid) {        // padding sample: contributes nothing
@@ -82,6 +95,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs
             } else {
                 uint64_t x = sobol_state(a.vdir, nm0, d, (uint64_t)(a.index0 + s));
                 if (a.shift) x ^= __ldg(a.shift + d);
+                if (sizeof(T) == 4) {              // FP32 form: inverse CDF in FP32
+                    w.q[d] = (double)(bsm_f32(x) * 0.70710678f);
+                    continue;
+                }
                 y = bsm(sobol_uniform(x));
             }
             w.q[d] = y / 1.4142135623730951;   // by /= sqrt(2.0)
@@ -90,7 +107,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs
         // 2. r = bohr * (x0 + MUa q)   (SCP3.cpp:208), FP64
         for (int c = lane; c < N3; c += 32) {
             double acc = 0.0;
-            for (int k = 0; k < nm0; k++) acc += __ldg(a.MUa + (size_t)k * N3 + c) * w.q[k];
+            for (int k = 0; k < nm0; k++) acc += MUa[(size_t)k * N3 + c] * w.q[k];
             w.crd[c] = (T)(kBohr * (__ldg(a.x0 + c) + acc));
         }
         __syncwarp();
@@ -156,14 +173,15 @@ int grid_for(int64_t nwarps_needed)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int64_t blocks = (nwarps_needed + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    const int64_t cap = (int64_t)sms * 16;
+    const int64_t cap = (int64_t)sms * 8;
     return (int)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
 }
 
 template <int PES, typename T>
 int launch_samples_t(const SampleArgs& a, cudaStream_t s)
 {
-    const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw);
+    const size_t mua_b = sizeof(double) * (size_t)9 * a.nw * a.nm0;
+    const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw) + (mua_b <= kMuaSmemMax ? (mua_b + 15) / 16 * 16 : 0);
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_kernel<PES, T>,
                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     samples_kernel<PES, T><<<grid_for(a.n), kWarpsPerBlock * 32, sm, s>>>(a);

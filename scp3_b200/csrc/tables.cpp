@@ -105,19 +105,47 @@ std::vector<uint32_t> pair_tasks(int nw)
 {
     std::vector<uint32_t> t;
     auto put = [&](uint32_t type, int a, int b) { t.push_back(type | ((uint32_t)a << 2) | ((uint32_t)b << 17)); };
-    for (int i = 0; i < nw; i++) {
-        for (int j = 0; j < nw; j++) {
-            if (i == j) continue;
-            for (int l = 1; l < 3; l++) put(0, i, 3 * j + l);
-        }
-        for (int j = i + 1; j < nw; j++) {
+    // grouped by type so that the lanes of a warp mostly take the same branch
+    for (int i = 0; i < nw; i++)
+        for (int j = 0; j < nw; j++)
+            if (i != j)
+                for (int l = 1; l < 3; l++) put(0, i, 3 * j + l);
+    for (int i = 0; i < nw; i++)
+        for (int j = i + 1; j < nw; j++)
             for (int a = 1; a < 3; a++)
                 for (int b = 1; b < 3; b++) put(1, 3 * i + a, 3 * j + b);
-            put(2, 3 * i, 3 * j);
-            put(3, i, j);
-        }
-    }
+    for (int i = 0; i < nw; i++)
+        for (int j = i + 1; j < nw; j++) put(2, 3 * i, 3 * j);
+    for (int i = 0; i < nw; i++)
+        for (int j = i + 1; j < nw; j++) put(3, i, j);
     return t;
+}
+
+// Each basis function as a product of three entries of a per-sample table
+// [1, h1(q_0..), h2(q_0..), h3(q_0..)]: entry indices a, b, c in bits 0..9,
+// 10..19, 20..29 (0 is the constant 1).
+std::vector<uint32_t> basis_factor_table(int nm, int n2, int n3)
+{
+    std::vector<uint32_t> d;
+    auto h1 = [&](int m) { return 1 + m; };
+    auto h2 = [&](int m) { return 1 + nm + m; };
+    auto h3 = [&](int m) { return 1 + 2 * nm + m; };
+    auto put = [&](int a, int b, int c) { d.push_back((uint32_t)a | ((uint32_t)b << 10) | ((uint32_t)c << 20)); };
+    put(0, 0, 0);
+    for (int m = 0; m < nm; m++) put(h1(m), 0, 0);
+    for (int m = 0; m < n2; m++) put(h2(m), 0, 0);
+    for (int m = 0; m < n2; m++)
+        for (int n = m + 1; n < n2; n++) put(h1(m), h1(n), 0);
+    for (int m = 0; m < n3; m++) put(h3(m), 0, 0);
+    for (int m = 0; m < n3; m++)
+        for (int n = m + 1; n < n3; n++) {
+            put(h2(m), h1(n), 0);
+            put(h1(m), h2(n), 0);
+        }
+    for (int m = 0; m < n3; m++)
+        for (int n = m + 1; n < n3; n++)
+            for (int p = n + 1; p < n3; p++) put(h1(m), h1(n), h1(p));
+    return d;
 }
 
 }  // namespace scp3

@@ -21,6 +21,7 @@ struct Plan {
     int* group_meta = nullptr;    // per flush block: first negative 16-group
     int2* tiles = nullptr;        // [ntiles] (ti, tj), in launch order
     int* tile_index = nullptr;    // [nt*nt] position of tile (ti, tj) in `tiles`
+    uint32_t* factors = nullptr;  // [nb] basis functions as products of Hermite-table entries
     double* partial = nullptr;    // [nsplit][ntiles][128*128] FP64
     void* tmap_hi = nullptr;      // CUtensorMap (host copy) for xhi / xlo
     void* tmap_lo = nullptr;
@@ -31,7 +32,7 @@ constexpr int kTile = 128;        // UMMA M = N = 128
 constexpr int kFlush = 4096;      // samples per sign-partition block (the FP64 flush is finer, see contract_tc.cu)
 constexpr int kSlotsPerFlush = kFlush + 64;  // sign partition pads each sign group to 16
 
-int create(Plan& p, int nb, int nm, int chunk_req, int sms, bool f16);
+int create(Plan& p, int nb, int nm, int n2, int n3, int chunk_req, int sms, bool f16);
 void destroy(Plan& p);
 int64_t pass_samples(const Plan& p, int64_t nvalid);
 int zero(Plan& p, cudaStream_t s);
