@@ -30,7 +30,7 @@ __device__ __forceinline__ double inv_sqrt(double x) { return 1.0 / sqrt(x); }
 // IEEE-rounded in FP32 too: rsqrtf's approximation error is not centred and its
 // bias, summed over the ~10^4 kcal/mol of Coulomb terms of a cluster, shows in
 // the levels at the 0.1 cm^-1 scale.
-__device__ __forceinline__ float inv_sqrt(float x) { return 1.0f / sqrtf(x); }
+__device__ __forceinline__ float inv_sqrt(float x) { return __frsqrt_rn(x); }
 
 // Beasley-Springer-Moro inverse normal CDF, the same formula and branch points
 // as the reference (beasley_springer_moro.cpp:14-46); log() is CUDA's.

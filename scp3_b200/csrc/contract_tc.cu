@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(1024) partition_kernel(const double* __restric
 // (g, r) handles slots 4g..4g+3 of rows r, r+8, ...: one 16-byte table read per
 // factor and 8-byte stores, so the 16 threads of a row write 128 contiguous
 // bytes per half.
-constexpr int kExpSlots = 64, kExpRows = 256, kExpThreads = 128;
+constexpr int kExpSlots = 64, kExpRows = 1024, kExpThreads = 128;
 
 template <bool F16>
 __device__ __forceinline__ void split4(float4 x, uint2& hi, uint2& lo)
@@ -443,13 +443,26 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const uint32_
         tab[e] = 1.0f;
         sv[e] = (s >= 0) ? (float)sqrt(fabs(v[s])) * (F16 ? kF16Scale : 1.0f) : 0.0f;
     }
-    for (int e = t; e < kExpSlots * nm; e += kExpThreads) {
-        const int l = e / nm, m = e - l * nm;
-        const int s = sample_of_slot[slot0 + l];
-        const float y = (s >= 0) ? q[(int64_t)s * nm + m] : 0.0f;
+    auto put = [&](int l, int m, float y) {
         tab[(1 + m) * kExpSlots + l] = 1.41421356f * y;                                  // ho1
         tab[(1 + nm + m) * kExpSlots + l] = (2.0f * y * y - 1.0f) * 0.70710678f;          // ho2
         tab[(1 + 2 * nm + m) * kExpSlots + l] = (2.0f * y * y - 3.0f) * y * 0.57735027f;  // ho3
+    };
+    if ((nm & 3) == 0) {            // 16-byte gathers of each slot's q row
+        const int n4 = nm >> 2;
+        for (int e = t; e < kExpSlots * n4; e += kExpThreads) {
+            const int l = e / n4, m4 = e - l * n4;
+            const int s = sample_of_slot[slot0 + l];
+            const float4 y = (s >= 0) ? reinterpret_cast<const float4*>(q + (int64_t)s * nm)[m4]
+                                      : make_float4(0.f, 0.f, 0.f, 0.f);
+            put(l, 4 * m4, y.x), put(l, 4 * m4 + 1, y.y), put(l, 4 * m4 + 2, y.z), put(l, 4 * m4 + 3, y.w);
+        }
+    } else {
+        for (int e = t; e < kExpSlots * nm; e += kExpThreads) {
+            const int l = e / nm, m = e - l * nm;
+            const int s = sample_of_slot[slot0 + l];
+            put(l, m, (s >= 0) ? q[(int64_t)s * nm + m] : 0.0f);
+        }
     }
     __syncthreads();
     const int g = t & 15, rl = t >> 4;
@@ -572,10 +585,12 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
                     tindex[(size_t)i * p.nt + j] = (int)t.size();
                     t.push_back(make_int2(i, j));
                 }
-    SCP3_CUDA(cudaMalloc(&p.xhi, sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
-    SCP3_CUDA(cudaMalloc(&p.xlo, sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
-    SCP3_CUDA(cudaMalloc(&p.slot_of, sizeof(int) * (size_t)p.slots));
-    SCP3_CUDA(cudaMalloc(&p.group_meta, sizeof(int) * nflush));
+    for (int b = 0; b < 2; b++) {
+        SCP3_CUDA(cudaMalloc(&p.xhi[b], sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
+        SCP3_CUDA(cudaMalloc(&p.xlo[b], sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
+        SCP3_CUDA(cudaMalloc(&p.slot_of[b], sizeof(int) * (size_t)p.slots));
+        SCP3_CUDA(cudaMalloc(&p.group_meta[b], sizeof(int) * nflush));
+    }
     SCP3_CUDA(cudaMalloc(&p.tiles, sizeof(int2) * t.size()));
     SCP3_CUDA(cudaMemcpy(p.tiles, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice));
     const std::vector<uint32_t> fac = basis_factor_table(nm_for_factors, n2_for_factors, n3_for_factors);
@@ -586,21 +601,25 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
     SCP3_CUDA(cudaMalloc(&p.partial, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kTile));
     SCP3_CUDA(cudaMalloc(&p.err_flag, sizeof(int)));
     SCP3_CUDA(cudaMemset(p.err_flag, 0, sizeof(int)));
-    int rc = encode_map(&p.tmap_hi, p.xhi, p.slots, p.nb_pad);
-    if (!rc) rc = encode_map(&p.tmap_lo, p.xlo, p.slots, p.nb_pad);
-    if (rc) return rc;
+    for (int b = 0; b < 2; b++) {
+        int rc = encode_map(&p.tmap_hi[b], p.xhi[b], p.slots, p.nb_pad);
+        if (!rc) rc = encode_map(&p.tmap_lo[b], p.xlo[b], p.slots, p.nb_pad);
+        if (rc) return rc;
+    }
     SCP3_CUDA(cudaFuncSetAttribute(contract_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
     return SCP3GPU_OK;
 }
 
 void destroy(Plan& p)
 {
-    void* ptrs[] = {p.xhi, p.xlo, p.slot_of, p.sign_groups, p.group_meta, p.tiles, p.tile_index, p.factors, p.partial,
-                    p.err_flag};
+    void* ptrs[] = {p.xhi[0], p.xhi[1], p.xlo[0], p.xlo[1], p.slot_of[0], p.slot_of[1], p.group_meta[0],
+                    p.group_meta[1], p.tiles, p.tile_index, p.factors, p.partial, p.err_flag};
     for (void* q : ptrs)
         if (q) cudaFree(q);
-    delete static_cast<CUtensorMap*>(p.tmap_hi);
-    delete static_cast<CUtensorMap*>(p.tmap_lo);
+    for (int b = 0; b < 2; b++) {
+        delete static_cast<CUtensorMap*>(p.tmap_hi[b]);
+        delete static_cast<CUtensorMap*>(p.tmap_lo[b]);
+    }
     p = Plan{};
 }
 
@@ -617,32 +636,48 @@ int zero(Plan& p, cudaStream_t s)
     return SCP3GPU_OK;
 }
 
-int accumulate_pass(Plan& p, const uint32_t* desc, int nb, int nm, const float* q32, const double* v, int64_t n,
-                    cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind)
+int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v, int64_t n, cudaStream_t s,
+            std::vector<cudaEvent_t>* pev, std::vector<int>* pkind)
 {
-    if (n % kFlush != 0 || n > p.chunk) return fail(SCP3GPU_ERR_ARG, "tc pass: sample count not in flush blocks");
+    if (n % kFlush != 0 || n > p.chunk || buf < 0 || buf > 1)
+        return fail(SCP3GPU_ERR_ARG, "tc pass: sample count not in flush blocks");
     const int nflush = (int)(n / kFlush);
     const int64_t slots = (int64_t)nflush * kSlotsPerFlush;
     record(pev, pkind, 1, s);
-    partition_kernel<<<nflush, 1024, 0, s>>>(v, p.slot_of, p.group_meta);
+    partition_kernel<<<nflush, 1024, 0, s>>>(v, p.slot_of[buf], p.group_meta[buf]);
     SCP3_CUDA(cudaGetLastError());
     const size_t sm = sizeof(float) * (size_t)(3 * nm + 2) * kExpSlots;
     auto kern = p.f16 ? expand_split_kernel<true> : expand_split_kernel<false>;
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     dim3 eg((unsigned)(slots / kExpSlots), (unsigned)((p.nb_pad + kExpRows - 1) / kExpRows));
-    kern<<<eg, kExpThreads, sm, s>>>(p.factors, nb, p.nb_pad, nm, q32, v, p.slot_of, p.slots, p.xhi, p.xlo);
+    kern<<<eg, kExpThreads, sm, s>>>(p.factors, nb, p.nb_pad, nm, q32, v, p.slot_of[buf], p.slots, p.xhi[buf],
+                                     p.xlo[buf]);
     SCP3_CUDA(cudaGetLastError());
     record(pev, pkind, 1, s);
+    return SCP3GPU_OK;
+}
+
+int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind)
+{
+    const int nflush = (int)(n / kFlush);
     record(pev, pkind, 2, s);
     const int nsplit = p.nsplit < nflush ? p.nsplit : nflush;
     dim3 grid(p.ntiles, nsplit);
-    contract_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(*static_cast<CUtensorMap*>(p.tmap_hi),
-                                                              *static_cast<CUtensorMap*>(p.tmap_lo), p.tiles,
-                                                              p.group_meta, nflush, p.ntiles, p.products, (int)p.f16,
-                                                              p.partial, p.err_flag);
+    contract_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(*static_cast<CUtensorMap*>(p.tmap_hi[buf]),
+                                                              *static_cast<CUtensorMap*>(p.tmap_lo[buf]), p.tiles,
+                                                              p.group_meta[buf], nflush, p.ntiles, p.products,
+                                                              (int)p.f16, p.partial, p.err_flag);
     SCP3_CUDA(cudaGetLastError());
     record(pev, pkind, 2, s);
     return SCP3GPU_OK;
+}
+
+int accumulate_pass(Plan& p, const uint32_t* desc, int nb, int nm, const float* q32, const double* v, int64_t n,
+                    cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind)
+{
+    (void)desc;
+    int rc = prepare(p, 0, nb, nm, q32, v, n, s, pev, pkind);
+    return rc ? rc : contract(p, 0, n, s, pev, pkind);
 }
 
 int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s)

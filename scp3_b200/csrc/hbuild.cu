@@ -80,8 +80,10 @@ struct scp3gpu_hbuild {
     std::vector<double> omega_sel;
     double zpe_inactive = 0.0;
     int dev = 0;
-    cudaStream_t stream = nullptr, copy_stream = nullptr;
+    cudaStream_t stream = nullptr, copy_stream = nullptr, prep_stream = nullptr;
     cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
+    cudaEvent_t prepared[2] = {nullptr, nullptr}, contracted[2] = {nullptr, nullptr};
+    int64_t pass = 0;                 // split form: passes launched (buffer = pass & 1)
     int nb = 0, nb_pad = 0, ntasks = 0, nsplit = 1;
     int64_t chunk = 0;
     TileMap tm{};
@@ -95,8 +97,10 @@ struct scp3gpu_hbuild {
     uint32_t *tasks = nullptr, *desc = nullptr;
     // per chunk
     double* q64 = nullptr;
-    float* q32 = nullptr;
+    float* q32 = nullptr;             // split form: q32 / vv[buffer]
     double* v = nullptr;
+    float* q32b[2] = {nullptr, nullptr};
+    double* vb[2] = {nullptr, nullptr};
     double* normals[2] = {nullptr, nullptr};
     double *phi = nullptr, *w = nullptr;
     double* partial = nullptr;
@@ -121,14 +125,18 @@ int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 struct Timed {
     scp3gpu_hbuild* h;
     int kind;
-    Timed(scp3gpu_hbuild* h_, int kind_) : h(h_), kind(kind_) { mark(); }
+    cudaStream_t st;
+    Timed(scp3gpu_hbuild* h_, int kind_, cudaStream_t s = nullptr) : h(h_), kind(kind_), st(s ? s : h_->stream)
+    {
+        mark();
+    }
     ~Timed() { mark(); }
     void mark()
     {
         if (!h->prof) return;
         cudaEvent_t e;
         if (cudaEventCreate(&e) != cudaSuccess) return;
-        cudaEventRecord(e, h->stream);
+        cudaEventRecord(e, st);
         h->pev.push_back(e);
         h->pkind.push_back(kind);
     }
@@ -150,9 +158,16 @@ void plan_fp64(scp3gpu_hbuild* h, int sms)
     h->nsplit = nsplit;
 }
 
-int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double* normals_dev)
+// One pass.  Plain form: everything on the handle's stream.  Split form: the
+// per-sample kernel, sign partition and expansion run on the prepare stream into
+// pass buffer (pass & 1) while the previous pass contracts on the main stream;
+// events order buffer reuse.  `copied` (may be null): event the normals copy of
+// this pass completes; the pass records `consumed` once it has read them.
+int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double* normals_dev,
+                 cudaEvent_t copied = nullptr, cudaEvent_t consumed = nullptr)
 {
     const bool fp32 = h->pes_fp32;
+    const int b = (int)(h->pass & 1);
     SampleArgs a{};
     a.nw = h->cfg.nw;
     a.nm0 = h->cfg.nmodes0;
@@ -170,19 +185,38 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     a.n = h->split_form ? tc::pass_samples(h->tcp, nvalid) : round_up(nvalid, 16ll * h->nsplit);
     a.nvalid = nvalid;
     a.q64 = h->split_form ? nullptr : h->q64;
-    a.q32 = h->split_form ? h->q32 : nullptr;
-    a.v = h->v;
+    a.q32 = h->split_form ? h->q32b[b] : nullptr;
+    a.v = h->split_form ? h->vb[b] : h->v;
     a.counters = h->counters;
     int rc;
+    if (h->split_form) {
+        cudaStream_t ps = h->prep_stream;
+        SCP3_CUDA(cudaStreamWaitEvent(ps, h->contracted[b], 0));   // buffer b free again
+        if (copied) SCP3_CUDA(cudaStreamWaitEvent(ps, copied, 0));
+        {
+            Timed t(h, 0, ps);
+            rc = launch_samples(h->cfg.pes, fp32, a, ps);
+        }
+        if (rc) return rc;
+        if (consumed) SCP3_CUDA(cudaEventRecord(consumed, ps));
+        rc = tc::prepare(h->tcp, b, h->nb, h->cfg.nmodes, a.q32, a.v, a.n, ps, h->prof ? &h->pev : nullptr,
+                         h->prof ? &h->pkind : nullptr);
+        if (rc) return rc;
+        SCP3_CUDA(cudaEventRecord(h->prepared[b], ps));
+        SCP3_CUDA(cudaStreamWaitEvent(h->stream, h->prepared[b], 0));
+        rc = tc::contract(h->tcp, b, a.n, h->stream, h->prof ? &h->pev : nullptr, h->prof ? &h->pkind : nullptr);
+        if (rc) return rc;
+        SCP3_CUDA(cudaEventRecord(h->contracted[b], h->stream));
+        h->pass++;
+        return SCP3GPU_OK;
+    }
+    if (copied) SCP3_CUDA(cudaStreamWaitEvent(h->stream, copied, 0));
     {
         Timed t(h, 0);
         rc = launch_samples(h->cfg.pes, fp32, a, h->stream);
     }
     if (rc) return rc;
-    if (h->split_form) {
-        return tc::accumulate_pass(h->tcp, h->desc, h->nb, h->cfg.nmodes, h->q32, h->v, a.n, h->stream,
-                                   h->prof ? &h->pev : nullptr, h->prof ? &h->pkind : nullptr);
-    }
+    if (consumed) SCP3_CUDA(cudaEventRecord(consumed, h->stream));
     {
         Timed t(h, 1);
         rc = launch_expand_fp64(h->desc, h->nb, h->nb_pad, h->cfg.nmodes, h->q64, h->v, a.n, h->chunk, h->phi, h->w,
@@ -191,6 +225,13 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     if (rc) return rc;
     Timed t(h, 2);
     return launch_contract_fp64(h->phi, h->w, h->chunk, a.n, h->nb_pad, h->tm, h->nsplit, h->partial, h->stream);
+}
+
+// Work on the prepare stream (split form) finished before the host goes on.
+int drain_prep(scp3gpu_hbuild* h)
+{
+    if (h->prep_stream) SCP3_CUDA(cudaStreamSynchronize(h->prep_stream));
+    return SCP3GPU_OK;
 }
 
 int zero_sums(scp3gpu_hbuild* h)
@@ -316,7 +357,9 @@ int scp3gpu_hbuild_destroy(scp3gpu_hbuild* h)
     DeviceGuard g(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
-    void* ptrs[] = {h->vdir, h->shift, h->x0, h->MUa, h->omega, h->modes, h->tasks, h->desc, h->q64, h->q32,
+    if (h->prep_stream) cudaStreamSynchronize(h->prep_stream);
+    void* ptrs[] = {h->vdir, h->shift, h->x0, h->MUa, h->omega, h->modes, h->tasks, h->desc, h->q64, h->q32b[0],
+                    h->q32b[1], h->vb[0], h->vb[1],
                     h->v, h->normals[0], h->normals[1], h->phi, h->w, h->partial, h->dense, h->hodiag,
                     h->counters};
     for (void* p : ptrs)
@@ -325,7 +368,10 @@ int scp3gpu_hbuild_destroy(scp3gpu_hbuild* h)
     for (int b = 0; b < 2; b++) {
         if (h->copied[b]) cudaEventDestroy(h->copied[b]);
         if (h->consumed[b]) cudaEventDestroy(h->consumed[b]);
+        if (h->prepared[b]) cudaEventDestroy(h->prepared[b]);
+        if (h->contracted[b]) cudaEventDestroy(h->contracted[b]);
     }
+    if (h->prep_stream) cudaStreamDestroy(h->prep_stream);
     if (h->stream) cudaStreamDestroy(h->stream);
     if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     delete h;
@@ -383,11 +429,14 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
         return code;
     };
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+        cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->prep_stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(SCP3GPU_ERR_CUDA, "stream creation failed"));
     for (int b = 0; b < 2; b++)
         if (cudaEventCreateWithFlags(&h->copied[b], cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&h->consumed[b], cudaEventDisableTiming) != cudaSuccess)
+            cudaEventCreateWithFlags(&h->consumed[b], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->prepared[b], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->contracted[b], cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(SCP3GPU_ERR_CUDA, "event creation failed"));
 
     std::vector<int64_t> vd;
@@ -410,8 +459,11 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
             return bail(rc);
         h->chunk = h->tcp.chunk;
         h->nb_pad = h->tcp.nb_pad;
-        if ((rc = dalloc(&h->q32, (size_t)h->chunk * c->nmodes)) || (rc = dalloc(&h->v, (size_t)h->chunk)))
-            return bail(rc);
+        for (int b = 0; b < 2; b++)
+            if ((rc = dalloc(&h->q32b[b], (size_t)h->chunk * c->nmodes)) || (rc = dalloc(&h->vb[b], (size_t)h->chunk)))
+                return bail(rc);
+        h->q32 = h->q32b[0];
+        h->v = h->vb[0];
     } else {
         plan_fp64(h, sms);
         if ((rc = dalloc(&h->q64, (size_t)h->chunk * c->nmodes)) || (rc = dalloc(&h->v, (size_t)h->chunk)) ||
@@ -429,7 +481,8 @@ int scp3gpu_hbuild_reset(scp3gpu_hbuild* h)
 {
     if (!h) return fail(SCP3GPU_ERR_ARG, "null handle");
     DeviceGuard g(h->dev);
-    int rc = zero_sums(h);
+    int rc = drain_prep(h);
+    if (!rc) rc = zero_sums(h);
     if (rc) return rc;
     SCP3_CUDA(cudaMemsetAsync(h->counters, 0, 2 * sizeof(unsigned long long), h->stream));
     h->count = 0;
@@ -471,9 +524,7 @@ int scp3gpu_hbuild_accumulate_normals(scp3gpu_hbuild* h, const double* normals, 
         SCP3_CUDA(cudaMemcpyAsync(h->normals[b], normals + off * nm0, sizeof(double) * c * nm0,
                                   cudaMemcpyHostToDevice, h->copy_stream));
         SCP3_CUDA(cudaEventRecord(h->copied[b], h->copy_stream));
-        SCP3_CUDA(cudaStreamWaitEvent(h->stream, h->copied[b], 0));
-        if ((rc = launch_chunk(h, 0, c, h->normals[b]))) return rc;
-        SCP3_CUDA(cudaEventRecord(h->consumed[b], h->stream));
+        if ((rc = launch_chunk(h, 0, c, h->normals[b], h->copied[b], h->consumed[b]))) return rc;
         h->count += c;
     }
     SCP3_CUDA(cudaStreamSynchronize(h->copy_stream));
@@ -485,6 +536,8 @@ int scp3gpu_hbuild_add_epot(scp3gpu_hbuild* h, const double* q, const double* V,
     if (!h || n < 0 || (n > 0 && (!q || !V))) return fail(SCP3GPU_ERR_ARG, "add_epot: bad arguments");
     DeviceGuard g(h->dev);
     const int nm = h->cfg.nmodes;
+    if (int rc0 = drain_prep(h)) return rc0;
+    SCP3_CUDA(cudaStreamSynchronize(h->stream));
     for (int64_t off = 0; off < n; off += h->chunk) {
         const int64_t c = std::min(h->chunk, n - off);
         const int64_t kn = h->split_form ? tc::pass_samples(h->tcp, c) : round_up(c, 16ll * h->nsplit);
@@ -624,6 +677,7 @@ int scp3gpu_hbuild_profile(scp3gpu_hbuild* h, int enable, double* ms, int64_t* l
     int64_t cnt[4] = {0, 0, 0, 0};
     int rc = SCP3GPU_OK;
     if (!enable) {
+        if (h->prep_stream) cudaStreamSynchronize(h->prep_stream);
         cudaError_t e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) rc = cuda_fail(e, "profile sync");
         for (size_t k = 0; !rc && k + 1 < h->pev.size(); k += 2) {
@@ -648,6 +702,8 @@ int scp3gpu_hbuild_status(scp3gpu_hbuild* h, int64_t* nonfinite, int64_t* not_co
     if (!h) return fail(SCP3GPU_ERR_ARG, "null handle");
     DeviceGuard g(h->dev);
     unsigned long long c[2] = {0, 0};
+    int rc0 = drain_prep(h);
+    if (rc0) return rc0;
     SCP3_CUDA(cudaMemcpyAsync(c, h->counters, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
     SCP3_CUDA(cudaStreamSynchronize(h->stream));
     if (nonfinite) *nonfinite = (int64_t)c[0];

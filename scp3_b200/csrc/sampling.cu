@@ -18,6 +18,7 @@ namespace scp3 {
 namespace {
 
 constexpr int kWarpsPerBlock = 8;
+constexpr int kRun = 16;          // consecutive samples per warp (Gray-code walk)
 
 template <typename T>
 struct WarpSlot {
@@ -77,8 +78,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs
     }
     char* slots = smem + (mua_in_smem ? (mua_b + 15) / 16 * 16 : 0);
     WarpSlot<T> w = warp_slot<T>(slots + wib * slot_bytes<T>(PES, nm0, nw), PES, nm0, nw);
+    // Each warp takes runs of kRun consecutive samples: the Sobol state of the
+    // first is formed from the Gray code of its index, the next ones by one XOR
+    // per dimension (index k differs from k-1 in direction number ctz(k)).
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
-    for (int64_t s = (int64_t)blockIdx.x * kWarpsPerBlock + wib; s < a.n; s += nwarps) {
+    const int64_t nruns = (a.n + kRun - 1) / kRun;
+    constexpr int kDimsPerLane = 4;           // dimensions up to 128 keep their state in registers
+    for (int64_t run = (int64_t)blockIdx.x * kWarpsPerBlock + wib; run < nruns; run += nwarps) {
+        uint64_t st[kDimsPerLane];
+        const int64_t s_first = run * kRun;
+        const bool sobol = a.normals == nullptr;
+      for (int64_t s = s_first; s < s_first + kRun && s < a.n; s++) {
         if (s >= a.nvalid) {        // padding sample: contributes nothing
             if (lane == 0) a.v[s] = 0.0;
             for (int m = lane; m < a.nm; m += 32) {
@@ -88,13 +98,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs
             continue;
         }
         // 1. standard normals -> q   (SCP3.cpp:196-201)
-        for (int d = lane; d < nm0; d += 32) {
+        const uint64_t idx = (uint64_t)(a.index0 + s);
+#pragma unroll
+        for (int j = 0; j < kDimsPerLane; j++) {
+            const int d = lane + 32 * j;
+            if (d >= nm0) break;
             double y;
-            if (a.normals) {
+            if (!sobol) {
                 y = a.normals[s * nm0 + d];
             } else {
-                uint64_t x = sobol_state(a.vdir, nm0, d, (uint64_t)(a.index0 + s));
-                if (a.shift) x ^= __ldg(a.shift + d);
+                if (s == s_first) st[j] = sobol_state(a.vdir, nm0, d, idx);
+                else st[j] ^= (uint64_t)__ldg(a.vdir + (size_t)(__ffsll((long long)idx) - 1) * nm0 + d);
+                const uint64_t x = a.shift ? st[j] ^ __ldg(a.shift + d) : st[j];
                 if (sizeof(T) == 4) {              // FP32 form: inverse CDF in FP32
                     w.q[d] = (double)(bsm_f32(x) * 0.70710678f);
                     continue;
@@ -103,12 +118,25 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs
             }
             w.q[d] = y / 1.4142135623730951;   // by /= sqrt(2.0)
         }
+        for (int d = lane + 32 * kDimsPerLane; d < nm0; d += 32) {   // beyond 128 dimensions
+            double y = sobol ? bsm(sobol_uniform((a.shift ? __ldg(a.shift + d) : 0ull) ^
+                                                 sobol_state(a.vdir, nm0, d, idx)))
+                             : a.normals[s * nm0 + d];
+            w.q[d] = y / 1.4142135623730951;
+        }
         __syncwarp();
-        // 2. r = bohr * (x0 + MUa q)   (SCP3.cpp:208), FP64
-        for (int c = lane; c < N3; c += 32) {
-            double acc = 0.0;
-            for (int k = 0; k < nm0; k++) acc += MUa[(size_t)k * N3 + c] * w.q[k];
-            w.crd[c] = (T)(kBohr * (__ldg(a.x0 + c) + acc));
+        // 2. r = bohr * (x0 + MUa q)   (SCP3.cpp:208), FP64; a lane's two coordinates in one pass
+        for (int c = lane; c < N3; c += 64) {
+            const bool two = c + 32 < N3;
+            double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll 4
+            for (int k = 0; k < nm0; k++) {
+                const double qk = w.q[k];
+                acc0 += MUa[(size_t)k * N3 + c] * qk;
+                if (two) acc1 += MUa[(size_t)k * N3 + c + 32] * qk;
+            }
+            w.crd[c] = (T)(kBohr * (__ldg(a.x0 + c) + acc0));
+            if (two) w.crd[c + 32] = (T)(kBohr * (__ldg(a.x0 + c + 32) + acc1));
         }
         __syncwarp();
         // 3. V in hartree, anharmonic residual   (SCP3.cpp:219-223)
@@ -130,6 +158,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs
             if (a.q32) a.q32[s * a.nm + m] = (float)qm;
         }
         __syncwarp();
+      }
     }
 }
 
@@ -184,7 +213,7 @@ int launch_samples_t(const SampleArgs& a, cudaStream_t s)
     const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw) + (mua_b <= kMuaSmemMax ? (mua_b + 15) / 16 * 16 : 0);
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_kernel<PES, T>,
                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    samples_kernel<PES, T><<<grid_for(a.n), kWarpsPerBlock * 32, sm, s>>>(a);
+    samples_kernel<PES, T><<<grid_for((a.n + kRun - 1) / kRun), kWarpsPerBlock * 32, sm, s>>>(a);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }

@@ -14,17 +14,17 @@ struct Plan {
     bool f16 = false;             // halves in FP16 (operand scaled by 2^6) instead of BF16
     int64_t slots = 0;            // K slots per pass after sign partition and padding
     // device buffers
-    uint16_t* xhi = nullptr;      // [nb_pad][slots] bf16: sqrt|V| Phi, high part
-    uint16_t* xlo = nullptr;      // [nb_pad][slots] bf16: low part
-    int* slot_of = nullptr;       // [chunk] sample -> K slot
-    uint32_t* sign_groups = nullptr;  // [slots/16] bit per 16-sample group: 1 = negative V
-    int* group_meta = nullptr;    // per flush block: first negative 16-group
+    // two pass buffers, so one pass can be prepared while the previous contracts
+    uint16_t* xhi[2] = {nullptr, nullptr};   // [nb_pad][slots] 16-bit: sqrt|V| Phi, high part
+    uint16_t* xlo[2] = {nullptr, nullptr};   // [nb_pad][slots] 16-bit: low part
+    int* slot_of[2] = {nullptr, nullptr};    // [slots] K slot -> sample (-1: zero padding)
+    int* group_meta[2] = {nullptr, nullptr}; // per 4096-sample block: first negative 16-group
     int2* tiles = nullptr;        // [ntiles] (ti, tj), in launch order
     int* tile_index = nullptr;    // [nt*nt] position of tile (ti, tj) in `tiles`
     uint32_t* factors = nullptr;  // [nb] basis functions as products of Hermite-table entries
     double* partial = nullptr;    // [nsplit][ntiles][128*128] FP64
-    void* tmap_hi = nullptr;      // CUtensorMap (host copy) for xhi / xlo
-    void* tmap_lo = nullptr;
+    void* tmap_hi[2] = {nullptr, nullptr};   // CUtensorMap (host copies) for xhi / xlo
+    void* tmap_lo[2] = {nullptr, nullptr};
     int* err_flag = nullptr;      // bounded-wait failures
 };
 
@@ -38,6 +38,12 @@ int64_t pass_samples(const Plan& p, int64_t nvalid);
 int zero(Plan& p, cudaStream_t s);
 // pev/pkind (may be null): when given, an event pair is recorded around every
 // launch with its kind (1 preparation, 2 contraction) for the handle's timing.
+// prepare: sign partition + expansion of n samples (q32, v) into pass buffer buf.
+int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v, int64_t n, cudaStream_t s,
+            std::vector<cudaEvent_t>* pev, std::vector<int>* pkind);
+// contract: the tensor-core accumulation of pass buffer buf into the partials.
+int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind);
+// both, on one stream, buffer 0
 int accumulate_pass(Plan& p, const uint32_t* desc, int nb, int nm, const float* q32, const double* v, int64_t n,
                     cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind);
 int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s);
