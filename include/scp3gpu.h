@@ -178,6 +178,40 @@ int scp3gpu_add_epot_static(int nmodes, int n2, int n3, const double* q_dev, con
  * Stored contiguous rather than chunked + deflate. */
 int scp3gpu_save_h5(const char* path, const double* M, int64_t n_rows, int64_t n_cols);
 
+/* ------------------------------------------------------------------ surrogate
+ * The learned control variate (no counterpart in the reference, which always
+ * evaluates the exact potential, SCP3.cpp:205-225): an n_in -> hidden -> hidden
+ * -> hidden -> 1 GELU network with BF16 weights and FP32 accumulation, trained
+ * and evaluated by this library's kernels.  Host buffers; q is n x n_in
+ * (sample-major), t and y are n targets/outputs in the units of V_anh. */
+typedef struct scp3gpu_mlp scp3gpu_mlp;
+int scp3gpu_mlp_create(int n_in, int hidden, int max_batch, uint64_t seed, int device, scp3gpu_mlp** out);
+int scp3gpu_mlp_destroy(scp3gpu_mlp* m);
+int64_t scp3gpu_mlp_num_params(const scp3gpu_mlp* m);
+/* flat parameters: for each layer l = 0..3, W_l (out x in, row-major) then b_l */
+int scp3gpu_mlp_get_params(scp3gpu_mlp* m, float* p, int64_t n);
+int scp3gpu_mlp_set_params(scp3gpu_mlp* m, const float* p, int64_t n);
+/* output = raw * scale + shift (targets are fitted in raw units) */
+int scp3gpu_mlp_set_output(scp3gpu_mlp* m, float scale, float shift);
+int scp3gpu_mlp_forward(scp3gpu_mlp* m, const float* q, int64_t n, float* y);
+/* mean-squared-error loss (raw units) of one batch (n a multiple of 64) and its
+ * gradient in the flat parameter order */
+int scp3gpu_mlp_grad(scp3gpu_mlp* m, const float* q, const float* t, int n, float* loss, float* grad);
+int scp3gpu_mlp_train(scp3gpu_mlp* m, const float* q, const float* t, int64_t n, int epochs, int batch, float lr,
+                      uint64_t seed, float* final_loss);
+
+#define SCP3GPU_SURROGATE_NONE 0
+#define SCP3GPU_SURROGATE_REPLACE 1  /* V_anh := V_nn(q); the potential is not evaluated */
+#define SCP3GPU_SURROGATE_RESIDUAL 2 /* V_anh := V_anh - V_nn(q)                         */
+/* Attach a surrogate to a split-form build (its input is the selected modes'
+ * q; max_batch >= the build's pass size); the control-variate estimate is
+ * M_replace / N_replace + M_residual / N_residual over two builds. */
+int scp3gpu_hbuild_set_surrogate(scp3gpu_hbuild* h, scp3gpu_mlp* m, int mode);
+/* The per-sample stage alone for points index0..index0+n-1: q of the selected
+ * modes (n x nmodes, FP32) and V_anh (n, FP64) into host buffers -- training
+ * data for the surrogate. */
+int scp3gpu_hbuild_sample(scp3gpu_hbuild* h, int64_t index0, int64_t n, float* q, double* v);
+
 /* Kernel timing (no counterpart in the reference, which has no in-code timing;
  * only a VTune build profile, config/vtune.mk:1-4).  enable = 1 clears and starts
  * recording CUDA events around every kernel the handle launches on its stream;

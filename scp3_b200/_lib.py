@@ -22,6 +22,9 @@ EXPORTS = [
     "scp3gpu_hbuild_accumulate", "scp3gpu_hbuild_accumulate_normals", "scp3gpu_hbuild_add_epot",
     "scp3gpu_hbuild_sample_count", "scp3gpu_hbuild_read", "scp3gpu_hbuild_read_dev", "scp3gpu_hbuild_eigvals", "scp3gpu_hbuild_status",
     "scp3gpu_hbuild_profile", "scp3gpu_add_epot_static", "scp3gpu_save_h5",
+    "scp3gpu_mlp_create", "scp3gpu_mlp_destroy", "scp3gpu_mlp_num_params", "scp3gpu_mlp_get_params",
+    "scp3gpu_mlp_set_params", "scp3gpu_mlp_set_output", "scp3gpu_mlp_forward", "scp3gpu_mlp_grad", "scp3gpu_mlp_train",
+    "scp3gpu_hbuild_set_surrogate", "scp3gpu_hbuild_sample",
 ]
 
 

@@ -10,6 +10,12 @@
 
 #include "internal.h"
 #include "tc.h"
+#include "mlp.h"
+
+namespace scp3 {
+mlp::Net* mlp_net(scp3gpu_mlp* m);
+int mlp_device(const scp3gpu_mlp* m);
+}
 
 namespace scp3 {
 
@@ -110,6 +116,10 @@ struct scp3gpu_hbuild {
     double* hodiag = nullptr;
     unsigned long long* counters = nullptr;
     int64_t count = 0;
+    // learned surrogate
+    scp3gpu_mlp* sur = nullptr;
+    int sur_mode = SCP3GPU_SURROGATE_NONE;
+    float* ybuf = nullptr;
     // kernel timing
     bool prof = false;
     std::vector<cudaEvent_t> pev;
@@ -158,6 +168,14 @@ void plan_fp64(scp3gpu_hbuild* h, int sms)
     h->nsplit = nsplit;
 }
 
+}  // namespace
+namespace scp3 {
+namespace hb {
+int launch_combine(int mode, double* v, const float* y, int64_t nvalid, cudaStream_t s);
+}
+}  // namespace scp3
+namespace {
+
 // One pass.  Plain form: everything on the handle's stream.  Split form: the
 // per-sample kernel, sign partition and expansion run on the prepare stream into
 // pass buffer (pass & 1) while the previous pass contracts on the main stream;
@@ -188,6 +206,7 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     a.q32 = h->split_form ? h->q32b[b] : nullptr;
     a.v = h->split_form ? h->vb[b] : h->v;
     a.counters = h->counters;
+    a.skip_pes = h->sur_mode == SCP3GPU_SURROGATE_REPLACE;
     int rc;
     if (h->split_form) {
         cudaStream_t ps = h->prep_stream;
@@ -199,6 +218,12 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
         }
         if (rc) return rc;
         if (consumed) SCP3_CUDA(cudaEventRecord(consumed, ps));
+        if (h->sur) {
+            Timed t(h, 1, ps);
+            rc = mlp_net(h->sur)->forward(a.q32, (int)a.n, h->ybuf, ps);
+            if (!rc) rc = hb::launch_combine(h->sur_mode, a.v, h->ybuf, nvalid, ps);
+            if (rc) return rc;
+        }
         rc = tc::prepare(h->tcp, b, h->nb, h->cfg.nmodes, a.q32, a.v, a.n, ps, h->prof ? &h->pev : nullptr,
                          h->prof ? &h->pkind : nullptr);
         if (rc) return rc;
@@ -226,6 +251,29 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     Timed t(h, 2);
     return launch_contract_fp64(h->phi, h->w, h->chunk, a.n, h->nb_pad, h->tm, h->nsplit, h->partial, h->stream);
 }
+
+}  // namespace
+
+namespace scp3 {
+namespace hb {
+__global__ void combine_kernel(int mode, double* __restrict__ v, const float* __restrict__ y, int64_t n)
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    v[s] = mode == SCP3GPU_SURROGATE_REPLACE ? (double)y[s] : v[s] - (double)y[s];
+}
+
+int launch_combine(int mode, double* v, const float* y, int64_t nvalid, cudaStream_t s)
+{
+    if (nvalid <= 0) return SCP3GPU_OK;
+    combine_kernel<<<(unsigned)((nvalid + 255) / 256), 256, 0, s>>>(mode, v, y, nvalid);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+}  // namespace hb
+}  // namespace scp3
+
+namespace {
 
 // Work on the prepare stream (split form) finished before the host goes on.
 int drain_prep(scp3gpu_hbuild* h)
@@ -358,7 +406,7 @@ int scp3gpu_hbuild_destroy(scp3gpu_hbuild* h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     if (h->prep_stream) cudaStreamSynchronize(h->prep_stream);
-    void* ptrs[] = {h->vdir, h->shift, h->x0, h->MUa, h->omega, h->modes, h->tasks, h->desc, h->q64, h->q32b[0],
+    void* ptrs[] = {h->ybuf, h->vdir, h->shift, h->x0, h->MUa, h->omega, h->modes, h->tasks, h->desc, h->q64, h->q32b[0],
                     h->q32b[1], h->vb[0], h->vb[1],
                     h->v, h->normals[0], h->normals[1], h->phi, h->w, h->partial, h->dense, h->hodiag,
                     h->counters};
@@ -498,6 +546,7 @@ int scp3gpu_hbuild_accumulate(scp3gpu_hbuild* h, int64_t index0, int64_t n)
     if (!h || index0 < 0 || n < 0) return fail(SCP3GPU_ERR_ARG, "accumulate: bad handle or range");
     if (index0 + n > (1ll << 62)) return fail(SCP3GPU_ERR_ARG, "accumulate: Sobol index beyond 2^62");
     DeviceGuard g(h->dev);
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     for (int64_t off = 0; off < n; off += h->chunk) {
         const int64_t c = std::min(h->chunk, n - off);
         int rc = launch_chunk(h, index0 + off, c, nullptr);
@@ -511,6 +560,7 @@ int scp3gpu_hbuild_accumulate_normals(scp3gpu_hbuild* h, const double* normals, 
 {
     if (!h || n < 0 || (n > 0 && !normals)) return fail(SCP3GPU_ERR_ARG, "accumulate_normals: bad arguments");
     DeviceGuard g(h->dev);
+    (void)cudaGetLastError();
     const int nm0 = h->cfg.nmodes0;
     int rc = SCP3GPU_OK;
     for (int b = 0; b < 2 && !h->normals[b]; b++)
@@ -667,6 +717,63 @@ int scp3gpu_hbuild_eigvals(scp3gpu_hbuild* h, int64_t nsub, int k, double* evals
     if (sol) cusolverDnDestroy(sol);
     cudaFree(A), cudaFree(W), cudaFree(work), cudaFree(info);
     return rc;
+}
+
+int scp3gpu_hbuild_set_surrogate(scp3gpu_hbuild* h, scp3gpu_mlp* m, int mode)
+{
+    if (!h) return fail(SCP3GPU_ERR_ARG, "null handle");
+    if (mode == SCP3GPU_SURROGATE_NONE) {
+        h->sur = nullptr;
+        h->sur_mode = mode;
+        return SCP3GPU_OK;
+    }
+    if (mode != SCP3GPU_SURROGATE_REPLACE && mode != SCP3GPU_SURROGATE_RESIDUAL)
+        return fail(SCP3GPU_ERR_ARG, "unknown surrogate mode");
+    if (!m || !h->split_form) return fail(SCP3GPU_ERR_ARG, "a surrogate needs a split-form build and a network");
+    mlp::Net* net = mlp_net(m);
+    if (net->n_in != h->cfg.nmodes || net->max_batch < h->chunk || mlp_device(m) != h->dev)
+        return fail(SCP3GPU_ERR_ARG, "surrogate: input width must equal nmodes, max_batch >= pass size, same device");
+    DeviceGuard g(h->dev);
+    if (int rc = drain_prep(h)) return rc;
+    if (!h->ybuf && cudaMalloc(&h->ybuf, sizeof(float) * (size_t)h->chunk) != cudaSuccess)
+        return fail(SCP3GPU_ERR_NOMEM, "surrogate output buffer");
+    h->sur = m;
+    h->sur_mode = mode;
+    return SCP3GPU_OK;
+}
+
+int scp3gpu_hbuild_sample(scp3gpu_hbuild* h, int64_t index0, int64_t n, float* q, double* v)
+{
+    if (!h || index0 < 0 || n < 0 || (n > 0 && (!q || !v))) return fail(SCP3GPU_ERR_ARG, "sample: bad arguments");
+    DeviceGuard g(h->dev);
+    if (int rc = drain_prep(h)) return rc;
+    SCP3_CUDA(cudaStreamSynchronize(h->stream));
+    const int nm = h->cfg.nmodes;
+    std::vector<double> qd;
+    for (int64_t off = 0; off < n; off += h->chunk) {
+        const int64_t c = std::min(h->chunk, n - off);
+        SampleArgs a{};
+        a.nw = h->cfg.nw, a.nm0 = h->cfg.nmodes0, a.nm = nm;
+        a.x0 = h->x0, a.MUa = h->MUa, a.omega = h->omega, a.modes = h->modes, a.vdir = h->vdir, a.shift = h->shift;
+        a.tasks = h->tasks, a.ntasks = h->ntasks, a.index0 = index0 + off, a.n = c, a.nvalid = c;
+        a.q64 = h->split_form ? nullptr : h->q64;
+        a.q32 = h->split_form ? h->q32b[0] : nullptr;
+        a.v = h->split_form ? h->vb[0] : h->v;
+        a.counters = h->counters;
+        int rc = launch_samples(h->cfg.pes, h->pes_fp32, a, h->stream);
+        if (rc) return rc;
+        if (h->split_form) {
+            SCP3_CUDA(cudaMemcpyAsync(q + off * nm, a.q32, sizeof(float) * c * nm, cudaMemcpyDeviceToHost, h->stream));
+        } else {
+            qd.resize((size_t)c * nm);
+            SCP3_CUDA(cudaMemcpyAsync(qd.data(), a.q64, sizeof(double) * c * nm, cudaMemcpyDeviceToHost, h->stream));
+        }
+        SCP3_CUDA(cudaMemcpyAsync(v + off, a.v, sizeof(double) * c, cudaMemcpyDeviceToHost, h->stream));
+        SCP3_CUDA(cudaStreamSynchronize(h->stream));
+        if (!h->split_form)
+            for (size_t i = 0; i < qd.size(); i++) q[off * nm + i] = (float)qd[i];
+    }
+    return SCP3GPU_OK;
 }
 
 int scp3gpu_hbuild_profile(scp3gpu_hbuild* h, int enable, double* ms, int64_t* launches)

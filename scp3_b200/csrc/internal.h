@@ -15,10 +15,12 @@ void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 
-#define SCP3_CUDA(call)                                                  \
-    do {                                                                 \
-        cudaError_t e_ = (call);                                         \
-        if (e_ != cudaSuccess) return ::scp3::cuda_fail(e_, #call);      \
+#define SCP3_STR2(x) #x
+#define SCP3_STR(x) SCP3_STR2(x)
+#define SCP3_CUDA(call)                                                                         \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) return ::scp3::cuda_fail(e_, __FILE__ ":" SCP3_STR(__LINE__) " " #call); \
     } while (0)
 
 constexpr int kLogMax = 62;           // bits of the Sobol state (sobol.cpp:27700)
@@ -73,6 +75,7 @@ struct SampleArgs {
     float* q32;                   // [n x nm] selected q, FP32 (may be nullptr)
     double* v;                    // [n] V_anh (hartree)
     unsigned long long* counters; // [2] non-finite, not converged
+    int skip_pes;                 // 1: q only, V_anh = 0 (the surrogate supplies V)
 };
 // pes: SCP3GPU_PES_*, fp32: run the potential in FP32.
 int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s);

@@ -141,11 +141,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs
         __syncwarp();
         // 3. V in hartree, anharmonic residual   (SCP3.cpp:219-223)
         int iters = 0;
-        const double e = potential<PES, T>(w, nw, a.tasks, a.ntasks, lane, &iters);
-        double h = 0.0;
-        for (int d = lane; d < nm0; d += 32) h += w.q[d] * (__ldg(a.omega + d) * w.q[d]);
-        h = warp_sum(h);
-        const double V = e / kAuToKcalPerMol - 0.5 * h;
+        double V = 0.0;
+        if (!a.skip_pes) {
+            const double e = potential<PES, T>(w, nw, a.tasks, a.ntasks, lane, &iters);
+            double h = 0.0;
+            for (int d = lane; d < nm0; d += 32) h += w.q[d] * (__ldg(a.omega + d) * w.q[d]);
+            h = warp_sum(h);
+            V = e / kAuToKcalPerMol - 0.5 * h;
+        }
         if (lane == 0) {
             a.v[s] = V;
             if (!isfinite(V)) atomicAdd(a.counters + 0, 1ull);

@@ -1,0 +1,90 @@
+"""The learned surrogate: forward and gradients of the library's kernels
+against the float64 oracle (oracle/mlp_oracle.py), a training run, and the
+control-variate estimator against the plain one (what the network gains)."""
+import numpy as np
+import pytest
+
+from conftest import load_hbuild_case
+
+pytestmark = pytest.mark.gpu
+AUTOCM = 2.194746313e5
+
+
+@pytest.fixture(scope="module")
+def sur():
+    import torch
+    assert torch.cuda.is_available()
+    from scp3_b200 import surrogate
+    return surrogate
+
+
+def test_forward_and_gradients_match_oracle(sur):
+    from oracle import mlp_oracle as mo
+    rng = np.random.default_rng(0)
+    net = sur.MLP(48, hidden=256, max_batch=256, seed=3)
+    net.set_output(0.02, -0.06)
+    q = rng.normal(scale=np.sqrt(0.5), size=(128, 48)).astype(np.float32)
+    t = (-0.06 + 0.02 * np.tanh(q[:, :4].sum(1))).astype(np.float32)
+    p = net.get_params()
+    y = net(q)
+    y_or, _ = mo.forward(p, q, 48, 256, 0.02, -0.06)
+    assert np.allclose(y, y_or, rtol=2e-3, atol=1e-5), np.abs(y - y_or).max()
+    loss, g = net.loss_and_grad(q, t)
+    loss_or, g_or = mo.loss_and_grad(p, q, t, 48, 256, 0.02, -0.06)
+    assert loss == pytest.approx(loss_or, rel=2e-3)
+    err = np.linalg.norm(g - g_or) / np.linalg.norm(g_or)
+    assert err <= 1e-2, err
+    # per layer too (weights and biases)
+    k = 0
+    for o, i in ((256, 48), (256, 256), (256, 256), (1, 256)):
+        for n in (o * i, o):
+            seg = slice(k, k + n)
+            assert np.linalg.norm(g[seg] - g_or[seg]) <= 2e-2 * np.linalg.norm(g_or[seg]) + 1e-9
+            k += n
+
+
+def test_training_fits_a_smooth_function(sur):
+    rng = np.random.default_rng(1)
+    q = rng.normal(scale=np.sqrt(0.5), size=(1 << 14, 48)).astype(np.float32)
+    t = (0.01 * (q[:, :8] ** 2).sum(1) - 0.002 * q[:, 0] * q[:, 1] + 0.001 * q[:, 2] ** 3).astype(np.float32)
+    net = sur.MLP(48, hidden=256, max_batch=4096, seed=5)
+    net.set_output(float(t.std()), float(t.mean()))
+    y0 = net(q)
+    before = float(np.mean((y0 - t) ** 2))
+    net.fit(q, t, epochs=40, batch=1024, lr=2e-3)
+    after = float(np.mean((net(q) - t) ** 2))
+    assert after < 0.02 * before, (before, after)
+
+
+def test_control_variate_gains_over_plain(sur):
+    """Dimer doubles basis: the surrogate trained on 2^13 exact samples, then
+    M_cv with 2^17 surrogate points + 2^12 exact residual points against the plain
+    estimator with the same 2^12 exact points; errors of the 10 lowest levels
+    judged against a 2^20-point plain build."""
+    import scp3_b200
+    c = load_hbuild_case("dimer_qtip4pf")
+
+    def make(prec="bf16x3"):
+        return scp3_b200.HBuild(2, c["x0"], c["MUa"], c["omega"], n2=12, n3=0, precision=prec, scramble_seed=0x5C3)
+
+    def levels(Mraw, hb):
+        M = np.asfortranarray(Mraw.copy())
+        scp3_b200.ScaledMatrixElements(c["omega"], 12, 0).addHODiagonal(M)
+        return np.linalg.eigvalsh(M)[:10]
+
+    hb = make()
+    qtr, vtr = sur.sample(hb, 1 << 30, 1 << 13)
+    net = sur.MLP(12, hidden=256, max_batch=1 << 17, seed=9)
+    net.fit(qtr, vtr.astype(np.float32), epochs=60, batch=1024, lr=2e-3)
+    ref = make()
+    ref.accumulate(0, 1 << 20)
+    e_ref = levels(ref.read(0) / (1 << 20), ref)
+    plain = make()
+    plain.accumulate(0, 1 << 12)
+    e_plain = levels(plain.read(0) / (1 << 12), plain)
+    Mcv = sur.control_variate(make, net, 1 << 17, 1 << 12, 1 << 40, 0)
+    e_cv = levels(Mcv, hb)
+    err_plain = np.abs(e_plain - e_ref).max() * AUTOCM
+    err_cv = np.abs(e_cv - e_ref).max() * AUTOCM
+    print("levels error cm-1: plain %.3f  control variate %.3f" % (err_plain, err_cv))
+    assert err_cv < err_plain
