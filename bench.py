@@ -181,8 +181,11 @@ def run_triples(args):
             t_compute += t1 - t0
             if Mh is not None and not args.no_dump:
                 hb.read(1, out=Mh)
-                h5.save(os.path.join(outdir, "sM_%07d.h5" % (c0 + chunk)), Mh)
+                path = os.path.join(outdir, "sM_%07d.h5" % (c0 + chunk))
+                h5.save(path, Mh)
                 t_dump += time.perf_counter() - t1
+                if c0 > 0:          # keep only the newest dump on disk (1.7 GB each)
+                    os.remove(os.path.join(outdir, "sM_%07d.h5" % c0))
         t0 = time.perf_counter()
         ev = hb.eigvals(10)
         t_eig = time.perf_counter() - t0
@@ -199,6 +202,77 @@ def run_triples(args):
                       "max_abs_err_cm1_vs_fp64": err, "h5_dir": outdir}))
 
 
+def run_cv(args):
+    """The learned control variate on the TTM3-F hexamer prism, doubles basis
+    (1225 functions): the surrogate trained on 2^18 exact samples, then
+    V_nn over 2^24 points + (V - V_nn) over 2^20 exact points, against the
+    plain exact estimator with 2^21 points and with as many points as the
+    control variate's GPU time buys; level errors against a 2^23-point exact
+    build.  One JSON line; not the benchmark's default."""
+    import torch
+    import scp3_b200
+    from scp3_b200 import inputs, surrogate
+    torch.cuda.set_device(0)
+    nw, x0, MUa, omega = inputs.load("prism_ttm3f")
+    autocm = scp3_b200.constants.autocm
+    prec = args.precision
+
+    def make():
+        return scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=0, pes="ttm3f", precision=prec,
+                                scramble_seed=SCRAMBLE_SEED)
+
+    sme = scp3_b200.ScaledMatrixElements(omega, 48, 0)
+
+    def levels(Mavg):
+        M = np.asfortranarray(Mavg.copy())
+        sme.addHODiagonal(M)
+        return np.linalg.eigvalsh(M)[:10] * autocm
+
+    def plain(n, i0=0):
+        hb = make()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hb.accumulate(i0, n)
+        M = hb.read(0) / n
+        t = time.perf_counter() - t0
+        hb.close()
+        return M, t
+
+    M_ref, t_ref = plain(1 << 23, 1 << 42)
+    e_ref = levels(M_ref)
+    hb = make()
+    t0 = time.perf_counter()
+    q, v = surrogate.sample(hb, 1 << 44, 1 << 18)
+    t_sample = time.perf_counter() - t0
+    hb.close()
+    net = surrogate.MLP(48, hidden=256, max_batch=1 << 17, seed=11)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = net.fit(q, v.astype(np.float32), epochs=args.cv_epochs, batch=4096, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    y = net(q[:1 << 16])
+    r2 = 1.0 - float(np.var(v[:1 << 16] - y) / np.var(v[:1 << 16]))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    M_cv = surrogate.control_variate(make, net, 1 << 24, 1 << 20, 1 << 40, 0)
+    torch.cuda.synchronize()
+    t_cv = time.perf_counter() - t0
+    M_p21, t_p21 = plain(1 << 21)
+    n_eq = int(min(1 << 24, (1 << 21) * t_cv / t_p21)) // 4096 * 4096
+    M_eq, t_eq = plain(n_eq)
+    err = lambda M: float(np.abs(levels(M) - e_ref).max())
+    print(json.dumps({"config": {"workload": "hexamer prism TTM3-F, doubles basis Nb=1225; surrogate 48-256-256-256-1 "
+                                             "GELU trained on 2^18 exact samples; V_nn over 2^24 + residual over 2^20",
+                                 "precision": prec},
+                      "train": {"samples": 1 << 18, "epochs": args.cv_epochs, "sample_s": t_sample,
+                                "train_s": t_train, "final_batch_loss": loss, "r2_heldin": r2},
+                      "control_variate": {"gpu_s": t_cv, "max_level_err_cm1": err(M_cv)},
+                      "plain_2^21": {"gpu_s": t_p21, "max_level_err_cm1": err(M_p21)},
+                      "plain_equal_time": {"samples": n_eq, "gpu_s": t_eq, "max_level_err_cm1": err(M_eq)},
+                      "reference": {"samples": 1 << 23, "gpu_s": t_ref, "lowest10_cm1": [float(x) for x in e_ref]}}))
+
+
 def main():
     global SAMPLES
     ap = argparse.ArgumentParser()
@@ -209,13 +283,19 @@ def main():
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--config", default="doubles", choices=["doubles", "triples"],
-                    help="doubles: the benchmark (hexamer, Nb=1225); triples: the TTM3-F triples build")
+    ap.add_argument("--config", default="doubles", choices=["doubles", "triples", "cv"],
+                    help="doubles: the benchmark (hexamer, Nb=1225); triples: the TTM3-F triples build; "
+                         "cv: the learned control variate")
+    ap.add_argument("--cv-epochs", type=int, default=30)
+    ap.add_argument("--no-levels", action="store_true", help="skip the FP64 level check (profiler captures)")
     ap.add_argument("--no-dump", action="store_true", help="triples: skip the sM_*.h5 dumps")
     ap.add_argument("--samples", type=int, default=SAMPLES,
                     help="samples per step (the benchmark is 2^20; smaller only for profiler captures)")
     args = ap.parse_args()
     SAMPLES = args.samples
+    if args.config == "cv":
+        run_cv(args)
+        return
     if args.config == "triples":
         if args.samples == 1 << 20:
             args.samples = 1 << 21
@@ -310,7 +390,7 @@ def main():
             "kernel_ms": {"per_sample": ms[0], "expand": ms[1], "contract": ms[2], "readout": ms[3]},
             "clocks": clk, "status": {"rc": rc, "nonfinite": nonfinite, "not_converged": notconv}}
 
-    if rank == 0 and args.precision != "fp64":
+    if rank == 0 and args.precision != "fp64" and not args.no_levels:
         # quality gate of the metric: the same 2^20 points through the FP64 plain form
         hb.reset()
         hb.accumulate(base, SAMPLES)

@@ -315,6 +315,7 @@ int64_t scp3gpu_sub_basis_size(int nm, int n2, int n3, int level)
 
 int scp3gpu_pes_energy_dev(int pes, int nw, int64_t n, const double* crd_dev, double* E_dev, int device)
 {
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (pes != SCP3GPU_PES_QTIP4PF && pes != SCP3GPU_PES_TTM3F) return fail(SCP3GPU_ERR_ARG, "unknown potential");
     if (nw < 1 || nw > kMaxWaters || n < 0 || (n > 0 && (!crd_dev || !E_dev)))
         return fail(SCP3GPU_ERR_ARG, "pes_energy: bad nw, n or pointer");
@@ -335,6 +336,7 @@ int scp3gpu_pes_energy_dev(int pes, int nw, int64_t n, const double* crd_dev, do
 
 int scp3gpu_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters)
 {
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (pes != SCP3GPU_PES_QTIP4PF && pes != SCP3GPU_PES_TTM3F) return fail(SCP3GPU_ERR_ARG, "unknown potential");
     if (nw < 1 || nw > kMaxWaters || n < 0 || (n > 0 && (!crd || !E)))
         return fail(SCP3GPU_ERR_ARG, "pes_energy: bad nw, n or pointer");
@@ -372,6 +374,7 @@ int scp3gpu_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E,
 
 int scp3gpu_sobol_std_normal(int dims, int64_t index0, int64_t n, int scramble, uint64_t seed, double* out)
 {
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (dims < 1 || dims > 1111 || index0 < 0 || n < 0 || (n > 0 && !out))
         return fail(SCP3GPU_ERR_ARG, "sobol_std_normal: bad dims, index or pointer");
     if (n == 0) return SCP3GPU_OK;
@@ -428,6 +431,7 @@ int scp3gpu_hbuild_destroy(scp3gpu_hbuild* h)
 
 int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
 {
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (!c || !out) return fail(SCP3GPU_ERR_ARG, "null config or output");
     *out = nullptr;
     if (c->nw < 1 || c->nw > kMaxWaters) return fail(SCP3GPU_ERR_ARG, "nw must be 1..16");
@@ -527,6 +531,7 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
 
 int scp3gpu_hbuild_reset(scp3gpu_hbuild* h)
 {
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (!h) return fail(SCP3GPU_ERR_ARG, "null handle");
     DeviceGuard g(h->dev);
     int rc = drain_prep(h);
@@ -583,6 +588,7 @@ int scp3gpu_hbuild_accumulate_normals(scp3gpu_hbuild* h, const double* normals, 
 
 int scp3gpu_hbuild_add_epot(scp3gpu_hbuild* h, const double* q, const double* V, int64_t n)
 {
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (!h || n < 0 || (n > 0 && (!q || !V))) return fail(SCP3GPU_ERR_ARG, "add_epot: bad arguments");
     DeviceGuard g(h->dev);
     const int nm = h->cfg.nmodes;
@@ -657,6 +663,7 @@ static int build_dense(scp3gpu_hbuild* h, int mode)
 
 int scp3gpu_hbuild_read(scp3gpu_hbuild* h, double* M, int64_t ld, int mode)
 {
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (!h || !M || ld < h->nb || (mode != 0 && mode != 1)) return fail(SCP3GPU_ERR_ARG, "read: bad arguments");
     DeviceGuard g(h->dev);
     int rc = build_dense(h, mode);
@@ -669,6 +676,7 @@ int scp3gpu_hbuild_read(scp3gpu_hbuild* h, double* M, int64_t ld, int mode)
 
 int scp3gpu_hbuild_read_dev(scp3gpu_hbuild* h, double* M_dev, int64_t ld, int mode)
 {
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (!h || !M_dev || ld < h->nb || (mode != 0 && mode != 1)) return fail(SCP3GPU_ERR_ARG, "read_dev: bad arguments");
     DeviceGuard g(h->dev);
     int rc = build_dense(h, mode);
@@ -680,6 +688,7 @@ int scp3gpu_hbuild_read_dev(scp3gpu_hbuild* h, double* M_dev, int64_t ld, int mo
 
 int scp3gpu_hbuild_eigvals(scp3gpu_hbuild* h, int64_t nsub, int k, double* evals)
 {
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (!h || nsub < 1 || nsub > h->nb || k < 1 || k > nsub || !evals)
         return fail(SCP3GPU_ERR_ARG, "eigvals: bad arguments");
     DeviceGuard g(h->dev);
@@ -744,6 +753,7 @@ int scp3gpu_hbuild_set_surrogate(scp3gpu_hbuild* h, scp3gpu_mlp* m, int mode)
 
 int scp3gpu_hbuild_sample(scp3gpu_hbuild* h, int64_t index0, int64_t n, float* q, double* v)
 {
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (!h || index0 < 0 || n < 0 || (n > 0 && (!q || !v))) return fail(SCP3GPU_ERR_ARG, "sample: bad arguments");
     DeviceGuard g(h->dev);
     if (int rc = drain_prep(h)) return rc;

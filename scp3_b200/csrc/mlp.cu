@@ -470,6 +470,7 @@ int scp3gpu_mlp_destroy(scp3gpu_mlp* m)
 
 int scp3gpu_mlp_create(int n_in, int hidden, int max_batch, uint64_t seed, int device, scp3gpu_mlp** out)
 {
+    (void)cudaGetLastError();
     if (!out || n_in < 1 || n_in > 1024 || hidden < 64 || hidden % 64 != 0 || max_batch < 64)
         return fail(SCP3GPU_ERR_ARG, "mlp_create: n_in 1..1024, hidden a multiple of 64, max_batch >= 64");
     *out = nullptr;
@@ -496,8 +497,11 @@ int scp3gpu_mlp_create(int n_in, int hidden, int max_batch, uint64_t seed, int d
         const double a = std::sqrt(6.0 / (fi + fo));
         std::vector<float> w((size_t)fi * fo), b(fo, 0.0f);
         for (float& x : w) x = (float)(a * (2.0 * ((sm64(st) >> 11) * 0x1p-53) - 1.0));
-        cudaMemcpy(m->net.w[l], w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice);
-        cudaMemcpy(m->net.b[l], b.data(), sizeof(float) * b.size(), cudaMemcpyHostToDevice);
+        if (cudaMemcpy(m->net.w[l], w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(m->net.b[l], b.data(), sizeof(float) * b.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            scp3gpu_mlp_destroy(m);
+            return fail(SCP3GPU_ERR_CUDA, "mlp init copy failed");
+        }
     }
     if ((rc = m->net.sync_bf16(m->s)) || cudaStreamSynchronize(m->s) != cudaSuccess) {
         scp3gpu_mlp_destroy(m);
@@ -532,6 +536,7 @@ int scp3gpu_mlp_get_params(scp3gpu_mlp* m, float* p, int64_t n)
 
 int scp3gpu_mlp_set_params(scp3gpu_mlp* m, const float* p, int64_t n)
 {
+    (void)cudaGetLastError();
     if (!m || !p || n != scp3gpu_mlp_num_params(m)) return fail(SCP3GPU_ERR_ARG, "mlp_set_params: bad size");
     Dev g(m->dev);
     SCP3_CUDA(cudaStreamSynchronize(m->s));
@@ -550,6 +555,7 @@ int scp3gpu_mlp_set_params(scp3gpu_mlp* m, const float* p, int64_t n)
 
 int scp3gpu_mlp_forward(scp3gpu_mlp* m, const float* q, int64_t n, float* y)
 {
+    (void)cudaGetLastError();
     if (!m || n < 0 || (n > 0 && (!q || !y))) return fail(SCP3GPU_ERR_ARG, "mlp_forward: bad arguments");
     Dev g(m->dev);
     const int nin = m->net.n_in, B = m->net.max_batch;
@@ -566,6 +572,7 @@ int scp3gpu_mlp_forward(scp3gpu_mlp* m, const float* q, int64_t n, float* y)
 
 int scp3gpu_mlp_grad(scp3gpu_mlp* m, const float* q, const float* t, int n, float* loss, float* grad)
 {
+    (void)cudaGetLastError();
     if (!m || !q || !t || n < 64 || n % 64 != 0 || n > m->net.max_batch)
         return fail(SCP3GPU_ERR_ARG, "mlp_grad: n must be a multiple of 64 within the batch size");
     Dev g(m->dev);
@@ -592,6 +599,7 @@ int scp3gpu_mlp_grad(scp3gpu_mlp* m, const float* q, const float* t, int n, floa
 int scp3gpu_mlp_train(scp3gpu_mlp* m, const float* q, const float* t, int64_t n, int epochs, int batch, float lr,
                       uint64_t seed, float* final_loss)
 {
+    (void)cudaGetLastError();
     if (!m || !q || !t || n < batch || batch < 64 || batch % 64 != 0 || batch > m->net.max_batch || epochs < 1)
         return fail(SCP3GPU_ERR_ARG, "mlp_train: bad sizes");
     Dev g(m->dev);
@@ -604,8 +612,11 @@ int scp3gpu_mlp_train(scp3gpu_mlp* m, const float* q, const float* t, int64_t n,
         cudaFree(qd), cudaFree(td), cudaFree(idx);
         return fail(SCP3GPU_ERR_NOMEM, "mlp_train: data allocation failed");
     }
-    cudaMemcpyAsync(qd, q, sizeof(float) * (size_t)n * nin, cudaMemcpyHostToDevice, m->s);
-    cudaMemcpyAsync(td, t, sizeof(float) * n, cudaMemcpyHostToDevice, m->s);
+    if (cudaMemcpyAsync(qd, q, sizeof(float) * (size_t)n * nin, cudaMemcpyHostToDevice, m->s) != cudaSuccess ||
+        cudaMemcpyAsync(td, t, sizeof(float) * n, cudaMemcpyHostToDevice, m->s) != cudaSuccess) {
+        cudaFree(qd), cudaFree(td), cudaFree(idx);
+        return fail(SCP3GPU_ERR_CUDA, "mlp_train: data copy failed");
+    }
     std::vector<int> perm(n);
     for (int64_t i = 0; i < n; i++) perm[i] = (int)i;
     uint64_t st = seed;
@@ -614,7 +625,8 @@ int scp3gpu_mlp_train(scp3gpu_mlp* m, const float* q, const float* t, int64_t n,
     float loss = 0.0f;
     for (int e = 0; e < epochs && !rc; e++) {
         for (int64_t i = n - 1; i > 0; i--) std::swap(perm[i], perm[sm64(st) % (uint64_t)(i + 1)]);
-        cudaMemcpyAsync(idx, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, m->s);
+        if (cudaMemcpyAsync(idx, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, m->s) != cudaSuccess)
+            rc = fail(SCP3GPU_ERR_CUDA, "mlp_train: permutation copy failed");
         for (int64_t bi = 0; bi < nbatch && !rc; bi++, k++) {
             gather_rows<<<(unsigned)((batch * nin + 255) / 256), 256, 0, m->s>>>(qd, idx + bi * batch, batch, nin, m->qbuf);
             gather_rows<<<(unsigned)((batch + 255) / 256), 256, 0, m->s>>>(td, idx + bi * batch, batch, 1, m->tbuf);

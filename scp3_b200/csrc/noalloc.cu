@@ -80,6 +80,7 @@ using namespace scp3;
 extern "C" int scp3gpu_add_epot_static(int nmodes, int n2, int n3, const double* q_dev, const double* V_dev, int64_t n,
                                        double* M_dev, int64_t ld, void* stream)
 {
+    (void)cudaGetLastError();
     const int64_t nb64 = scp3gpu_basis_size(nmodes, n2, n3);
     if (nb64 < 0 || nmodes < 1 || nmodes > kMaxModes) return fail(SCP3GPU_ERR_ARG, "add_epot_static: bad mode counts");
     if (n < 0 || (n > 0 && (!q_dev || !V_dev)) || !M_dev || ld < nb64)
