@@ -273,6 +273,99 @@ def run_cv(args):
                       "reference": {"samples": 1 << 23, "gpu_s": t_ref, "lowest10_cm1": [float(x) for x in e_ref]}}))
 
 
+def run_batch(args):
+    """The batched build: 32 qTIP4P/f clusters of 2..8 waters (doubles bases of
+    91..946 functions, scp3_b200.inputs.batch_clusters), 2^18 scrambled points
+    per cluster, built in one batch (one CUDA graph replay per step, autotuned
+    contraction work shape) against 32 sequential single builds of the same
+    precision and 32 sequential plain FP64 builds.  Levels of every cluster
+    against its FP64 build.  One JSON line; not the benchmark's default."""
+    import torch
+    import scp3_b200
+    from scp3_b200 import inputs
+    torch.cuda.set_device(0)
+    n = args.samples if args.samples != 1 << 20 else 1 << 18
+    cl = inputs.batch_clusters()
+    for c in cl:
+        c["scramble_seed"] = SCRAMBLE_SEED
+    spec = [{k: v for k, v in c.items() if k != "name"} for c in cl]
+    autocm = scp3_b200.constants.autocm
+    t0 = time.perf_counter()
+    b = scp3_b200.Batch(spec, precision=args.precision)
+    t_create = time.perf_counter() - t0
+    nsplit, ctas, chunk, tuned_ms = b.shape()
+
+    def timed_batch(bb, steps, warmup):
+        st = torch.cuda.ExternalStream(bb.stream)
+        for k in range(warmup):
+            bb.reset()
+            bb.accumulate(k * n, n)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = []
+        for k in range(steps):
+            bb.reset()
+            e0.record(st)
+            bb.accumulate(0, n)
+            e1.record(st)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    ms_graph = timed_batch(b, args.steps, args.warmup)
+    bd = scp3_b200.Batch(spec, precision=args.precision, graph=False)
+    ms_direct = timed_batch(bd, args.steps, 1)
+    bd.close()
+
+    def sequential(prec):
+        hbs = [scp3_b200.HBuild(c["nw"], c["x0"], c["MUa"], c["omega"], modes=c["modes"], n2=c["n2"], n3=0,
+                                precision=prec, scramble_seed=SCRAMBLE_SEED) for c in spec]
+        for hb in hbs:             # warm-up
+            hb.accumulate(0, 4096)
+        torch.cuda.synchronize()
+        for hb in hbs:
+            hb.reset()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for hb in hbs:
+            hb.accumulate(0, n)
+        torch.cuda.synchronize()
+        return hbs, 1e3 * (time.perf_counter() - t0)
+
+    seq, ms_seq = sequential(args.precision)
+    seq64, ms_seq64 = sequential("fp64")
+    # accuracy: the batch against the same-precision single builds (same kernels) and FP64 levels
+    b.reset()
+    b.accumulate(0, n)
+    worst_same, worst_lvl, per = 0.0, 0.0, []
+    for i, c in enumerate(cl):
+        M = b.read(i, 0)
+        R = seq[i].read(0)
+        worst_same = max(worst_same, float(np.abs(M - R).max() / np.abs(R).max()))
+        e_b = np.linalg.eigvalsh(b.read(i, 1))[:10] * autocm
+        e_64 = np.linalg.eigvalsh(seq64[i].read(1))[:10] * autocm
+        err = float(np.abs(e_b - e_64).max())
+        worst_lvl = max(worst_lvl, err)
+        per.append({"name": c["name"], "nw": c["nw"], "nmodes": int(c["modes"].size), "nb": b.nb[i],
+                    "max_level_err_cm1": err})
+    for hb in seq + seq64:
+        hb.close()
+    total = len(cl) * n
+    print(json.dumps({
+        "config": {"workload": "32 qTIP4P/f clusters, 2..8 waters, 12..42 modes, doubles bases 91..946, "
+                               "2^18 scrambled Sobol points per cluster", "precision": args.precision,
+                   "clusters": len(cl), "samples_per_cluster": n, "basis_sizes": b.nb},
+        "metric": "cluster-samples/s", "unit": "samples/s",
+        "batch_graph": {"ms": ms_graph, "value": total / (ms_graph * 1e-3)},
+        "batch_direct": {"ms": ms_direct, "value": total / (ms_direct * 1e-3)},
+        "sequential_same_precision": {"ms": ms_seq, "value": total / (ms_seq * 1e-3)},
+        "sequential_fp64": {"ms": ms_seq64, "value": total / (ms_seq64 * 1e-3)},
+        "speedup_vs_sequential": ms_seq / ms_graph, "speedup_vs_sequential_fp64": ms_seq64 / ms_graph,
+        "work_shape": {"nsplit": nsplit, "ctas": ctas, "samples_per_pass": chunk, "tuned_contract_ms": tuned_ms,
+                       "create_s": t_create},
+        "max_rel_diff_vs_single_builds": worst_same, "max_level_err_cm1_vs_fp64": worst_lvl, "clusters": per}))
+
+
 def main():
     global SAMPLES
     ap = argparse.ArgumentParser()
@@ -280,12 +373,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16x3"])
+    ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16x3", "f16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--config", default="doubles", choices=["doubles", "triples", "cv"],
+    ap.add_argument("--config", default="doubles", choices=["doubles", "triples", "cv", "batch"],
                     help="doubles: the benchmark (hexamer, Nb=1225); triples: the TTM3-F triples build; "
-                         "cv: the learned control variate")
+                         "cv: the learned control variate; batch: 32 clusters in one batched build")
     ap.add_argument("--cv-epochs", type=int, default=30)
     ap.add_argument("--no-levels", action="store_true", help="skip the FP64 level check (profiler captures)")
     ap.add_argument("--no-dump", action="store_true", help="triples: skip the sM_*.h5 dumps")
@@ -295,6 +388,9 @@ def main():
     SAMPLES = args.samples
     if args.config == "cv":
         run_cv(args)
+        return
+    if args.config == "batch":
+        run_batch(args)
         return
     if args.config == "triples":
         if args.samples == 1 << 20:

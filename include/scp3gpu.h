@@ -157,6 +157,37 @@ int scp3gpu_hbuild_eigvals(scp3gpu_hbuild* h, int64_t nsub, int k, double* evals
  * V, TTM3-F samples that hit the sweep cap. */
 int scp3gpu_hbuild_status(scp3gpu_hbuild* h, int64_t* nonfinite, int64_t* not_converged);
 
+/* ------------------------------------------------------------------ batch
+ * Several clusters of uneven size and basis built together (no counterpart in
+ * the reference, which builds one cluster per SCP3 run, SCP3.cpp:154-272).
+ * Every cluster has its own config (geometry, modes, N2/N3, Sobol seed); all
+ * share one potential, one split precision (FP64 is rejected with
+ * SCP3GPU_ERR_UNSUPPORTED) and one device.  Each pass runs one launch per
+ * stage for all clusters; an accumulate call is one CUDA graph replay.  At
+ * creation the contraction's work shape is chosen by timing (unless
+ * SCP3GPU_BATCH_NO_AUTOTUNE).  Every cluster sees the same Sobol index range,
+ * as separate scp3gpu_hbuild handles given the same calls would. */
+typedef struct scp3gpu_batch scp3gpu_batch;
+#define SCP3GPU_BATCH_NO_GRAPH 1    /* launch the passes directly instead of replaying a graph */
+#define SCP3GPU_BATCH_NO_AUTOTUNE 2 /* keep the default work shape                          */
+/* chunk: samples per pass (multiple of 4096; 0 = sized for ~3 GB of operand per pass buffer) */
+int scp3gpu_batch_create(const scp3gpu_config* cfgs, int ncl, int64_t chunk, int flags, scp3gpu_batch** out);
+int scp3gpu_batch_destroy(scp3gpu_batch* b);
+int scp3gpu_batch_reset(scp3gpu_batch* b);
+int scp3gpu_batch_size(const scp3gpu_batch* b);
+int64_t scp3gpu_batch_basis_size(const scp3gpu_batch* b, int cluster);
+int64_t scp3gpu_batch_sample_count(const scp3gpu_batch* b);
+void* scp3gpu_batch_stream(const scp3gpu_batch* b);
+/* the chosen work shape: sample ranges per tile and pass, CTAs of the
+ * contraction launch (0 = one per work unit), samples per pass, and the timed
+ * contraction of one pass in ms (0 without autotuning); pointers may be NULL */
+int scp3gpu_batch_shape(const scp3gpu_batch* b, int* nsplit, int* ctas, int64_t* chunk, double* ms);
+/* Sobol points index0 .. index0+n-1 for every cluster (asynchronous) */
+int scp3gpu_batch_accumulate(scp3gpu_batch* b, int64_t index0, int64_t n);
+/* as scp3gpu_hbuild_read for one cluster */
+int scp3gpu_batch_read(scp3gpu_batch* b, int cluster, double* M, int64_t ld, int mode);
+int scp3gpu_batch_status(scp3gpu_batch* b, int cluster, int64_t* nonfinite, int64_t* not_converged);
+
 /* addEpot of the -G path without any device allocation, for callers that
  * cannot call cudaMalloc (a host framework that owns all device memory and hands
  * out only its own buffers, a locked-down allocator, an allocation-free hot

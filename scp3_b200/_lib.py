@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "libscp3gpu.so")
 OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_NOT_CONVERGED, ERR_NONFINITE, ERR_TIMEOUT, ERR_UNSUPPORTED = range(8)
 PREC_FP64, PREC_BF16X3, PREC_BF16X3_PES64, PREC_F16X3, PREC_F16X3_PES64 = 0, 1, 2, 3, 4
 SOBOL_REFERENCE, SOBOL_SCRAMBLED = 0, 1
+BATCH_NO_GRAPH, BATCH_NO_AUTOTUNE = 1, 2
 
 # every symbol include/scp3gpu.h declares (checked by the CPU tests)
 EXPORTS = [
@@ -25,6 +26,9 @@ EXPORTS = [
     "scp3gpu_mlp_create", "scp3gpu_mlp_destroy", "scp3gpu_mlp_num_params", "scp3gpu_mlp_get_params",
     "scp3gpu_mlp_set_params", "scp3gpu_mlp_set_output", "scp3gpu_mlp_forward", "scp3gpu_mlp_grad", "scp3gpu_mlp_train",
     "scp3gpu_hbuild_set_surrogate", "scp3gpu_hbuild_sample",
+    "scp3gpu_batch_create", "scp3gpu_batch_destroy", "scp3gpu_batch_reset", "scp3gpu_batch_size",
+    "scp3gpu_batch_basis_size", "scp3gpu_batch_sample_count", "scp3gpu_batch_stream", "scp3gpu_batch_shape",
+    "scp3gpu_batch_accumulate", "scp3gpu_batch_read", "scp3gpu_batch_status",
 ]
 
 
@@ -93,6 +97,21 @@ def lib():
     L.scp3gpu_add_epot_static.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, i64, vp, i64, vp]
     L.scp3gpu_save_h5.argtypes = [ctypes.c_char_p, dp, i64, i64]
     L.scp3gpu_hbuild_status.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64)]
+    L.scp3gpu_batch_create.argtypes = [ctypes.POINTER(Config), ctypes.c_int, i64, ctypes.c_int, ctypes.POINTER(vp)]
+    L.scp3gpu_batch_destroy.argtypes = [vp]
+    L.scp3gpu_batch_reset.argtypes = [vp]
+    L.scp3gpu_batch_size.argtypes = [vp]
+    L.scp3gpu_batch_basis_size.restype = i64
+    L.scp3gpu_batch_basis_size.argtypes = [vp, ctypes.c_int]
+    L.scp3gpu_batch_sample_count.restype = i64
+    L.scp3gpu_batch_sample_count.argtypes = [vp]
+    L.scp3gpu_batch_stream.restype = vp
+    L.scp3gpu_batch_stream.argtypes = [vp]
+    L.scp3gpu_batch_shape.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(i64), dp]
+    L.scp3gpu_batch_accumulate.argtypes = [vp, i64, i64]
+    L.scp3gpu_batch_read.argtypes = [vp, ctypes.c_int, dp, i64, ctypes.c_int]
+    L.scp3gpu_batch_status.argtypes = [vp, ctypes.c_int, ctypes.POINTER(i64), ctypes.POINTER(i64)]
     _lib = L
     return L
 

@@ -90,32 +90,40 @@ def std_normal(dims, seed):
     return u
 
 
+PRECISIONS = {"fp64": _lib.PREC_FP64, "bf16x3": _lib.PREC_BF16X3, "bf16x3_pes64": _lib.PREC_BF16X3_PES64,
+              "f16x3": _lib.PREC_F16X3, "f16x3_pes64": _lib.PREC_F16X3_PES64}
+
+
+def _fill_config(obj, nw, x0, MUa, omega, modes, n2, n3, pes, precision, scramble_seed, chunk, device):
+    """Fill obj._cfg (a Config) and keep the arrays it points to alive on obj."""
+    obj.x0 = np.ascontiguousarray(x0, dtype=np.float64)
+    obj.MUa = np.asfortranarray(MUa, dtype=np.float64)
+    obj.omega = np.ascontiguousarray(omega, dtype=np.float64)
+    nm0 = obj.omega.size
+    obj.modes = np.arange(nm0, dtype=np.int32) if modes is None else np.ascontiguousarray(modes, dtype=np.int32)
+    n2 = obj.modes.size if n2 is None else n2      # SCP3.cpp:305
+    obj.n2, obj.n3 = n2, n3
+    cfg = _lib.Config()
+    cfg.nw, cfg.nmodes0 = nw, nm0
+    cfg.x0, cfg.MUa, cfg.omega = _p(obj.x0), obj.MUa.ctypes.data_as(_dp), _p(obj.omega)
+    cfg.nmodes = obj.modes.size
+    cfg.modes = obj.modes.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    cfg.n2, cfg.n3 = n2, n3
+    cfg.pes = C.PES_IDS[pes] if isinstance(pes, str) else int(pes)
+    cfg.precision = PRECISIONS[precision]
+    cfg.scramble = _lib.SOBOL_SCRAMBLED if scramble_seed is not None else _lib.SOBOL_REFERENCE
+    cfg.scramble_seed = scramble_seed or 0
+    cfg.chunk, cfg.device = chunk, device
+    obj._cfg = cfg
+
+
 class HBuild:
     """One device-side Hamiltonian build: ScaledMatrixElements + the SCP3_a loop."""
 
     def __init__(self, nw, x0, MUa, omega, modes=None, n2=None, n3=0, pes="qtip4pf", precision="fp64",
                  scramble_seed=None, chunk=0, device=0):
-        self.x0 = np.ascontiguousarray(x0, dtype=np.float64)
-        self.MUa = np.asfortranarray(MUa, dtype=np.float64)
-        self.omega = np.ascontiguousarray(omega, dtype=np.float64)
-        nm0 = self.omega.size
-        self.modes = np.arange(nm0, dtype=np.int32) if modes is None else np.ascontiguousarray(modes, dtype=np.int32)
-        n2 = self.modes.size if n2 is None else n2      # SCP3.cpp:305
-        self.n2, self.n3 = n2, n3
-        cfg = _lib.Config()
-        cfg.nw, cfg.nmodes0 = nw, nm0
-        cfg.x0, cfg.MUa, cfg.omega = _p(self.x0), self.MUa.ctypes.data_as(_dp), _p(self.omega)
-        cfg.nmodes = self.modes.size
-        cfg.modes = self.modes.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
-        cfg.n2, cfg.n3 = n2, n3
-        cfg.pes = C.PES_IDS[pes] if isinstance(pes, str) else int(pes)
-        cfg.precision = {"fp64": _lib.PREC_FP64, "bf16x3": _lib.PREC_BF16X3,
-                         "bf16x3_pes64": _lib.PREC_BF16X3_PES64, "f16x3": _lib.PREC_F16X3,
-                         "f16x3_pes64": _lib.PREC_F16X3_PES64}[precision]
-        cfg.scramble = _lib.SOBOL_SCRAMBLED if scramble_seed is not None else _lib.SOBOL_REFERENCE
-        cfg.scramble_seed = scramble_seed or 0
-        cfg.chunk, cfg.device = chunk, device
-        self._cfg = cfg
+        _fill_config(self, nw, x0, MUa, omega, modes, n2, n3, pes, precision, scramble_seed, chunk, device)
+        cfg = self._cfg
         h = ctypes.c_void_p()
         _lib.check(_lib.lib().scp3gpu_hbuild_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -235,3 +243,75 @@ class ScaledMatrixElements:
               for j in range(l + 1, self.Nmodes3)]
         M[np.diag_indices(len(d))] += np.array(d)
         return M
+
+
+class _ClusterCfg:
+    pass
+
+
+class Batch:
+    """Several clusters built together (scp3gpu_batch_*): one launch per stage
+    for all clusters, each accumulate one CUDA graph replay.
+
+    clusters: sequence of dicts with keys nw, x0, MUa, omega and optionally
+    modes, n2, n3, scramble_seed (default: the batch's)."""
+
+    def __init__(self, clusters, pes="qtip4pf", precision="bf16x3", scramble_seed=None, chunk=0, graph=True,
+                 autotune=True, device=0):
+        self._keep = []
+        arr = (_lib.Config * len(clusters))()
+        for i, c in enumerate(clusters):
+            k = _ClusterCfg()
+            _fill_config(k, c["nw"], c["x0"], c["MUa"], c["omega"], c.get("modes"), c.get("n2"), c.get("n3", 0),
+                         pes, precision, c.get("scramble_seed", scramble_seed), 0, device)
+            self._keep.append(k)
+            arr[i] = k._cfg
+        flags = (0 if graph else _lib.BATCH_NO_GRAPH) | (0 if autotune else _lib.BATCH_NO_AUTOTUNE)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().scp3gpu_batch_create(arr, len(clusters), chunk, flags, ctypes.byref(h)))
+        self._h = h
+        self.ncl = len(clusters)
+        self.nb = [int(_lib.lib().scp3gpu_batch_basis_size(h, i)) for i in range(self.ncl)]
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().scp3gpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return _lib.lib().scp3gpu_batch_stream(self._h)
+
+    def shape(self):
+        """(nsplit, ctas, samples per pass, timed contraction ms) of the chosen work shape."""
+        ns, ct, ch, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64(), ctypes.c_double()
+        _lib.check(_lib.lib().scp3gpu_batch_shape(self._h, ctypes.byref(ns), ctypes.byref(ct), ctypes.byref(ch),
+                                                  ctypes.byref(ms)))
+        return ns.value, ct.value, ch.value, ms.value
+
+    def reset(self):
+        _lib.check(_lib.lib().scp3gpu_batch_reset(self._h))
+
+    def accumulate(self, index0, n):
+        _lib.check(_lib.lib().scp3gpu_batch_accumulate(self._h, index0, n))
+
+    def sample_count(self):
+        return int(_lib.lib().scp3gpu_batch_sample_count(self._h))
+
+    def read(self, cluster, mode=0):
+        nb = self.nb[cluster]
+        M = np.zeros((nb, nb), order="F")
+        _lib.check(_lib.lib().scp3gpu_batch_read(self._h, cluster, M.ctypes.data_as(_dp), nb, mode))
+        return M
+
+    def status(self, cluster):
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        rc = _lib.lib().scp3gpu_batch_status(self._h, cluster, ctypes.byref(a), ctypes.byref(b))
+        return rc, a.value, b.value

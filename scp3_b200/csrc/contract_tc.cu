@@ -37,6 +37,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 
 #include "common.cuh"
@@ -174,11 +175,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
     for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[j]);
 }
 
-// grid: (ntiles, nsplit).  Split s takes flush blocks [s*nflush/nsplit, (s+1)*nflush/nsplit).
+// Work units: unit u = split * nitems + item takes work item `item` over flush
+// blocks [split*nflush/nsplit, (split+1)*nflush/nsplit).  CTA b runs units b,
+// b + gridDim.x, ...: with one CTA per unit this is the plain launch, with fewer
+// CTAs (one per SM) it is persistent, and the loads and MMAs of a CTA's next
+// unit overlap the FP64 write-back of the previous one.  Pipeline counters
+// (stage, phase, accumulator use) run on across units.
 __global__ void __launch_bounds__(kThreads, 1)
     contract_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
-                           const int2* __restrict__ tiles, const int* __restrict__ neg_group, int nflush, int ntiles,
-                           int products, int f16, double* __restrict__ partial, int* __restrict__ err_flag)
+                           const WorkItem* __restrict__ items, const int* __restrict__ neg_group, int nflush,
+                           int nitems, int nsplit, int products, int f16, double* __restrict__ partial,
+                           int* __restrict__ err_flag)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -192,10 +199,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int2 tt = tiles[blockIdx.x];
-    const bool diag = tt.x == tt.y;
-    const int split = blockIdx.y, nsplit = gridDim.y;
-    const int f0 = (int)((int64_t)split * nflush / nsplit), f1 = (int)((int64_t)(split + 1) * nflush / nsplit);
+    const int nunits = nitems * nsplit;
+    auto flush_range = [&](int split, int& f0, int& f1) {
+        f0 = (int)((int64_t)split * nflush / nsplit);
+        f1 = (int)((int64_t)(split + 1) * nflush / nsplit);
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; s++) {
@@ -221,28 +229,38 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     if (warp == 0) {
         if (lane == 0) {
-            const uint32_t bytes = diag ? 2 * kTileBytes : 4 * kTileBytes;
             int stage = 0;
             uint32_t phase = 0;
             int issued[kStages] = {0, 0, 0};
             uint32_t issued_phase[kStages] = {0, 0, 0};
-            for (int f = f0; f < f1 && !*abort; f++) {
-                for (int kb = 0; kb < kKBlocks; kb++) {
-                    if (!mbar_wait(empty + stage, phase ^ 1, abort)) break;
-                    uint8_t* st = smem + stage * kStageBytes;
-                    mbar_expect_tx(full + stage, bytes);
-                    const int x = f * kSlotsPerFlush + kb * kBK;
-                    tma_load_2d(&map_hi, full + stage, st, x, tt.x * kTile);
-                    tma_load_2d(&map_lo, full + stage, st + kTileBytes, x, tt.x * kTile);
-                    if (!diag) {
-                        tma_load_2d(&map_hi, full + stage, st + 2 * kTileBytes, x, tt.y * kTile);
-                        tma_load_2d(&map_lo, full + stage, st + 3 * kTileBytes, x, tt.y * kTile);
-                    }
-                    issued[stage] = 1;
-                    issued_phase[stage] = phase;
-                    if (++stage == kStages) {
-                        stage = 0;
-                        phase ^= 1;
+            bool ok = true;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                const WorkItem wi = items[u % nitems];
+                const bool diag = wi.arow == wi.brow;
+                const uint32_t bytes = diag ? 2 * kTileBytes : 4 * kTileBytes;
+                int f0, f1;
+                flush_range(u / nitems, f0, f1);
+                for (int f = f0; f < f1 && ok; f++) {
+                    for (int kb = 0; kb < kKBlocks; kb++) {
+                        if (!mbar_wait(empty + stage, phase ^ 1, abort)) {
+                            ok = false;
+                            break;
+                        }
+                        uint8_t* st = smem + stage * kStageBytes;
+                        mbar_expect_tx(full + stage, bytes);
+                        const int x = f * kSlotsPerFlush + kb * kBK;
+                        tma_load_2d(&map_hi, full + stage, st, x, wi.arow);
+                        tma_load_2d(&map_lo, full + stage, st + kTileBytes, x, wi.arow);
+                        if (!diag) {
+                            tma_load_2d(&map_hi, full + stage, st + 2 * kTileBytes, x, wi.brow);
+                            tma_load_2d(&map_lo, full + stage, st + 3 * kTileBytes, x, wi.brow);
+                        }
+                        issued[stage] = 1;
+                        issued_phase[stage] = phase;
+                        if (++stage == kStages) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
                     }
                 }
             }
@@ -259,45 +277,52 @@ __global__ void __launch_bounds__(kThreads, 1)
             int stage = 0, use = 0;
             uint32_t phase = 0;
             bool ok = true;
-            for (int f = f0; f < f1 && ok && !*abort; f++) {
-                const int neg0 = neg_group[f];
-                for (int seg = 0; seg < kSegments && ok; seg++, use++) {
-                    const int a = use & 1;
-                    if (!mbar_wait(acc_empty + a, ((use >> 1) & 1) ^ 1, abort)) {
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint32_t dhh = tmem + (uint32_t)(a * 2 * kTile), dx = dhh + kTile;
-                    const int kb1 = min(kKBlocks, (seg + 1) * kDrainKB);
-                    for (int kb = seg * kDrainKB; kb < kb1; kb++) {
-                        if (!mbar_wait(full + stage, phase, abort)) {
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                const WorkItem wi = items[u % nitems];
+                const bool diag = wi.arow == wi.brow;
+                int f0, f1;
+                flush_range(u / nitems, f0, f1);
+                for (int f = f0; f < f1 && ok; f++) {
+                    const int neg0 = neg_group[wi.neg_off + f];
+                    for (int seg = 0; seg < kSegments && ok; seg++, use++) {
+                        const int a = use & 1;
+                        if (!mbar_wait(acc_empty + a, ((use >> 1) & 1) ^ 1, abort)) {
                             ok = false;
                             break;
                         }
                         tc_fence_after();
-                        uint8_t* st = smem + stage * kStageBytes;
-                        const uint64_t ahi = smem_desc(st), alo = smem_desc(st + kTileBytes);
-                        const uint64_t bhi = diag ? ahi : smem_desc(st + 2 * kTileBytes);
-                        const uint64_t blo = diag ? alo : smem_desc(st + 3 * kTileBytes);
+                        const uint32_t dhh = tmem + (uint32_t)(a * 2 * kTile), dx = dhh + kTile;
+                        const int kb1 = min(kKBlocks, (seg + 1) * kDrainKB);
+                        for (int kb = seg * kDrainKB; kb < kb1; kb++) {
+                            if (!mbar_wait(full + stage, phase, abort)) {
+                                ok = false;
+                                break;
+                            }
+                            tc_fence_after();
+                            uint8_t* st = smem + stage * kStageBytes;
+                            const uint64_t ahi = smem_desc(st), alo = smem_desc(st + kTileBytes);
+                            const uint64_t bhi = diag ? ahi : smem_desc(st + 2 * kTileBytes);
+                            const uint64_t blo = diag ? alo : smem_desc(st + 3 * kTileBytes);
 #pragma unroll
-                        for (int kk = 0; kk < kBK / 16; kk++) {
-                            const bool neg = kb * 4 + kk >= neg0;
-                            const uint32_t idesc = f16 ? (neg ? kIdescF16NegA : kIdescF16) : (neg ? kIdescNegA : kIdesc);
-                            const uint64_t adv = (uint64_t)(kk * 2);    // 32 B along K inside the swizzle atom
-                            const uint32_t acc = (kb != seg * kDrainKB) | (kk != 0);
-                            mma_bf16(dhh, ahi + adv, bhi + adv, idesc, acc);
-                            mma_bf16(dx, ahi + adv, blo + adv, idesc, acc);
-                            mma_bf16(dx, alo + adv, bhi + adv, idesc, 1);
-                            if (products == 4) mma_bf16(dx, alo + adv, blo + adv, idesc, 1);
+                            for (int kk = 0; kk < kBK / 16; kk++) {
+                                const bool neg = kb * 4 + kk >= neg0;
+                                const uint32_t idesc =
+                                    f16 ? (neg ? kIdescF16NegA : kIdescF16) : (neg ? kIdescNegA : kIdesc);
+                                const uint64_t adv = (uint64_t)(kk * 2);    // 32 B along K inside the swizzle atom
+                                const uint32_t acc = (kb != seg * kDrainKB) | (kk != 0);
+                                mma_bf16(dhh, ahi + adv, bhi + adv, idesc, acc);
+                                mma_bf16(dx, ahi + adv, blo + adv, idesc, acc);
+                                mma_bf16(dx, alo + adv, bhi + adv, idesc, 1);
+                                if (products == 4) mma_bf16(dx, alo + adv, blo + adv, idesc, 1);
+                            }
+                            mma_commit(empty + stage);      // frees the stage once these MMAs have read it
+                            if (++stage == kStages) {
+                                stage = 0;
+                                phase ^= 1;
+                            }
                         }
-                        mma_commit(empty + stage);      // frees the stage once these MMAs have read it
-                        if (++stage == kStages) {
-                            stage = 0;
-                            phase ^= 1;
-                        }
+                        if (ok) mma_commit(acc_full + a);
                     }
-                    if (ok) mma_commit(acc_full + a);
                 }
             }
             mma_commit(drain);                     // completes when every MMA above has
@@ -308,33 +333,45 @@ __global__ void __launch_bounds__(kThreads, 1)
         // epilogue: warps 2..9; warp w reads TMEM lane quadrant w%4 and column half (w-2)/4
         const int quad = warp & 3, half = (warp - 2) >> 2;
         const int row = quad * 32 + lane;
-        double acc[64];
-#pragma unroll
-        for (int j = 0; j < 64; j++) acc[j] = 0.0;
-        const int nseg = (f1 - f0) * kSegments;
-        for (int use = 0; use < nseg; use++) {
-            const int a = use & 1;
-            if (!mbar_wait(acc_full + a, (use >> 1) & 1, abort)) break;
-            tc_fence_after();
-            const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * 2 * kTile + half * 64);
-#pragma unroll
-            for (int c0 = 0; c0 < 64; c0 += 32) {
-#pragma unroll
-                for (int part = 0; part < 2; part++) {     // hi*hi, then the cross terms
-                    float t[32];
-                    tmem_ld32(base + part * kTile + c0, t);
-#pragma unroll
-                    for (int j = 0; j < 32; j++) acc[c0 + j] += (double)t[j];
-                }
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(acc_empty + a);
-        }
-        double* P = partial + ((size_t)split * ntiles + blockIdx.x) * (kTile * kTile);
         const double unscale = f16 ? kF16Unscale : 1.0;
+        int use = 0;
+        bool ok = true;
+        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+            const WorkItem wi = items[u % nitems];
+            const int split = u / nitems;
+            int f0, f1;
+            flush_range(split, f0, f1);
+            double acc[64];
 #pragma unroll
-        for (int j = 0; j < 64; j++) P[(size_t)(half * 64 + j) * kTile + row] += acc[j] * unscale;
+            for (int j = 0; j < 64; j++) acc[j] = 0.0;
+            const int nseg = (f1 - f0) * kSegments;
+            for (int k = 0; k < nseg; k++, use++) {
+                const int a = use & 1;
+                if (!mbar_wait(acc_full + a, (use >> 1) & 1, abort)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * 2 * kTile + half * 64);
+#pragma unroll
+                for (int c0 = 0; c0 < 64; c0 += 32) {
+#pragma unroll
+                    for (int part = 0; part < 2; part++) {     // hi*hi, then the cross terms
+                        float t[32];
+                        tmem_ld32(base + part * kTile + c0, t);
+#pragma unroll
+                        for (int j = 0; j < 32; j++) acc[c0 + j] += (double)t[j];
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acc_empty + a);
+            }
+            if (!ok) break;
+            double* P = partial + (size_t)split * nitems * (kTile * kTile) + wi.poff;
+#pragma unroll
+            for (int j = 0; j < 64; j++) P[(size_t)(half * 64 + j) * kTile + row] += acc[j] * unscale;
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -349,11 +386,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 // partition of its samples by the sign of V into K slots; writes slot -> sample
 // (-1 = zero padding) and the first negative 16-group of the block.
 __global__ void __launch_bounds__(1024) partition_kernel(const double* __restrict__ v, int* __restrict__ sample_of_slot,
-                                                         int* __restrict__ neg_group)
+                                                         int* __restrict__ neg_group, int64_t v_stride,
+                                                         int64_t slot_stride, int neg_stride)
 {
     static_assert(kFlush == 4096, "four samples per thread");
     __shared__ int wpos[32], tot;
     const int b = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
+    v += blockIdx.y * v_stride;              // cluster blockIdx.y of a batch
+    sample_of_slot += blockIdx.y * slot_stride;
+    neg_group += blockIdx.y * neg_stride;
     const int64_t s0 = (int64_t)b * kFlush + 4 * t;
     int flags = 0, np = 0;
 #pragma unroll
@@ -427,13 +468,19 @@ __device__ __forceinline__ void split4(float4 x, uint2& hi, uint2& lo)
 }
 
 template <bool F16>
-__global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const uint32_t* __restrict__ factors, int nb,
-                                                                    int nb_pad, int nm, const float* __restrict__ q,
-                                                                    const double* __restrict__ v,
-                                                                    const int* __restrict__ sample_of_slot,
-                                                                    int64_t ldk, uint16_t* __restrict__ xhi,
-                                                                    uint16_t* __restrict__ xlo)
+__global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandDesc* __restrict__ descs, int64_t ldk,
+                                                                    uint16_t* __restrict__ xhi_all,
+                                                                    uint16_t* __restrict__ xlo_all)
 {
+    const ExpandDesc dsc = descs[blockIdx.z];        // one cluster of a batch per z
+    if ((int)blockIdx.y * kExpRows >= dsc.nb_pad) return;
+    const uint32_t* __restrict__ factors = dsc.factors;
+    const int nb = dsc.nb, nb_pad = dsc.nb_pad, nm = dsc.nm;
+    const float* __restrict__ q = dsc.q;
+    const double* __restrict__ v = dsc.v;
+    const int* __restrict__ sample_of_slot = dsc.slot_of;
+    uint16_t* __restrict__ xhi = xhi_all + (size_t)dsc.row0 * ldk;
+    uint16_t* __restrict__ xlo = xlo_all + (size_t)dsc.row0 * ldk;
     extern __shared__ __align__(16) float tab[];      // [3nm+1][kExpSlots], then sqrt|V| [kExpSlots]
     float* sv = tab + (size_t)(3 * nm + 1) * kExpSlots;
     const int t = threadIdx.x;
@@ -488,14 +535,14 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const uint32_
 // Dense column-major nb x nb from the tile partials (tile-local column-major).
 __global__ void unpack_tc_kernel(const double* __restrict__ partial, const int* __restrict__ tile_index, int nt,
                                  int ntiles, int nsplit, int nb, double divisor, const double* __restrict__ diag,
-                                 double zpe, double* __restrict__ M, int64_t ld)
+                                 double zpe, double* __restrict__ M, int64_t ld, int64_t item0)
 {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (int64_t)nb * nb) return;
     const int j = (int)(e / nb), i = (int)(e - (int64_t)j * nb);
     const int r = min(i, j), c = max(i, j);
     const int ti = r / kTile, tj = c / kTile;
-    const int t = tile_index[(size_t)ti * nt + tj];
+    const int64_t t = item0 + tile_index[(size_t)ti * nt + tj];
     const size_t off = (size_t)t * kTile * kTile + (size_t)(c - tj * kTile) * kTile + (r - ti * kTile);
     double val = 0.0;
     for (int s = 0; s < nsplit; s++) val += partial[(size_t)s * ntiles * kTile * kTile + off];
@@ -576,14 +623,15 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
     // (row-major order would stream ~150 distinct panels per wave for the
     // triples basis).
     const int G = 12;
-    std::vector<int2> t;
+    std::vector<WorkItem> t;
     std::vector<int> tindex((size_t)p.nt * p.nt, -1);
     for (int bi = 0; bi < p.nt; bi += G)
         for (int bj = bi; bj < p.nt; bj += G)
             for (int i = bi; i < std::min(bi + G, p.nt); i++)
                 for (int j = std::max(i, bj); j < std::min(bj + G, p.nt); j++) {
                     tindex[(size_t)i * p.nt + j] = (int)t.size();
-                    t.push_back(make_int2(i, j));
+                    WorkItem w{i * kTile, j * kTile, 0, 0, (long long)t.size() * kTile * kTile};
+                    t.push_back(w);
                 }
     for (int b = 0; b < 2; b++) {
         SCP3_CUDA(cudaMalloc(&p.xhi[b], sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
@@ -591,11 +639,12 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
         SCP3_CUDA(cudaMalloc(&p.slot_of[b], sizeof(int) * (size_t)p.slots));
         SCP3_CUDA(cudaMalloc(&p.group_meta[b], sizeof(int) * nflush));
     }
-    SCP3_CUDA(cudaMalloc(&p.tiles, sizeof(int2) * t.size()));
-    SCP3_CUDA(cudaMemcpy(p.tiles, t.data(), sizeof(int2) * t.size(), cudaMemcpyHostToDevice));
+    SCP3_CUDA(cudaMalloc(&p.tiles, sizeof(WorkItem) * t.size()));
+    SCP3_CUDA(cudaMemcpy(p.tiles, t.data(), sizeof(WorkItem) * t.size(), cudaMemcpyHostToDevice));
     const std::vector<uint32_t> fac = basis_factor_table(nm_for_factors, n2_for_factors, n3_for_factors);
     SCP3_CUDA(cudaMalloc(&p.factors, sizeof(uint32_t) * fac.size()));
     SCP3_CUDA(cudaMemcpy(p.factors, fac.data(), sizeof(uint32_t) * fac.size(), cudaMemcpyHostToDevice));
+    SCP3_CUDA(cudaMalloc(&p.desc_dev, sizeof(ExpandDesc) * 2));
     SCP3_CUDA(cudaMalloc(&p.tile_index, sizeof(int) * tindex.size()));
     SCP3_CUDA(cudaMemcpy(p.tile_index, tindex.data(), sizeof(int) * tindex.size(), cudaMemcpyHostToDevice));
     SCP3_CUDA(cudaMalloc(&p.partial, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kTile));
@@ -613,7 +662,7 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
 void destroy(Plan& p)
 {
     void* ptrs[] = {p.xhi[0], p.xhi[1], p.xlo[0], p.xlo[1], p.slot_of[0], p.slot_of[1], p.group_meta[0],
-                    p.group_meta[1], p.tiles, p.tile_index, p.factors, p.partial, p.err_flag};
+                    p.group_meta[1], p.tiles, p.tile_index, p.factors, p.partial, p.err_flag, p.desc_dev};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     for (int b = 0; b < 2; b++) {
@@ -636,6 +685,55 @@ int zero(Plan& p, cudaStream_t s)
     return SCP3GPU_OK;
 }
 
+int launch_partition(const double* v, int64_t v_stride, int* slot_of, int64_t slot_stride, int* neg, int neg_stride,
+                     int nflush, int nclusters, cudaStream_t s)
+{
+    partition_kernel<<<dim3(nflush, nclusters), 1024, 0, s>>>(v, slot_of, neg, v_stride, slot_stride, neg_stride);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
+int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t ldk,
+                  uint16_t* xhi, uint16_t* xlo, bool f16, cudaStream_t s)
+{
+    const size_t sm = sizeof(float) * (size_t)(3 * max_nm + 2) * kExpSlots;
+    auto kern = f16 ? expand_split_kernel<true> : expand_split_kernel<false>;
+    if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    dim3 eg((unsigned)(slots / kExpSlots), (unsigned)((max_nb_pad + kExpRows - 1) / kExpRows), (unsigned)nclusters);
+    kern<<<eg, kExpThreads, sm, s>>>(descs_dev, ldk, xhi, xlo);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
+int launch_contract(const void* map_hi, const void* map_lo, const WorkItem* items, int nitems, const int* neg,
+                    int nflush, int nsplit, int products, bool f16, double* partial, int* err_flag, cudaStream_t s,
+                    int max_ctas)
+{
+    if (nitems <= 0 || nsplit <= 0) return SCP3GPU_OK;
+    SCP3_CUDA(cudaFuncSetAttribute(contract_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    const int64_t units = (int64_t)nitems * nsplit;
+    const int grid = (int)(max_ctas > 0 ? std::min<int64_t>(units, max_ctas) : units);
+    contract_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(*static_cast<const CUtensorMap*>(map_hi),
+                                                              *static_cast<const CUtensorMap*>(map_lo), items, neg,
+                                                              nflush, nitems, nsplit, products, (int)f16, partial,
+                                                              err_flag);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
+int launch_unpack(const double* partial, const int* tile_index, int nt, int nitems_total, int nsplit, int64_t item0,
+                  int nb, double divisor, const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s)
+{
+    const int64_t total = (int64_t)nb * nb;
+    unpack_tc_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(partial, tile_index, nt, nitems_total, nsplit, nb,
+                                                                      divisor, diag, zpe, M, ld, item0);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
+int encode_operand_map(void** out, void* base, int64_t slots, int rows) { return encode_map(out, base, slots, rows); }
+void free_operand_map(void* map) { delete static_cast<CUtensorMap*>(map); }
+
 int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v, int64_t n, cudaStream_t s,
             std::vector<cudaEvent_t>* pev, std::vector<int>* pkind)
 {
@@ -644,15 +742,16 @@ int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v,
     const int nflush = (int)(n / kFlush);
     const int64_t slots = (int64_t)nflush * kSlotsPerFlush;
     record(pev, pkind, 1, s);
-    partition_kernel<<<nflush, 1024, 0, s>>>(v, p.slot_of[buf], p.group_meta[buf]);
-    SCP3_CUDA(cudaGetLastError());
-    const size_t sm = sizeof(float) * (size_t)(3 * nm + 2) * kExpSlots;
-    auto kern = p.f16 ? expand_split_kernel<true> : expand_split_kernel<false>;
-    if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    dim3 eg((unsigned)(slots / kExpSlots), (unsigned)((p.nb_pad + kExpRows - 1) / kExpRows));
-    kern<<<eg, kExpThreads, sm, s>>>(p.factors, nb, p.nb_pad, nm, q32, v, p.slot_of[buf], p.slots, p.xhi[buf],
-                                     p.xlo[buf]);
-    SCP3_CUDA(cudaGetLastError());
+    int rc = launch_partition(v, 0, p.slot_of[buf], 0, p.group_meta[buf], 0, nflush, 1, s);
+    if (rc) return rc;
+    const ExpandDesc d{p.factors, nb, p.nb_pad, nm, 0, q32, v, p.slot_of[buf]};
+    if (std::memcmp(&d, &p.desc_host[buf], sizeof(d)) != 0) {
+        // pageable source: the copy has read it when the call returns
+        SCP3_CUDA(cudaMemcpyAsync(p.desc_dev + buf, &d, sizeof(d), cudaMemcpyHostToDevice, s));
+        p.desc_host[buf] = d;
+    }
+    rc = launch_expand(p.desc_dev + buf, 1, p.nb_pad, nm, slots, p.slots, p.xhi[buf], p.xlo[buf], p.f16, s);
+    if (rc) return rc;
     record(pev, pkind, 1, s);
     return SCP3GPU_OK;
 }
@@ -662,12 +761,9 @@ int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_
     const int nflush = (int)(n / kFlush);
     record(pev, pkind, 2, s);
     const int nsplit = p.nsplit < nflush ? p.nsplit : nflush;
-    dim3 grid(p.ntiles, nsplit);
-    contract_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(*static_cast<CUtensorMap*>(p.tmap_hi[buf]),
-                                                              *static_cast<CUtensorMap*>(p.tmap_lo[buf]), p.tiles,
-                                                              p.group_meta[buf], nflush, p.ntiles, p.products,
-                                                              (int)p.f16, p.partial, p.err_flag);
-    SCP3_CUDA(cudaGetLastError());
+    int rc = launch_contract(p.tmap_hi[buf], p.tmap_lo[buf], p.tiles, p.ntiles, p.group_meta[buf], nflush, nsplit,
+                             p.products, p.f16, p.partial, p.err_flag, s);
+    if (rc) return rc;
     record(pev, pkind, 2, s);
     return SCP3GPU_OK;
 }
@@ -687,10 +783,8 @@ int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, doub
     SCP3_CUDA(cudaStreamSynchronize(s));
     if (err) return fail(SCP3GPU_ERR_TIMEOUT, "tensor-core contraction: a bounded pipeline wait expired");
     const int64_t total = (int64_t)nb * nb;
-    unpack_tc_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p.partial, p.tile_index, p.nt, p.ntiles,
-                                                                      p.nsplit, nb, divisor, diag, zpe, M, ld);
-    SCP3_CUDA(cudaGetLastError());
-    return SCP3GPU_OK;
+    (void)total;
+    return launch_unpack(p.partial, p.tile_index, p.nt, p.ntiles, p.nsplit, 0, nb, divisor, diag, zpe, M, ld, s);
 }
 
 }  // namespace tc

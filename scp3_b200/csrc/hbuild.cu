@@ -32,51 +32,6 @@ int cuda_fail(cudaError_t e, const char* what)
     return e == cudaErrorMemoryAllocation ? SCP3GPU_ERR_NOMEM : SCP3GPU_ERR_CUDA;
 }
 
-namespace {
-
-template <typename T>
-int dalloc(T** p, size_t count)
-{
-    *p = nullptr;
-    if (count == 0) return SCP3GPU_OK;
-    SCP3_CUDA(cudaMalloc((void**)p, count * sizeof(T)));
-    return SCP3GPU_OK;
-}
-
-template <typename T>
-int upload(T** p, const T* host, size_t count)
-{
-    int rc = dalloc(p, count);
-    if (rc) return rc;
-    if (count) SCP3_CUDA(cudaMemcpy(*p, host, count * sizeof(T), cudaMemcpyHostToDevice));
-    return SCP3GPU_OK;
-}
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev)
-    {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard()
-    {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
-
-int check_device(int dev)
-{
-    int n = 0;
-    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(SCP3GPU_ERR_UNSUPPORTED, "no CUDA device");
-    if (dev < 0 || dev >= n) return fail(SCP3GPU_ERR_ARG, "device ordinal out of range");
-    int major = 0;
-    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-    if (major != 10) return fail(SCP3GPU_ERR_UNSUPPORTED, "libscp3gpu is built for sm_100a (B200) only");
-    return SCP3GPU_OK;
-}
-
-}  // namespace
 }  // namespace scp3
 
 using namespace scp3;
@@ -629,27 +584,7 @@ static int build_dense(scp3gpu_hbuild* h, int mode)
     if (mode == 1) {
         if (h->count <= 0) return fail(SCP3GPU_ERR_ARG, "read: no samples accumulated");
         if (!h->hodiag) {
-            // addHODiagonal (ScaledMatrixElements.cpp:735-784)
-            const int nm = h->cfg.nmodes, n2 = h->cfg.n2, n3 = h->cfg.n3;
-            const std::vector<double>& w = h->omega_sel;
-            std::vector<double> d;
-            double e0 = 0;
-            for (double x : w) e0 += x;
-            e0 *= 0.5;
-            d.push_back(e0);
-            for (int k = 0; k < nm; k++) d.push_back(e0 + w[k]);
-            for (int k = 0; k < n2; k++) d.push_back(e0 + 2 * w[k]);
-            for (int k = 0; k < n2; k++)
-                for (int l = k + 1; l < n2; l++) d.push_back(e0 + w[k] + w[l]);
-            for (int k = 0; k < n3; k++) d.push_back(e0 + 3.0 * w[k]);
-            for (int k = 0; k < n3; k++)
-                for (int l = k + 1; l < n3; l++) {
-                    d.push_back(e0 + 2.0 * w[k] + w[l]);
-                    d.push_back(e0 + w[k] + 2.0 * w[l]);
-                }
-            for (int k = 0; k < n3; k++)
-                for (int l = k + 1; l < n3; l++)
-                    for (int j = l + 1; j < n3; j++) d.push_back(e0 + w[k] + w[l] + w[j]);
+            const std::vector<double> d = ho_diagonal(h->omega_sel, h->cfg.n2, h->cfg.n3);
             if ((rc = upload(&h->hodiag, d.data(), d.size()))) return rc;
         }
         diag = h->hodiag;

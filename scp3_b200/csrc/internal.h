@@ -23,6 +23,50 @@ int cuda_fail(cudaError_t e, const char* what);
         if (e_ != cudaSuccess) return ::scp3::cuda_fail(e_, __FILE__ ":" SCP3_STR(__LINE__) " " #call); \
     } while (0)
 
+// ---------------------------------------------------------------- device helpers
+template <typename T>
+inline int dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) return SCP3GPU_OK;
+    SCP3_CUDA(cudaMalloc((void**)p, count * sizeof(T)));
+    return SCP3GPU_OK;
+}
+
+template <typename T>
+inline int upload(T** p, const T* host, size_t count)
+{
+    int rc = dalloc(p, count);
+    if (rc) return rc;
+    if (count) SCP3_CUDA(cudaMemcpy(*p, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    return SCP3GPU_OK;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+inline int check_device(int dev)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(SCP3GPU_ERR_UNSUPPORTED, "no CUDA device");
+    if (dev < 0 || dev >= n) return fail(SCP3GPU_ERR_ARG, "device ordinal out of range");
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) return fail(SCP3GPU_ERR_UNSUPPORTED, "libscp3gpu is built for sm_100a (B200) only");
+    return SCP3GPU_OK;
+}
+
+
 constexpr int kLogMax = 62;           // bits of the Sobol state (sobol.cpp:27700)
 constexpr int kMaxModes = 255;        // modes fit the 8-bit fields of a basis descriptor
 constexpr int kMaxWaters = 16;        // per-sample kernels keep one geometry per warp in smem
@@ -48,6 +92,7 @@ std::vector<uint32_t> basis_descriptors(int nm, int n2, int n3);
 
 // The same basis as products of entries of a per-sample Hermite table
 // [1, h1(q_m), h2(q_m), h3(q_m)] (indices a, b, c in 10-bit fields).
+std::vector<double> ho_diagonal(const std::vector<double>& omega_sel, int n2, int n3);
 std::vector<uint32_t> basis_factor_table(int nm, int n2, int n3);
 
 // Pair tasks of the water potentials, in one list per cluster size: type in
@@ -79,6 +124,12 @@ struct SampleArgs {
 };
 // pes: SCP3GPU_PES_*, fp32: run the potential in FP32.
 int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s);
+
+// All clusters of a batch in one launch: cluster c (grid.y) runs args_dev[c]
+// (args_host: a host copy of the same array, for the launch shape), n samples
+// each.
+int launch_samples_batch(int pes, bool fp32, const SampleArgs* args_host, const SampleArgs* args_dev, int ncl,
+                         int64_t n, cudaStream_t s);
 
 int launch_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters,
                       const uint32_t* tasks, int ntasks, cudaStream_t s);

@@ -10,6 +10,7 @@
 #include "pes_ttm3f.cuh"
 #include "ps_coeffs.h"
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 
@@ -62,9 +63,27 @@ __device__ inline double potential(const WarpSlot<T>& w, int nw, const uint32_t*
 constexpr size_t kMuaSmemMax = 64 * 1024;
 
 template <int PES, typename T>
+__device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem);
+
+template <int PES, typename T>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs a)
 {
     extern __shared__ __align__(16) char smem[];
+    samples_body<PES, T>(a, smem);
+}
+
+// Several clusters of a batch: cluster blockIdx.y takes args[blockIdx.y].
+template <int PES, typename T>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_batch_kernel(const SampleArgs* __restrict__ args)
+{
+    extern __shared__ __align__(16) char smem[];
+    const SampleArgs a = args[blockIdx.y];
+    samples_body<PES, T>(a, smem);
+}
+
+template <int PES, typename T>
+__device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
+{
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int nw = a.nw, nm0 = a.nm0, N3 = 9 * nw;
     const size_t mua_b = sizeof(double) * (size_t)N3 * nm0;
@@ -221,7 +240,43 @@ int launch_samples_t(const SampleArgs& a, cudaStream_t s)
     return SCP3GPU_OK;
 }
 
+template <int PES, typename T>
+int launch_samples_batch_t(const SampleArgs* args_host, const SampleArgs* args_dev, int ncl, int64_t n, cudaStream_t s)
+{
+    // Shared memory for the largest cluster: warp slots of the largest (nm0, nw)
+    // plus the largest MUa that a cluster stages (each cluster decides as the
+    // single-cluster kernel does, so its layout fits).
+    int nm0 = 0, nw = 0;
+    size_t mua = 0;
+    for (int c = 0; c < ncl; c++) {
+        nm0 = std::max(nm0, args_host[c].nm0);
+        nw = std::max(nw, args_host[c].nw);
+        const size_t b = sizeof(double) * (size_t)9 * args_host[c].nw * args_host[c].nm0;
+        if (b <= kMuaSmemMax) mua = std::max(mua, (b + 15) / 16 * 16);
+    }
+    const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, nm0, nw) + mua;
+    if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_batch_kernel<PES, T>,
+                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int per = grid_for((n + kRun - 1) / kRun);   // per cluster; the clusters share the SMs
+    samples_batch_kernel<PES, T><<<dim3((unsigned)per, (unsigned)ncl), kWarpsPerBlock * 32, sm, s>>>(args_dev);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
 }  // namespace
+
+int launch_samples_batch(int pes, bool fp32, const SampleArgs* args_host, const SampleArgs* args_dev, int ncl,
+                         int64_t n, cudaStream_t s)
+{
+    if (n <= 0 || ncl <= 0) return SCP3GPU_OK;
+    if (pes == SCP3GPU_PES_QTIP4PF)
+        return fp32 ? launch_samples_batch_t<SCP3GPU_PES_QTIP4PF, float>(args_host, args_dev, ncl, n, s)
+                    : launch_samples_batch_t<SCP3GPU_PES_QTIP4PF, double>(args_host, args_dev, ncl, n, s);
+    if (pes == SCP3GPU_PES_TTM3F)
+        return fp32 ? launch_samples_batch_t<SCP3GPU_PES_TTM3F, float>(args_host, args_dev, ncl, n, s)
+                    : launch_samples_batch_t<SCP3GPU_PES_TTM3F, double>(args_host, args_dev, ncl, n, s);
+    return fail(SCP3GPU_ERR_ARG, "unknown potential id");
+}
 
 int ttm_init_device()
 {

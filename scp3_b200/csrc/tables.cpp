@@ -148,4 +148,30 @@ std::vector<uint32_t> basis_factor_table(int nm, int n2, int n3)
     return d;
 }
 
+// addHODiagonal (ScaledMatrixElements.cpp:735-784): the harmonic energy of
+// every basis function, in basis order, from the selected modes' frequencies.
+std::vector<double> ho_diagonal(const std::vector<double>& w, int n2, int n3)
+{
+    const int nm = (int)w.size();
+    std::vector<double> d;
+    double e0 = 0;
+    for (double x : w) e0 += x;
+    e0 *= 0.5;
+    d.push_back(e0);
+    for (int k = 0; k < nm; k++) d.push_back(e0 + w[k]);
+    for (int k = 0; k < n2; k++) d.push_back(e0 + 2 * w[k]);
+    for (int k = 0; k < n2; k++)
+        for (int l = k + 1; l < n2; l++) d.push_back(e0 + w[k] + w[l]);
+    for (int k = 0; k < n3; k++) d.push_back(e0 + 3.0 * w[k]);
+    for (int k = 0; k < n3; k++)
+        for (int l = k + 1; l < n3; l++) {
+            d.push_back(e0 + 2.0 * w[k] + w[l]);
+            d.push_back(e0 + w[k] + 2.0 * w[l]);
+        }
+    for (int k = 0; k < n3; k++)
+        for (int l = k + 1; l < n3; l++)
+            for (int j = l + 1; j < n3; j++) d.push_back(e0 + w[k] + w[l] + w[j]);
+    return d;
+}
+
 }  // namespace scp3

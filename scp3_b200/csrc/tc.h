@@ -5,6 +5,27 @@
 namespace scp3 {
 namespace tc {
 
+// One CTA's share of the contraction: the A and B row bases (128-row panels of
+// the operand, which may hold several clusters' bases one after another), the
+// offset of its cluster's per-block sign-group table, and the offset of its
+// FP64 partial tile (per sample-range split, after split * nitems tiles).
+struct WorkItem {
+    int arow, brow;     // first operand rows of the tile's A and B panels
+    int neg_off;        // index of the cluster's first entry in the sign-group table
+    int pad;
+    long long poff;     // partial offset in doubles (tile index * 128 * 128)
+};
+
+// Per-cluster inputs of the split-operand expansion.
+struct ExpandDesc {
+    const uint32_t* factors;   // [nb] basis factor table
+    int nb, nb_pad, nm;
+    int row0;                  // first operand row of this cluster
+    const float* q;            // [samples][nm]
+    const double* v;           // [samples]
+    const int* slot_of;        // [slots] K slot -> sample
+};
+
 struct Plan {
     int nb = 0, nb_pad = 0, nm = 0;
     int nt = 0, ntiles = 0;       // 128-row tiles per side, upper tiles
@@ -19,9 +40,11 @@ struct Plan {
     uint16_t* xlo[2] = {nullptr, nullptr};   // [nb_pad][slots] 16-bit: low part
     int* slot_of[2] = {nullptr, nullptr};    // [slots] K slot -> sample (-1: zero padding)
     int* group_meta[2] = {nullptr, nullptr}; // per 4096-sample block: first negative 16-group
-    int2* tiles = nullptr;        // [ntiles] (ti, tj), in launch order
+    WorkItem* tiles = nullptr;    // [ntiles] work items, in launch order
     int* tile_index = nullptr;    // [nt*nt] position of tile (ti, tj) in `tiles`
     uint32_t* factors = nullptr;  // [nb] basis functions as products of Hermite-table entries
+    ExpandDesc* desc_dev = nullptr;   // [2] expansion descriptors of the two pass buffers
+    ExpandDesc desc_host[2] = {};     // what desc_dev holds (uploaded again only when it changes)
     double* partial = nullptr;    // [nsplit][ntiles][128*128] FP64
     void* tmap_hi[2] = {nullptr, nullptr};   // CUtensorMap (host copies) for xhi / xlo
     void* tmap_lo[2] = {nullptr, nullptr};
@@ -47,6 +70,20 @@ int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_
 int accumulate_pass(Plan& p, const uint32_t* desc, int nb, int nm, const float* q32, const double* v, int64_t n,
                     cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind);
 int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s);
+
+// Launchers shared by the single build and the batch (several clusters in one launch).
+int launch_partition(const double* v, int64_t v_stride, int* slot_of, int64_t slot_stride, int* neg, int neg_stride,
+                     int nflush, int nclusters, cudaStream_t s);
+int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t ldk,
+                  uint16_t* xhi, uint16_t* xlo, bool f16, cudaStream_t s);
+// max_ctas > 0: at most that many CTAs, each looping over work units (persistent); 0: one CTA per unit.
+int launch_contract(const void* map_hi, const void* map_lo, const WorkItem* items, int nitems, const int* neg,
+                    int nflush, int nsplit, int products, bool f16, double* partial, int* err_flag, cudaStream_t s,
+                    int max_ctas = 0);
+int launch_unpack(const double* partial, const int* tile_index, int nt, int nitems_total, int nsplit, int64_t item0,
+                  int nb, double divisor, const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s);
+int encode_operand_map(void** out, void* base, int64_t slots, int rows);
+void free_operand_map(void* map);
 
 }  // namespace tc
 }  // namespace scp3

@@ -8,6 +8,9 @@ potentials and cached under scp3_b200/data/.
                   qTIP4P/f: 48 modes
   prism_ttm3f     the same start relaxed on TTM3-F
   cluster_<n>_<seed>  seeded random n-water cluster relaxed on qTIP4P/f
+
+batch_clusters() assembles the batched-build workload from cluster_<n>_<seed>
+inputs.
 """
 import os
 
@@ -60,3 +63,31 @@ def load(name, build_if_missing=True):
     _, mass, x0, H = modes.ohhohh(mass, x0, H)
     omega, MUa, _ = modes.normal_modes(H, mass)
     return x0.size // 9, x0, MUa, omega
+
+
+def batch_clusters(count=32, seed=7, max_modes=42, min_omega_cm1=20.0, build_if_missing=True):
+    """The batched-build workload: `count` clusters, n drawn uniformly from 2..8
+    waters (numpy generator seeded with `seed`), each a seeded random placement
+    relaxed on qTIP4P/f (input cluster_<n>_<s>, s = 100 * i + t); a placement
+    whose relaxed Hessian has a frequency below min_omega_cm1 or an imaginary one
+    (a saddle point or an unconverged relaxation) is replaced by the next t.
+    Active modes: the max_modes highest-frequency modes (every mode up to five
+    waters), N2 = all active modes, no triples -- 12..42 modes and doubles bases
+    of 91..946 functions.  Returns a list of dicts for scp3_b200.Batch (plus
+    'name')."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(2, 9, size=count)
+    out = []
+    for i, n in enumerate(ns):
+        for t in range(100):
+            name = "cluster_%d_%d" % (n, 100 * i + t)
+            nw, x0, MUa, omega = load(name, build_if_missing)
+            if np.all(np.isfinite(omega)) and omega.min() * C.autocm >= min_omega_cm1:
+                break
+        else:
+            raise RuntimeError("no valid placement for cluster %d" % i)
+        nm0 = omega.size
+        nm = min(nm0, max_modes)
+        modes = np.arange(nm0 - nm, nm0, dtype=np.int32)    # normal modes come in ascending frequency
+        out.append(dict(name=name, nw=nw, x0=x0, MUa=MUa, omega=omega, modes=modes, n2=nm, n3=0))
+    return out
