@@ -153,6 +153,14 @@ int scp3gpu_hbuild_read_dev(scp3gpu_hbuild* h, double* M_dev, int64_t ld, int mo
  * singles/doubles readouts of SCP3.cpp:241-247), FP64 on the device. */
 int scp3gpu_hbuild_eigvals(scp3gpu_hbuild* h, int64_t nsub, int k, double* evals);
 
+/* The k lowest eigenvalues (ascending) and, with Z != NULL, their eigenvectors
+ * (columns of Z, leading dimension ldz) of the symmetric n x n host matrix A
+ * (column-major, leading dimension lda), FP64 on the device -- replaces
+ * dsyevr(A, IU = k, &C) of the eigensolver tool (eigensolver.cpp:20-84): the
+ * upper triangle is read unless A(0, n-1) == 0, then the lower one. */
+int scp3gpu_syevr_lowest(const double* A, int64_t n, int64_t lda, int k, double* W, double* Z, int64_t ldz,
+                         int device);
+
 /* Per-sample status counters since create/reset: samples with a non-finite
  * V, TTM3-F samples that hit the sweep cap. */
 int scp3gpu_hbuild_status(scp3gpu_hbuild* h, int64_t* nonfinite, int64_t* not_converged);
@@ -208,6 +216,15 @@ int scp3gpu_add_epot_static(int nmodes, int n2, int n3, const double* q_dev, con
  * (DiskIO.cpp:201-227), which SCP3 calls every 2^17 samples (SCP3.cpp:252-255).
  * Stored contiguous rather than chunked + deflate. */
 int scp3gpu_save_h5(const char* path, const double* M, int64_t n_rows, int64_t n_cols);
+/* As scp3gpu_save_h5 with the storage chosen: deflate = 0..9 writes the
+ * reference's chunked layout (chunks of min(n_cols, ceil(131072 / n_rows))
+ * whole columns, each deflated at that level -- 6 in DiskIO.cpp:214-216,
+ * compressed on all host threads); deflate = -1 writes it contiguous. */
+int scp3gpu_save_h5_layout(const char* path, const double* M, int64_t n_rows, int64_t n_cols, int deflate);
+/* load_hdf5(name, M) (DiskIO.cpp:267-289): dataset "M" (dims {n_cols, n_rows},
+ * float32 or float64, contiguous or chunked with deflate) into column-major M
+ * (leading dimension n_rows).  M == NULL returns the shape only. */
+int scp3gpu_load_h5(const char* path, double* M, int64_t* n_rows, int64_t* n_cols);
 
 /* ------------------------------------------------------------------ surrogate
  * The learned control variate (no counterpart in the reference, which always

@@ -22,7 +22,8 @@ EXPORTS = [
     "scp3gpu_hbuild_destroy", "scp3gpu_hbuild_reset", "scp3gpu_hbuild_basis_size", "scp3gpu_hbuild_stream",
     "scp3gpu_hbuild_accumulate", "scp3gpu_hbuild_accumulate_normals", "scp3gpu_hbuild_add_epot",
     "scp3gpu_hbuild_sample_count", "scp3gpu_hbuild_read", "scp3gpu_hbuild_read_dev", "scp3gpu_hbuild_eigvals", "scp3gpu_hbuild_status",
-    "scp3gpu_hbuild_profile", "scp3gpu_add_epot_static", "scp3gpu_save_h5",
+    "scp3gpu_hbuild_profile", "scp3gpu_add_epot_static", "scp3gpu_save_h5", "scp3gpu_save_h5_layout",
+    "scp3gpu_load_h5", "scp3gpu_syevr_lowest",
     "scp3gpu_mlp_create", "scp3gpu_mlp_destroy", "scp3gpu_mlp_num_params", "scp3gpu_mlp_get_params",
     "scp3gpu_mlp_set_params", "scp3gpu_mlp_set_output", "scp3gpu_mlp_forward", "scp3gpu_mlp_grad", "scp3gpu_mlp_train",
     "scp3gpu_hbuild_set_surrogate", "scp3gpu_hbuild_sample",
@@ -96,6 +97,9 @@ def lib():
     L.scp3gpu_hbuild_profile.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(i64)]
     L.scp3gpu_add_epot_static.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, i64, vp, i64, vp]
     L.scp3gpu_save_h5.argtypes = [ctypes.c_char_p, dp, i64, i64]
+    L.scp3gpu_save_h5_layout.argtypes = [ctypes.c_char_p, dp, i64, i64, ctypes.c_int]
+    L.scp3gpu_syevr_lowest.argtypes = [dp, i64, i64, ctypes.c_int, dp, dp, i64, ctypes.c_int]
+    L.scp3gpu_load_h5.argtypes = [ctypes.c_char_p, dp, ctypes.POINTER(i64), ctypes.POINTER(i64)]
     L.scp3gpu_hbuild_status.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64)]
     L.scp3gpu_batch_create.argtypes = [ctypes.POINTER(Config), ctypes.c_int, i64, ctypes.c_int, ctypes.POINTER(vp)]
     L.scp3gpu_batch_destroy.argtypes = [vp]

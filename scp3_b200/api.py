@@ -245,6 +245,21 @@ class ScaledMatrixElements:
         return M
 
 
+def dsyevr(A, IU=0, vectors=True, device=0):
+    """The lowest IU eigenpairs of the symmetric matrix A on the GPU (FP64), as
+    dsyevr(A, IU, &C) of the eigensolver tool (eigensolver.cpp:20-84): the upper
+    triangle is read unless A[0, n-1] == 0.  IU = 0: all of them.  Returns W, or
+    (W, C) with the eigenvectors as columns of C."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    n = A.shape[0]
+    k = n if IU <= 0 else IU
+    W = np.zeros(k)
+    C = np.zeros((n, k), order="F") if vectors else None
+    _lib.check(_lib.lib().scp3gpu_syevr_lowest(A.ctypes.data_as(_dp), n, n, k, _p(W),
+                                               C.ctypes.data_as(_dp) if vectors else None, n, device))
+    return (W, C) if vectors else W
+
+
 class _ClusterCfg:
     pass
 

@@ -42,3 +42,17 @@ def test_cli_rejects_gradient_path_and_bad_options(cli, tmp_path):
     assert r.returncode == 1 and "too large" in r.stderr
     r = subprocess.run([cli, "-G"], cwd=tmp_path, capture_output=True, text=True)
     assert r.returncode == 1 and "No input file" in r.stderr
+
+
+def test_eigensolver_cli_arguments(cli, tmp_path):
+    """eigensolver (eigensolver.cpp over the library): usage and file errors are
+    reported before any GPU work."""
+    eig = os.path.join(ROOT, "scp3_b200", "eigensolver")
+    r = subprocess.run([eig], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "usage" in r.stderr
+    r = subprocess.run([eig, "sM_missing.h5", "5"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "cannot open" in r.stderr
+    from scp3_b200 import h5
+    h5.save(str(tmp_path / "sM_0000001.h5"), np.eye(4), deflate=6)
+    r = subprocess.run([eig, "sM_0000001.h5", "9"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "n_eigenpairs" in r.stderr
