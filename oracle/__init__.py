@@ -68,6 +68,17 @@ def lib():
                                  ctypes.c_int64, _c_dp, _c_dp]
         L.or_accumulate.argtypes = [ctypes.c_int] * 3 + [_c_dp, _c_dp, ctypes.c_int64, _c_dp]
         L.or_accumulate_abs.argtypes = [ctypes.c_int] * 3 + [_c_dp, _c_dp, ctypes.c_int64, _c_dp]
+        L.or_basis_modes.restype = ctypes.c_int
+        L.or_basis_modes.argtypes = [ctypes.c_int] * 3 + [ctypes.c_int64, ctypes.POINTER(ctypes.c_int),
+                                                          ctypes.POINTER(ctypes.c_int)]
+        L.or_qtip4pf_grad.restype = ctypes.c_double
+        L.or_qtip4pf_grad.argtypes = [ctypes.c_int, _c_dp, _c_dp]
+        L.or_samples_grad.argtypes = [ctypes.c_int, _c_dp, _c_dp, _c_dp, ctypes.c_int, _c_dp, ctypes.c_int64,
+                                      _c_dp, _c_dp, _c_dp]
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.or_stein_term.restype = ctypes.c_double
+        L.or_stein_term.argtypes = [_c_dp, ctypes.c_double, _c_dp, ctypes.c_int, ip, ip, ctypes.c_int, ip, ip]
+        L.or_accumulate_stein.argtypes = [ctypes.c_int] * 3 + [_c_dp, _c_dp, _c_dp, ctypes.c_int64, _c_dp]
         _lib = L
     return _lib
 
@@ -171,6 +182,58 @@ def add_ho_diagonal(M, omega_sel, n2, n3, zpe_inactive=0.0):
 
 # ---------------------------------------------------------------- the reference itself
 _ref = {}
+
+
+def basis_modes(nm, n2, n3, R):
+    """(mode, level) pairs of basis function R (the order of get_bra)."""
+    m = (ctypes.c_int * 3)()
+    lv = (ctypes.c_int * 3)()
+    k = lib().or_basis_modes(nm, n2, n3, R, m, lv)
+    return [(m[t], lv[t]) for t in range(k)]
+
+
+def qtip4pf_grad(crd):
+    crd = np.ascontiguousarray(crd, dtype=np.float64)
+    g = np.zeros(crd.size)
+    e = lib().or_qtip4pf_grad(crd.size // 9, _dp(crd), _dp(g))
+    return e, g
+
+
+def samples_grad(nw, x0, MUa, omega, normals):
+    """(q, V_anh, dV_anh/dq) of the gradient path, all nm0 modes (qTIP4P/f)."""
+    normals = np.ascontiguousarray(normals, dtype=np.float64)
+    n, nm0 = normals.shape
+    MUa = np.asfortranarray(MUa, dtype=np.float64)
+    q = np.zeros((n, nm0))
+    v = np.zeros(n)
+    vq = np.zeros((n, nm0))
+    lib().or_samples_grad(nw, _dp(np.ascontiguousarray(x0, dtype=np.float64)), _dp(MUa),
+                          _dp(np.ascontiguousarray(omega, dtype=np.float64)), nm0, _dp(normals), n, _dp(q), _dp(v),
+                          _dp(vq))
+    return q, v, vq
+
+
+def stein_term(q, V, vq, bra, ket):
+    """One sample's gradient-estimator value for <bra|V|ket>, each a list of (mode, level)."""
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    vq = np.ascontiguousarray(vq, dtype=np.float64)
+    mi = (ctypes.c_int * 3)(*[b[0] for b in bra])
+    li = (ctypes.c_int * 3)(*[b[1] for b in bra])
+    mj = (ctypes.c_int * 3)(*[b[0] for b in ket])
+    lj = (ctypes.c_int * 3)(*[b[1] for b in ket])
+    return lib().or_stein_term(_dp(q), float(V), _dp(vq), len(bra), mi, li, len(ket), mj, lj)
+
+
+def accumulate_stein(q_sel, v, vq_sel, n2, n3, M=None):
+    """Upper triangle of sum_s estimate_ij(s) (addEpot(q, V, Vq, M)), column-major nb x nb."""
+    q_sel = np.ascontiguousarray(q_sel, dtype=np.float64)
+    vq_sel = np.ascontiguousarray(vq_sel, dtype=np.float64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    n, nm = q_sel.shape
+    nb = basis_size(nm, n2, n3)
+    out = np.zeros((nb, nb), order="F") if M is None else M
+    lib().or_accumulate_stein(nm, n2, n3, _dp(q_sel), _dp(v), _dp(vq_sel), n, out.ctypes.data_as(_c_dp))
+    return out
 
 
 def ref_available(fast=False):

@@ -613,3 +613,256 @@ void or_accumulate_abs(int nm, int n2, int n3, const double* q_sel, const double
     }
     free(bra);
 }
+
+/* ------------------------------------------------------------------------- */
+/* The gradient (default) path.                                               */
+/* ------------------------------------------------------------------------- */
+
+/* qTIP4P/f energy and gradient (qtip4pf.cpp:252-397): kcal/mol and kcal/mol/A.
+ * The M site is a fixed linear combination of O, H, H, so a force on it goes to
+ * the three atoms with the weights gammaM, gamma1, gamma1. */
+static void qt_monomer_grad(const double* w, double* g, double* e)
+{
+    double d1[3], d2[3], r1 = 0, r2 = 0, c = 0;
+    for (int k = 0; k < 3; k++) {
+        d1[k] = w[3 + k] - w[k];
+        d2[k] = w[6 + k] - w[k];
+        r1 += d1[k] * d1[k];
+        r2 += d2[k] * d2[k];
+        c += d1[k] * d2[k];
+    }
+    r1 = sqrt(r1);
+    r2 = sqrt(r2);
+    const double x1 = QT_ALPHAR * (r1 - QT_ROHEQ), x2 = QT_ALPHAR * (r2 - QT_ROHEQ);
+    const double v1 = x1 * x1 * (1.0 - x1 * (1.0 - (7.0 / 12.0) * x1)) * QT_DR;
+    const double v2 = x2 * x2 * (1.0 - x2 * (1.0 - (7.0 / 12.0) * x2)) * QT_DR;
+    /* d/dx of x^2 - x^3 + 7/12 x^4 */
+    const double dv1 = QT_DR * QT_ALPHAR * x1 * (2.0 - x1 * (3.0 - (7.0 / 3.0) * x1));
+    const double dv2 = QT_DR * QT_ALPHAR * x2 * (2.0 - x2 * (3.0 - (7.0 / 3.0) * x2));
+    const double cs = c / (r1 * r2);
+    const double th = acos(cs);
+    const double dth = th - QT_AHOHEQ * M_PI / 180.0;
+    *e += v1 + v2 + 0.5 * QT_KTHETA * dth * dth;
+    /* dE/dcos = k dth * dth/dcos = -k dth / sin(th) */
+    const double de_dc = -QT_KTHETA * dth / sqrt(1.0 - cs * cs);
+    for (int k = 0; k < 3; k++) {
+        const double u1 = d1[k] / r1, u2 = d2[k] / r2;
+        const double gh1 = dv1 * u1 + de_dc * (u2 - cs * u1) / r1;
+        const double gh2 = dv2 * u2 + de_dc * (u1 - cs * u2) / r2;
+        g[3 + k] += gh1;
+        g[6 + k] += gh2;
+        g[k] -= gh1 + gh2;
+    }
+}
+
+/* charge-charge term q_a q_b / r between points a and b: energy, and the
+ * gradient added into ga (at a) and gb (at b) */
+static double qt_coulomb(double qq, const double* a, const double* b, double* ga, double* gb)
+{
+    double d[3], r2 = 0;
+    for (int k = 0; k < 3; k++) {
+        d[k] = a[k] - b[k];
+        r2 += d[k] * d[k];
+    }
+    const double ir = 1.0 / sqrt(r2), e = qq * ir, f = -e * ir * ir;
+    for (int k = 0; k < 3; k++) {
+        ga[k] += f * d[k];
+        gb[k] -= f * d[k];
+    }
+    return e;
+}
+
+double or_qtip4pf_grad(int nw, const double* crd, double* grad)
+{
+    double msite[3 * 64], gm[3 * 64];
+    if (nw > 64) return NAN;
+    double e = 0;
+    for (int i = 0; i < 9 * nw; i++) grad[i] = 0.0;
+    for (int i = 0; i < 3 * nw; i++) gm[i] = 0.0;
+    for (int i = 0; i < nw; i++) {
+        const double* w = crd + 9 * i;
+        for (int k = 0; k < 3; k++) msite[3 * i + k] = QT_GAMMAM * w[k] + QT_GAMMA1 * (w[3 + k] + w[6 + k]);
+        qt_monomer_grad(w, grad + 9 * i, &e);
+    }
+    for (int i = 0; i < nw; i++) {
+        for (int j = 0; j < nw; j++) {
+            if (i == j) continue;
+            for (int l = 1; l < 3; l++)
+                e += qt_coulomb(QT_QH * qt_qM, msite + 3 * i, crd + 9 * j + 3 * l, gm + 3 * i, grad + 9 * j + 3 * l);
+        }
+        for (int j = i + 1; j < nw; j++) {
+            for (int a = 1; a < 3; a++)
+                for (int b = 1; b < 3; b++)
+                    e += qt_coulomb(QT_QH * QT_QH, crd + 9 * i + 3 * a, crd + 9 * j + 3 * b, grad + 9 * i + 3 * a,
+                                    grad + 9 * j + 3 * b);
+            double d[3], r2 = 0;
+            for (int k = 0; k < 3; k++) {
+                d[k] = crd[9 * i + k] - crd[9 * j + k];
+                r2 += d[k] * d[k];
+            }
+            const double s2 = QT_SIGMA * QT_SIGMA / r2, s6 = s2 * s2 * s2;
+            e += 4 * QT_EPS * s6 * (s6 - 1.0);
+            /* dE/dx_i = 2 dE/dr2 d, dE/dr2 = 4 eps (3 s6 - 6 s12) / r2 */
+            const double f = 2.0 * 4 * QT_EPS * (3.0 * s6 - 6.0 * s6 * s6) / r2;
+            for (int k = 0; k < 3; k++) {
+                grad[9 * i + k] += f * d[k];
+                grad[9 * j + k] -= f * d[k];
+            }
+            e += qt_coulomb(qt_qM * qt_qM, msite + 3 * i, msite + 3 * j, gm + 3 * i, gm + 3 * j);
+        }
+    }
+    for (int i = 0; i < nw; i++)
+        for (int k = 0; k < 3; k++) {
+            grad[9 * i + k] += QT_GAMMAM * gm[3 * i + k];
+            grad[9 * i + 3 + k] += QT_GAMMA1 * gm[3 * i + k];
+            grad[9 * i + 6 + k] += QT_GAMMA1 * gm[3 * i + k];
+        }
+    return e;
+}
+
+/* Per-sample stage of the gradient path (SCP3.cpp:205-223, use_gradient):
+ * V_anh as or_samples, and Vq = MUa^T (bohr dV/dr / autokcal) - omega % q for
+ * all nm0 modes (n x nm0, sample-major).  qTIP4P/f only. */
+void or_samples_grad(int nw, const double* x0, const double* MUa, const double* omega, int nm0,
+                     const double* normals, int64_t n, double* q_out, double* v_out, double* vq_out)
+{
+    const double bohr = 0.52917721092, kcal = 627.509474277194;
+    const int N3 = 9 * nw;
+    double* r = (double*)malloc(sizeof(double) * N3);
+    double* g = (double*)malloc(sizeof(double) * N3);
+    for (int64_t s = 0; s < n; s++) {
+        double* q = q_out + s * nm0;
+        for (int k = 0; k < nm0; k++) q[k] = normals[s * nm0 + k] / sqrt(2.0);
+        for (int a = 0; a < N3; a++) {
+            double acc = 0.0;
+            for (int k = 0; k < nm0; k++) acc += MUa[(size_t)k * N3 + a] * q[k];
+            r[a] = bohr * (x0[a] + acc);
+        }
+        const double V = or_qtip4pf_grad(nw, r, g) / kcal;
+        for (int a = 0; a < N3; a++) g[a] *= bohr / kcal;
+        double h = 0.0;
+        for (int k = 0; k < nm0; k++) h += q[k] * (omega[k] * q[k]);
+        v_out[s] = V - 0.5 * h;
+        for (int k = 0; k < nm0; k++) {
+            double acc = 0.0;
+            for (int a = 0; a < N3; a++) acc += MUa[(size_t)k * N3 + a] * g[a];
+            vq_out[s * nm0 + k] = acc - omega[k] * q[k];
+        }
+    }
+    free(r);
+    free(g);
+}
+
+/* The gradient (Stein) estimator of <i|V|j> (ScaledMatrixElements.cpp:102-725,
+ * TripleExcitations.h), restated by the rule its formulas follow: with
+ * phi_i phi_j = prod_m p_m(q_m) over the set S of modes either function
+ * excites, every mode m in S contributes the Stein identity
+ * E[q g(q)] = 1/2 E[g'(q)] (q ~ N(0, 1/2)) applied to the factor q_m of
+ * p_m = p_m(0) + q_m r_m(q_m):
+ *     T_m = R_m [ (p_m(0) + r_m'/2) V + (r_m/2) dV/dq_m ],  R_m = prod_{m' != m} p_m',
+ * and the estimate is the mean of T_m over S (V itself for <0|V|0>).  One
+ * exception reproduces the reference as written: see <3_m|V|3_m> below.
+ * Per mode, with h_0..h_3 the oscillator functions (levels a, b):
+ *     r_ab = d_a h_b + h_a(0) d_b,  d_a = (h_a(q) - h_a(0)) / q. */
+static void ho_parts(int a, double q, double* h, double* h0, double* dh, double* d, double* dd)
+{
+    const double s2 = sqrt(2.0), s3 = sqrt(3.0);
+    switch (a) {
+        case 0: *h = 1, *h0 = 1, *dh = 0, *d = 0, *dd = 0; break;
+        case 1: *h = s2 * q, *h0 = 0, *dh = s2, *d = s2, *dd = 0; break;
+        case 2: *h = (2 * q * q - 1) / s2, *h0 = -1 / s2, *dh = 2 * s2 * q, *d = s2 * q, *dd = s2; break;
+        default: *h = (2 * q * q - 3) * q / s3, *h0 = 0, *dh = (6 * q * q - 3) / s3, *d = (2 * q * q - 3) / s3,
+                 *dd = 4 * q / s3; break;
+    }
+}
+
+/* One sample's estimate for the pair of functions given as (mode, level) lists. */
+double or_stein_term(const double* q, double V, const double* vq, int ni, const int* mi, const int* li, int nj,
+                     const int* mj, const int* lj)
+{
+    int S[8], A[8], B[8], ns = 0;
+    for (int k = 0; k < ni; k++) S[ns] = mi[k], A[ns] = li[k], B[ns] = 0, ns++;
+    for (int k = 0; k < nj; k++) {
+        int f = -1;
+        for (int t = 0; t < ns; t++)
+            if (S[t] == mj[k]) f = t;
+        if (f >= 0) B[f] = lj[k];
+        else S[ns] = mj[k], A[ns] = 0, B[ns] = lj[k], ns++;
+    }
+    if (ns == 0) return V;
+    double p[8], u[8], w[8];
+    for (int t = 0; t < ns; t++) {
+        double ha, ha0, dha, da, dda, hb, hb0, dhb, db, ddb;
+        const double x = q[S[t]];
+        ho_parts(A[t], x, &ha, &ha0, &dha, &da, &dda);
+        ho_parts(B[t], x, &hb, &hb0, &dhb, &db, &ddb);
+        const double r = da * hb + ha0 * db;
+        const double dr = dda * hb + da * dhb + ha0 * ddb;
+        p[t] = ha * hb;
+        u[t] = ha0 * hb0 + 0.5 * dr;
+        w[t] = 0.5 * r;
+        /* <3_m|V|3_m>: the reference's formula (TripleExcitations.h:763-773) has
+         * (q^2 - 3) V where the identity gives (10 q^2 - 3) V; kept for parity */
+        if (A[t] == 3 && B[t] == 3) u[t] = (2 * x * x - 3) * (x * x - 3) / 6.0;
+    }
+    double sum = 0.0;
+    for (int t = 0; t < ns; t++) {
+        double R = 1.0;
+        for (int o = 0; o < ns; o++)
+            if (o != t) R *= p[o];
+        sum += R * (u[t] * V + w[t] * vq[S[t]]);
+    }
+    return sum / ns;
+}
+
+/* (mode, level) list of basis function R in the order of or_get_bra */
+static int basis_modes(int nm, int n2, int n3, size_t R, int* m, int* l)
+{
+    size_t k = 0;
+    if (R == k) return 0;
+    k++;
+    if (R < k + (size_t)nm) { m[0] = (int)(R - k), l[0] = 1; return 1; }
+    k += nm;
+    if (R < k + (size_t)n2) { m[0] = (int)(R - k), l[0] = 2; return 1; }
+    k += n2;
+    for (int a = 0; a < n2; a++)
+        for (int b = a + 1; b < n2; b++, k++)
+            if (R == k) { m[0] = a, l[0] = 1, m[1] = b, l[1] = 1; return 2; }
+    if (R < k + (size_t)n3) { m[0] = (int)(R - k), l[0] = 3; return 1; }
+    k += n3;
+    for (int a = 0; a < n3; a++)
+        for (int b = a + 1; b < n3; b++) {
+            if (R == k) { m[0] = a, l[0] = 2, m[1] = b, l[1] = 1; return 2; }
+            k++;
+            if (R == k) { m[0] = a, l[0] = 1, m[1] = b, l[1] = 2; return 2; }
+            k++;
+        }
+    for (int a = 0; a < n3; a++)
+        for (int b = a + 1; b < n3; b++)
+            for (int c = b + 1; c < n3; c++, k++)
+                if (R == k) { m[0] = a, l[0] = 1, m[1] = b, l[1] = 1, m[2] = c, l[2] = 1; return 3; }
+    return -1;
+}
+
+int or_basis_modes(int nm, int n2, int n3, int64_t R, int* m, int* l) { return basis_modes(nm, n2, n3, (size_t)R, m, l); }
+
+/* addEpot(q, V, Vq, M) (ScaledMatrixElements.cpp:704-719): M_upper[i,j] += sum_s
+ * estimate_ij(s), i <= j.  q_sel, vq_sel: n x nm (selected modes), M nb x nb. */
+void or_accumulate_stein(int nm, int n2, int n3, const double* q_sel, const double* v, const double* vq_sel, int64_t n,
+                         double* M)
+{
+    const size_t nb = or_basis_size(nm, n2, n3);
+    int* mm = (int*)malloc(sizeof(int) * 3 * nb);
+    int* ll = (int*)malloc(sizeof(int) * 3 * nb);
+    int* cnt = (int*)malloc(sizeof(int) * nb);
+    for (size_t R = 0; R < nb; R++) cnt[R] = basis_modes(nm, n2, n3, R, mm + 3 * R, ll + 3 * R);
+    for (size_t j = 0; j < nb; j++)
+        for (size_t i = 0; i <= j; i++) {
+            double acc = 0.0;
+            for (int64_t s = 0; s < n; s++)
+                acc += or_stein_term(q_sel + s * nm, v[s], vq_sel + s * nm, cnt[i], mm + 3 * i, ll + 3 * i, cnt[j],
+                                     mm + 3 * j, ll + 3 * j);
+            M[j * nb + i] += acc;
+        }
+    free(mm), free(ll), free(cnt);
+}

@@ -17,6 +17,14 @@ Fixtures:
   hbuild_ref.npz  the -G sample loop (SCP3.cpp:187-232 with get_bra + dsyr2k,
                   ScaledMatrixElements.cpp:870-971) for small dimer/hexamer bases,
                   with the normal-mode inputs it used.
+  stein_ref.npz   the gradient path: every formula of TripleExcitations.h (the
+                  reference's gradient estimator, oracle/_ref/libscp3ref_stein.so)
+                  on seeded data; qTIP4P/f gradients (qtip4pf.cpp:252-397) on the
+                  pes_ref geometries; and a dimer matrix (N2 = 12, N3 = 4) summed
+                  from the reference's formulas over samples whose V and dV/dq
+                  come from the reference's potential (SCP3.cpp:205-223).
+
+    python tests/golden/make_golden.py stein      # only stein_ref.npz
 """
 import os
 import sys
@@ -141,12 +149,145 @@ def gen_hbuild(L, dimer, prism):
     np.savez_compressed(os.path.join(OUT, "hbuild_ref.npz"), **flat)
 
 
+def parse_formula(name, params):
+    """TripleExcitations.h names a formula by its bra and ket, e.g.
+    m2_n1_f_k1_l1_j1(m, n, k, l, j) = <2_m 1_n | V | 1_k 1_l 1_j>: per side a
+    list of (parameter index, level)."""
+    bra, ket = name.split("f_") if name.startswith("f_") is False else ("", name[2:])
+    if not name.startswith("f_"):
+        bra, ket = name.split("_f_")
+    side = lambda t: [(params.index(tok[0]), int(tok[1])) for tok in t.split("_") if tok]
+    return side(bra), side(ket)
+
+
+def ref_stein_lib():
+    import ctypes
+    Ls = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libscp3ref_stein.so"))
+    Ls.ref_stein_name.restype = ctypes.c_char_p
+    Ls.ref_stein_params.restype = ctypes.c_char_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    Ls.ref_stein_eval.restype = ctypes.c_double
+    Ls.ref_stein_eval.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    names = [Ls.ref_stein_name(i).decode() for i in range(Ls.ref_stein_count())]
+    params = [Ls.ref_stein_params(i).decode().split(",") for i in range(Ls.ref_stein_count())]
+    return Ls, names, params
+
+
+def ref_stein_eval(Ls, i, args, qT, V, VqT):
+    import ctypes
+    dp = ctypes.POINTER(ctypes.c_double)
+    a = np.asarray(args, dtype=np.int32)
+    return Ls.ref_stein_eval(i, qT.ctypes.data_as(dp), V.ctypes.data_as(dp), VqT.ctypes.data_as(dp), V.size,
+                             a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+
+
+def gen_stein(L, dimer):
+    import ctypes
+    import itertools
+    Ls, names, params = ref_stein_lib()
+    rng = np.random.default_rng(2024)
+    nm, n = 10, 64
+    q = rng.normal(scale=np.sqrt(0.5), size=(n, nm))
+    V = rng.normal(size=n)
+    Vq = rng.normal(size=(n, nm))
+    qT, VqT = np.ascontiguousarray(q.T), np.ascontiguousarray(Vq.T)
+    args = np.full((len(names), 6), -1, dtype=np.int32)
+    vals = np.zeros(len(names))
+    for i, (nmx, pr) in enumerate(zip(names, params)):
+        a = rng.choice(nm, size=len(pr), replace=False)
+        args[i, :len(pr)] = a
+        vals[i] = ref_stein_eval(Ls, i, a, qT, V, VqT)
+    # qTIP4P/f gradients of the reference on the pes_ref geometries
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.ref_qtip4pf_energy_grad.restype = ctypes.c_double
+    L.ref_qtip4pf_energy_grad.argtypes = [ctypes.c_int, dp, dp]
+    z = np.load(os.path.join(OUT, "pes_ref.npz"), allow_pickle=True)
+    grads = []
+    for x in z["geoms"]:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        g = np.zeros(x.size)
+        L.ref_qtip4pf_energy_grad(x.size // 9, x.ctypes.data_as(dp), g.ctypes.data_as(dp))
+        grads.append(g)
+    # the dimer matrix: each upper element from the reference formula with its bra and ket
+    x0, MUa, omega = setup_modes(L, dimer)
+    nm0 = omega.size
+    n2, n3, ns, sseed = 12, 4, 256, 0x5C3
+    normals = oracle.std_normals(nm0, 0, ns, scramble_seed=sseed)
+    bohr, kcal = C.bohr, C.autokcalpmol
+    qs = normals / np.sqrt(2.0)
+    Vs = np.zeros(ns)
+    Vqs = np.zeros((ns, nm0))
+    for s in range(ns):
+        r = np.ascontiguousarray(bohr * (x0 + MUa @ qs[s]))
+        g = np.zeros(r.size)
+        e = L.ref_qtip4pf_energy_grad(r.size // 9, r.ctypes.data_as(dp), g.ctypes.data_as(dp)) / kcal
+        Vs[s] = e - 0.5 * np.dot(qs[s], omega * qs[s])
+        Vqs[s] = MUa.T @ (g * bohr / kcal) - omega * qs[s]
+    nb = oracle.basis_size(nm0, n2, n3)
+    funcs = [oracle.basis_modes(nm0, n2, n3, R) for R in range(nb)]
+    parsed = [parse_formula(nmx, pr) for nmx, pr in zip(names, params)]
+    qT, VqT = np.ascontiguousarray(qs.T), np.ascontiguousarray(Vqs.T)
+    Mu = np.zeros(nb * (nb + 1) // 2)
+    k = 0
+    used = set()
+    for C_ in range(nb):
+        for R in range(C_ + 1):
+            if R == 0 and C_ == 0:
+                Mu[k] = Vs.sum()            # M(0,0) += sum(V), ScaledMatrixElements.cpp:711
+                k += 1
+                continue
+            hit = None
+            # a formula names <bra|V|ket>; the estimate is symmetric, so either
+            # function of the pair may be its bra (the loops of
+            # ScaledMatrixElements.cpp:102-702 use both orders)
+            for i, (pb, pk), (bra, ket) in ((i, pp, bk) for bk in ((funcs[R], funcs[C_]), (funcs[C_], funcs[R]))
+                                            for i, pp in enumerate(parsed)):
+                if len(pb) != len(bra) or len(pk) != len(ket):
+                    continue
+                for perm_b in itertools.permutations(range(len(bra))):
+                    ok = all(bra[perm_b[t]][1] == pb[t][1] for t in range(len(pb)))
+                    if not ok:
+                        continue
+                    amap = {pb[t][0]: bra[perm_b[t]][0] for t in range(len(pb))}
+                    for perm_k in itertools.permutations(range(len(ket))):
+                        a2 = dict(amap)
+                        good = True
+                        for t in range(len(pk)):
+                            md, lv = ket[perm_k[t]]
+                            if lv != pk[t][1] or a2.get(pk[t][0], md) != md:
+                                good = False
+                                break
+                            a2[pk[t][0]] = md
+                        if good and len(set(a2.values())) == len(a2) and len(a2) == len(params[i]):
+                            hit = (i, [a2[j] for j in range(len(params[i]))])
+                            break
+                    if hit:
+                        break
+                if hit:
+                    break
+            if hit is None:
+                raise RuntimeError("no formula for <%s|V|%s>" % (funcs[R], funcs[C_]))
+            used.add(hit[0])
+            Mu[k] = ref_stein_eval(Ls, hit[0], hit[1], qT, Vs, VqT)
+            k += 1
+    print("stein: %d formulas, %d used by the dimer matrix" % (len(names), len(used)))
+    np.savez_compressed(os.path.join(OUT, "stein_ref.npz"), names=np.array(names), params=np.array(
+        [",".join(p) for p in params]), args=args, values=vals, q=q, V=V, Vq=Vq, pes_geoms_grad=np.array(
+        grads, dtype=object), dimer_x0=x0, dimer_MUa=MUa, dimer_omega=omega, dimer_n2=n2, dimer_n3=n3,
+        dimer_nsamples=ns, dimer_scramble_seed=sseed, dimer_q=qs, dimer_V=Vs, dimer_Vq=Vqs, dimer_M_upper=Mu)
+
+
 def main():
     oracle.build(REF)
     L = oracle.ref_lib()
+    if sys.argv[1:] == ["stein"]:
+        z = np.load(os.path.join(OUT, "pes_ref.npz"), allow_pickle=True)
+        gen_stein(L, np.asarray(z["geoms"][7], dtype=np.float64))   # the relaxed dimer (gen_pes bases[1])
+        return
     gen_sobol(L)
     dimer, prism = gen_pes(L)
     gen_hbuild(L, dimer, prism)
+    gen_stein(L, dimer)
 
 
 if __name__ == "__main__":
