@@ -107,7 +107,14 @@ typedef struct scp3gpu_config {
     uint64_t scramble_seed;
     int chunk;              /* samples per device pass; multiple of 4096, 0 = auto     */
     int device;             /* CUDA device ordinal                                     */
+    int estimator;          /* SCP3GPU_ESTIMATOR_*                                     */
 } scp3gpu_config;
+
+/* matrix-element estimator (SCP3.cpp:226-231) */
+#define SCP3GPU_ESTIMATOR_DIRECT 0   /* -G: sum_s Phi V Phi^T (ScaledMatrixElements.cpp:951-971)         */
+#define SCP3GPU_ESTIMATOR_GRADIENT 1 /* the default: Stein estimator from V and dV/dq
+                                        (ScaledMatrixElements.cpp:102-725, TripleExcitations.h); plain
+                                        FP64 form, qTIP4P/f (its gradient, qtip4pf.cpp:252-397)          */
 
 /* Replaces ScaledMatrixElements(omega(modes), N2, N3) + M.zeros (SCP3.cpp:164-169). */
 int scp3gpu_hbuild_create(const scp3gpu_config* cfg, scp3gpu_hbuild** out);
@@ -160,6 +167,11 @@ int scp3gpu_hbuild_eigvals(scp3gpu_hbuild* h, int64_t nsub, int k, double* evals
  * upper triangle is read unless A(0, n-1) == 0, then the lower one. */
 int scp3gpu_syevr_lowest(const double* A, int64_t n, int64_t lda, int k, double* W, double* Z, int64_t ldz,
                          int device);
+
+/* addEpot(q, V, Vq, M) of the gradient path (ScaledMatrixElements.cpp:704-719):
+ * n samples of the selected modes' q and dV_anh/dq (n x nmodes, sample-major)
+ * and V_anh into the sums of a SCP3GPU_ESTIMATOR_GRADIENT handle. */
+int scp3gpu_hbuild_add_epot_grad(scp3gpu_hbuild* h, const double* q, const double* V, const double* Vq, int64_t n);
 
 /* Per-sample status counters since create/reset: samples with a non-finite
  * V, TTM3-F samples that hit the sweep cap. */

@@ -14,6 +14,7 @@ OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_NOT_CONVERGED, ERR_NONFINITE, ERR_TIMEOUT,
 PREC_FP64, PREC_BF16X3, PREC_BF16X3_PES64, PREC_F16X3, PREC_F16X3_PES64 = 0, 1, 2, 3, 4
 SOBOL_REFERENCE, SOBOL_SCRAMBLED = 0, 1
 BATCH_NO_GRAPH, BATCH_NO_AUTOTUNE = 1, 2
+ESTIMATOR_DIRECT, ESTIMATOR_GRADIENT = 0, 1
 
 # every symbol include/scp3gpu.h declares (checked by the CPU tests)
 EXPORTS = [
@@ -26,7 +27,7 @@ EXPORTS = [
     "scp3gpu_load_h5", "scp3gpu_syevr_lowest",
     "scp3gpu_mlp_create", "scp3gpu_mlp_destroy", "scp3gpu_mlp_num_params", "scp3gpu_mlp_get_params",
     "scp3gpu_mlp_set_params", "scp3gpu_mlp_set_output", "scp3gpu_mlp_forward", "scp3gpu_mlp_grad", "scp3gpu_mlp_train",
-    "scp3gpu_hbuild_set_surrogate", "scp3gpu_hbuild_sample",
+    "scp3gpu_hbuild_set_surrogate", "scp3gpu_hbuild_sample", "scp3gpu_hbuild_add_epot_grad",
     "scp3gpu_batch_create", "scp3gpu_batch_destroy", "scp3gpu_batch_reset", "scp3gpu_batch_size",
     "scp3gpu_batch_basis_size", "scp3gpu_batch_sample_count", "scp3gpu_batch_stream", "scp3gpu_batch_shape",
     "scp3gpu_batch_accumulate", "scp3gpu_batch_read", "scp3gpu_batch_status",
@@ -47,7 +48,7 @@ class Config(ctypes.Structure):
         ("nmodes", ctypes.c_int), ("modes", ctypes.POINTER(ctypes.c_int)),
         ("n2", ctypes.c_int), ("n3", ctypes.c_int), ("pes", ctypes.c_int), ("precision", ctypes.c_int),
         ("scramble", ctypes.c_int), ("scramble_seed", ctypes.c_uint64), ("chunk", ctypes.c_int),
-        ("device", ctypes.c_int),
+        ("device", ctypes.c_int), ("estimator", ctypes.c_int),
     ]
 
 
@@ -89,6 +90,7 @@ def lib():
     L.scp3gpu_hbuild_accumulate.argtypes = [vp, i64, i64]
     L.scp3gpu_hbuild_accumulate_normals.argtypes = [vp, dp, i64]
     L.scp3gpu_hbuild_add_epot.argtypes = [vp, dp, dp, i64]
+    L.scp3gpu_hbuild_add_epot_grad.argtypes = [vp, dp, dp, dp, i64]
     L.scp3gpu_hbuild_sample_count.restype = i64
     L.scp3gpu_hbuild_sample_count.argtypes = [vp]
     L.scp3gpu_hbuild_read.argtypes = [vp, dp, i64, ctypes.c_int]

@@ -94,7 +94,8 @@ PRECISIONS = {"fp64": _lib.PREC_FP64, "bf16x3": _lib.PREC_BF16X3, "bf16x3_pes64"
               "f16x3": _lib.PREC_F16X3, "f16x3_pes64": _lib.PREC_F16X3_PES64}
 
 
-def _fill_config(obj, nw, x0, MUa, omega, modes, n2, n3, pes, precision, scramble_seed, chunk, device):
+def _fill_config(obj, nw, x0, MUa, omega, modes, n2, n3, pes, precision, scramble_seed, chunk, device,
+                 estimator="direct"):
     """Fill obj._cfg (a Config) and keep the arrays it points to alive on obj."""
     obj.x0 = np.ascontiguousarray(x0, dtype=np.float64)
     obj.MUa = np.asfortranarray(MUa, dtype=np.float64)
@@ -114,6 +115,7 @@ def _fill_config(obj, nw, x0, MUa, omega, modes, n2, n3, pes, precision, scrambl
     cfg.scramble = _lib.SOBOL_SCRAMBLED if scramble_seed is not None else _lib.SOBOL_REFERENCE
     cfg.scramble_seed = scramble_seed or 0
     cfg.chunk, cfg.device = chunk, device
+    cfg.estimator = {"direct": _lib.ESTIMATOR_DIRECT, "gradient": _lib.ESTIMATOR_GRADIENT}[estimator]
     obj._cfg = cfg
 
 
@@ -121,8 +123,12 @@ class HBuild:
     """One device-side Hamiltonian build: ScaledMatrixElements + the SCP3_a loop."""
 
     def __init__(self, nw, x0, MUa, omega, modes=None, n2=None, n3=0, pes="qtip4pf", precision="fp64",
-                 scramble_seed=None, chunk=0, device=0):
-        _fill_config(self, nw, x0, MUa, omega, modes, n2, n3, pes, precision, scramble_seed, chunk, device)
+                 scramble_seed=None, chunk=0, device=0, estimator="direct"):
+        """estimator: "direct" (-G, sum Phi V Phi^T) or "gradient" (the reference's
+        default Stein estimator from V and dV/dq; FP64, qTIP4P/f)."""
+        _fill_config(self, nw, x0, MUa, omega, modes, n2, n3, pes, precision, scramble_seed, chunk, device,
+                     estimator)
+        self.estimator = estimator
         cfg = self._cfg
         h = ctypes.c_void_p()
         _lib.check(_lib.lib().scp3gpu_hbuild_create(ctypes.byref(cfg), ctypes.byref(h)))
@@ -165,6 +171,13 @@ class HBuild:
         q = np.ascontiguousarray(q, dtype=np.float64)
         V = np.ascontiguousarray(V, dtype=np.float64)
         _lib.check(_lib.lib().scp3gpu_hbuild_add_epot(self._h, _p(q), _p(V), V.size))
+
+    def add_epot_grad(self, q, V, Vq):
+        """addEpot(q, V, Vq, M) of the gradient path: q, Vq n x nmodes, V n."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        Vq = np.ascontiguousarray(Vq, dtype=np.float64)
+        _lib.check(_lib.lib().scp3gpu_hbuild_add_epot_grad(self._h, _p(q), _p(V), _p(Vq), V.size))
 
     def sample_count(self):
         return int(_lib.lib().scp3gpu_hbuild_sample_count(self._h))

@@ -64,6 +64,8 @@ struct scp3gpu_hbuild {
     double* vb[2] = {nullptr, nullptr};
     double* normals[2] = {nullptr, nullptr};
     double *phi = nullptr, *w = nullptr;
+    double* vq = nullptr;             // gradient path: dV_anh/dq of the selected modes, [chunk][nmodes]
+    bool gradient = false;
     double* partial = nullptr;
     tc::Plan tcp{};
     // read-out
@@ -162,6 +164,7 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     a.v = h->split_form ? h->vb[b] : h->v;
     a.counters = h->counters;
     a.skip_pes = h->sur_mode == SCP3GPU_SURROGATE_REPLACE;
+    a.vq = h->gradient ? h->vq : nullptr;
     int rc;
     if (h->split_form) {
         cudaStream_t ps = h->prep_stream;
@@ -197,6 +200,11 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     }
     if (rc) return rc;
     if (consumed) SCP3_CUDA(cudaEventRecord(consumed, h->stream));
+    if (h->gradient) {
+        Timed t(h, 2);
+        return launch_stein_fp64(h->desc, h->nb, h->cfg.nmodes, h->q64, h->v, h->vq, a.n, h->tm, h->nsplit,
+                                 h->partial, h->stream);
+    }
     {
         Timed t(h, 1);
         rc = launch_expand_fp64(h->desc, h->nb, h->nb_pad, h->cfg.nmodes, h->q64, h->v, a.n, h->chunk, h->phi, h->w,
@@ -364,7 +372,7 @@ int scp3gpu_hbuild_destroy(scp3gpu_hbuild* h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     if (h->prep_stream) cudaStreamSynchronize(h->prep_stream);
-    void* ptrs[] = {h->ybuf, h->vdir, h->shift, h->x0, h->MUa, h->omega, h->modes, h->tasks, h->desc, h->q64, h->q32b[0],
+    void* ptrs[] = {h->vq, h->ybuf, h->vdir, h->shift, h->x0, h->MUa, h->omega, h->modes, h->tasks, h->desc, h->q64, h->q32b[0],
                     h->q32b[1], h->vb[0], h->vb[1],
                     h->v, h->normals[0], h->normals[1], h->phi, h->w, h->partial, h->dense, h->hodiag,
                     h->counters};
@@ -404,6 +412,11 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
         return fail(SCP3GPU_ERR_ARG, "unknown precision");
     if (c->pes == SCP3GPU_PES_TTM3F && c->nw > 8) return fail(SCP3GPU_ERR_ARG, "TTM3-F kernel supports nw <= 8");
     if (c->chunk < 0 || c->chunk % 4096 != 0) return fail(SCP3GPU_ERR_ARG, "chunk must be a multiple of 4096");
+    if (c->estimator != SCP3GPU_ESTIMATOR_DIRECT && c->estimator != SCP3GPU_ESTIMATOR_GRADIENT)
+        return fail(SCP3GPU_ERR_ARG, "unknown estimator");
+    if (c->estimator == SCP3GPU_ESTIMATOR_GRADIENT &&
+        (c->precision != SCP3GPU_PREC_FP64 || c->pes != SCP3GPU_PES_QTIP4PF))
+        return fail(SCP3GPU_ERR_UNSUPPORTED, "gradient estimator: plain FP64 form with qTIP4P/f only");
     for (int m = 0; m < c->nmodes; m++)
         if (c->modes[m] < 0 || c->modes[m] >= c->nmodes0) return fail(SCP3GPU_ERR_ARG, "mode index out of range");
     int rc = check_device(c->device);
@@ -472,11 +485,17 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
         h->q32 = h->q32b[0];
         h->v = h->vb[0];
     } else {
+        h->gradient = c->estimator == SCP3GPU_ESTIMATOR_GRADIENT;
         plan_fp64(h, sms);
         if ((rc = dalloc(&h->q64, (size_t)h->chunk * c->nmodes)) || (rc = dalloc(&h->v, (size_t)h->chunk)) ||
-            (rc = dalloc(&h->phi, (size_t)h->nb_pad * h->chunk)) || (rc = dalloc(&h->w, (size_t)h->nb_pad * h->chunk)) ||
             (rc = dalloc(&h->partial, (size_t)h->nsplit * h->tm.ntiles * 64 * 64)))
             return bail(rc);
+        if (h->gradient) {
+            if ((rc = dalloc(&h->vq, (size_t)h->chunk * c->nmodes))) return bail(rc);
+        } else if ((rc = dalloc(&h->phi, (size_t)h->nb_pad * h->chunk)) ||
+                   (rc = dalloc(&h->w, (size_t)h->nb_pad * h->chunk))) {
+            return bail(rc);
+        }
     }
     if ((rc = zero_sums(h))) return bail(rc);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(fail(SCP3GPU_ERR_CUDA, "create sync failed"));
@@ -545,6 +564,7 @@ int scp3gpu_hbuild_add_epot(scp3gpu_hbuild* h, const double* q, const double* V,
 {
     (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
     if (!h || n < 0 || (n > 0 && (!q || !V))) return fail(SCP3GPU_ERR_ARG, "add_epot: bad arguments");
+    if (h->gradient) return fail(SCP3GPU_ERR_ARG, "add_epot: a gradient-estimator build takes add_epot_grad");
     DeviceGuard g(h->dev);
     const int nm = h->cfg.nmodes;
     if (int rc0 = drain_prep(h)) return rc0;
@@ -569,6 +589,33 @@ int scp3gpu_hbuild_add_epot(scp3gpu_hbuild* h, const double* q, const double* V,
                                                h->stream);
             SCP3_CUDA(cudaStreamSynchronize(h->stream));
         }
+        if (rc) return rc;
+        h->count += c;
+    }
+    return SCP3GPU_OK;
+}
+
+int scp3gpu_hbuild_add_epot_grad(scp3gpu_hbuild* h, const double* q, const double* V, const double* Vq, int64_t n)
+{
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
+    if (!h || n < 0 || (n > 0 && (!q || !V || !Vq))) return fail(SCP3GPU_ERR_ARG, "add_epot_grad: bad arguments");
+    if (!h->gradient) return fail(SCP3GPU_ERR_ARG, "add_epot_grad: the build was created with the direct estimator");
+    DeviceGuard g(h->dev);
+    const int nm = h->cfg.nmodes;
+    SCP3_CUDA(cudaStreamSynchronize(h->stream));
+    for (int64_t off = 0; off < n; off += h->chunk) {
+        const int64_t c = std::min(h->chunk, n - off);
+        const int64_t kn = round_up(c, 16ll * h->nsplit);
+        // padding samples carry V = 0 and dV/dq = 0 and so contribute nothing
+        SCP3_CUDA(cudaMemsetAsync(h->v, 0, sizeof(double) * kn, h->stream));
+        SCP3_CUDA(cudaMemsetAsync(h->q64, 0, sizeof(double) * kn * nm, h->stream));
+        SCP3_CUDA(cudaMemsetAsync(h->vq, 0, sizeof(double) * kn * nm, h->stream));
+        SCP3_CUDA(cudaMemcpyAsync(h->v, V + off, sizeof(double) * c, cudaMemcpyHostToDevice, h->stream));
+        SCP3_CUDA(cudaMemcpyAsync(h->q64, q + off * nm, sizeof(double) * c * nm, cudaMemcpyHostToDevice, h->stream));
+        SCP3_CUDA(cudaMemcpyAsync(h->vq, Vq + off * nm, sizeof(double) * c * nm, cudaMemcpyHostToDevice, h->stream));
+        int rc = launch_stein_fp64(h->desc, h->nb, nm, h->q64, h->v, h->vq, kn, h->tm, h->nsplit, h->partial,
+                                   h->stream);
+        SCP3_CUDA(cudaStreamSynchronize(h->stream));
         if (rc) return rc;
         h->count += c;
     }

@@ -121,6 +121,8 @@ struct SampleArgs {
     double* v;                    // [n] V_anh (hartree)
     unsigned long long* counters; // [2] non-finite, not converged
     int skip_pes;                 // 1: q only, V_anh = 0 (the surrogate supplies V)
+    double* vq;                   // [n x nm] dV_anh/dq of the selected modes, FP64 (gradient path; qTIP4P/f,
+                                  // FP64 potential), or nullptr
 };
 // pes: SCP3GPU_PES_*, fp32: run the potential in FP32.
 int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s);
@@ -140,6 +142,12 @@ int launch_std_normal(int dims, int64_t index0, int64_t n, const int64_t* vdir, 
 // FP64 plain form: Phi[i][s] and W[i][s] = V_s Phi[i][s], rows i < nb_pad, K = ldk.
 int launch_expand_fp64(const uint32_t* desc, int nb, int nb_pad, int nm, const double* q, const double* v,
                        int64_t n, int64_t ldk, double* phi, double* w, cudaStream_t s);
+
+struct TileMap;
+// Gradient (Stein) estimator, FP64: partial[split][tile] += sum over this split's
+// samples of the estimate of every upper element (q, vq: [k][nm], v: [k]).
+int launch_stein_fp64(const uint32_t* desc, int nb, int nm, const double* q, const double* v, const double* vq,
+                      int64_t k, const TileMap& tm, int nsplit, double* partial, cudaStream_t s);
 
 struct TileMap {
     int tile;          // tile edge (64 FP64, 128 tensor-core)

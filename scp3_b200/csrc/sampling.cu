@@ -27,24 +27,33 @@ struct WarpSlot {
     T* crd;         // 9nw
     T* ms;          // 3nw
     T* ttm;         // TTM3-F scratch
+    double* g;      // 9nw gradient (gradient path)
+    double* gm;     // 3nw forces on the M sites
 };
 
 template <typename T>
-__host__ __device__ inline size_t slot_bytes(int pes, int nm0, int nw)
+__host__ __device__ inline size_t slot_bytes(int pes, int nm0, int nw, bool grad = false)
 {
     size_t b = sizeof(double) * (size_t)((nm0 + 1) & ~1) + sizeof(T) * (size_t)(12 * nw);
     if (pes == SCP3GPU_PES_TTM3F) b += sizeof(T) * ttm::scratch_elems(nw);
+    b = (b + 7) & ~(size_t)7;
+    if (grad) b += sizeof(double) * (size_t)(12 * nw);
     return (b + 15) & ~(size_t)15;
 }
 
 template <typename T>
-__device__ inline WarpSlot<T> warp_slot(char* base, int pes, int nm0, int nw)
+__device__ inline WarpSlot<T> warp_slot(char* base, int pes, int nm0, int nw, bool grad = false)
 {
     WarpSlot<T> s;
     s.q = reinterpret_cast<double*>(base);
     s.crd = reinterpret_cast<T*>(s.q + ((nm0 + 1) & ~1));
     s.ms = s.crd + 9 * nw;
     s.ttm = s.ms + 3 * nw;
+    size_t off = sizeof(double) * (size_t)((nm0 + 1) & ~1) + sizeof(T) * (size_t)(12 * nw);
+    if (pes == SCP3GPU_PES_TTM3F) off += sizeof(T) * ttm::scratch_elems(nw);
+    off = (off + 7) & ~(size_t)7;
+    s.g = grad ? reinterpret_cast<double*>(base + off) : nullptr;
+    s.gm = grad ? s.g + 9 * nw : nullptr;
     return s;
 }
 
@@ -96,7 +105,8 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
         __syncthreads();
     }
     char* slots = smem + (mua_in_smem ? (mua_b + 15) / 16 * 16 : 0);
-    WarpSlot<T> w = warp_slot<T>(slots + wib * slot_bytes<T>(PES, nm0, nw), PES, nm0, nw);
+    const bool grad = a.vq != nullptr;
+    WarpSlot<T> w = warp_slot<T>(slots + wib * slot_bytes<T>(PES, nm0, nw, grad), PES, nm0, nw, grad);
     // Each warp takes runs of kRun consecutive samples: the Sobol state of the
     // first is formed from the Gray code of its index, the next ones by one XOR
     // per dimension (index k differs from k-1 in direction number ctz(k)).
@@ -113,6 +123,7 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
             for (int m = lane; m < a.nm; m += 32) {
                 if (a.q64) a.q64[s * a.nm + m] = 0.0;
                 if (a.q32) a.q32[s * a.nm + m] = 0.0f;
+                if (a.vq) a.vq[s * a.nm + m] = 0.0;
             }
             continue;
         }
@@ -161,7 +172,26 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
         // 3. V in hartree, anharmonic residual   (SCP3.cpp:219-223)
         int iters = 0;
         double V = 0.0;
-        if (!a.skip_pes) {
+        if constexpr (PES == SCP3GPU_PES_QTIP4PF && sizeof(T) == 8) {
+            if (grad) {
+                // gradient path (SCP3.cpp:209-216): V and dV/dr, then
+                // dV_anh/dq = MUa^T (bohr dV/dr / autokcal) - omega % q, selected modes
+                const double e = qt::energy_grad_warp(reinterpret_cast<const double*>(w.crd),
+                                                      reinterpret_cast<double*>(w.ms), w.g, w.gm, nw, a.tasks,
+                                                      a.ntasks, lane);
+                double h = 0.0;
+                for (int d = lane; d < nm0; d += 32) h += w.q[d] * (__ldg(a.omega + d) * w.q[d]);
+                h = warp_sum(h);
+                V = e / kAuToKcalPerMol - 0.5 * h;
+                for (int m = lane; m < a.nm; m += 32) {
+                    const int k = __ldg(a.modes + m);
+                    double acc = 0.0;
+                    for (int c = 0; c < N3; c++) acc += MUa[(size_t)k * N3 + c] * w.g[c];
+                    a.vq[s * a.nm + m] = acc * (kBohr / kAuToKcalPerMol) - __ldg(a.omega + k) * w.q[k];
+                }
+            }
+        }
+        if (!a.skip_pes && !grad) {
             const double e = potential<PES, T>(w, nw, a.tasks, a.ntasks, lane, &iters);
             double h = 0.0;
             for (int d = lane; d < nm0; d += 32) h += w.q[d] * (__ldg(a.omega + d) * w.q[d]);
@@ -232,7 +262,8 @@ template <int PES, typename T>
 int launch_samples_t(const SampleArgs& a, cudaStream_t s)
 {
     const size_t mua_b = sizeof(double) * (size_t)9 * a.nw * a.nm0;
-    const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw) + (mua_b <= kMuaSmemMax ? (mua_b + 15) / 16 * 16 : 0);
+    const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw, a.vq != nullptr) +
+                      (mua_b <= kMuaSmemMax ? (mua_b + 15) / 16 * 16 : 0);
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_kernel<PES, T>,
                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     samples_kernel<PES, T><<<grid_for((a.n + kRun - 1) / kRun), kWarpsPerBlock * 32, sm, s>>>(a);
@@ -315,6 +346,8 @@ int ttm_init_device()
 int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s)
 {
     if (a.n <= 0) return SCP3GPU_OK;
+    if (a.vq && (fp32 || pes != SCP3GPU_PES_QTIP4PF))
+        return fail(SCP3GPU_ERR_UNSUPPORTED, "gradient path: qTIP4P/f with an FP64 potential only");
     if (pes == SCP3GPU_PES_QTIP4PF)
         return fp32 ? launch_samples_t<SCP3GPU_PES_QTIP4PF, float>(a, s)
                     : launch_samples_t<SCP3GPU_PES_QTIP4PF, double>(a, s);

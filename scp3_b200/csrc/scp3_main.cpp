@@ -9,9 +9,9 @@
 // on the GPU: E0_sd.dat every 2^14 samples (SCP3.cpp:234-250), sM_%07d.h5 every
 // 2^17 (SCP3.cpp:252-255), omega0.dat at start (SCP3.cpp:300-302).
 //
-// Only the -G estimator (ScaledMatrixElements.cpp:951-971) runs on the GPU; the
-// gradient estimator of the reference's default path is not built, so -G is
-// required.
+// Without -G the reference's default gradient estimator runs
+// (ScaledMatrixElements.cpp:102-725): on the GPU in FP64 with the qTIP4P/f
+// gradient; other potentials or precisions need -G (ScaledMatrixElements.cpp:951-971).
 #include <getopt.h>
 
 #include <cmath>
@@ -245,8 +245,8 @@ void check(int rc, const char* what)
 int main(int argc, char** argv)
 {
     Options o = parse(argc, argv);
-    if (o.use_gradient)
-        die("The gradient estimator (the reference's default path) is not built on the GPU; run with -G.");
+    if (o.use_gradient && (o.pes != "qtip4pf" || o.precision != "fp64"))
+        die("The gradient estimator runs with -p qtip4pf in FP64; run other potentials or precisions with -G.");
     vector<double> mass, x0, H;
     load_input(o.input, mass, x0, H);
     ohhohh(mass, x0, H);
@@ -289,6 +289,7 @@ int main(int argc, char** argv)
     c.scramble = o.scramble ? SCP3GPU_SOBOL_SCRAMBLED : SCP3GPU_SOBOL_REFERENCE;
     c.scramble_seed = o.scramble_seed;
     c.device = o.device;
+    c.estimator = o.use_gradient ? SCP3GPU_ESTIMATOR_GRADIENT : SCP3GPU_ESTIMATOR_DIRECT;
     scp3gpu_hbuild* h = nullptr;
     check(scp3gpu_hbuild_create(&c, &h), "create");
     const int64_t nb = scp3gpu_hbuild_basis_size(h);
