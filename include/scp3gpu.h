@@ -69,6 +69,11 @@ int scp3gpu_version(void);
  * TTM3-F geometry hit the 500-sweep cap (its energy is still written). */
 int scp3gpu_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters);
 
+/* Energies and gradients (kcal/mol/Angstrom, n x 9*nw) -- h2o::PES::operator()(nw,
+ * crd, grad) (PES.h:14-22), qtip4pf.cpp:252-397.  qTIP4P/f; TTM3-F returns
+ * SCP3GPU_ERR_UNSUPPORTED. */
+int scp3gpu_pes_energy_grad(int pes, int nw, int64_t n, const double* crd, double* E, double* grad);
+
 /* Device-buffer variant (crd_dev, E_dev on `device`), ordered on the legacy
  * default stream of that device. */
 int scp3gpu_pes_energy_dev(int pes, int nw, int64_t n, const double* crd_dev, double* E_dev, int device);

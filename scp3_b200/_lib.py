@@ -18,7 +18,7 @@ ESTIMATOR_DIRECT, ESTIMATOR_GRADIENT = 0, 1
 
 # every symbol include/scp3gpu.h declares (checked by the CPU tests)
 EXPORTS = [
-    "scp3gpu_last_error", "scp3gpu_version", "scp3gpu_pes_energy", "scp3gpu_pes_energy_dev",
+    "scp3gpu_last_error", "scp3gpu_version", "scp3gpu_pes_energy", "scp3gpu_pes_energy_dev", "scp3gpu_pes_energy_grad",
     "scp3gpu_sobol_std_normal", "scp3gpu_basis_size", "scp3gpu_sub_basis_size", "scp3gpu_hbuild_create",
     "scp3gpu_hbuild_destroy", "scp3gpu_hbuild_reset", "scp3gpu_hbuild_basis_size", "scp3gpu_hbuild_stream",
     "scp3gpu_hbuild_accumulate", "scp3gpu_hbuild_accumulate_normals", "scp3gpu_hbuild_add_epot",
@@ -74,6 +74,7 @@ def lib():
     i64 = ctypes.c_int64
     L.scp3gpu_last_error.restype = ctypes.c_char_p
     L.scp3gpu_pes_energy.argtypes = [ctypes.c_int, ctypes.c_int, i64, dp, dp, ip]
+    L.scp3gpu_pes_energy_grad.argtypes = [ctypes.c_int, ctypes.c_int, i64, dp, dp, dp]
     L.scp3gpu_pes_energy_dev.argtypes = [ctypes.c_int, ctypes.c_int, i64, vp, vp, ctypes.c_int]
     L.scp3gpu_sobol_std_normal.argtypes = [ctypes.c_int, i64, i64, ctypes.c_int, ctypes.c_uint64, dp]
     L.scp3gpu_basis_size.restype = i64

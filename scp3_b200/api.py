@@ -55,10 +55,28 @@ class PES:
             _lib.check(rc)
         return (E, it) if return_iters else E
 
-    def __call__(self, nw, crd):
+    def energies_grad(self, crd):
+        """Energies (kcal/mol) and gradients (kcal/mol/A, n x 9nw) of a batch of
+        geometries (qTIP4P/f)."""
+        crd = np.ascontiguousarray(np.atleast_2d(crd), dtype=np.float64)
+        n, w = crd.shape
+        if w % 9:
+            raise ValueError("a geometry has 9*nw coordinates")
+        E = np.zeros(n)
+        G = np.zeros((n, w))
+        _lib.check(_lib.lib().scp3gpu_pes_energy_grad(self.pes_id, w // 9, n, _p(crd), _p(E), _p(G)))
+        return E, G
+
+    def __call__(self, nw, crd, grad=None):
+        """h2o::PES::operator()(nw, crd[, grad]) (PES.h:14-22): the energy; with a
+        9nw array `grad`, the gradient is written into it."""
         crd = np.asarray(crd, dtype=np.float64).reshape(1, -1)
         if crd.shape[1] != 9 * nw:
             raise ValueError("crd must hold 9*nw coordinates")
+        if grad is not None:
+            E, G = self.energies_grad(crd)
+            grad[:] = G[0]
+            return float(E[0])
         return float(self.energies(crd)[0])
 
 

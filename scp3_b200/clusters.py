@@ -201,3 +201,41 @@ def hessian(energy, x_angstrom, mass, h=1e-3):
     P = np.eye(n) - T @ T.T
     H = P @ H @ P
     return 0.5 * (H + H.T), xb
+
+
+def relax_grad(energy_grad, x, gtol=1e-7, maxiter=5000):
+    """Minimisation with analytic gradients: ``energy_grad(X) -> (E, G)`` for a
+    batch X (n x 9nw, Angstrom; kcal/mol, kcal/mol/A).  L-BFGS (scipy), then the
+    same |g|max test as relax().  Returns (x, E, |g|max, iterations)."""
+    from scipy.optimize import minimize
+    x = np.array(x, dtype=np.float64)
+
+    def fg(v):
+        E, G = energy_grad(v[None, :])
+        return float(E[0]), G[0]
+
+    res = minimize(fg, x, jac=True, method="L-BFGS-B",
+                   options=dict(maxiter=maxiter, gtol=gtol, ftol=1e-15, maxcor=50))
+    e, g = fg(res.x)
+    return res.x, e, float(np.abs(g).max()), int(res.nit)
+
+
+def hessian_grad(energy_grad, x_angstrom, mass, h=1e-4):
+    """As hessian(), from central differences of analytic gradients (step h bohr):
+    one batch of 2n gradient evaluations."""
+    xb = np.asarray(x_angstrom, dtype=np.float64) / C.bohr
+    n = xb.size
+    X = np.repeat(xb[None, :], 2 * n, axis=0)
+    idx = np.arange(n)
+    X[2 * idx, idx] += h
+    X[2 * idx + 1, idx] -= h
+    _, G = energy_grad(X * C.bohr)
+    G = G * C.bohr / C.autokcalpmol                  # hartree / bohr
+    K = (G[0::2] - G[1::2]) / (2 * h)
+    K = 0.5 * (K + K.T)
+    ism = 1.0 / np.sqrt(mass)
+    H = K * ism[:, None] * ism[None, :]
+    T = _transrot_basis(xb, mass)
+    P = np.eye(n) - T @ T.T
+    H = P @ H @ P
+    return 0.5 * (H + H.T), xb

@@ -235,7 +235,7 @@ int zero_sums(scp3gpu_batch* b)
 // the fastest.  The trial sums are discarded afterwards.
 int autotune(scp3gpu_batch* b)
 {
-    int rc = stage_args(b, 0, b->chunk, 1);
+    int rc = stage_args(b, 1ll << 30, b->chunk, 1);   // trial points from the reference's default skip
     if (rc) return rc;
     // one direct pass prepares buffer 0 (and sets the kernels' attributes before any capture)
     const int keep_split = b->nsplit, keep_ctas = b->ctas;
@@ -483,7 +483,7 @@ int scp3gpu_batch_create(const scp3gpu_config* cfgs, int ncl, int64_t chunk, int
         if ((rc = autotune(b))) return bail(rc);
     } else {
         // set the kernels' attributes outside any capture with one direct pass, then clear its sums
-        if ((rc = stage_args(b, 0, b->chunk, 1)) || (rc = enqueue(b, 1, b->chunk)) || (rc = zero_sums(b)))
+        if ((rc = stage_args(b, 1ll << 30, b->chunk, 1)) || (rc = enqueue(b, 1, b->chunk)) || (rc = zero_sums(b)))
             return bail(rc);
     }
     if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bail(fail(SCP3GPU_ERR_CUDA, "batch create sync failed"));

@@ -335,6 +335,37 @@ int scp3gpu_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E,
     return capped ? fail(SCP3GPU_ERR_NOT_CONVERGED, "TTM3-F dipoles hit the iteration cap") : SCP3GPU_OK;
 }
 
+int scp3gpu_pes_energy_grad(int pes, int nw, int64_t n, const double* crd, double* E, double* grad)
+{
+    (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
+    if (pes == SCP3GPU_PES_TTM3F)
+        return fail(SCP3GPU_ERR_UNSUPPORTED, "pes_energy_grad: the TTM3-F gradient is not built (qTIP4P/f only)");
+    if (pes != SCP3GPU_PES_QTIP4PF) return fail(SCP3GPU_ERR_ARG, "unknown potential");
+    if (nw < 1 || nw > kMaxWaters || n < 0 || (n > 0 && (!crd || !E || !grad)))
+        return fail(SCP3GPU_ERR_ARG, "pes_energy_grad: bad nw, n or pointer");
+    if (n == 0) return SCP3GPU_OK;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int rc = check_device(dev);
+    if (rc) return rc;
+    std::vector<uint32_t> t = pair_tasks(nw);
+    uint32_t* td = nullptr;
+    double *cd = nullptr, *ed = nullptr, *gd = nullptr;
+    if ((rc = upload(&td, t.data(), t.size())) || (rc = upload(&cd, crd, (size_t)n * 9 * nw)) ||
+        (rc = dalloc(&ed, (size_t)n)) || (rc = dalloc(&gd, (size_t)n * 9 * nw))) {
+        cudaFree(td), cudaFree(cd), cudaFree(ed), cudaFree(gd);
+        return rc;
+    }
+    rc = launch_pes_energy_grad(nw, n, cd, ed, gd, td, (int)t.size(), 0);
+    if (!rc) {
+        cudaError_t e = cudaMemcpy(E, ed, sizeof(double) * n, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(grad, gd, sizeof(double) * n * 9 * nw, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = cuda_fail(e, "pes_energy_grad copy-out");
+    }
+    cudaFree(td), cudaFree(cd), cudaFree(ed), cudaFree(gd);
+    return rc;
+}
+
 int scp3gpu_sobol_std_normal(int dims, int64_t index0, int64_t n, int scramble, uint64_t seed, double* out)
 {
     (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's

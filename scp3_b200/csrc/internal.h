@@ -133,6 +133,10 @@ int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s);
 int launch_samples_batch(int pes, bool fp32, const SampleArgs* args_host, const SampleArgs* args_dev, int ncl,
                          int64_t n, cudaStream_t s);
 
+// qTIP4P/f energies (kcal/mol) and gradients (kcal/mol/A, [n][9nw]) of n geometries
+int launch_pes_energy_grad(int nw, int64_t n, const double* crd, double* E, double* G, const uint32_t* tasks,
+                           int ntasks, cudaStream_t s);
+
 int launch_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters,
                       const uint32_t* tasks, int ntasks, cudaStream_t s);
 

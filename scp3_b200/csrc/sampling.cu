@@ -236,6 +236,27 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     }
 }
 
+// qTIP4P/f energy and gradient of n geometries, one warp each (the E+g operator,
+// qtip4pf.cpp:252-397).
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    pes_energy_grad_kernel(int nw, int64_t n, const double* __restrict__ crd, double* __restrict__ E,
+                           double* __restrict__ G, const uint32_t* __restrict__ tasks, int ntasks)
+{
+    extern __shared__ __align__(16) double gsm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double* x = gsm + (size_t)wib * 24 * nw;
+    double *ms = x + 9 * nw, *g = ms + 3 * nw, *gm = g + 9 * nw;
+    const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
+    for (int64_t k = (int64_t)blockIdx.x * kWarpsPerBlock + wib; k < n; k += nwarps) {
+        for (int c = lane; c < 9 * nw; c += 32) x[c] = crd[k * 9 * nw + c];
+        __syncwarp();
+        const double e = qt::energy_grad_warp(x, ms, g, gm, nw, tasks, ntasks, lane);
+        if (lane == 0) E[k] = e;
+        for (int c = lane; c < 9 * nw; c += 32) G[k * 9 * nw + c] = g[c];
+        __syncwarp();
+    }
+}
+
 __global__ void std_normal_kernel(int dims, int64_t index0, int64_t n, const int64_t* __restrict__ vdir,
                                   const uint64_t* __restrict__ shift, double* __restrict__ out)
 {
@@ -355,6 +376,18 @@ int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s)
         return fp32 ? launch_samples_t<SCP3GPU_PES_TTM3F, float>(a, s)
                     : launch_samples_t<SCP3GPU_PES_TTM3F, double>(a, s);
     return fail(SCP3GPU_ERR_ARG, "unknown potential id");
+}
+
+int launch_pes_energy_grad(int nw, int64_t n, const double* crd, double* E, double* G, const uint32_t* tasks,
+                           int ntasks, cudaStream_t s)
+{
+    if (n <= 0) return SCP3GPU_OK;
+    const size_t sm = sizeof(double) * kWarpsPerBlock * 24 * (size_t)nw;
+    if (sm > 48 * 1024)
+        SCP3_CUDA(cudaFuncSetAttribute(pes_energy_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    pes_energy_grad_kernel<<<grid_for(n), kWarpsPerBlock * 32, sm, s>>>(nw, n, crd, E, G, tasks, ntasks);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
 }
 
 int launch_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters, const uint32_t* tasks,

@@ -41,10 +41,16 @@ def build_input(name, path=None, energy=None):
     from .api import PES
     x = _start(name)
     nw = x.size // 9
-    en = energy or PES(_pes_of(name)).energies
-    xr, e, g, it = clusters.relax(en, x)
     mass = np.tile(np.repeat([C.Omass, C.Hmass, C.Hmass], 3), nw)
-    H, x0 = clusters.hessian(en, xr, mass)
+    if energy is None and _pes_of(name) == "qtip4pf" and name.startswith("cluster_"):
+        # analytic gradients of the GPU potential: L-BFGS and a gradient-difference Hessian
+        eg = PES("qtip4pf").energies_grad
+        xr, e, g, it = clusters.relax_grad(eg, x)
+        H, x0 = clusters.hessian_grad(eg, xr, mass)
+    else:
+        en = energy or PES(_pes_of(name)).energies
+        xr, e, g, it = clusters.relax(en, x)
+        H, x0 = clusters.hessian(en, xr, mass)
     species = ["O", "H", "H"] * nw
     path = path or os.path.join(DATA, name + ".dat")
     os.makedirs(os.path.dirname(path), exist_ok=True)

@@ -77,10 +77,11 @@ def test_batch_graph_equals_direct_and_calls_compose(scp3):
     g = scp3.Batch(cl, precision="bf16x3", chunk=4096, graph=True, autotune=False)
     d = scp3.Batch(cl, precision="bf16x3", chunk=4096, graph=False, autotune=False)
     assert g.shape()[:3] == d.shape()[:3]
-    g.accumulate(0, 3 * 4096)            # one graph of three passes
-    g.accumulate(3 * 4096, 2 * 4096)     # a second graph (two passes) ...
-    g.accumulate(5 * 4096, 2 * 4096)     # ... replayed with new Sobol offsets
-    d.accumulate(0, 7 * 4096)
+    i0 = 1 << 30                         # the reference's skip: point 0 of the unscrambled sequence is u = 0
+    g.accumulate(i0, 3 * 4096)           # one graph of three passes
+    g.accumulate(i0 + 3 * 4096, 2 * 4096)    # a second graph (two passes) ...
+    g.accumulate(i0 + 5 * 4096, 2 * 4096)    # ... replayed with new Sobol offsets
+    d.accumulate(i0, 7 * 4096)
     for i in range(len(cl)):
         A, B = g.read(i, 0), d.read(i, 0)
         assert np.array_equal(A, B), i
@@ -93,9 +94,9 @@ def test_batch_autotuned_shape_is_valid(scp3):
     assert chunk == 16384 and nsplit in (1, 2, 4) and ms > 0
     assert ctas >= 0
     # tuning trials leave no trace in the sums
-    b.accumulate(0, 4096)
+    b.accumulate(7, 4096)
     ref = scp3.Batch(cl, precision="bf16x3", chunk=16384, autotune=False)
-    ref.accumulate(0, 4096)
+    ref.accumulate(7, 4096)
     for i in range(len(cl)):
         A, B = b.read(i, 0), ref.read(i, 0)
         assert np.abs(A - B).max() <= 1e-11 * np.abs(B).max()
@@ -127,10 +128,10 @@ def test_batch_ttm3f(scp3):
     cs = [load_hbuild_case(n) for n in ["dimer_ttm3f", "hexamer_ttm3f"]]
     cl = [_cluster(c) for c in cs]
     b = scp3.Batch(cl, pes="ttm3f", precision="bf16x3", chunk=4096)
-    b.accumulate(0, 4096)
+    b.accumulate(7, 4096)
     for i, d in enumerate(cl):
         hb = _single(scp3, d, "ttm3f", "bf16x3")
-        hb.accumulate(0, 4096)
+        hb.accumulate(7, 4096)
         ref = hb.read(0)
         assert np.abs(b.read(i, 0) - ref).max() <= 1e-11 * np.abs(ref).max()
         assert b.status(i)[0] == 0

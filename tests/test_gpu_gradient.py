@@ -74,3 +74,17 @@ def test_gradient_estimator_limits(scp3, z):
     d = scp3.HBuild(2, z["dimer_x0"], z["dimer_MUa"], z["dimer_omega"])
     with pytest.raises(scp3.SCP3GPUError):
         d.add_epot_grad(np.zeros((4, 12)), np.zeros(4), np.zeros((4, 12)))
+
+
+def test_pes_energy_grad_matches_reference(scp3, z):
+    """h2o::PES::operator()(nw, crd, grad) on the GPU against the reference's
+    qTIP4P/f gradient (qtip4pf.cpp:252-397) on the pes_ref geometries."""
+    p = np.load(os.path.join(GOLDEN, "pes_ref.npz"), allow_pickle=True)
+    pes = scp3.PES("qtip4pf")
+    for x, e_ref, g_ref in zip(p["geoms"], p["e_qtip4pf"], z["pes_geoms_grad"]):
+        x = np.asarray(x, dtype=np.float64)
+        E, G = pes.energies_grad(x[None, :])
+        assert abs(E[0] - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
+        assert np.abs(G[0] - g_ref).max() <= 1e-11 * max(1.0, np.abs(g_ref).max())
+    with pytest.raises(scp3.SCP3GPUError):
+        scp3.PES("ttm3f").energies_grad(np.asarray(p["geoms"][0], dtype=np.float64)[None, :])
