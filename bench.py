@@ -33,6 +33,10 @@ SCRAMBLE_SEED = 0x5C3
 WORKLOAD = "hexamer prism qTIP4P/f, 48 modes, doubles basis Nb=1225, 2^20 scrambled Sobol points per GPU per step"
 METRIC = "Sobol samples/s (hexamer H-build) at <=0.1 cm^-1 on 10 lowest levels vs FP64"
 FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (vector and tensor) nominal; no measured FP64 peak on this pool
+# DRAM bytes (read + write) of one BF16x3 contraction launch of 2^17 samples on the hexamer doubles
+# basis, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum = 859.5 + 51.6 MB); the
+# traffic grows with the samples per launch
+CONTRACT_DRAM_BYTES_PER_SAMPLE = (859.509504e6 + 51.570432e6) / 131072
 
 
 def load_peaks():
@@ -472,9 +476,11 @@ def main():
                 "note": "FP64 DFMA contraction; peak is B200 nominal FP64 (no measured FP64 peak)"}
     else:
         pk = peaks["bf16_tflops"]
+        traffic = CONTRACT_DRAM_BYTES_PER_SAMPLE * samples_per_launch if nb == 1225 else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
-                "traffic": None, "note": "algorithmic Nb(Nb+1) flops/sample; BF16x3 issues 3 tensor products each "
-                                         "(ceiling 1/3); peak " + peak_src}
+                "traffic": traffic, "note": "algorithmic Nb(Nb+1) flops/sample; BF16x3 issues 3 tensor products each "
+                                            "(ceiling 1/3); peak " + peak_src + "; traffic: ncu DRAM bytes per "
+                                            "launch (read + write; operand 5200 B/sample)"}
 
     line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
