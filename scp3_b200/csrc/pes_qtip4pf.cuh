@@ -148,7 +148,7 @@ __device__ __forceinline__ double pair_grad(uint32_t task, const double* crd, co
 
 // Energy (all lanes) and gradient g[9nw] (shared, complete after the call) of
 // the geometry crd; ms[3nw] and gm[3nw] are shared scratch (M sites, their forces).
-__device__ double energy_grad_warp(const double* crd, double* ms, double* g, double* gm, int nw,
+__device__ inline double energy_grad_warp(const double* crd, double* ms, double* g, double* gm, int nw,
                                    const uint32_t* __restrict__ tasks, int ntasks, int lane)
 {
     for (int c = lane; c < 9 * nw; c += 32) g[c] = 0.0;
