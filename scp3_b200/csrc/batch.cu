@@ -66,8 +66,7 @@ struct scp3gpu_batch {
     double* v[kBuffers] = {};
     int* slot_of[kBuffers] = {};
     int* neg[kBuffers] = {};
-    uint16_t *xhi[kBuffers] = {}, *xlo[kBuffers] = {};
-    void *tmap_hi[kBuffers] = {}, *tmap_lo[kBuffers] = {};
+    uint16_t* x[kBuffers] = {};        // the operand (box layout of contract_tc.cu), rows x slots x 2 halves
     tc::ExpandDesc* desc_dev[kBuffers] = {};
     // per-pass sample arguments [pass][cluster]
     SampleArgs* args_dev = nullptr;
@@ -159,12 +158,12 @@ int enqueue(scp3gpu_batch* b, int64_t passes, int64_t last)
                                       b->args_dev + (size_t)p * b->ncl, b->ncl, npad, b->prep);
         if (!rc) rc = tc::launch_partition(b->v[buf], b->chunk, b->slot_of[buf], b->slots, b->neg[buf], b->nflush,
                                            nflush, b->ncl, b->prep);
-        if (!rc) rc = tc::launch_expand(b->desc_dev[buf], b->ncl, round_up(b->max_nb, tc::kTile), b->max_nm, slots, b->slots,
-                                        b->xhi[buf], b->xlo[buf], b->f16, b->prep);
+        if (!rc) rc = tc::launch_expand(b->desc_dev[buf], b->ncl, round_up(b->max_nb, tc::kTile), b->max_nm, slots, b->slots / 64,
+                                        b->x[buf], b->f16, b->prep);
         if (rc) return rc;
         SCP3_CUDA(cudaEventRecord(b->prepared[buf], b->prep));
         SCP3_CUDA(cudaStreamWaitEvent(b->stream, b->prepared[buf], 0));
-        rc = tc::launch_contract(b->tmap_hi[buf], b->tmap_lo[buf], b->items, b->nitems, b->neg[buf], nflush,
+        rc = tc::launch_contract(b->x[buf], b->slots / 64, b->items, b->nitems, b->neg[buf], nflush,
                                  std::min(b->nsplit, nflush), 3, b->f16, b->partial, b->err_flag, b->stream, b->ctas);
         if (rc) return rc;
         SCP3_CUDA(cudaEventRecord(b->contracted[buf], b->stream));
@@ -253,7 +252,7 @@ int autotune(scp3gpu_batch* b)
             float ms_best = 1e30f;
             for (int rep = 0; rep < 3 && rc == 0; rep++) {
                 cudaEventRecord(e0, b->stream);
-                rc = tc::launch_contract(b->tmap_hi[0], b->tmap_lo[0], b->items, b->nitems, b->neg[0], b->nflush, ns, 3,
+                rc = tc::launch_contract(b->x[0], b->slots / 64, b->items, b->nitems, b->neg[0], b->nflush, ns, 3,
                                          b->f16, b->partial, b->err_flag, b->stream, ctas);
                 cudaEventRecord(e1, b->stream);
                 if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(SCP3GPU_ERR_CUDA, "batch: autotune sync");
@@ -331,11 +330,9 @@ int scp3gpu_batch_destroy(scp3gpu_batch* b)
             if (p) cudaFree(p);
     }
     for (int i = 0; i < kBuffers; i++) {
-        void* ptrs[] = {b->q32[i], b->v[i], b->slot_of[i], b->neg[i], b->xhi[i], b->xlo[i], b->desc_dev[i]};
+        void* ptrs[] = {b->q32[i], b->v[i], b->slot_of[i], b->neg[i], b->x[i], b->desc_dev[i]};
         for (void* p : ptrs)
             if (p) cudaFree(p);
-        tc::free_operand_map(b->tmap_hi[i]);
-        tc::free_operand_map(b->tmap_lo[i]);
         if (b->prepared[i]) cudaEventDestroy(b->prepared[i]);
         if (b->contracted[i]) cudaEventDestroy(b->contracted[i]);
     }
@@ -464,10 +461,7 @@ int scp3gpu_batch_create(const scp3gpu_config* cfgs, int ncl, int64_t chunk, int
     for (int i = 0; i < kBuffers; i++) {
         if ((rc = dalloc(&b->q32[i], (size_t)b->chunk * sum_nm)) || (rc = dalloc(&b->v[i], (size_t)b->chunk * ncl)) ||
             (rc = dalloc(&b->slot_of[i], (size_t)b->slots * ncl)) || (rc = dalloc(&b->neg[i], (size_t)b->nflush * ncl)) ||
-            (rc = dalloc(&b->xhi[i], (size_t)b->rows * b->slots)) || (rc = dalloc(&b->xlo[i], (size_t)b->rows * b->slots)))
-            return bail(rc);
-        if ((rc = tc::encode_operand_map(&b->tmap_hi[i], b->xhi[i], b->slots, b->rows)) ||
-            (rc = tc::encode_operand_map(&b->tmap_lo[i], b->xlo[i], b->slots, b->rows)))
+            (rc = dalloc(&b->x[i], (size_t)2 * b->rows * b->slots)))
             return bail(rc);
         std::vector<tc::ExpandDesc> d(ncl);
         for (int c = 0; c < ncl; c++) {

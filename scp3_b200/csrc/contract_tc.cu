@@ -26,15 +26,19 @@
 // accumulator put ~0.45 cm^-1 into the levels, 1024-slot runs in split
 // accumulators ~0.08, 512-slot runs ~0.06 (BF16) / 0.04 (FP16 halves).
 //
-// Warp roles (320 threads): warp 0 lane 0 issues the TMA loads (SWIZZLE_128B,
-// 64 K-slots x 128 rows per box), warp 1 owns TMEM (512 columns) and lane 0
+// Operand layout.  The expansion writes X in boxes of 128 rows x 64 K slots
+// (16 KB), each already in the 128-byte-swizzled order the MMA descriptors
+// read (16-byte chunk c of row r at chunk c ^ (r & 7)), the hi and lo boxes of
+// a (row block, k-block) next to each other: [row block][k-block][hi, lo][16 KB].
+// A stage is then two contiguous 32 KB bulk copies (A and B), and the
+// expansion's stores are sequential.
+//
+// Warp roles (320 threads): warp 0 lane 0 issues the bulk copies, warp 1 owns TMEM (512 columns) and lane 0
 // issues the MMAs and commits, warps 2..9 drain the accumulators.  Every mbarrier wait is
 // bounded (4 s of %globaltimer); on expiry the CTA records an error, stops
 // issuing, waits (bounded) for its own loads and MMAs, frees TMEM and returns.
-#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cstring>
@@ -124,13 +128,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
     }
 }
 
-__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y)
+// 1-D bulk copy global -> this CTA's shared memory, completing on an mbarrier
+// (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            smem_u32(dst)),
-        "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 // K-major, SWIZZLE_128B shared-memory matrix descriptor: start address >> 4,
@@ -182,7 +187,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
 // unit overlap the FP64 write-back of the previous one.  Pipeline counters
 // (stage, phase, accumulator use) run on across units.
 __global__ void __launch_bounds__(kThreads, 1)
-    contract_bf16x3_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
+    contract_bf16x3_kernel(const uint16_t* __restrict__ xop, long long nkb,
                            const WorkItem* __restrict__ items, const int* __restrict__ neg_group, int nflush,
                            int nitems, int nsplit, int products, int f16, double* __restrict__ partial,
                            int* __restrict__ err_flag)
@@ -248,13 +253,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                         uint8_t* st = smem + stage * kStageBytes;
                         mbar_expect_tx(full + stage, bytes);
-                        const int x = f * kSlotsPerFlush + kb * kBK;
-                        tma_load_2d(&map_hi, full + stage, st, x, wi.arow);
-                        tma_load_2d(&map_lo, full + stage, st + kTileBytes, x, wi.arow);
-                        if (!diag) {
-                            tma_load_2d(&map_hi, full + stage, st + 2 * kTileBytes, x, wi.brow);
-                            tma_load_2d(&map_lo, full + stage, st + 3 * kTileBytes, x, wi.brow);
-                        }
+                        const long long kbi = (long long)f * kKBlocks + kb;
+                        bulk_load(st, xop + ((wi.arow / kTile) * nkb + kbi) * (2 * kTile * kBK), 2 * kTileBytes,
+                                  full + stage);
+                        if (!diag)
+                            bulk_load(st + 2 * kTileBytes, xop + ((wi.brow / kTile) * nkb + kbi) * (2 * kTile * kBK),
+                                      2 * kTileBytes, full + stage);
                         issued[stage] = 1;
                         issued_phase[stage] = phase;
                         if (++stage == kStages) {
@@ -438,13 +442,13 @@ __global__ void __launch_bounds__(1024) partition_kernel(const double* __restric
 }
 
 // Expansion into the split operand X = sqrt|V| Phi (hi + lo halves).  A block
-// covers 64 K slots and up to 256 basis rows: it first tabulates, per slot,
+// covers 64 K slots and up to 2048 basis rows: it first tabulates, per slot,
 // [1, h1(q_m), h2(q_m), h3(q_m)] for all modes in shared memory, then every basis
 // value is the product of three table entries (basis_factor_table).  Thread
 // (g, r) handles slots 4g..4g+3 of rows r, r+8, ...: one 16-byte table read per
 // factor and 8-byte stores, so the 16 threads of a row write 128 contiguous
 // bytes per half.
-constexpr int kExpSlots = 64, kExpRows = 1024, kExpThreads = 128;
+constexpr int kExpSlots = 64, kExpRows = 2048, kExpThreads = 128;
 
 template <bool F16>
 __device__ __forceinline__ void split4(float4 x, uint2& hi, uint2& lo)
@@ -468,9 +472,8 @@ __device__ __forceinline__ void split4(float4 x, uint2& hi, uint2& lo)
 }
 
 template <bool F16>
-__global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandDesc* __restrict__ descs, int64_t ldk,
-                                                                    uint16_t* __restrict__ xhi_all,
-                                                                    uint16_t* __restrict__ xlo_all)
+__global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandDesc* __restrict__ descs, int64_t nkb,
+                                                                    uint16_t* __restrict__ xop)
 {
     const ExpandDesc dsc = descs[blockIdx.z];        // one cluster of a batch per z
     if ((int)blockIdx.y * kExpRows >= dsc.nb_pad) return;
@@ -479,8 +482,6 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandD
     const float* __restrict__ q = dsc.q;
     const double* __restrict__ v = dsc.v;
     const int* __restrict__ sample_of_slot = dsc.slot_of;
-    uint16_t* __restrict__ xhi = xhi_all + (size_t)dsc.row0 * ldk;
-    uint16_t* __restrict__ xlo = xlo_all + (size_t)dsc.row0 * ldk;
     extern __shared__ __align__(16) float tab[];      // [3nm+1][kExpSlots], then sqrt|V| [kExpSlots]
     float* sv = tab + (size_t)(3 * nm + 1) * kExpSlots;
     const int t = threadIdx.x;
@@ -515,20 +516,36 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandD
     const int g = t & 15, rl = t >> 4;
     const float4 w = reinterpret_cast<const float4*>(sv)[g];
     const int r0 = blockIdx.y * kExpRows, r1 = min(r0 + kExpRows, nb_pad);
-    for (int r = r0 + rl; r < r1; r += kExpThreads / 16) {
-        uint2 hi = make_uint2(0, 0), lo = make_uint2(0, 0);
-        if (r < nb) {
-            const uint32_t d = __ldg(factors + r);
-            const float4 A = reinterpret_cast<const float4*>(tab + (d & 1023u) * kExpSlots)[g];
-            const float4 B = reinterpret_cast<const float4*>(tab + ((d >> 10) & 1023u) * kExpSlots)[g];
-            const float4 C = reinterpret_cast<const float4*>(tab + (d >> 20) * kExpSlots)[g];
-            const float4 x = make_float4(w.x * (A.x * B.x * C.x), w.y * (A.y * B.y * C.y), w.z * (A.z * B.z * C.z),
-                                         w.w * (A.w * B.w * C.w));
-            split4<F16>(x, hi, lo);
+    // four rows per trip, their descriptors loaded first so the loads overlap
+    constexpr int kStep = kExpThreads / 16;
+    constexpr uint32_t kNone = 0xffffffffu;      // rows beyond nb (zero padding); real factors < 2^30
+    for (int r = r0 + rl; r < r1; r += 4 * kStep) {
+        uint32_t d[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int rr = r + u * kStep;
+            d[u] = (rr < nb && rr < r1) ? __ldg(factors + rr) : kNone;
         }
-        const size_t off = (size_t)r * ldk + slot0 + 4 * g;
-        *reinterpret_cast<uint2*>(xhi + off) = hi;
-        *reinterpret_cast<uint2*>(xlo + off) = lo;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int rr = r + u * kStep;
+            if (rr >= r1) break;
+            uint2 hi = make_uint2(0, 0), lo = make_uint2(0, 0);
+            if (d[u] != kNone) {
+                const float4 A = reinterpret_cast<const float4*>(tab + (d[u] & 1023u) * kExpSlots)[g];
+                const float4 B = reinterpret_cast<const float4*>(tab + ((d[u] >> 10) & 1023u) * kExpSlots)[g];
+                const float4 C = reinterpret_cast<const float4*>(tab + (d[u] >> 20) * kExpSlots)[g];
+                const float4 x = make_float4(w.x * (A.x * B.x * C.x), w.y * (A.y * B.y * C.y),
+                                             w.z * (A.z * B.z * C.z), w.w * (A.w * B.w * C.w));
+                split4<F16>(x, hi, lo);
+            }
+            // box (row block, k-block blockIdx.x), swizzled: 16-byte chunk g/2 of row rin at (g/2) ^ (rin & 7)
+            const int row = dsc.row0 + rr, rin = row & (kTile - 1);
+            uint16_t* box = xop + ((size_t)(row / kTile) * nkb + blockIdx.x) * (2 * kTile * kExpSlots);
+            const int off = rin * kExpSlots + (((g >> 1) ^ (rin & 7)) << 3) + ((g & 1) << 2);
+            *reinterpret_cast<uint2*>(box + off) = hi;
+            *reinterpret_cast<uint2*>(box + kTile * kExpSlots + off) = lo;
+        }
     }
 }
 
@@ -549,42 +566,6 @@ __global__ void unpack_tc_kernel(const double* __restrict__ partial, const int* 
     val = val / divisor;
     if (diag && i == j) val = (val + diag[i]) + zpe;
     M[(size_t)j * ld + i] = val;
-}
-
-PFN_cuTensorMapEncodeTiled_v12000 get_encode()
-{
-    static std::mutex mu;
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!fn) {
-        cudaDriverEntryPointQueryResult q;
-        void* p = nullptr;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-    }
-    return fn;
-}
-
-int encode_map(void** out, void* base, int64_t slots, int rows)
-// (the 16-bit element type of the map does not matter to the copy: BF16 and FP16 share size and swizzle)
-{
-    auto enc = get_encode();
-    if (!enc) return fail(SCP3GPU_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
-    CUtensorMap* m = new CUtensorMap;
-    cuuint64_t dims[2] = {(cuuint64_t)slots, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)slots * 2};
-    cuuint32_t box[2] = {kBK, kTile};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) {
-        delete m;
-        return fail(SCP3GPU_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    }
-    *out = m;
-    return SCP3GPU_OK;
 }
 
 void record(std::vector<cudaEvent_t>* pev, std::vector<int>* pkind, int kind, cudaStream_t s)
@@ -634,8 +615,7 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
                     t.push_back(w);
                 }
     for (int b = 0; b < 2; b++) {
-        SCP3_CUDA(cudaMalloc(&p.xhi[b], sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
-        SCP3_CUDA(cudaMalloc(&p.xlo[b], sizeof(uint16_t) * (size_t)p.nb_pad * p.slots));
+        SCP3_CUDA(cudaMalloc(&p.x[b], sizeof(uint16_t) * 2 * (size_t)p.nb_pad * p.slots));
         SCP3_CUDA(cudaMalloc(&p.slot_of[b], sizeof(int) * (size_t)p.slots));
         SCP3_CUDA(cudaMalloc(&p.group_meta[b], sizeof(int) * nflush));
     }
@@ -650,25 +630,16 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
     SCP3_CUDA(cudaMalloc(&p.partial, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kTile));
     SCP3_CUDA(cudaMalloc(&p.err_flag, sizeof(int)));
     SCP3_CUDA(cudaMemset(p.err_flag, 0, sizeof(int)));
-    for (int b = 0; b < 2; b++) {
-        int rc = encode_map(&p.tmap_hi[b], p.xhi[b], p.slots, p.nb_pad);
-        if (!rc) rc = encode_map(&p.tmap_lo[b], p.xlo[b], p.slots, p.nb_pad);
-        if (rc) return rc;
-    }
     SCP3_CUDA(cudaFuncSetAttribute(contract_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
     return SCP3GPU_OK;
 }
 
 void destroy(Plan& p)
 {
-    void* ptrs[] = {p.xhi[0], p.xhi[1], p.xlo[0], p.xlo[1], p.slot_of[0], p.slot_of[1], p.group_meta[0],
+    void* ptrs[] = {p.x[0], p.x[1], p.slot_of[0], p.slot_of[1], p.group_meta[0],
                     p.group_meta[1], p.tiles, p.tile_index, p.factors, p.partial, p.err_flag, p.desc_dev};
     for (void* q : ptrs)
         if (q) cudaFree(q);
-    for (int b = 0; b < 2; b++) {
-        delete static_cast<CUtensorMap*>(p.tmap_hi[b]);
-        delete static_cast<CUtensorMap*>(p.tmap_lo[b]);
-    }
     p = Plan{};
 }
 
@@ -693,30 +664,27 @@ int launch_partition(const double* v, int64_t v_stride, int* slot_of, int64_t sl
     return SCP3GPU_OK;
 }
 
-int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t ldk,
-                  uint16_t* xhi, uint16_t* xlo, bool f16, cudaStream_t s)
+int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t nkb,
+                  uint16_t* x, bool f16, cudaStream_t s)
 {
     const size_t sm = sizeof(float) * (size_t)(3 * max_nm + 2) * kExpSlots;
     auto kern = f16 ? expand_split_kernel<true> : expand_split_kernel<false>;
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     dim3 eg((unsigned)(slots / kExpSlots), (unsigned)((max_nb_pad + kExpRows - 1) / kExpRows), (unsigned)nclusters);
-    kern<<<eg, kExpThreads, sm, s>>>(descs_dev, ldk, xhi, xlo);
+    kern<<<eg, kExpThreads, sm, s>>>(descs_dev, nkb, x);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }
 
-int launch_contract(const void* map_hi, const void* map_lo, const WorkItem* items, int nitems, const int* neg,
-                    int nflush, int nsplit, int products, bool f16, double* partial, int* err_flag, cudaStream_t s,
-                    int max_ctas)
+int launch_contract(const uint16_t* x, int64_t nkb, const WorkItem* items, int nitems, const int* neg, int nflush,
+                    int nsplit, int products, bool f16, double* partial, int* err_flag, cudaStream_t s, int max_ctas)
 {
     if (nitems <= 0 || nsplit <= 0) return SCP3GPU_OK;
     SCP3_CUDA(cudaFuncSetAttribute(contract_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
     const int64_t units = (int64_t)nitems * nsplit;
     const int grid = (int)(max_ctas > 0 ? std::min<int64_t>(units, max_ctas) : units);
-    contract_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(*static_cast<const CUtensorMap*>(map_hi),
-                                                              *static_cast<const CUtensorMap*>(map_lo), items, neg,
-                                                              nflush, nitems, nsplit, products, (int)f16, partial,
-                                                              err_flag);
+    contract_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(x, (long long)nkb, items, neg, nflush, nitems, nsplit,
+                                                              products, (int)f16, partial, err_flag);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }
@@ -731,8 +699,6 @@ int launch_unpack(const double* partial, const int* tile_index, int nt, int nite
     return SCP3GPU_OK;
 }
 
-int encode_operand_map(void** out, void* base, int64_t slots, int rows) { return encode_map(out, base, slots, rows); }
-void free_operand_map(void* map) { delete static_cast<CUtensorMap*>(map); }
 
 int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v, int64_t n, cudaStream_t s,
             std::vector<cudaEvent_t>* pev, std::vector<int>* pkind)
@@ -750,7 +716,7 @@ int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v,
         SCP3_CUDA(cudaMemcpyAsync(p.desc_dev + buf, &d, sizeof(d), cudaMemcpyHostToDevice, s));
         p.desc_host[buf] = d;
     }
-    rc = launch_expand(p.desc_dev + buf, 1, p.nb_pad, nm, slots, p.slots, p.xhi[buf], p.xlo[buf], p.f16, s);
+    rc = launch_expand(p.desc_dev + buf, 1, p.nb_pad, nm, slots, p.slots / kBK, p.x[buf], p.f16, s);
     if (rc) return rc;
     record(pev, pkind, 1, s);
     return SCP3GPU_OK;
@@ -761,7 +727,7 @@ int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_
     const int nflush = (int)(n / kFlush);
     record(pev, pkind, 2, s);
     const int nsplit = p.nsplit < nflush ? p.nsplit : nflush;
-    int rc = launch_contract(p.tmap_hi[buf], p.tmap_lo[buf], p.tiles, p.ntiles, p.group_meta[buf], nflush, nsplit,
+    int rc = launch_contract(p.x[buf], p.slots / kBK, p.tiles, p.ntiles, p.group_meta[buf], nflush, nsplit,
                              p.products, p.f16, p.partial, p.err_flag, s);
     if (rc) return rc;
     record(pev, pkind, 2, s);

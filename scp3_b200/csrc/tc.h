@@ -36,8 +36,8 @@ struct Plan {
     int64_t slots = 0;            // K slots per pass after sign partition and padding
     // device buffers
     // two pass buffers, so one pass can be prepared while the previous contracts
-    uint16_t* xhi[2] = {nullptr, nullptr};   // [nb_pad][slots] 16-bit: sqrt|V| Phi, high part
-    uint16_t* xlo[2] = {nullptr, nullptr};   // [nb_pad][slots] 16-bit: low part
+    // [row block][k-block][hi, lo][128 x 64] 16-bit sqrt|V| Phi, each box in the swizzled MMA order
+    uint16_t* x[2] = {nullptr, nullptr};
     int* slot_of[2] = {nullptr, nullptr};    // [slots] K slot -> sample (-1: zero padding)
     int* group_meta[2] = {nullptr, nullptr}; // per 4096-sample block: first negative 16-group
     WorkItem* tiles = nullptr;    // [ntiles] work items, in launch order
@@ -46,8 +46,6 @@ struct Plan {
     ExpandDesc* desc_dev = nullptr;   // [2] expansion descriptors of the two pass buffers
     ExpandDesc desc_host[2] = {};     // what desc_dev holds (uploaded again only when it changes)
     double* partial = nullptr;    // [nsplit][ntiles][128*128] FP64
-    void* tmap_hi[2] = {nullptr, nullptr};   // CUtensorMap (host copies) for xhi / xlo
-    void* tmap_lo[2] = {nullptr, nullptr};
     int* err_flag = nullptr;      // bounded-wait failures
 };
 
@@ -74,16 +72,15 @@ int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, doub
 // Launchers shared by the single build and the batch (several clusters in one launch).
 int launch_partition(const double* v, int64_t v_stride, int* slot_of, int64_t slot_stride, int* neg, int neg_stride,
                      int nflush, int nclusters, cudaStream_t s);
-int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t ldk,
-                  uint16_t* xhi, uint16_t* xlo, bool f16, cudaStream_t s);
+// slots: K slots of this pass (k-blocks of 64); nkb: k-blocks per row block in the operand's allocation
+int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t nkb,
+                  uint16_t* x, bool f16, cudaStream_t s);
 // max_ctas > 0: at most that many CTAs, each looping over work units (persistent); 0: one CTA per unit.
-int launch_contract(const void* map_hi, const void* map_lo, const WorkItem* items, int nitems, const int* neg,
-                    int nflush, int nsplit, int products, bool f16, double* partial, int* err_flag, cudaStream_t s,
+int launch_contract(const uint16_t* x, int64_t nkb, const WorkItem* items, int nitems, const int* neg, int nflush,
+                    int nsplit, int products, bool f16, double* partial, int* err_flag, cudaStream_t s,
                     int max_ctas = 0);
 int launch_unpack(const double* partial, const int* tile_index, int nt, int nitems_total, int nsplit, int64_t item0,
                   int nb, double divisor, const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s);
-int encode_operand_map(void** out, void* base, int64_t slots, int rows);
-void free_operand_map(void* map);
 
 }  // namespace tc
 }  // namespace scp3
