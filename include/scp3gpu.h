@@ -69,9 +69,9 @@ int scp3gpu_version(void);
  * TTM3-F geometry hit the 500-sweep cap (its energy is still written). */
 int scp3gpu_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters);
 
-/* Energies and gradients (kcal/mol/Angstrom, n x 9*nw) -- h2o::PES::operator()(nw,
- * crd, grad) (PES.h:14-22), qtip4pf.cpp:252-397.  qTIP4P/f; TTM3-F returns
- * SCP3GPU_ERR_UNSUPPORTED. */
+/* Energies and gradients (kcal/mol/Angstrom, n x 9*nw), FP64 -- h2o::PES::operator()(nw,
+ * crd, grad) (PES.h:14-22): qtip4pf.cpp:252-397, ttm3f.cpp:325-720.
+ * SCP3GPU_ERR_NOT_CONVERGED if a TTM3-F geometry hit the dipole sweep cap. */
 int scp3gpu_pes_energy_grad(int pes, int nw, int64_t n, const double* crd, double* E, double* grad);
 
 /* Device-buffer variant (crd_dev, E_dev on `device`), ordered on the legacy
@@ -119,7 +119,7 @@ typedef struct scp3gpu_config {
 #define SCP3GPU_ESTIMATOR_DIRECT 0   /* -G: sum_s Phi V Phi^T (ScaledMatrixElements.cpp:951-971)         */
 #define SCP3GPU_ESTIMATOR_GRADIENT 1 /* the default: Stein estimator from V and dV/dq
                                         (ScaledMatrixElements.cpp:102-725, TripleExcitations.h); plain
-                                        FP64 form, qTIP4P/f (its gradient, qtip4pf.cpp:252-397)          */
+                                        FP64 form (qtip4pf.cpp:252-397, ttm3f.cpp:325-720 gradients)     */
 
 /* Replaces ScaledMatrixElements(omega(modes), N2, N3) + M.zeros (SCP3.cpp:164-169). */
 int scp3gpu_hbuild_create(const scp3gpu_config* cfg, scp3gpu_hbuild** out);

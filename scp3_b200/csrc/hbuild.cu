@@ -338,32 +338,38 @@ int scp3gpu_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E,
 int scp3gpu_pes_energy_grad(int pes, int nw, int64_t n, const double* crd, double* E, double* grad)
 {
     (void)cudaGetLastError();   // a pending error of an earlier, unrelated call is not this call's
-    if (pes == SCP3GPU_PES_TTM3F)
-        return fail(SCP3GPU_ERR_UNSUPPORTED, "pes_energy_grad: the TTM3-F gradient is not built (qTIP4P/f only)");
-    if (pes != SCP3GPU_PES_QTIP4PF) return fail(SCP3GPU_ERR_ARG, "unknown potential");
+    if (pes != SCP3GPU_PES_QTIP4PF && pes != SCP3GPU_PES_TTM3F) return fail(SCP3GPU_ERR_ARG, "unknown potential");
     if (nw < 1 || nw > kMaxWaters || n < 0 || (n > 0 && (!crd || !E || !grad)))
         return fail(SCP3GPU_ERR_ARG, "pes_energy_grad: bad nw, n or pointer");
+    if (pes == SCP3GPU_PES_TTM3F && nw > 8) return fail(SCP3GPU_ERR_ARG, "TTM3-F kernel supports nw <= 8");
     if (n == 0) return SCP3GPU_OK;
     int dev = 0;
     cudaGetDevice(&dev);
     int rc = check_device(dev);
     if (rc) return rc;
+    if (pes == SCP3GPU_PES_TTM3F && (rc = ttm_init_device())) return rc;
     std::vector<uint32_t> t = pair_tasks(nw);
     uint32_t* td = nullptr;
     double *cd = nullptr, *ed = nullptr, *gd = nullptr;
+    int* id = nullptr;
     if ((rc = upload(&td, t.data(), t.size())) || (rc = upload(&cd, crd, (size_t)n * 9 * nw)) ||
-        (rc = dalloc(&ed, (size_t)n)) || (rc = dalloc(&gd, (size_t)n * 9 * nw))) {
-        cudaFree(td), cudaFree(cd), cudaFree(ed), cudaFree(gd);
+        (rc = dalloc(&ed, (size_t)n)) || (rc = dalloc(&gd, (size_t)n * 9 * nw)) || (rc = dalloc(&id, (size_t)n))) {
+        cudaFree(td), cudaFree(cd), cudaFree(ed), cudaFree(gd), cudaFree(id);
         return rc;
     }
-    rc = launch_pes_energy_grad(nw, n, cd, ed, gd, td, (int)t.size(), 0);
+    rc = launch_pes_energy_grad(pes, nw, n, cd, ed, gd, id, td, (int)t.size(), 0);
+    std::vector<int> it(n);
     if (!rc) {
         cudaError_t e = cudaMemcpy(E, ed, sizeof(double) * n, cudaMemcpyDeviceToHost);
         if (e == cudaSuccess) e = cudaMemcpy(grad, gd, sizeof(double) * n * 9 * nw, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(it.data(), id, sizeof(int) * n, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) rc = cuda_fail(e, "pes_energy_grad copy-out");
     }
-    cudaFree(td), cudaFree(cd), cudaFree(ed), cudaFree(gd);
-    return rc;
+    cudaFree(td), cudaFree(cd), cudaFree(ed), cudaFree(gd), cudaFree(id);
+    if (rc) return rc;
+    for (int64_t k = 0; k < n; k++)
+        if (it[k] > kTtmMaxIter) return fail(SCP3GPU_ERR_NOT_CONVERGED, "TTM3-F dipoles hit the iteration cap");
+    return SCP3GPU_OK;
 }
 
 int scp3gpu_sobol_std_normal(int dims, int64_t index0, int64_t n, int scramble, uint64_t seed, double* out)
@@ -445,9 +451,8 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     if (c->chunk < 0 || c->chunk % 4096 != 0) return fail(SCP3GPU_ERR_ARG, "chunk must be a multiple of 4096");
     if (c->estimator != SCP3GPU_ESTIMATOR_DIRECT && c->estimator != SCP3GPU_ESTIMATOR_GRADIENT)
         return fail(SCP3GPU_ERR_ARG, "unknown estimator");
-    if (c->estimator == SCP3GPU_ESTIMATOR_GRADIENT &&
-        (c->precision != SCP3GPU_PREC_FP64 || c->pes != SCP3GPU_PES_QTIP4PF))
-        return fail(SCP3GPU_ERR_UNSUPPORTED, "gradient estimator: plain FP64 form with qTIP4P/f only");
+    if (c->estimator == SCP3GPU_ESTIMATOR_GRADIENT && c->precision != SCP3GPU_PREC_FP64)
+        return fail(SCP3GPU_ERR_UNSUPPORTED, "gradient estimator: plain FP64 form only");
     for (int m = 0; m < c->nmodes; m++)
         if (c->modes[m] < 0 || c->modes[m] >= c->nmodes0) return fail(SCP3GPU_ERR_ARG, "mode index out of range");
     int rc = check_device(c->device);

@@ -121,8 +121,8 @@ struct SampleArgs {
     double* v;                    // [n] V_anh (hartree)
     unsigned long long* counters; // [2] non-finite, not converged
     int skip_pes;                 // 1: q only, V_anh = 0 (the surrogate supplies V)
-    double* vq;                   // [n x nm] dV_anh/dq of the selected modes, FP64 (gradient path; qTIP4P/f,
-                                  // FP64 potential), or nullptr
+    double* vq;                   // [n x nm] dV_anh/dq of the selected modes, FP64 (gradient path; FP64
+                                  // potential), or nullptr
 };
 // pes: SCP3GPU_PES_*, fp32: run the potential in FP32.
 int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s);
@@ -133,9 +133,10 @@ int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s);
 int launch_samples_batch(int pes, bool fp32, const SampleArgs* args_host, const SampleArgs* args_dev, int ncl,
                          int64_t n, cudaStream_t s);
 
-// qTIP4P/f energies (kcal/mol) and gradients (kcal/mol/A, [n][9nw]) of n geometries
-int launch_pes_energy_grad(int nw, int64_t n, const double* crd, double* E, double* G, const uint32_t* tasks,
-                           int ntasks, cudaStream_t s);
+// Energies (kcal/mol) and gradients (kcal/mol/A, [n][9nw]) of n geometries, FP64;
+// iters (may be null): TTM3-F dipole sweeps per geometry
+int launch_pes_energy_grad(int pes, int nw, int64_t n, const double* crd, double* E, double* G, int* iters,
+                           const uint32_t* tasks, int ntasks, cudaStream_t s);
 
 int launch_pes_energy(int pes, int nw, int64_t n, const double* crd, double* E, int* iters,
                       const uint32_t* tasks, int ntasks, cudaStream_t s);

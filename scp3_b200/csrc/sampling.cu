@@ -35,7 +35,7 @@ template <typename T>
 __host__ __device__ inline size_t slot_bytes(int pes, int nm0, int nw, bool grad = false)
 {
     size_t b = sizeof(double) * (size_t)((nm0 + 1) & ~1) + sizeof(T) * (size_t)(12 * nw);
-    if (pes == SCP3GPU_PES_TTM3F) b += sizeof(T) * ttm::scratch_elems(nw);
+    if (pes == SCP3GPU_PES_TTM3F) b += sizeof(T) * ttm::scratch_elems(nw, grad);
     b = (b + 7) & ~(size_t)7;
     if (grad) b += sizeof(double) * (size_t)(12 * nw);
     return (b + 15) & ~(size_t)15;
@@ -50,7 +50,7 @@ __device__ inline WarpSlot<T> warp_slot(char* base, int pes, int nm0, int nw, bo
     s.ms = s.crd + 9 * nw;
     s.ttm = s.ms + 3 * nw;
     size_t off = sizeof(double) * (size_t)((nm0 + 1) & ~1) + sizeof(T) * (size_t)(12 * nw);
-    if (pes == SCP3GPU_PES_TTM3F) off += sizeof(T) * ttm::scratch_elems(nw);
+    if (pes == SCP3GPU_PES_TTM3F) off += sizeof(T) * ttm::scratch_elems(nw, grad);
     off = (off + 7) & ~(size_t)7;
     s.g = grad ? reinterpret_cast<double*>(base + off) : nullptr;
     s.gm = grad ? s.g + 9 * nw : nullptr;
@@ -172,13 +172,18 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
         // 3. V in hartree, anharmonic residual   (SCP3.cpp:219-223)
         int iters = 0;
         double V = 0.0;
-        if constexpr (PES == SCP3GPU_PES_QTIP4PF && sizeof(T) == 8) {
+        if constexpr (sizeof(T) == 8) {
             if (grad) {
                 // gradient path (SCP3.cpp:209-216): V and dV/dr, then
                 // dV_anh/dq = MUa^T (bohr dV/dr / autokcal) - omega % q, selected modes
-                const double e = qt::energy_grad_warp(reinterpret_cast<const double*>(w.crd),
-                                                      reinterpret_cast<double*>(w.ms), w.g, w.gm, nw, a.tasks,
-                                                      a.ntasks, lane);
+                double e;
+                if constexpr (PES == SCP3GPU_PES_QTIP4PF)
+                    e = qt::energy_grad_warp(reinterpret_cast<const double*>(w.crd), reinterpret_cast<double*>(w.ms),
+                                             w.g, w.gm, nw, a.tasks, a.ntasks, lane);
+                else
+                    e = ttm::energy_grad_warp(reinterpret_cast<const double*>(w.crd),
+                                              reinterpret_cast<double*>(w.ms), reinterpret_cast<double*>(w.ttm),
+                                              w.g, nw, a.tasks, a.ntasks, lane, &iters);
                 double h = 0.0;
                 for (int d = lane; d < nm0; d += 32) h += w.q[d] * (__ldg(a.omega + d) * w.q[d]);
                 h = warp_sum(h);
@@ -238,20 +243,29 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 
 // qTIP4P/f energy and gradient of n geometries, one warp each (the E+g operator,
 // qtip4pf.cpp:252-397).
+template <int PES>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     pes_energy_grad_kernel(int nw, int64_t n, const double* __restrict__ crd, double* __restrict__ E,
-                           double* __restrict__ G, const uint32_t* __restrict__ tasks, int ntasks)
+                           double* __restrict__ G, int* __restrict__ iters_out, const uint32_t* __restrict__ tasks,
+                           int ntasks)
 {
     extern __shared__ __align__(16) double gsm[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double* x = gsm + (size_t)wib * 24 * nw;
-    double *ms = x + 9 * nw, *g = ms + 3 * nw, *gm = g + 9 * nw;
+    const size_t per = 24 * (size_t)nw + (PES == SCP3GPU_PES_TTM3F ? ttm::scratch_elems(nw, true) : 0);
+    double* x = gsm + (size_t)wib * per;
+    double *ms = x + 9 * nw, *g = ms + 3 * nw, *gm = g + 9 * nw, *sc = gm + 3 * nw;
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
     for (int64_t k = (int64_t)blockIdx.x * kWarpsPerBlock + wib; k < n; k += nwarps) {
         for (int c = lane; c < 9 * nw; c += 32) x[c] = crd[k * 9 * nw + c];
         __syncwarp();
-        const double e = qt::energy_grad_warp(x, ms, g, gm, nw, tasks, ntasks, lane);
-        if (lane == 0) E[k] = e;
+        int iters = 0;
+        double e;
+        if constexpr (PES == SCP3GPU_PES_QTIP4PF) e = qt::energy_grad_warp(x, ms, g, gm, nw, tasks, ntasks, lane);
+        else e = ttm::energy_grad_warp(x, ms, sc, g, nw, tasks, ntasks, lane, &iters);
+        if (lane == 0) {
+            E[k] = e;
+            if (iters_out) iters_out[k] = iters;
+        }
         for (int c = lane; c < 9 * nw; c += 32) G[k * 9 * nw + c] = g[c];
         __syncwarp();
     }
@@ -367,8 +381,7 @@ int ttm_init_device()
 int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s)
 {
     if (a.n <= 0) return SCP3GPU_OK;
-    if (a.vq && (fp32 || pes != SCP3GPU_PES_QTIP4PF))
-        return fail(SCP3GPU_ERR_UNSUPPORTED, "gradient path: qTIP4P/f with an FP64 potential only");
+    if (a.vq && fp32) return fail(SCP3GPU_ERR_UNSUPPORTED, "gradient path: FP64 potential only");
     if (pes == SCP3GPU_PES_QTIP4PF)
         return fp32 ? launch_samples_t<SCP3GPU_PES_QTIP4PF, float>(a, s)
                     : launch_samples_t<SCP3GPU_PES_QTIP4PF, double>(a, s);
@@ -378,14 +391,16 @@ int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s)
     return fail(SCP3GPU_ERR_ARG, "unknown potential id");
 }
 
-int launch_pes_energy_grad(int nw, int64_t n, const double* crd, double* E, double* G, const uint32_t* tasks,
-                           int ntasks, cudaStream_t s)
+int launch_pes_energy_grad(int pes, int nw, int64_t n, const double* crd, double* E, double* G, int* iters,
+                           const uint32_t* tasks, int ntasks, cudaStream_t s)
 {
     if (n <= 0) return SCP3GPU_OK;
-    const size_t sm = sizeof(double) * kWarpsPerBlock * 24 * (size_t)nw;
-    if (sm > 48 * 1024)
-        SCP3_CUDA(cudaFuncSetAttribute(pes_energy_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    pes_energy_grad_kernel<<<grid_for(n), kWarpsPerBlock * 32, sm, s>>>(nw, n, crd, E, G, tasks, ntasks);
+    const bool ttm = pes == SCP3GPU_PES_TTM3F;
+    const size_t per = 24 * (size_t)nw + (ttm ? ttm::scratch_elems(nw, true) : 0);
+    const size_t sm = sizeof(double) * kWarpsPerBlock * per;
+    auto kern = ttm ? pes_energy_grad_kernel<SCP3GPU_PES_TTM3F> : pes_energy_grad_kernel<SCP3GPU_PES_QTIP4PF>;
+    if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<grid_for(n), kWarpsPerBlock * 32, sm, s>>>(nw, n, crd, E, G, iters, tasks, ntasks);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }

@@ -10,8 +10,8 @@
 // 2^17 (SCP3.cpp:252-255), omega0.dat at start (SCP3.cpp:300-302).
 //
 // Without -G the reference's default gradient estimator runs
-// (ScaledMatrixElements.cpp:102-725): on the GPU in FP64 with the qTIP4P/f
-// gradient; other potentials or precisions need -G (ScaledMatrixElements.cpp:951-971).
+// (ScaledMatrixElements.cpp:102-725): on the GPU in FP64 with the potential's
+// gradient; the split precisions need -G (ScaledMatrixElements.cpp:951-971).
 #include <getopt.h>
 
 #include <cmath>
@@ -245,8 +245,8 @@ void check(int rc, const char* what)
 int main(int argc, char** argv)
 {
     Options o = parse(argc, argv);
-    if (o.use_gradient && (o.pes != "qtip4pf" || o.precision != "fp64"))
-        die("The gradient estimator runs with -p qtip4pf in FP64; run other potentials or precisions with -G.");
+    if (o.use_gradient && o.precision != "fp64")
+        die("The gradient estimator runs in FP64; run the split precisions with -G.");
     vector<double> mass, x0, H;
     load_input(o.input, mass, x0, H);
     ohhohh(mass, x0, H);

@@ -202,16 +202,41 @@ def gen_stein(L, dimer):
     L.ref_qtip4pf_energy_grad.restype = ctypes.c_double
     L.ref_qtip4pf_energy_grad.argtypes = [ctypes.c_int, dp, dp]
     z = np.load(os.path.join(OUT, "pes_ref.npz"), allow_pickle=True)
-    grads = []
+    L.ref_ttm3f_energy_grad.restype = ctypes.c_double
+    L.ref_ttm3f_energy_grad.argtypes = [ctypes.c_int, dp, dp]
+    grads, grads_t, e_t = [], [], []
     for x in z["geoms"]:
         x = np.ascontiguousarray(x, dtype=np.float64)
         g = np.zeros(x.size)
         L.ref_qtip4pf_energy_grad(x.size // 9, x.ctypes.data_as(dp), g.ctypes.data_as(dp))
         grads.append(g)
-    # the dimer matrix: each upper element from the reference formula with its bra and ket
+        # TTM3-F E+g twice: its dipole iteration starts from the previous call's field
+        # (ttm3f.cpp:344-345 zeroes Efd/Efq/phi/dM here, so one call suffices; two agree)
+        g = np.zeros(x.size)
+        L.ref_ttm3f_energy_grad(x.size // 9, x.ctypes.data_as(dp), g.ctypes.data_as(dp))
+        e_t.append(L.ref_ttm3f_energy_grad(x.size // 9, x.ctypes.data_as(dp), g.ctypes.data_as(dp)))
+        grads_t.append(g)
+    out = dict(names=np.array(names), params=np.array([",".join(p) for p in params]), args=args, values=vals,
+               q=q, V=V, Vq=Vq, pes_geoms_grad=np.array(grads, dtype=object),
+               pes_geoms_grad_ttm3f=np.array(grads_t, dtype=object), pes_geoms_e_ttm3f=np.array(e_t))
     x0, MUa, omega = setup_modes(L, dimer)
+    for tag, fn in (("dimer", L.ref_qtip4pf_energy_grad), ("dimer_ttm3f", L.ref_ttm3f_energy_grad)):
+        n2, n3, ns, sseed = 12, 4, 256, 0x5C3
+        qs, Vs, Vqs, Mu = stein_matrix(Ls, names, params, fn, x0, MUa, omega, n2, n3, ns, sseed)
+        out.update({tag + "_x0": x0, tag + "_MUa": MUa, tag + "_omega": omega, tag + "_n2": n2, tag + "_n3": n3,
+                    tag + "_nsamples": ns, tag + "_scramble_seed": sseed, tag + "_q": qs, tag + "_V": Vs,
+                    tag + "_Vq": Vqs, tag + "_M_upper": Mu})
+    np.savez_compressed(os.path.join(OUT, "stein_ref.npz"), **out)
+
+
+def stein_matrix(Ls, names, params, egrad, x0, MUa, omega, n2, n3, ns, sseed):
+    """A gradient-path matrix from the reference: V and dV/dq from the
+    reference's E+g operator (SCP3.cpp:205-223) and every upper element from
+    the reference formula for its bra and ket."""
+    import ctypes
+    import itertools
+    dp = ctypes.POINTER(ctypes.c_double)
     nm0 = omega.size
-    n2, n3, ns, sseed = 12, 4, 256, 0x5C3
     normals = oracle.std_normals(nm0, 0, ns, scramble_seed=sseed)
     bohr, kcal = C.bohr, C.autokcalpmol
     qs = normals / np.sqrt(2.0)
@@ -220,7 +245,8 @@ def gen_stein(L, dimer):
     for s in range(ns):
         r = np.ascontiguousarray(bohr * (x0 + MUa @ qs[s]))
         g = np.zeros(r.size)
-        e = L.ref_qtip4pf_energy_grad(r.size // 9, r.ctypes.data_as(dp), g.ctypes.data_as(dp)) / kcal
+        egrad(r.size // 9, r.ctypes.data_as(dp), g.ctypes.data_as(dp))
+        e = egrad(r.size // 9, r.ctypes.data_as(dp), g.ctypes.data_as(dp)) / kcal
         Vs[s] = e - 0.5 * np.dot(qs[s], omega * qs[s])
         Vqs[s] = MUa.T @ (g * bohr / kcal) - omega * qs[s]
     nb = oracle.basis_size(nm0, n2, n3)
@@ -271,10 +297,7 @@ def gen_stein(L, dimer):
             Mu[k] = ref_stein_eval(Ls, hit[0], hit[1], qT, Vs, VqT)
             k += 1
     print("stein: %d formulas, %d used by the dimer matrix" % (len(names), len(used)))
-    np.savez_compressed(os.path.join(OUT, "stein_ref.npz"), names=np.array(names), params=np.array(
-        [",".join(p) for p in params]), args=args, values=vals, q=q, V=V, Vq=Vq, pes_geoms_grad=np.array(
-        grads, dtype=object), dimer_x0=x0, dimer_MUa=MUa, dimer_omega=omega, dimer_n2=n2, dimer_n3=n3,
-        dimer_nsamples=ns, dimer_scramble_seed=sseed, dimer_q=qs, dimer_V=Vs, dimer_Vq=Vqs, dimer_M_upper=Mu)
+    return qs, Vs, Vqs, Mu
 
 
 def main():

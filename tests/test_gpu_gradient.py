@@ -1,11 +1,12 @@
-"""GPU parity of the gradient (default) path: the qTIP4P/f gradient in the
-per-sample kernel, dV/dq = MUa^T dV/dr - omega q (SCP3.cpp:209-216), and the
-Stein estimator of every upper element (ScaledMatrixElements.cpp:102-725,
+"""GPU parity of the gradient (default) path: the qTIP4P/f and TTM3-F gradients
+in the per-sample kernel, dV/dq = MUa^T dV/dr - omega q (SCP3.cpp:209-216),
+and the Stein estimator of every upper element (ScaledMatrixElements.cpp:102-725,
 TripleExcitations.h) in FP64.
 
-Against the reference: the dimer matrix of tests/golden/stein_ref.npz (N2 =
-12, N3 = 4, 256 scrambled points), summed from the reference's own formulas
-with the reference's potential gradient, to 1e-11 of its largest element.
+Against the reference: the dimer matrices of tests/golden/stein_ref.npz (N2 =
+12, N3 = 4, 256 scrambled points, both potentials), summed from the
+reference's own formulas with the reference's potential gradients, to 1e-11 of
+the largest element; the gradients themselves on the pes_ref geometries.
 Against the oracle: addEpot(q, V, Vq) on the hexamer basis with N3 = 6."""
 import os
 
@@ -30,19 +31,20 @@ def z():
     return np.load(os.path.join(GOLDEN, "stein_ref.npz"), allow_pickle=True)
 
 
-def test_dimer_gradient_build_matches_reference(scp3, z):
-    n2, n3, ns = int(z["dimer_n2"]), int(z["dimer_n3"]), int(z["dimer_nsamples"])
-    hb = scp3.HBuild(2, z["dimer_x0"], z["dimer_MUa"], z["dimer_omega"], n2=n2, n3=n3,
-                     scramble_seed=int(z["dimer_scramble_seed"]), estimator="gradient")
+@pytest.mark.parametrize("tag,pes", [("dimer", "qtip4pf"), ("dimer_ttm3f", "ttm3f")])
+def test_dimer_gradient_build_matches_reference(scp3, z, tag, pes):
+    n2, n3, ns = int(z[tag + "_n2"]), int(z[tag + "_n3"]), int(z[tag + "_nsamples"])
+    hb = scp3.HBuild(2, z[tag + "_x0"], z[tag + "_MUa"], z[tag + "_omega"], n2=n2, n3=n3, pes=pes,
+                     scramble_seed=int(z[tag + "_scramble_seed"]), estimator="gradient")
     hb.accumulate(0, ns)
     M = hb.read(0)
     assert hb.status()[0] == 0
     got = M.T[np.tril_indices(M.shape[0])]        # upper triangle column by column
-    ref = z["dimer_M_upper"]
+    ref = z[tag + "_M_upper"]
     assert np.abs(got - ref).max() <= 1e-11 * np.abs(ref).max(), np.abs(got - ref).max() / np.abs(ref).max()
     # Mout adds the same HO diagonal as the direct path
-    d = scp3.HBuild(2, z["dimer_x0"], z["dimer_MUa"], z["dimer_omega"], n2=n2, n3=n3,
-                    scramble_seed=int(z["dimer_scramble_seed"]))
+    d = scp3.HBuild(2, z[tag + "_x0"], z[tag + "_MUa"], z[tag + "_omega"], n2=n2, n3=n3, pes=pes,
+                    scramble_seed=int(z[tag + "_scramble_seed"]))
     d.accumulate(0, ns)
     diag_g = np.diag(hb.read(1)) - np.diag(M) / ns
     diag_d = np.diag(d.read(1)) - np.diag(d.read(0)) / ns
@@ -68,23 +70,22 @@ def test_add_epot_grad_matches_oracle(scp3, oracle_mod):
 
 
 def test_gradient_estimator_limits(scp3, z):
-    for kw in (dict(pes="ttm3f"), dict(precision="bf16x3")):
-        with pytest.raises(scp3.SCP3GPUError):
-            scp3.HBuild(2, z["dimer_x0"], z["dimer_MUa"], z["dimer_omega"], estimator="gradient", **kw)
+    with pytest.raises(scp3.SCP3GPUError):
+        scp3.HBuild(2, z["dimer_x0"], z["dimer_MUa"], z["dimer_omega"], estimator="gradient", precision="bf16x3")
     d = scp3.HBuild(2, z["dimer_x0"], z["dimer_MUa"], z["dimer_omega"])
     with pytest.raises(scp3.SCP3GPUError):
         d.add_epot_grad(np.zeros((4, 12)), np.zeros(4), np.zeros((4, 12)))
 
 
-def test_pes_energy_grad_matches_reference(scp3, z):
+@pytest.mark.parametrize("pes,ekey,gkey", [("qtip4pf", "e_qtip4pf", "pes_geoms_grad"),
+                                           ("ttm3f", "e_ttm3f", "pes_geoms_grad_ttm3f")])
+def test_pes_energy_grad_matches_reference(scp3, z, pes, ekey, gkey):
     """h2o::PES::operator()(nw, crd, grad) on the GPU against the reference's
-    qTIP4P/f gradient (qtip4pf.cpp:252-397) on the pes_ref geometries."""
+    gradients (qtip4pf.cpp:252-397, ttm3f.cpp:325-720) on the pes_ref geometries."""
     p = np.load(os.path.join(GOLDEN, "pes_ref.npz"), allow_pickle=True)
-    pes = scp3.PES("qtip4pf")
-    for x, e_ref, g_ref in zip(p["geoms"], p["e_qtip4pf"], z["pes_geoms_grad"]):
+    P = scp3.PES(pes)
+    for x, e_ref, g_ref in zip(p["geoms"], p[ekey], z[gkey]):
         x = np.asarray(x, dtype=np.float64)
-        E, G = pes.energies_grad(x[None, :])
-        assert abs(E[0] - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
-        assert np.abs(G[0] - g_ref).max() <= 1e-11 * max(1.0, np.abs(g_ref).max())
-    with pytest.raises(scp3.SCP3GPUError):
-        scp3.PES("ttm3f").energies_grad(np.asarray(p["geoms"][0], dtype=np.float64)[None, :])
+        E, G = P.energies_grad(x[None, :])
+        assert abs(E[0] - e_ref) <= 1e-11 * max(1.0, abs(e_ref)), (E[0], e_ref)
+        assert np.abs(G[0] - g_ref).max() <= 1e-10 * max(1.0, np.abs(g_ref).max()), np.abs(G[0] - g_ref).max()

@@ -56,3 +56,13 @@ def test_dimer_gradient_path(oracle_mod, z):
     got = M.T[np.tril_indices(nb)]        # upper triangle column by column, as the fixture stores it
     ref = z["dimer_M_upper"]
     assert np.abs(got - ref).max() <= 1e-11 * np.abs(ref).max(), np.abs(got - ref).max()
+
+
+def test_dimer_ttm3f_gradient_path_matrix(oracle_mod, z):
+    """The same rule on V and dV/dq from the reference's TTM3-F E+g operator
+    (ttm3f.cpp:325-720)."""
+    n2, n3 = int(z["dimer_ttm3f_n2"]), int(z["dimer_ttm3f_n3"])
+    M = oracle_mod.accumulate_stein(z["dimer_ttm3f_q"], z["dimer_ttm3f_V"], z["dimer_ttm3f_Vq"], n2, n3)
+    got = M.T[np.tril_indices(M.shape[0])]
+    ref = z["dimer_ttm3f_M_upper"]
+    assert np.abs(got - ref).max() <= 1e-11 * np.abs(ref).max()
