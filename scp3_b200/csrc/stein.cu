@@ -15,11 +15,16 @@
 // carries (q^2 - 3) V where the identity gives (10 q^2 - 3) V.
 //
 // Layout: a CTA owns one upper 64x64 tile and one range of samples (split);
-// 256 threads hold a 4x4 fragment each.  The samples' q, V and dV/dq (FP64,
-// sample-major) are staged in shared memory in chunks; every thread forms the
-// mode set of each of its elements from the row and column descriptors and
-// sums the estimate over the chunk.  Partials: [split][tile][64 x 64] row-major
-// within the tile, as the plain -G form, so the same read-out applies.
+// 256 threads hold a 4x4 fragment each.  Every factor above depends on one
+// mode, its two levels and the sample, so the samples are taken in small
+// chunks and, per sample and mode, a table of the 16 level pairs (a, b) holds
+// p_ab and t_ab = (p_ab(0) + r_ab'/2) V + (r_ab/2) dV/dq_m.  An element is
+// then up to six table slots (its mode set; spare slots point at an entry with
+// p = 1, t = 0, and <0|V|0> at one with t = V), and its estimate is
+// (1/|S|) sum_u t_u prod_{u' != u} p_u' from prefix and suffix products.  The
+// slot indices of the thread's 16 elements are formed once and kept in
+// registers.  Partials: [split][tile][64 x 64] row-major within the tile, as
+// the plain -G form, so the same read-out applies.
 #include <algorithm>
 
 #include "internal.h"
@@ -61,16 +66,33 @@ __device__ __forceinline__ void ho_parts(int a, double q, double& h, double& h0,
     }
 }
 
-__global__ void __launch_bounds__(256) stein_fp64_kernel(const uint32_t* __restrict__ desc, int nb, int nm,
-                                                          const double* __restrict__ q, const double* __restrict__ v,
-                                                          const double* __restrict__ vq, int64_t kps, int chunk,
-                                                          int nt, int ntiles, double* __restrict__ partial)
+// Table entry of mode m, levels (a, b) at q = x: p and the two Stein coefficients.
+__device__ __forceinline__ void stein_entry(int a, int b, double x, double& p, double& u, double& w)
 {
-    extern __shared__ __align__(16) double sm[];
-    double* sq = sm;                              // [chunk][nm]
-    double* svq = sq + (size_t)chunk * nm;        // [chunk][nm]
-    double* sv = svq + (size_t)chunk * nm;        // [chunk]
-    __shared__ uint32_t rdesc[kT], cdesc[kT];
+    double ha, ha0, dha, da, dda, hb, hb0, dhb, db, ddb;
+    ho_parts(a, x, ha, ha0, dha, da, dda);
+    ho_parts(b, x, hb, hb0, dhb, db, ddb);
+    const double r = da * hb + ha0 * db;
+    const double dr = dda * hb + da * dhb + ha0 * ddb;
+    p = ha * hb;
+    u = ha0 * hb0 + 0.5 * dr;
+    w = 0.5 * r;
+    if (a == 3 && b == 3) u = (2 * x * x - 3) * (x * x - 3) * (1.0 / 6.0);   // TripleExcitations.h:763-773
+}
+
+constexpr int kSlots = 6;
+__constant__ double kInvNs[kSlots + 1] = {0.0, 1.0, 1.0 / 2, 1.0 / 3, 1.0 / 4, 1.0 / 5, 1.0 / 6};
+
+__global__ void __launch_bounds__(256, 2) stein_fp64_kernel(const uint32_t* __restrict__ desc, int nb, int nm,
+                                                             const double* __restrict__ q,
+                                                             const double* __restrict__ v,
+                                                             const double* __restrict__ vq, int64_t kps, int chunk,
+                                                             int nt, int ntiles, double* __restrict__ partial)
+{
+    extern __shared__ __align__(16) double2 tab[];   // [chunk][nm * 16 + 2] (p, t), then the slot words
+    const int per = nm * 16 + 2;                     // + the p = 1, t = 0 entry and the t = V entry
+    uint32_t* slw = reinterpret_cast<uint32_t*>(tab + (size_t)chunk * per);   // [16 x 3 words][thread]
+    const int kOne = nm * 16, kV = nm * 16 + 1;
     int t = blockIdx.x, ti = 0;
     while (t >= nt - ti) {
         t -= nt - ti;
@@ -78,33 +100,22 @@ __global__ void __launch_bounds__(256) stein_fp64_kernel(const uint32_t* __restr
     }
     const int tj = ti + t;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    if (tid < kT) {
-        const int r = ti * kT + tid, c = tj * kT + tid;
-        rdesc[tid] = r < nb ? desc[r] : 0xffffffffu;
-        cdesc[tid] = c < nb ? desc[c] : 0xffffffffu;
-    }
-    const int64_t s0 = (int64_t)blockIdx.y * kps;
-    double acc[16];
-#pragma unroll
-    for (int e = 0; e < 16; e++) acc[e] = 0.0;
-    for (int64_t c0 = 0; c0 < kps; c0 += chunk) {
-        const int nc = (int)(kps - c0 < chunk ? kps - c0 : chunk);
-        __syncthreads();
-        for (int e = tid; e < nc * nm; e += blockDim.x) {
-            sq[e] = q[(s0 + c0) * nm + e];
-            svq[e] = vq[(s0 + c0) * nm + e];
-        }
-        for (int e = tid; e < nc; e += blockDim.x) sv[e] = v[s0 + c0 + e];
-        __syncthreads();
+
+    // slot indices of the thread's 16 elements, two 16-bit indices per word; the
+    // element's |S| rides in bits 12-15 of word 0 (|S| <= 6; 0 = skip).  Kept in
+    // shared memory, [word][thread], so the registers stay with the arithmetic.
+    auto SL = [&](int e, int wd) -> uint32_t& { return slw[(size_t)(3 * e + wd) * 256 + tid]; };
 #pragma unroll 1
-        for (int e = 0; e < 16; e++) {
-            const int lr = ty + 16 * (e >> 2), lc = tx + 16 * (e & 3);
-            const int gi = ti * kT + lr, gj = tj * kT + lc;
-            if (gi > gj || rdesc[lr] == 0xffffffffu || cdesc[lc] == 0xffffffffu) continue;
-            // the mode set S of the pair and the two levels in each mode
+    for (int e = 0; e < 16; e++) {
+        const int gi = ti * kT + ty + 16 * (e >> 2), gj = tj * kT + tx + 16 * (e & 3);
+        int idx[kSlots];
+#pragma unroll
+        for (int u = 0; u < kSlots; u++) idx[u] = kOne;
+        int ns = 0;
+        if (gi <= gj && gj < nb) {
             int mi[3], li[3], mj[3], lj[3];
-            const int ni = decode(rdesc[lr], mi, li), nj = decode(cdesc[lc], mj, lj);
-            int S[kMaxS], A[kMaxS], B[kMaxS], ns = 0;
+            const int ni = decode(__ldg(desc + gi), mi, li), nj = decode(__ldg(desc + gj), mj, lj);
+            int S[kSlots], A[kSlots], B[kSlots];
             for (int k = 0; k < ni; k++) S[ns] = mi[k], A[ns] = li[k], B[ns] = 0, ns++;
             for (int k = 0; k < nj; k++) {
                 int f = -1;
@@ -113,41 +124,69 @@ __global__ void __launch_bounds__(256) stein_fp64_kernel(const uint32_t* __restr
                 if (f >= 0) B[f] = lj[k];
                 else S[ns] = mj[k], A[ns] = 0, B[ns] = lj[k], ns++;
             }
-            double sum = 0.0;
-            if (ns == 0) {
-                for (int s = 0; s < nc; s++) sum += sv[s];
-            } else {
-                const double inv_ns = 1.0 / ns;
-                for (int s = 0; s < nc; s++) {
-                    const double* qs = sq + (size_t)s * nm;
-                    const double* gs = svq + (size_t)s * nm;
-                    double p[kMaxS], term[kMaxS];
 #pragma unroll
-                    for (int u = 0; u < kMaxS; u++) {
-                        if (u >= ns) break;
-                        const double x = qs[S[u]];
-                        double ha, ha0, dha, da, dda, hb, hb0, dhb, db, ddb;
-                        ho_parts(A[u], x, ha, ha0, dha, da, dda);
-                        ho_parts(B[u], x, hb, hb0, dhb, db, ddb);
-                        const double r = da * hb + ha0 * db;
-                        const double dr = dda * hb + da * dhb + ha0 * ddb;
-                        double uu = ha0 * hb0 + 0.5 * dr;
-                        if (A[u] == 3 && B[u] == 3) uu = (2 * x * x - 3) * (x * x - 3) * (1.0 / 6.0);
-                        p[u] = ha * hb;
-                        term[u] = uu * sv[s] + 0.5 * r * gs[S[u]];
-                    }
-                    // sum_u term_u prod_{u' != u} p_u'  (prefix and suffix products)
-                    double pre = 1.0, tot = 0.0, suf[kMaxS];
-                    suf[ns - 1] = 1.0;
-                    for (int u = ns - 1; u > 0; u--) suf[u - 1] = suf[u] * p[u];
-                    for (int u = 0; u < ns; u++) {
-                        tot += term[u] * pre * suf[u];
-                        pre *= p[u];
-                    }
-                    sum += tot * inv_ns;
-                }
+            for (int u = 0; u < kSlots; u++)
+                if (u < ns) idx[u] = S[u] * 16 + A[u] * 4 + B[u];
+            if (ns == 0) {                 // <0|V|0> = V
+                idx[0] = kV;
+                ns = 1;
             }
-            acc[e] += sum;
+        }
+        SL(e, 0) = (uint32_t)idx[0] | ((uint32_t)ns << 12) | ((uint32_t)idx[1] << 16);
+        SL(e, 1) = (uint32_t)idx[2] | ((uint32_t)idx[3] << 16);
+        SL(e, 2) = (uint32_t)idx[4] | ((uint32_t)idx[5] << 16);
+    }
+    double acc[16];
+#pragma unroll
+    for (int e = 0; e < 16; e++) acc[e] = 0.0;
+
+    const int64_t s0 = (int64_t)blockIdx.y * kps;
+    for (int64_t c0 = 0; c0 < kps; c0 += chunk) {
+        const int nc = (int)(kps - c0 < chunk ? kps - c0 : chunk);
+        __syncthreads();
+        for (int k = tid; k < nc * per; k += blockDim.x) {
+            const int j = k / per, id = k - j * per;
+            const int64_t smp = s0 + c0 + j;
+            double2 ent;
+            if (id >= kOne) {
+                ent = make_double2(1.0, id == kV ? v[smp] : 0.0);
+            } else {
+                const int m = id >> 4, a = (id >> 2) & 3, b = id & 3;
+                double p, u, w;
+                stein_entry(a, b, q[smp * nm + m], p, u, w);
+                ent = make_double2(p, u * v[smp] + w * vq[smp * nm + m]);
+            }
+            tab[k] = ent;
+        }
+        __syncthreads();
+        for (int j = 0; j < nc; j++) {
+            const double2* T = tab + (size_t)j * per;
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                const uint32_t w0 = SL(e, 0);
+                const int ns = (int)((w0 >> 12) & 15u);
+                if (ns == 0) continue;
+                const uint32_t w1 = SL(e, 1), w2 = SL(e, 2);
+                double2 x[kSlots];
+                x[0] = T[w0 & 0xfffu];
+                x[1] = T[w0 >> 16];
+                x[2] = T[w1 & 0xffffu];
+                x[3] = T[w1 >> 16];
+                x[4] = T[w2 & 0xffffu];
+                x[5] = T[w2 >> 16];
+                // sum_u t_u prod_{u' != u} p_u' over the six slots (spare ones p = 1, t = 0)
+                double pre = 1.0, tot = 0.0;
+                double suf[kSlots];
+                suf[kSlots - 1] = 1.0;
+#pragma unroll
+                for (int u = kSlots - 1; u > 0; u--) suf[u - 1] = suf[u] * x[u].x;
+#pragma unroll
+                for (int u = 0; u < kSlots; u++) {
+                    tot += x[u].y * (pre * suf[u]);
+                    pre *= x[u].x;
+                }
+                acc[e] += tot * kInvNs[ns];
+            }
         }
     }
     double* P = partial + ((size_t)blockIdx.y * ntiles + blockIdx.x) * (kT * kT);
@@ -164,9 +203,11 @@ int launch_stein_fp64(const uint32_t* desc, int nb, int nm, const double* q, con
                       int64_t k, const TileMap& tm, int nsplit, double* partial, cudaStream_t s)
 {
     if (tm.tile != kT || k % nsplit != 0) return fail(SCP3GPU_ERR_ARG, "stein: shapes not tiled");
+    if (nm * 16 + 2 > 0xfff) return fail(SCP3GPU_ERR_ARG, "stein: too many modes for the slot encoding");
     if (k == 0) return SCP3GPU_OK;
-    const int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(32, (40 * 1024) / (int64_t)(16 * nm + 8)));
-    const size_t sm = sizeof(double) * ((size_t)chunk * (2 * nm + 1));
+    const size_t per = (size_t)(nm * 16 + 2) * sizeof(double2);
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(4, (48 * 1024) / per));
+    const size_t sm = per * chunk + sizeof(uint32_t) * 48 * 256;   // table chunk + slot words
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(stein_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        (int)sm));
     dim3 grid(tm.ntiles, nsplit);
