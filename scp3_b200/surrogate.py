@@ -118,6 +118,12 @@ def sample(hb, index0, n):
     return q, v
 
 
+def attach(hb, net, mode):
+    """Attach the network to a split-form build: SURROGATE_REPLACE (V_nn for V)
+    or SURROGATE_RESIDUAL (V - V_nn); SURROGATE_NONE detaches."""
+    _lib.check(_bind().scp3gpu_hbuild_set_surrogate(hb._h, net.handle if net is not None else None, mode))
+
+
 def control_variate(make_build, net, n_replace, n_residual, index_replace, index_residual):
     """Raw control-variate matrix M_cv (the estimate of sum V Phi Phi^T / N) from two
     builds made by make_build(): the surrogate alone over n_replace points and the
