@@ -77,6 +77,7 @@ struct scp3gpu_hbuild {
     scp3gpu_mlp* sur = nullptr;
     int sur_mode = SCP3GPU_SURROGATE_NONE;
     float* ybuf = nullptr;
+    __nv_bfloat16* sur_ws = nullptr;  // the network's activations for this build's passes
     // kernel timing
     bool prof = false;
     std::vector<cudaEvent_t> pev;
@@ -178,7 +179,11 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
         if (consumed) SCP3_CUDA(cudaEventRecord(consumed, ps));
         if (h->sur) {
             Timed t(h, 1, ps);
-            rc = mlp_net(h->sur)->forward(a.q32, (int)a.n, h->ybuf, ps);
+            const mlp::Net* net = mlp_net(h->sur);
+            const size_t mp = (size_t)(a.n + 63) / 64 * 64;
+            __nv_bfloat16* X = h->sur_ws;
+            __nv_bfloat16* Ha = X + mp * net->kin;
+            rc = net->infer(a.q32, (int)a.n, h->ybuf, ps, X, Ha, Ha + mp * net->hid);
             if (!rc) rc = hb::launch_combine(h->sur_mode, a.v, h->ybuf, nvalid, ps);
             if (rc) return rc;
         }
@@ -409,7 +414,7 @@ int scp3gpu_hbuild_destroy(scp3gpu_hbuild* h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     if (h->prep_stream) cudaStreamSynchronize(h->prep_stream);
-    void* ptrs[] = {h->vq, h->ybuf, h->vdir, h->shift, h->x0, h->MUa, h->omega, h->modes, h->tasks, h->desc, h->q64, h->q32b[0],
+    void* ptrs[] = {h->sur_ws, h->vq, h->ybuf, h->vdir, h->shift, h->x0, h->MUa, h->omega, h->modes, h->tasks, h->desc, h->q64, h->q32b[0],
                     h->q32b[1], h->vb[0], h->vb[1],
                     h->v, h->normals[0], h->normals[1], h->phi, h->w, h->partial, h->dense, h->hodiag,
                     h->counters};
@@ -764,6 +769,11 @@ int scp3gpu_hbuild_set_surrogate(scp3gpu_hbuild* h, scp3gpu_mlp* m, int mode)
     if (int rc = drain_prep(h)) return rc;
     if (!h->ybuf && cudaMalloc(&h->ybuf, sizeof(float) * (size_t)h->chunk) != cudaSuccess)
         return fail(SCP3GPU_ERR_NOMEM, "surrogate output buffer");
+    // a workspace per build, so builds sharing one network can run at once
+    if (h->sur_ws) cudaFree(h->sur_ws);
+    h->sur_ws = nullptr;
+    if (cudaMalloc(&h->sur_ws, sizeof(__nv_bfloat16) * net->infer_workspace((int)h->chunk)) != cudaSuccess)
+        return fail(SCP3GPU_ERR_NOMEM, "surrogate workspace");
     h->sur = m;
     h->sur_mode = mode;
     return SCP3GPU_OK;

@@ -326,6 +326,34 @@ int Net::forward(const float* q, int M, float* y, cudaStream_t s)
     return apply_output(y, M, s);
 }
 
+__global__ void affine_kernel(float* y, int M, const float* b, float scale, float shift);
+
+size_t Net::infer_workspace(int M) const
+{
+    const size_t Mp = (size_t)(M + 63) / 64 * 64;
+    return Mp * kin + 2 * Mp * hid;
+}
+
+int Net::infer(const float* q, int M, float* y, cudaStream_t s, __nv_bfloat16* Xw, __nv_bfloat16* Ha,
+               __nv_bfloat16* Hb) const
+{
+    if (M <= 0) return SCP3GPU_OK;
+    const int Mp = (M + 63) / 64 * 64;
+    input_kernel<<<blocks((int64_t)Mp * kin, 256), 256, 0, s>>>(q, M, n_in, kin, Xw);
+    if (Mp > M) SCP3_CUDA(cudaMemsetAsync(Xw + (size_t)M * kin, 0, sizeof(__nv_bfloat16) * (size_t)(Mp - M) * kin, s));
+    const __nv_bfloat16* in_act = Xw;
+    __nv_bfloat16* outs[3] = {Ha, Hb, Ha};
+    for (int l = 0; l < 3; l++) {
+        dim3 grid(Mp / kGM, hid / kGN);
+        gemm_bias_gelu<<<grid, 128, 0, s>>>(in_act, wb[l], b[l], Mp, hid, inpad[l], nullptr, outs[l], 1);
+        in_act = outs[l];
+    }
+    head_kernel<<<blocks(M, 8), 256, 0, s>>>(in_act, w[3], 0.0f, M, hid, 1.0f, 0.0f, y);
+    affine_kernel<<<blocks(M, 256), 256, 0, s>>>(y, M, b[3], out_scale, out_shift);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
 __global__ void affine_kernel(float* y, int M, const float* b, float scale, float shift)
 {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;

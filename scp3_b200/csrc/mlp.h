@@ -25,6 +25,11 @@ struct Net {
     void free_all();
     int sync_bf16(cudaStream_t s);
     int forward(const float* q, int M, float* y, cudaStream_t s);
+    // Inference on a caller's workspace (X: Mp x kin, Ha/Hb: Mp x hid, BF16, Mp = M rounded
+    // up to 64): reads only the weights, so several builds may run it at once on their streams.
+    int infer(const float* q, int M, float* y, cudaStream_t s, __nv_bfloat16* X, __nv_bfloat16* Ha,
+              __nv_bfloat16* Hb) const;
+    size_t infer_workspace(int M) const;   // BF16 elements for X + Ha + Hb
     int apply_output(float* y, int M, cudaStream_t s);
     int backward(const float* q, const float* t, int M, cudaStream_t s, float* loss_out);
     int adam(float lr, cudaStream_t s);

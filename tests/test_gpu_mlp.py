@@ -88,3 +88,32 @@ def test_control_variate_gains_over_plain(sur):
     err_cv = np.abs(e_cv - e_ref).max() * AUTOCM
     print("levels error cm-1: plain %.3f  control variate %.3f" % (err_plain, err_cv))
     assert err_cv < err_plain
+
+
+def test_builds_sharing_a_network_run_concurrently(sur):
+    """Two builds with the same network attached (the two halves of the control
+    variate) accumulate at the same time on their own streams: each has its own
+    activation workspace, so the result equals one build after the other."""
+    import scp3_b200
+    c = load_hbuild_case("dimer_qtip4pf")
+
+    def make():
+        return scp3_b200.HBuild(2, c["x0"], c["MUa"], c["omega"], n2=12, n3=0, precision="bf16x3",
+                                scramble_seed=0x5C3)
+
+    net = sur.MLP(12, hidden=256, max_batch=1 << 17, seed=5)
+    net.set_output(0.01, -0.01)
+    seq = []
+    for mode, i0 in ((sur.SURROGATE_REPLACE, 1 << 40), (sur.SURROGATE_RESIDUAL, 0)):
+        hb = make()
+        sur.attach(hb, net, mode)
+        hb.accumulate(i0, 1 << 18)
+        seq.append(hb.read(0))
+        hb.close()
+    a, b = make(), make()
+    sur.attach(a, net, sur.SURROGATE_REPLACE)
+    sur.attach(b, net, sur.SURROGATE_RESIDUAL)
+    a.accumulate(1 << 40, 1 << 18)     # asynchronous: both run before either is read
+    b.accumulate(0, 1 << 18)
+    assert np.array_equal(a.read(0), seq[0])
+    assert np.array_equal(b.read(0), seq[1])
