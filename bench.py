@@ -533,23 +533,34 @@ def main():
         line["levels"] = {"max_abs_err_cm1_vs_fp64": float(np.abs(e_split - e64).max() * autocm),
                           "lowest10_cm1_fp64": [float(x * autocm) for x in e64],
                           "samples": SAMPLES}
-    if rank == 0 and not args.no_e2e:
-        # the -r path with host buffers: normals in from pinned memory, Mout back to host
-        normals = torch.from_numpy(scp3_b200.std_normals(nm0, 1 << 41, SAMPLES, scramble_seed=SCRAMBLE_SEED))
+    if not args.no_e2e:
+        # the -r path with host buffers on every rank: normals in from pinned memory, Mout
+        # back to host; the slowest rank's time is the job's
+        normals = torch.from_numpy(scp3_b200.std_normals(nm0, (1 << 41) + rank * SAMPLES, SAMPLES,
+                                                          scramble_seed=SCRAMBLE_SEED))
         normals = normals.pin_memory().numpy()
         Mh = np.asfortranarray(torch.empty((nb, nb), dtype=torch.float64).pin_memory().numpy().T)
         hb.reset()
         hb.accumulate_normals(normals)
         hb.read(1, out=Mh)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
         t0 = time.perf_counter()
         ne = max(2, min(args.steps, 5))
         for k in range(ne):
             hb.accumulate_normals(normals)
             hb.read(1, out=Mh)
         e2e_s = (time.perf_counter() - t0) / ne
-        line["e2e"] = {"value": SAMPLES / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": int(normals.nbytes),
-                       "d2h_bytes_per_step": int(nb * nb * 8),
-                       "path": "scp3gpu_hbuild_accumulate_normals + scp3gpu_hbuild_read(mode 1), host buffers"}
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([e2e_s], dtype=torch.float64, device=local)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        line["e2e"] = {"value": world * SAMPLES / e2e_s, "unit": "samples/s",
+                       "h2d_bytes_per_step": int(normals.nbytes), "d2h_bytes_per_step": int(nb * nb * 8),
+                       "path": "scp3gpu_hbuild_accumulate_normals + scp3gpu_hbuild_read(mode 1), host buffers, "
+                               "every rank; bytes per rank"}
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         normals = scp3_b200.std_normals(nm0, 0, 1 << 17, scramble_seed=SCRAMBLE_SEED)
         line["cpu_baseline"] = cpu_reference(nw, x0, MUa, omega, np.arange(nm0, dtype=np.int32), 48, 0, normals)
