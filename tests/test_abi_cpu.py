@@ -70,3 +70,44 @@ def test_input_roundtrip_and_modes(tmp_path):
     G = MUa.T @ (m3[:, None] * MUa)
     assert np.allclose(G, np.diag(1 / omega), rtol=1e-10)
     assert list(modes.parse_modes("0-3,7,9-10")) == [0, 1, 2, 3, 7, 9, 10]
+
+
+def test_argument_errors_before_any_device_work():
+    """Entry points reject bad shapes and options with SCP3GPU_ERR_ARG (or
+    UNSUPPORTED for a form that is not built) before they touch a device, so the
+    checks run here without a GPU."""
+    from scp3_b200 import _lib, api
+    L = _lib.lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    # batch: FP64 is not a batched form; chunk must be whole 4096-sample blocks
+    class K:
+        pass
+    k = K()
+    x0 = np.zeros(18)
+    api._fill_config(k, 2, x0, np.zeros((18, 12)), np.ones(12), None, 12, 0, "qtip4pf", "fp64", None, 0, 0)
+    arr = (_lib.Config * 1)(k._cfg)
+    h = ctypes.c_void_p()
+    assert L.scp3gpu_batch_create(arr, 1, 0, 0, ctypes.byref(h)) == _lib.ERR_UNSUPPORTED
+    k._cfg.precision = _lib.PREC_BF16X3
+    arr = (_lib.Config * 1)(k._cfg)
+    assert L.scp3gpu_batch_create(arr, 1, 1000, 0, ctypes.byref(h)) == _lib.ERR_ARG
+    assert L.scp3gpu_batch_create(arr, 0, 0, 0, ctypes.byref(h)) == _lib.ERR_ARG
+    # a build: unknown estimator; gradient estimator in a split precision
+    k._cfg.estimator = 7
+    assert L.scp3gpu_hbuild_create(ctypes.byref(k._cfg), ctypes.byref(h)) == _lib.ERR_ARG
+    k._cfg.estimator = _lib.ESTIMATOR_GRADIENT
+    assert L.scp3gpu_hbuild_create(ctypes.byref(k._cfg), ctypes.byref(h)) == _lib.ERR_UNSUPPORTED
+    # eigenpairs: k out of range, null matrix
+    A = np.eye(4)
+    W = np.zeros(4)
+    assert L.scp3gpu_syevr_lowest(A.ctypes.data_as(dp), 4, 4, 5, W.ctypes.data_as(dp), None, 4, 0) == _lib.ERR_ARG
+    assert L.scp3gpu_syevr_lowest(None, 4, 4, 2, W.ctypes.data_as(dp), None, 4, 0) == _lib.ERR_ARG
+    # energies and gradients: unknown potential, too many waters for TTM3-F
+    E = np.zeros(1)
+    G = np.zeros(9 * 9)
+    crd = np.zeros(9 * 9)
+    assert L.scp3gpu_pes_energy_grad(5, 9, 1, crd.ctypes.data_as(dp), E.ctypes.data_as(dp),
+                                     G.ctypes.data_as(dp)) == _lib.ERR_ARG
+    assert L.scp3gpu_pes_energy_grad(1, 9, 1, crd.ctypes.data_as(dp), E.ctypes.data_as(dp),
+                                     G.ctypes.data_as(dp)) == _lib.ERR_ARG
+    assert "TTM3-F" in L.scp3gpu_last_error().decode()
