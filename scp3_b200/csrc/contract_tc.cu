@@ -441,111 +441,251 @@ __global__ void __launch_bounds__(1024) partition_kernel(const double* __restric
     if (t == 0) neg_group[b] = P16 / 16;
 }
 
-// Expansion into the split operand X = sqrt|V| Phi (hi + lo halves).  A block
-// covers 64 K slots and up to 2048 basis rows: it first tabulates, per slot,
-// [1, h1(q_m), h2(q_m), h3(q_m)] for all modes in shared memory, then every basis
-// value is the product of three table entries (basis_factor_table).  Thread
-// (g, r) handles slots 4g..4g+3 of rows r, r+8, ...: one 16-byte table read per
-// factor and 8-byte stores, so the 16 threads of a row write 128 contiguous
-// bytes per half.
-constexpr int kExpSlots = 64, kExpRows = 2048, kExpThreads = 128;
+// Expansion into the split operand X = sqrt|V| Phi (hi + lo halves).
+//
+// Work unit: one k-block (64 K slots) x one chunk of kExpChunk basis rows of one
+// cluster.  Units are numbered cluster by cluster, k-block-major, and a
+// persistent grid (as many CTAs as the SMs hold at once) gives each CTA one
+// contiguous, balanced range of them, so there is no tail wave and a CTA
+// rebuilds its table only when its k-block changes.
+//
+// Per k-block the CTA tabulates, per slot, [1, h1(q_m), h2(q_m), h3(q_m)] for
+// all modes in shared memory; every basis value is then the product of three
+// table entries (basis_factor_table).  Thread (g, r) handles slots 8g..8g+7 of
+// rows r, r+32, ...: two 16-byte table reads per factor (the table's columns
+// are permuted so these are conflict-free) and one 16-byte store per half, so
+// the 8 threads of a row write its 128 contiguous bytes.  While a
+// k-block's rows are written, its successor's q rows and V values are already
+// in flight into a staging area (cp.async), so the table build that follows
+// does not wait on the gathers; when the staging area does not fit next to the
+// table (very many modes) the gathers are made at build time instead.
+constexpr int kExpSlots = 64, kExpChunk = 256, kExpThreads = 256;
 
+// x = hi + lo for two values, each half packed in one 32-bit word (the first
+// value in the low 16 bits): hi = round(x), lo = round(x - hi), round-to-nearest.
 template <bool F16>
-__device__ __forceinline__ void split4(float4 x, uint2& hi, uint2& lo)
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo)
 {
-    const float v[4] = {x.x, x.y, x.z, x.w};
-    uint32_t h[4], l[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        if (F16) {
-            const __half a = __float2half_rn(v[k]);
-            h[k] = __half_as_ushort(a);
-            l[k] = __half_as_ushort(__float2half_rn(v[k] - __half2float(a)));
-        } else {
-            const __nv_bfloat16 a = __float2bfloat16_rn(v[k]);
-            h[k] = __bfloat16_as_ushort(a);
-            l[k] = __bfloat16_as_ushort(__float2bfloat16_rn(v[k] - __bfloat162float(a)));
-        }
+    if (F16) {
+        const __half2 h = __floats2half2_rn(x0, x1);
+        const float2 hf = __half22float2(h);
+        const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+        hi = *reinterpret_cast<const uint32_t*>(&h);
+        lo = *reinterpret_cast<const uint32_t*>(&l);
+    } else {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+        const float2 hf = __bfloat1622float2(h);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+        hi = *reinterpret_cast<const uint32_t*>(&h);
+        lo = *reinterpret_cast<const uint32_t*>(&l);
     }
-    hi = make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
-    lo = make_uint2(l[0] | (l[1] << 16), l[2] | (l[3] << 16));
+}
+
+// Table column of K slot l (0..63): slots 8g..8g+3 at columns 4g..4g+3 and slots
+// 8g+4..8g+7 at 32+4g..32+4g+3, so the 8 threads of a row, thread g taking
+// slots 8g..8g+7, read two contiguous 128-byte spans (no bank conflict).
+__device__ __forceinline__ int tab_col(int l) { return ((l >> 3) << 2) | (l & 3) | ((l & 4) << 3); }
+__device__ __forceinline__ int tab_slot(int c) { return (((c & 31) >> 2) << 3) | (c & 3) | ((c >> 5) << 2); }
+
+__device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes, bool valid)
+{
+    // zero-filled (nothing read) when !valid; src is then any mapped address
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    const int n = valid ? bytes : 0;
+    if (bytes == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+    else if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Shared memory of the expansion (floats): table [3nm+1][64], sqrt|V| [64], and
+// when staged, q [nm][64] (in 4-mode groups when nm % 4 == 0) and V [64] (doubles).
+__host__ __device__ inline size_t expand_smem(int nm, bool staged)
+{
+    size_t f = (size_t)(3 * nm + 1) * kExpSlots + kExpSlots;
+    if (staged) f += (size_t)nm * kExpSlots + 2 * kExpSlots;
+    return f * sizeof(float);
 }
 
 template <bool F16>
-__global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandDesc* __restrict__ descs, int64_t nkb,
+__global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandDesc* __restrict__ descs, int ncl,
+                                                                    int64_t nkbp, int64_t nkb, int staged,
                                                                     uint16_t* __restrict__ xop)
 {
-    const ExpandDesc dsc = descs[blockIdx.z];        // one cluster of a batch per z
-    if ((int)blockIdx.y * kExpRows >= dsc.nb_pad) return;
-    const uint32_t* __restrict__ factors = dsc.factors;
-    const int nb = dsc.nb, nb_pad = dsc.nb_pad, nm = dsc.nm;
-    const float* __restrict__ q = dsc.q;
-    const double* __restrict__ v = dsc.v;
-    const int* __restrict__ sample_of_slot = dsc.slot_of;
-    extern __shared__ __align__(16) float tab[];      // [3nm+1][kExpSlots], then sqrt|V| [kExpSlots]
-    float* sv = tab + (size_t)(3 * nm + 1) * kExpSlots;
+    extern __shared__ __align__(16) float smem_f[];
     const int t = threadIdx.x;
-    const int64_t slot0 = (int64_t)blockIdx.x * kExpSlots;
-    for (int e = t; e < kExpSlots; e += kExpThreads) {
-        const int s = sample_of_slot[slot0 + e];
-        tab[e] = 1.0f;
-        sv[e] = (s >= 0) ? (float)sqrt(fabs(v[s])) * (F16 ? kF16Scale : 1.0f) : 0.0f;
-    }
-    auto put = [&](int l, int m, float y) {
-        tab[(1 + m) * kExpSlots + l] = 1.41421356f * y;                                  // ho1
-        tab[(1 + nm + m) * kExpSlots + l] = (2.0f * y * y - 1.0f) * 0.70710678f;          // ho2
-        tab[(1 + 2 * nm + m) * kExpSlots + l] = (2.0f * y * y - 3.0f) * y * 0.57735027f;  // ho3
+    // units of the whole launch and this CTA's range
+    int64_t utot = 0;
+    for (int z = 0; z < ncl; z++) utot += nkbp * ((descs[z].nb_pad + kExpChunk - 1) / kExpChunk);
+    const int64_t u0 = utot * blockIdx.x / gridDim.x, u1 = utot * (blockIdx.x + 1) / gridDim.x;
+    if (u0 >= u1) return;
+    int max_nm = 0;
+    for (int z = 0; z < ncl; z++) max_nm = max(max_nm, descs[z].nm);
+    float* tab = smem_f;                                         // [3 nm + 1][64]
+    float* sv = tab + (size_t)(3 * max_nm + 1) * kExpSlots;     // [64]
+    float* stq = sv + kExpSlots;                                 // [nm][64] staged q
+    double* stv = reinterpret_cast<double*>(stq + (size_t)max_nm * kExpSlots);   // [64] staged V
+
+    // Group: the units of one (cluster, k-block) inside [u0, u1).
+    struct Group {
+        int z;
+        int64_t kb;
+        int r0, r1;     // basis rows [r0, r1) of the cluster
     };
-    if ((nm & 3) == 0) {            // 16-byte gathers of each slot's q row
-        const int n4 = nm >> 2;
-        for (int e = t; e < kExpSlots * n4; e += kExpThreads) {
-            const int l = e / n4, m4 = e - l * n4;
-            const int s = sample_of_slot[slot0 + l];
-            const float4 y = (s >= 0) ? reinterpret_cast<const float4*>(q + (int64_t)s * nm)[m4]
-                                      : make_float4(0.f, 0.f, 0.f, 0.f);
-            put(l, 4 * m4, y.x), put(l, 4 * m4 + 1, y.y), put(l, 4 * m4 + 2, y.z), put(l, 4 * m4 + 3, y.w);
+    int zc = 0;
+    int64_t pre = 0;    // first unit of cluster zc
+    auto group_at = [&](int64_t u) {
+        for (;;) {
+            const int64_t nu = nkbp * ((descs[zc].nb_pad + kExpChunk - 1) / kExpChunk);
+            if (u < pre + nu) break;
+            pre += nu;
+            zc++;
         }
-    } else {
-        for (int e = t; e < kExpSlots * nm; e += kExpThreads) {
-            const int l = e / nm, m = e - l * nm;
-            const int s = sample_of_slot[slot0 + l];
-            put(l, m, (s >= 0) ? q[(int64_t)s * nm + m] : 0.0f);
+        const int nrc = (descs[zc].nb_pad + kExpChunk - 1) / kExpChunk;
+        const int64_t w = u - pre;
+        Group g;
+        g.z = zc;
+        g.kb = w / nrc;
+        const int rc = (int)(w - g.kb * nrc);
+        const int64_t gend = min(u1, pre + (g.kb + 1) * nrc);      // first unit after the group
+        g.r0 = rc * kExpChunk;
+        g.r1 = min((int)(rc + (gend - u)) * kExpChunk, descs[zc].nb_pad);
+        return g;
+    };
+    // gathers of a group's q rows and V into the staging area
+    auto issue = [&](const Group& g) {
+        const ExpandDesc d = descs[g.z];
+        const int64_t slot0 = g.kb * kExpSlots;
+        const bool vec = (d.nm & 3) == 0;
+        const int nv = vec ? d.nm >> 2 : d.nm;
+        for (int e = t; e < (nv + 1) * kExpSlots; e += kExpThreads) {
+            const int l = e & (kExpSlots - 1), k = e >> 6;
+            const int s = d.slot_of[slot0 + l];
+            if (k == nv) cp_async(stv + l, d.v + (s >= 0 ? s : 0), 8, s >= 0);
+            else if (vec) cp_async(stq + (size_t)e * 4, d.q + (int64_t)(s >= 0 ? s : 0) * d.nm + 4 * k, 16, s >= 0);
+            else cp_async(stq + e, d.q + (int64_t)(s >= 0 ? s : 0) * d.nm + k, 4, s >= 0);
         }
-    }
-    __syncthreads();
-    const int g = t & 15, rl = t >> 4;
-    const float4 w = reinterpret_cast<const float4*>(sv)[g];
-    const int r0 = blockIdx.y * kExpRows, r1 = min(r0 + kExpRows, nb_pad);
-    // four rows per trip, their descriptors loaded first so the loads overlap
-    constexpr int kStep = kExpThreads / 16;
-    constexpr uint32_t kNone = 0xffffffffu;      // rows beyond nb (zero padding); real factors < 2^30
-    for (int r = r0 + rl; r < r1; r += 4 * kStep) {
-        uint32_t d[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int rr = r + u * kStep;
-            d[u] = (rr < nb && rr < r1) ? __ldg(factors + rr) : kNone;
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int rr = r + u * kStep;
-            if (rr >= r1) break;
-            uint2 hi = make_uint2(0, 0), lo = make_uint2(0, 0);
-            if (d[u] != kNone) {
-                const float4 A = reinterpret_cast<const float4*>(tab + (d[u] & 1023u) * kExpSlots)[g];
-                const float4 B = reinterpret_cast<const float4*>(tab + ((d[u] >> 10) & 1023u) * kExpSlots)[g];
-                const float4 C = reinterpret_cast<const float4*>(tab + (d[u] >> 20) * kExpSlots)[g];
-                const float4 x = make_float4(w.x * (A.x * B.x * C.x), w.y * (A.y * B.y * C.y),
-                                             w.z * (A.z * B.z * C.z), w.w * (A.w * B.w * C.w));
-                split4<F16>(x, hi, lo);
+    };
+    // the table of a group: from the staging area, or (unstaged) gathered here;
+    // slot l goes to table column tab_col(l)
+    auto build = [&](const Group& g) {
+        const ExpandDesc d = descs[g.z];
+        const int nm = d.nm;
+        const int64_t slot0 = g.kb * kExpSlots;
+        auto put = [&](int c, int m, float y) {
+            tab[(1 + m) * kExpSlots + c] = 1.41421356f * y;                                  // ho1
+            tab[(1 + nm + m) * kExpSlots + c] = (2.0f * y * y - 1.0f) * 0.70710678f;          // ho2
+            tab[(1 + 2 * nm + m) * kExpSlots + c] = (2.0f * y * y - 3.0f) * y * 0.57735027f;  // ho3
+        };
+        for (int c = t; c < kExpSlots; c += kExpThreads) {
+            const int l = tab_slot(c);
+            tab[c] = 1.0f;
+            double vv;
+            if (staged) {
+                vv = stv[l];
+            } else {
+                const int s = d.slot_of[slot0 + l];
+                vv = s >= 0 ? d.v[s] : 0.0;
             }
-            // box (row block, k-block blockIdx.x), swizzled: 16-byte chunk g/2 of row rin at (g/2) ^ (rin & 7)
-            const int row = dsc.row0 + rr, rin = row & (kTile - 1);
-            uint16_t* box = xop + ((size_t)(row / kTile) * nkb + blockIdx.x) * (2 * kTile * kExpSlots);
-            const int off = rin * kExpSlots + (((g >> 1) ^ (rin & 7)) << 3) + ((g & 1) << 2);
-            *reinterpret_cast<uint2*>(box + off) = hi;
-            *reinterpret_cast<uint2*>(box + kTile * kExpSlots + off) = lo;
+            sv[c] = (float)sqrt(fabs(vv)) * (F16 ? kF16Scale : 1.0f);
         }
+        if ((nm & 3) == 0) {
+            const int n4 = nm >> 2;
+            for (int e = t; e < n4 * kExpSlots; e += kExpThreads) {
+                const int c = e & (kExpSlots - 1), m4 = e >> 6, l = tab_slot(c);
+                float4 y;
+                if (staged) {
+                    y = reinterpret_cast<const float4*>(stq)[m4 * kExpSlots + l];
+                } else {
+                    const int s = d.slot_of[slot0 + l];
+                    y = s >= 0 ? reinterpret_cast<const float4*>(d.q + (int64_t)s * nm)[m4]
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                put(c, 4 * m4, y.x), put(c, 4 * m4 + 1, y.y), put(c, 4 * m4 + 2, y.z), put(c, 4 * m4 + 3, y.w);
+            }
+        } else {
+            for (int e = t; e < nm * kExpSlots; e += kExpThreads) {
+                const int c = e & (kExpSlots - 1), m = e >> 6, l = tab_slot(c);
+                float y;
+                if (staged) {
+                    y = stq[m * kExpSlots + l];
+                } else {
+                    const int s = d.slot_of[slot0 + l];
+                    y = s >= 0 ? d.q[(int64_t)s * nm + m] : 0.0f;
+                }
+                put(c, m, y);
+            }
+        }
+    };
+
+    const int g8 = t & 7, rl = t >> 3;
+    constexpr int kStep = kExpThreads / 8;                 // rows per trip of the CTA
+    constexpr uint32_t kNone = 0xffffffffu;                // rows beyond nb (zero padding); real factors < 2^30
+    Group cur = group_at(u0);
+    if (staged) {
+        issue(cur);
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    build(cur);
+    __syncthreads();
+    for (;;) {
+        const int64_t nxt_u = pre + (cur.kb + 1) * ((descs[cur.z].nb_pad + kExpChunk - 1) / kExpChunk);
+        const bool more = nxt_u < u1;
+        Group nxt{};
+        if (more) {
+            nxt = group_at(nxt_u);
+            if (staged) issue(nxt);
+        }
+        // rows [r0, r1) of (cluster, k-block)
+        {
+            const uint32_t* __restrict__ factors = descs[cur.z].factors;
+            const int nb = descs[cur.z].nb, row0 = descs[cur.z].row0;
+            const float4* tab4 = reinterpret_cast<const float4*>(tab);
+            const float4 w0 = reinterpret_cast<const float4*>(sv)[g8];
+            const float4 w1 = reinterpret_cast<const float4*>(sv)[g8 + 8];
+            uint16_t* xkb = xop + (size_t)cur.kb * (2 * kTile * kExpSlots);
+            for (int r = cur.r0 + rl; r < cur.r1; r += 4 * kStep) {
+                uint32_t f[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int rr = r + u * kStep;
+                    f[u] = (rr < nb && rr < cur.r1) ? __ldg(factors + rr) : kNone;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int rr = r + u * kStep;
+                    if (rr >= cur.r1) break;
+                    uint4 hi = make_uint4(0, 0, 0, 0), lo = hi;
+                    if (f[u] != kNone) {
+                        const float4* A = tab4 + (f[u] & 1023u) * (kExpSlots / 4) + g8;
+                        const float4* B = tab4 + ((f[u] >> 10) & 1023u) * (kExpSlots / 4) + g8;
+                        const float4* C = tab4 + (f[u] >> 20) * (kExpSlots / 4) + g8;
+                        const float4 a0 = A[0], a1 = A[8], b0 = B[0], b1 = B[8], c0 = C[0], c1 = C[8];
+                        split2<F16>(w0.x * (a0.x * b0.x * c0.x), w0.y * (a0.y * b0.y * c0.y), hi.x, lo.x);
+                        split2<F16>(w0.z * (a0.z * b0.z * c0.z), w0.w * (a0.w * b0.w * c0.w), hi.y, lo.y);
+                        split2<F16>(w1.x * (a1.x * b1.x * c1.x), w1.y * (a1.y * b1.y * c1.y), hi.z, lo.z);
+                        split2<F16>(w1.z * (a1.z * b1.z * c1.z), w1.w * (a1.w * b1.w * c1.w), hi.w, lo.w);
+                    }
+                    // box (row block, k-block), swizzled: 16-byte chunk g8 of row rin at g8 ^ (rin & 7)
+                    const int row = row0 + rr, rin = row & (kTile - 1);
+                    uint16_t* box = xkb + (size_t)(row / kTile) * nkb * (2 * kTile * kExpSlots);
+                    const int off = rin * kExpSlots + ((g8 ^ (rin & 7)) << 3);
+                    *reinterpret_cast<uint4*>(box + off) = hi;
+                    *reinterpret_cast<uint4*>(box + kTile * kExpSlots + off) = lo;
+                }
+            }
+        }
+        if (!more) break;
+        if (staged) cp_async_wait_all();
+        __syncthreads();          // every row of cur written: the table is free
+        build(nxt);
+        __syncthreads();
+        cur = nxt;
     }
 }
 
@@ -667,11 +807,19 @@ int launch_partition(const double* v, int64_t v_stride, int* slot_of, int64_t sl
 int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t nkb,
                   uint16_t* x, bool f16, cudaStream_t s)
 {
-    const size_t sm = sizeof(float) * (size_t)(3 * max_nm + 2) * kExpSlots;
+    constexpr size_t kMaxSmem = 227 * 1024;
+    const bool staged = expand_smem(max_nm, true) <= kMaxSmem;
+    const size_t sm = expand_smem(max_nm, staged);
     auto kern = f16 ? expand_split_kernel<true> : expand_split_kernel<false>;
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    dim3 eg((unsigned)(slots / kExpSlots), (unsigned)((max_nb_pad + kExpRows - 1) / kExpRows), (unsigned)nclusters);
-    kern<<<eg, kExpThreads, sm, s>>>(descs_dev, nkb, x);
+    int dev = 0, sms = 148, per = 0;
+    SCP3_CUDA(cudaGetDevice(&dev));
+    SCP3_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SCP3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kExpThreads, sm));
+    const int64_t nkbp = slots / kExpSlots;
+    const int64_t units_max = nkbp * nclusters * ((max_nb_pad + kExpChunk - 1) / kExpChunk);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)std::max(per, 1) * sms, units_max));
+    kern<<<grid, kExpThreads, sm, s>>>(descs_dev, nclusters, nkbp, nkb, staged ? 1 : 0, x);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }

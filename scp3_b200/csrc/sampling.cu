@@ -19,7 +19,8 @@ namespace scp3 {
 namespace {
 
 constexpr int kWarpsPerBlock = 8;
-constexpr int kRun = 16;          // consecutive samples per warp (Gray-code walk)
+constexpr int kRun = 16;          // samples per warp of a batch launch (Gray-code walk)
+constexpr int kMinRun = 8;        // fewest samples per warp of a single launch
 
 template <typename T>
 struct WarpSlot {
@@ -68,8 +69,17 @@ __device__ inline double potential(const WarpSlot<T>& w, int nw, const uint32_t*
     return ttm::energy_warp<T>(w.crd, w.ms, w.ttm, nw, tasks, ntasks, lane, iters);
 }
 
-// MUa is staged in shared memory (FP64) when it fits this many bytes.
+// MUa is staged in shared memory (FP64) when it fits this many bytes, as
+// coordinate pairs: for mode k and coordinate group g (64 coordinates), lane l
+// reads {MUa[k][64g + l], MUa[k][64g + 32 + l]} as one 16-byte word (zero past
+// the last coordinate).
 constexpr size_t kMuaSmemMax = 64 * 1024;
+
+__host__ __device__ inline int mua_groups(int nw) { return (9 * nw + 63) / 64; }
+__host__ __device__ inline size_t mua_smem_bytes(int nw, int nm0)
+{
+    return sizeof(double) * 64 * (size_t)mua_groups(nw) * nm0;
+}
 
 template <int PES, typename T>
 __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem);
@@ -95,29 +105,35 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
 {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int nw = a.nw, nm0 = a.nm0, N3 = 9 * nw;
-    const size_t mua_b = sizeof(double) * (size_t)N3 * nm0;
+    const size_t mua_b = mua_smem_bytes(nw, nm0);
     const bool mua_in_smem = mua_b <= kMuaSmemMax;
+    const int ng = mua_groups(nw);
     const double* MUa = a.MUa;
+    double2* mua2 = reinterpret_cast<double2*>(smem);      // [nm0][ng][32] coordinate pairs
     if (mua_in_smem) {
-        double* m = reinterpret_cast<double*>(smem);
-        for (int e = threadIdx.x; e < N3 * nm0; e += blockDim.x) m[e] = a.MUa[e];
-        MUa = m;
+        for (int e = threadIdx.x; e < nm0 * ng * 32; e += blockDim.x) {
+            const int l = e & 31, g = (e >> 5) % ng, k = (e >> 5) / ng, c = 64 * g + l;
+            mua2[e] = make_double2(c < N3 ? a.MUa[(size_t)k * N3 + c] : 0.0,
+                                   c + 32 < N3 ? a.MUa[(size_t)k * N3 + c + 32] : 0.0);
+        }
         __syncthreads();
     }
-    char* slots = smem + (mua_in_smem ? (mua_b + 15) / 16 * 16 : 0);
+    char* slots = smem + (mua_in_smem ? mua_b : 0);
     const bool grad = a.vq != nullptr;
     WarpSlot<T> w = warp_slot<T>(slots + wib * slot_bytes<T>(PES, nm0, nw, grad), PES, nm0, nw, grad);
-    // Each warp takes runs of kRun consecutive samples: the Sobol state of the
-    // first is formed from the Gray code of its index, the next ones by one XOR
-    // per dimension (index k differs from k-1 in direction number ctz(k)).
+    // Each warp takes one contiguous range of samples, the ranges balanced to
+    // within one sample (the grid is sized to the SMs, so there is no tail wave):
+    // the Sobol state of the first is formed from the Gray code of its index, the
+    // next ones by one XOR per dimension (index k differs from k-1 in direction
+    // number ctz(k)).
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
-    const int64_t nruns = (a.n + kRun - 1) / kRun;
+    const int64_t gw = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
     constexpr int kDimsPerLane = 4;           // dimensions up to 128 keep their state in registers
-    for (int64_t run = (int64_t)blockIdx.x * kWarpsPerBlock + wib; run < nruns; run += nwarps) {
+    {
         uint64_t st[kDimsPerLane];
-        const int64_t s_first = run * kRun;
+        const int64_t s_first = a.n * gw / nwarps, s_end = a.n * (gw + 1) / nwarps;
         const bool sobol = a.normals == nullptr;
-      for (int64_t s = s_first; s < s_first + kRun && s < a.n; s++) {
+      for (int64_t s = s_first; s < s_end; s++) {
         if (s >= a.nvalid) {        // padding sample: contributes nothing
             if (lane == 0) a.v[s] = 0.0;
             for (int m = lane; m < a.nm; m += 32) {
@@ -155,18 +171,47 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
             w.q[d] = y / 1.4142135623730951;
         }
         __syncwarp();
-        // 2. r = bohr * (x0 + MUa q)   (SCP3.cpp:208), FP64; a lane's two coordinates in one pass
-        for (int c = lane; c < N3; c += 64) {
-            const bool two = c + 32 < N3;
-            double acc0 = 0.0, acc1 = 0.0;
-#pragma unroll 4
-            for (int k = 0; k < nm0; k++) {
-                const double qk = w.q[k];
-                acc0 += MUa[(size_t)k * N3 + c] * qk;
-                if (two) acc1 += MUa[(size_t)k * N3 + c + 32] * qk;
+        // 2. r = bohr * (x0 + MUa q)   (SCP3.cpp:208), FP64; a lane's two coordinates
+        // (c, c + 32) in one pass, each summed over k in order
+        if (mua_in_smem) {
+            const double2* q2 = reinterpret_cast<const double2*>(w.q);
+            for (int g = 0; g < ng; g++) {
+                const int c = 64 * g + lane;
+                const double2* mg = mua2 + g * 32 + lane;
+                const int kstride = ng * 32;
+                double acc0 = 0.0, acc1 = 0.0;
+                int k = 0;
+#pragma unroll 2
+                for (; k + 1 < nm0; k += 2) {
+                    const double2 qq = q2[k >> 1];
+                    const double2 m0 = mg[k * kstride], m1 = mg[(k + 1) * kstride];
+                    acc0 += m0.x * qq.x;
+                    acc1 += m0.y * qq.x;
+                    acc0 += m1.x * qq.y;
+                    acc1 += m1.y * qq.y;
+                }
+                if (k < nm0) {
+                    const double qk = w.q[k];
+                    const double2 m0 = mg[k * kstride];
+                    acc0 += m0.x * qk;
+                    acc1 += m0.y * qk;
+                }
+                if (c < N3) w.crd[c] = (T)(kBohr * (__ldg(a.x0 + c) + acc0));
+                if (c + 32 < N3) w.crd[c + 32] = (T)(kBohr * (__ldg(a.x0 + c + 32) + acc1));
             }
-            w.crd[c] = (T)(kBohr * (__ldg(a.x0 + c) + acc0));
-            if (two) w.crd[c + 32] = (T)(kBohr * (__ldg(a.x0 + c + 32) + acc1));
+        } else {
+            for (int c = lane; c < N3; c += 64) {
+                const bool two = c + 32 < N3;
+                double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll 4
+                for (int k = 0; k < nm0; k++) {
+                    const double qk = w.q[k];
+                    acc0 += MUa[(size_t)k * N3 + c] * qk;
+                    if (two) acc1 += MUa[(size_t)k * N3 + c + 32] * qk;
+                }
+                w.crd[c] = (T)(kBohr * (__ldg(a.x0 + c) + acc0));
+                if (two) w.crd[c + 32] = (T)(kBohr * (__ldg(a.x0 + c + 32) + acc1));
+            }
         }
         __syncwarp();
         // 3. V in hartree, anharmonic residual   (SCP3.cpp:219-223)
@@ -283,6 +328,21 @@ __global__ void std_normal_kernel(int dims, int64_t index0, int64_t n, const int
     out[t] = bsm(sobol_uniform(x));
 }
 
+// Blocks of the per-sample kernel: one warp per kMinRun samples at least, and
+// no more blocks than the SMs hold at once.
+template <typename K>
+int sample_grid(K kern, size_t smem, int64_t n)
+{
+    int dev = 0, sms = 148, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kWarpsPerBlock * 32, smem) != cudaSuccess || per < 1)
+        per = 1;
+    const int64_t want = (n + (int64_t)kMinRun * kWarpsPerBlock - 1) / ((int64_t)kMinRun * kWarpsPerBlock);
+    const int64_t cap = (int64_t)per * sms;
+    return (int)std::max<int64_t>(1, std::min(want, cap));
+}
+
 int grid_for(int64_t nwarps_needed)
 {
     int dev = 0, sms = 148;
@@ -296,12 +356,12 @@ int grid_for(int64_t nwarps_needed)
 template <int PES, typename T>
 int launch_samples_t(const SampleArgs& a, cudaStream_t s)
 {
-    const size_t mua_b = sizeof(double) * (size_t)9 * a.nw * a.nm0;
+    const size_t mua_b = mua_smem_bytes(a.nw, a.nm0);
     const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw, a.vq != nullptr) +
-                      (mua_b <= kMuaSmemMax ? (mua_b + 15) / 16 * 16 : 0);
+                      (mua_b <= kMuaSmemMax ? mua_b : 0);
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_kernel<PES, T>,
                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    samples_kernel<PES, T><<<grid_for((a.n + kRun - 1) / kRun), kWarpsPerBlock * 32, sm, s>>>(a);
+    samples_kernel<PES, T><<<sample_grid(samples_kernel<PES, T>, sm, a.n), kWarpsPerBlock * 32, sm, s>>>(a);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }
@@ -317,8 +377,8 @@ int launch_samples_batch_t(const SampleArgs* args_host, const SampleArgs* args_d
     for (int c = 0; c < ncl; c++) {
         nm0 = std::max(nm0, args_host[c].nm0);
         nw = std::max(nw, args_host[c].nw);
-        const size_t b = sizeof(double) * (size_t)9 * args_host[c].nw * args_host[c].nm0;
-        if (b <= kMuaSmemMax) mua = std::max(mua, (b + 15) / 16 * 16);
+        const size_t b = mua_smem_bytes(args_host[c].nw, args_host[c].nm0);
+        if (b <= kMuaSmemMax) mua = std::max(mua, b);
     }
     const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, nm0, nw) + mua;
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_batch_kernel<PES, T>,
