@@ -55,18 +55,21 @@ __device__ __forceinline__ double bsm(double u)
 }
 
 // The same inverse CDF in FP32 for the FP32 form, from the 62-bit Sobol state x
-// (u = x 2^-62): the upper tail takes 1 - u = (2^62 - x) 2^-62 exactly from the
-// integer state instead of subtracting rounded floats.
+// (u = x 2^-62, one rounding to FP32): the upper tail takes 1 - u = (2^62 - x)
+// 2^-62 from the integer state instead of subtracting rounded floats.  The
+// central branch's rational function divides with __fdividef (the denominator
+// lies in [0.11, 1]; within 2 ulp).
 __device__ __forceinline__ float bsm_f32(uint64_t x)
 {
-    const float u = (float)((double)(int64_t)x * 0x1p-62);
+    const float u = (float)(int64_t)x * 0x1p-62f;
     const float y = u - 0.5f;
     if (fabsf(y) < 0.42f) {
         const float r = y * y;
-        return y * (((-25.44106049637f * r + 41.39119773534f) * r + -18.61500062529f) * r + 2.50662823884f) /
-               ((((3.13082909833f * r + -21.06224101826f) * r + 23.08336743743f) * r + -8.47351093090f) * r + 1.0f);
+        return __fdividef(
+            y * (((-25.44106049637f * r + 41.39119773534f) * r + -18.61500062529f) * r + 2.50662823884f),
+            (((3.13082909833f * r + -21.06224101826f) * r + 23.08336743743f) * r + -8.47351093090f) * r + 1.0f);
     }
-    const float tail = (y > 0) ? (float)((double)(int64_t)((1ull << 62) - x) * 0x1p-62) : u;
+    const float tail = (y > 0) ? (float)(int64_t)((1ull << 62) - x) * 0x1p-62f : u;
     const float r = logf(-logf(tail));
     const float t = 0.3374754822726147f +
                     r * (0.9761690190917186f +

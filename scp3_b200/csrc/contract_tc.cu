@@ -662,10 +662,14 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandD
                     if (rr >= cur.r1) break;
                     uint4 hi = make_uint4(0, 0, 0, 0), lo = hi;
                     if (f[u] != kNone) {
+                        // factor 0 is the constant 1: not read (most rows have one or two)
+                        const uint32_t ib = (f[u] >> 10) & 1023u, ic = f[u] >> 20;
                         const float4* A = tab4 + (f[u] & 1023u) * (kExpSlots / 4) + g8;
-                        const float4* B = tab4 + ((f[u] >> 10) & 1023u) * (kExpSlots / 4) + g8;
-                        const float4* C = tab4 + (f[u] >> 20) * (kExpSlots / 4) + g8;
-                        const float4 a0 = A[0], a1 = A[8], b0 = B[0], b1 = B[8], c0 = C[0], c1 = C[8];
+                        const float4 a0 = A[0], a1 = A[8];
+                        const float4 one = make_float4(1.f, 1.f, 1.f, 1.f);
+                        float4 b0 = one, b1 = one, c0 = one, c1 = one;
+                        if (ib) b0 = tab4[ib * (kExpSlots / 4) + g8], b1 = tab4[ib * (kExpSlots / 4) + g8 + 8];
+                        if (ic) c0 = tab4[ic * (kExpSlots / 4) + g8], c1 = tab4[ic * (kExpSlots / 4) + g8 + 8];
                         split2<F16>(w0.x * (a0.x * b0.x * c0.x), w0.y * (a0.y * b0.y * c0.y), hi.x, lo.x);
                         split2<F16>(w0.z * (a0.z * b0.z * c0.z), w0.w * (a0.w * b0.w * c0.w), hi.y, lo.y);
                         split2<F16>(w1.x * (a1.x * b1.x * c1.x), w1.y * (a1.y * b1.y * c1.y), hi.z, lo.z);

@@ -22,20 +22,26 @@ constexpr int kWarpsPerBlock = 8;
 constexpr int kRun = 16;          // samples per warp of a batch launch (Gray-code walk)
 constexpr int kMinRun = 8;        // fewest samples per warp of a single launch
 
+// Samples a warp carries through the back-transform together, so that every
+// shared-memory read of MUa serves this many samples (the back-transform is
+// bound by shared-memory bandwidth, MUa being re-read for every sample).
+constexpr int kGroup = 4;
+
 template <typename T>
 struct WarpSlot {
-    double* q;      // nm0
-    T* crd;         // 9nw
+    T* q;           // [group][qs] normal coordinates (the form's precision)
+    T* crd;         // [group][9nw] geometries
     T* ms;          // 3nw
     T* ttm;         // TTM3-F scratch
     double* g;      // 9nw gradient (gradient path)
     double* gm;     // 3nw forces on the M sites
+    int qs;         // q stride: nm0 rounded up to even (16-byte aligned rows)
 };
 
 template <typename T>
-__host__ __device__ inline size_t slot_bytes(int pes, int nm0, int nw, bool grad = false)
+__host__ __device__ inline size_t slot_bytes(int pes, int nm0, int nw, bool grad = false, int group = 1)
 {
-    size_t b = sizeof(double) * (size_t)((nm0 + 1) & ~1) + sizeof(T) * (size_t)(12 * nw);
+    size_t b = sizeof(T) * ((size_t)group * ((nm0 + 1) & ~1) + (size_t)(9 * nw * group + 3 * nw));
     if (pes == SCP3GPU_PES_TTM3F) b += sizeof(T) * ttm::scratch_elems(nw, grad);
     b = (b + 7) & ~(size_t)7;
     if (grad) b += sizeof(double) * (size_t)(12 * nw);
@@ -43,14 +49,15 @@ __host__ __device__ inline size_t slot_bytes(int pes, int nm0, int nw, bool grad
 }
 
 template <typename T>
-__device__ inline WarpSlot<T> warp_slot(char* base, int pes, int nm0, int nw, bool grad = false)
+__device__ inline WarpSlot<T> warp_slot(char* base, int pes, int nm0, int nw, bool grad = false, int group = 1)
 {
     WarpSlot<T> s;
-    s.q = reinterpret_cast<double*>(base);
-    s.crd = reinterpret_cast<T*>(s.q + ((nm0 + 1) & ~1));
-    s.ms = s.crd + 9 * nw;
+    s.qs = (nm0 + 1) & ~1;
+    s.q = reinterpret_cast<T*>(base);
+    s.crd = s.q + (size_t)group * s.qs;
+    s.ms = s.crd + 9 * nw * group;
     s.ttm = s.ms + 3 * nw;
-    size_t off = sizeof(double) * (size_t)((nm0 + 1) & ~1) + sizeof(T) * (size_t)(12 * nw);
+    size_t off = sizeof(T) * ((size_t)group * s.qs + (size_t)(9 * nw * group + 3 * nw));
     if (pes == SCP3GPU_PES_TTM3F) off += sizeof(T) * ttm::scratch_elems(nw, grad);
     off = (off + 7) & ~(size_t)7;
     s.g = grad ? reinterpret_cast<double*>(base + off) : nullptr;
@@ -59,27 +66,39 @@ __device__ inline WarpSlot<T> warp_slot(char* base, int pes, int nm0, int nw, bo
 }
 
 template <int PES, typename T>
-__device__ inline double potential(const WarpSlot<T>& w, int nw, const uint32_t* tasks, int ntasks, int lane,
-                                   int* iters)
+__device__ inline double potential(const T* crd, const WarpSlot<T>& w, int nw, const uint32_t* tasks, int ntasks,
+                                   int lane, int* iters)
 {
     if (PES == SCP3GPU_PES_QTIP4PF) {
         *iters = 0;
-        return qt::energy_warp<T>(w.crd, w.ms, nw, tasks, ntasks, lane);
+        return qt::energy_warp<T>(crd, w.ms, nw, tasks, ntasks, lane);
     }
-    return ttm::energy_warp<T>(w.crd, w.ms, w.ttm, nw, tasks, ntasks, lane, iters);
+    return ttm::energy_warp<T>(crd, w.ms, w.ttm, nw, tasks, ntasks, lane, iters);
 }
 
-// MUa is staged in shared memory (FP64) when it fits this many bytes, as
-// coordinate pairs: for mode k and coordinate group g (64 coordinates), lane l
-// reads {MUa[k][64g + l], MUa[k][64g + 32 + l]} as one 16-byte word (zero past
-// the last coordinate).
+// MUa is staged in shared memory, in the form's precision, when it fits this
+// many bytes, as coordinate pairs: for mode k and coordinate group g (64
+// coordinates), lane l reads {MUa[k][64g + l], MUa[k][64g + 32 + l]} as one
+// word (zero past the last coordinate).
 constexpr size_t kMuaSmemMax = 64 * 1024;
 
 __host__ __device__ inline int mua_groups(int nw) { return (9 * nw + 63) / 64; }
+template <typename T>
 __host__ __device__ inline size_t mua_smem_bytes(int nw, int nm0)
 {
-    return sizeof(double) * 64 * (size_t)mua_groups(nw) * nm0;
+    return sizeof(T) * 64 * (size_t)mua_groups(nw) * nm0;
 }
+
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+template <>
+struct Pair<float> {
+    using type = float2;
+};
 
 template <int PES, typename T>
 __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem);
@@ -105,162 +124,198 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
 {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int nw = a.nw, nm0 = a.nm0, N3 = 9 * nw;
-    const size_t mua_b = mua_smem_bytes(nw, nm0);
+    using T2 = typename Pair<T>::type;
+    const size_t mua_b = mua_smem_bytes<T>(nw, nm0);
     const bool mua_in_smem = mua_b <= kMuaSmemMax;
     const int ng = mua_groups(nw);
     const double* MUa = a.MUa;
-    double2* mua2 = reinterpret_cast<double2*>(smem);      // [nm0][ng][32] coordinate pairs
+    T2* mua2 = reinterpret_cast<T2*>(smem);      // [nm0][ng][32] coordinate pairs
     if (mua_in_smem) {
         for (int e = threadIdx.x; e < nm0 * ng * 32; e += blockDim.x) {
             const int l = e & 31, g = (e >> 5) % ng, k = (e >> 5) / ng, c = 64 * g + l;
-            mua2[e] = make_double2(c < N3 ? a.MUa[(size_t)k * N3 + c] : 0.0,
-                                   c + 32 < N3 ? a.MUa[(size_t)k * N3 + c + 32] : 0.0);
+            T2 m;
+            m.x = (T)(c < N3 ? a.MUa[(size_t)k * N3 + c] : 0.0);
+            m.y = (T)(c + 32 < N3 ? a.MUa[(size_t)k * N3 + c + 32] : 0.0);
+            mua2[e] = m;
         }
         __syncthreads();
     }
     char* slots = smem + (mua_in_smem ? mua_b : 0);
     const bool grad = a.vq != nullptr;
-    WarpSlot<T> w = warp_slot<T>(slots + wib * slot_bytes<T>(PES, nm0, nw, grad), PES, nm0, nw, grad);
+    WarpSlot<T> w = warp_slot<T>(slots + wib * slot_bytes<T>(PES, nm0, nw, grad, kGroup), PES, nm0, nw, grad, kGroup);
     // Each warp takes one contiguous range of samples, the ranges balanced to
     // within one sample (the grid is sized to the SMs, so there is no tail wave):
     // the Sobol state of the first is formed from the Gray code of its index, the
     // next ones by one XOR per dimension (index k differs from k-1 in direction
-    // number ctz(k)).
+    // number ctz(k)).  The range goes in groups of kGroup samples: normals for
+    // the group, one back-transform pass for the group, then the potential per
+    // sample.
     const int64_t nwarps = (int64_t)gridDim.x * kWarpsPerBlock;
     const int64_t gw = (int64_t)blockIdx.x * kWarpsPerBlock + wib;
     constexpr int kDimsPerLane = 4;           // dimensions up to 128 keep their state in registers
-    {
-        uint64_t st[kDimsPerLane];
-        const int64_t s_first = a.n * gw / nwarps, s_end = a.n * (gw + 1) / nwarps;
-        const bool sobol = a.normals == nullptr;
-      for (int64_t s = s_first; s < s_end; s++) {
-        if (s >= a.nvalid) {        // padding sample: contributes nothing
-            if (lane == 0) a.v[s] = 0.0;
-            for (int m = lane; m < a.nm; m += 32) {
-                if (a.q64) a.q64[s * a.nm + m] = 0.0;
-                if (a.q32) a.q32[s * a.nm + m] = 0.0f;
-                if (a.vq) a.vq[s * a.nm + m] = 0.0;
-            }
-            continue;
-        }
+    uint64_t st[kDimsPerLane];
+    const int64_t s_first = a.n * gw / nwarps, s_end = a.n * (gw + 1) / nwarps;
+    const bool sobol = a.normals == nullptr;
+    for (int64_t s0 = s_first; s0 < s_end; s0 += kGroup) {
+        const int gn = (int)(s_end - s0 < kGroup ? s_end - s0 : kGroup);
         // 1. standard normals -> q   (SCP3.cpp:196-201)
-        const uint64_t idx = (uint64_t)(a.index0 + s);
-#pragma unroll
-        for (int j = 0; j < kDimsPerLane; j++) {
-            const int d = lane + 32 * j;
-            if (d >= nm0) break;
-            double y;
-            if (!sobol) {
-                y = a.normals[s * nm0 + d];
-            } else {
-                if (s == s_first) st[j] = sobol_state(a.vdir, nm0, d, idx);
-                else st[j] ^= (uint64_t)__ldg(a.vdir + (size_t)(__ffsll((long long)idx) - 1) * nm0 + d);
-                const uint64_t x = a.shift ? st[j] ^ __ldg(a.shift + d) : st[j];
-                if (sizeof(T) == 4) {              // FP32 form: inverse CDF in FP32
-                    w.q[d] = (double)(bsm_f32(x) * 0.70710678f);
-                    continue;
-                }
-                y = bsm(sobol_uniform(x));
+        for (int j = 0; j < gn; j++) {
+            const int64_t s = s0 + j;
+            T* q = w.q + j * w.qs;
+            if (s >= a.nvalid) {        // padding sample (the range's tail): contributes nothing
+                for (int d = lane; d < nm0; d += 32) q[d] = T(0);
+                continue;
             }
-            w.q[d] = y / 1.4142135623730951;   // by /= sqrt(2.0)
-        }
-        for (int d = lane + 32 * kDimsPerLane; d < nm0; d += 32) {   // beyond 128 dimensions
-            double y = sobol ? bsm(sobol_uniform((a.shift ? __ldg(a.shift + d) : 0ull) ^
-                                                 sobol_state(a.vdir, nm0, d, idx)))
-                             : a.normals[s * nm0 + d];
-            w.q[d] = y / 1.4142135623730951;
+            const uint64_t idx = (uint64_t)(a.index0 + s);
+#pragma unroll
+            for (int jd = 0; jd < kDimsPerLane; jd++) {
+                const int d = lane + 32 * jd;
+                if (d >= nm0) break;
+                double y;
+                if (!sobol) {
+                    y = a.normals[s * nm0 + d];
+                } else {
+                    if (s == s_first) st[jd] = sobol_state(a.vdir, nm0, d, idx);
+                    else st[jd] ^= (uint64_t)__ldg(a.vdir + (size_t)(__ffsll((long long)idx) - 1) * nm0 + d);
+                    const uint64_t x = a.shift ? st[jd] ^ __ldg(a.shift + d) : st[jd];
+                    if (sizeof(T) == 4) {              // FP32 form: inverse CDF in FP32
+                        q[d] = (T)(bsm_f32(x) * 0.70710678f);
+                        continue;
+                    }
+                    y = bsm(sobol_uniform(x));
+                }
+                q[d] = (T)(y / 1.4142135623730951);   // by /= sqrt(2.0)
+            }
+            for (int d = lane + 32 * kDimsPerLane; d < nm0; d += 32) {   // beyond 128 dimensions
+                double y = sobol ? bsm(sobol_uniform((a.shift ? __ldg(a.shift + d) : 0ull) ^
+                                                     sobol_state(a.vdir, nm0, d, idx)))
+                                 : a.normals[s * nm0 + d];
+                q[d] = (T)(y / 1.4142135623730951);
+            }
         }
         __syncwarp();
-        // 2. r = bohr * (x0 + MUa q)   (SCP3.cpp:208), FP64; a lane's two coordinates
-        // (c, c + 32) in one pass, each summed over k in order
+        // 2. r = bohr * (x0 + MUa q)   (SCP3.cpp:208), in the form's precision (FP64
+        // for the plain form); a lane's two coordinates (c, c + 32) of every sample
+        // of the group in one pass, each summed over k in order (samples past gn
+        // compute stale values that are not used)
         if (mua_in_smem) {
-            const double2* q2 = reinterpret_cast<const double2*>(w.q);
             for (int g = 0; g < ng; g++) {
                 const int c = 64 * g + lane;
-                const double2* mg = mua2 + g * 32 + lane;
+                const T2* mg = mua2 + g * 32 + lane;
                 const int kstride = ng * 32;
-                double acc0 = 0.0, acc1 = 0.0;
+                T acc0[kGroup], acc1[kGroup];
+#pragma unroll
+                for (int j = 0; j < kGroup; j++) acc0[j] = acc1[j] = T(0);
                 int k = 0;
-#pragma unroll 2
                 for (; k + 1 < nm0; k += 2) {
-                    const double2 qq = q2[k >> 1];
-                    const double2 m0 = mg[k * kstride], m1 = mg[(k + 1) * kstride];
-                    acc0 += m0.x * qq.x;
-                    acc1 += m0.y * qq.x;
-                    acc0 += m1.x * qq.y;
-                    acc1 += m1.y * qq.y;
+                    const T2 m0 = mg[k * kstride], m1 = mg[(k + 1) * kstride];
+#pragma unroll
+                    for (int j = 0; j < kGroup; j++) {
+                        const T2 qq = reinterpret_cast<const T2*>(w.q + j * w.qs)[k >> 1];
+                        acc0[j] += m0.x * qq.x;
+                        acc1[j] += m0.y * qq.x;
+                        acc0[j] += m1.x * qq.y;
+                        acc1[j] += m1.y * qq.y;
+                    }
                 }
                 if (k < nm0) {
-                    const double qk = w.q[k];
-                    const double2 m0 = mg[k * kstride];
-                    acc0 += m0.x * qk;
-                    acc1 += m0.y * qk;
+                    const T2 m0 = mg[k * kstride];
+#pragma unroll
+                    for (int j = 0; j < kGroup; j++) {
+                        const T qk = w.q[j * w.qs + k];
+                        acc0[j] += m0.x * qk;
+                        acc1[j] += m0.y * qk;
+                    }
                 }
-                if (c < N3) w.crd[c] = (T)(kBohr * (__ldg(a.x0 + c) + acc0));
-                if (c + 32 < N3) w.crd[c + 32] = (T)(kBohr * (__ldg(a.x0 + c + 32) + acc1));
+                const T x0a = (T)(c < N3 ? __ldg(a.x0 + c) : 0.0), x0b = (T)(c + 32 < N3 ? __ldg(a.x0 + c + 32) : 0.0);
+#pragma unroll
+                for (int j = 0; j < kGroup; j++) {
+                    if (j >= gn) break;
+                    T* crd = w.crd + j * N3;
+                    if (c < N3) crd[c] = (T)kBohr * (x0a + acc0[j]);
+                    if (c + 32 < N3) crd[c + 32] = (T)kBohr * (x0b + acc1[j]);
+                }
             }
         } else {
-            for (int c = lane; c < N3; c += 64) {
-                const bool two = c + 32 < N3;
-                double acc0 = 0.0, acc1 = 0.0;
+            for (int j = 0; j < gn; j++) {
+                const T* q = w.q + j * w.qs;
+                T* crd = w.crd + j * N3;
+                for (int c = lane; c < N3; c += 64) {
+                    const bool two = c + 32 < N3;
+                    double acc0 = 0.0, acc1 = 0.0;
 #pragma unroll 4
-                for (int k = 0; k < nm0; k++) {
-                    const double qk = w.q[k];
-                    acc0 += MUa[(size_t)k * N3 + c] * qk;
-                    if (two) acc1 += MUa[(size_t)k * N3 + c + 32] * qk;
+                    for (int k = 0; k < nm0; k++) {
+                        const double qk = (double)q[k];
+                        acc0 += MUa[(size_t)k * N3 + c] * qk;
+                        if (two) acc1 += MUa[(size_t)k * N3 + c + 32] * qk;
+                    }
+                    crd[c] = (T)(kBohr * (__ldg(a.x0 + c) + acc0));
+                    if (two) crd[c + 32] = (T)(kBohr * (__ldg(a.x0 + c + 32) + acc1));
                 }
-                w.crd[c] = (T)(kBohr * (__ldg(a.x0 + c) + acc0));
-                if (two) w.crd[c + 32] = (T)(kBohr * (__ldg(a.x0 + c + 32) + acc1));
             }
         }
         __syncwarp();
-        // 3. V in hartree, anharmonic residual   (SCP3.cpp:219-223)
-        int iters = 0;
-        double V = 0.0;
-        if constexpr (sizeof(T) == 8) {
-            if (grad) {
-                // gradient path (SCP3.cpp:209-216): V and dV/dr, then
-                // dV_anh/dq = MUa^T (bohr dV/dr / autokcal) - omega % q, selected modes
-                double e;
-                if constexpr (PES == SCP3GPU_PES_QTIP4PF)
-                    e = qt::energy_grad_warp(reinterpret_cast<const double*>(w.crd), reinterpret_cast<double*>(w.ms),
-                                             w.g, w.gm, nw, a.tasks, a.ntasks, lane);
-                else
-                    e = ttm::energy_grad_warp(reinterpret_cast<const double*>(w.crd),
-                                              reinterpret_cast<double*>(w.ms), reinterpret_cast<double*>(w.ttm),
-                                              w.g, nw, a.tasks, a.ntasks, lane, &iters);
+        for (int j = 0; j < gn; j++) {
+            const int64_t s = s0 + j;
+            const T* q = w.q + j * w.qs;
+            const T* crd = w.crd + j * N3;
+            if (s >= a.nvalid) {
+                if (lane == 0) a.v[s] = 0.0;
+                for (int m = lane; m < a.nm; m += 32) {
+                    if (a.q64) a.q64[s * a.nm + m] = 0.0;
+                    if (a.q32) a.q32[s * a.nm + m] = 0.0f;
+                    if (a.vq) a.vq[s * a.nm + m] = 0.0;
+                }
+                continue;
+            }
+            // 3. V in hartree, anharmonic residual   (SCP3.cpp:219-223)
+            int iters = 0;
+            double V = 0.0;
+            if constexpr (sizeof(T) == 8) {
+                if (grad) {
+                    // gradient path (SCP3.cpp:209-216): V and dV/dr, then
+                    // dV_anh/dq = MUa^T (bohr dV/dr / autokcal) - omega % q, selected modes
+                    double e;
+                    if constexpr (PES == SCP3GPU_PES_QTIP4PF)
+                        e = qt::energy_grad_warp(reinterpret_cast<const double*>(crd),
+                                                 reinterpret_cast<double*>(w.ms), w.g, w.gm, nw, a.tasks, a.ntasks,
+                                                 lane);
+                    else
+                        e = ttm::energy_grad_warp(reinterpret_cast<const double*>(crd),
+                                                  reinterpret_cast<double*>(w.ms), reinterpret_cast<double*>(w.ttm),
+                                                  w.g, nw, a.tasks, a.ntasks, lane, &iters);
+                    double h = 0.0;
+                    for (int d = lane; d < nm0; d += 32) h += (double)q[d] * (__ldg(a.omega + d) * (double)q[d]);
+                    h = warp_sum(h);
+                    V = e / kAuToKcalPerMol - 0.5 * h;
+                    for (int m = lane; m < a.nm; m += 32) {
+                        const int k = __ldg(a.modes + m);
+                        double acc = 0.0;
+                        for (int c = 0; c < N3; c++) acc += MUa[(size_t)k * N3 + c] * w.g[c];
+                        a.vq[s * a.nm + m] = acc * (kBohr / kAuToKcalPerMol) - __ldg(a.omega + k) * (double)q[k];
+                    }
+                }
+            }
+            if (!a.skip_pes && !grad) {
+                const double e = potential<PES, T>(crd, w, nw, a.tasks, a.ntasks, lane, &iters);
                 double h = 0.0;
-                for (int d = lane; d < nm0; d += 32) h += w.q[d] * (__ldg(a.omega + d) * w.q[d]);
+                for (int d = lane; d < nm0; d += 32) h += (double)q[d] * (__ldg(a.omega + d) * (double)q[d]);
                 h = warp_sum(h);
                 V = e / kAuToKcalPerMol - 0.5 * h;
-                for (int m = lane; m < a.nm; m += 32) {
-                    const int k = __ldg(a.modes + m);
-                    double acc = 0.0;
-                    for (int c = 0; c < N3; c++) acc += MUa[(size_t)k * N3 + c] * w.g[c];
-                    a.vq[s * a.nm + m] = acc * (kBohr / kAuToKcalPerMol) - __ldg(a.omega + k) * w.q[k];
-                }
             }
+            if (lane == 0) {
+                a.v[s] = V;
+                if (!isfinite(V)) atomicAdd(a.counters + 0, 1ull);
+                if (iters > kTtmMaxIter) atomicAdd(a.counters + 1, 1ull);
+            }
+            // 4. selected modes, coalesced per sample
+            for (int m = lane; m < a.nm; m += 32) {
+                const T qm = q[__ldg(a.modes + m)];
+                if (a.q64) a.q64[s * a.nm + m] = (double)qm;
+                if (a.q32) a.q32[s * a.nm + m] = (float)qm;
+            }
+            __syncwarp();
         }
-        if (!a.skip_pes && !grad) {
-            const double e = potential<PES, T>(w, nw, a.tasks, a.ntasks, lane, &iters);
-            double h = 0.0;
-            for (int d = lane; d < nm0; d += 32) h += w.q[d] * (__ldg(a.omega + d) * w.q[d]);
-            h = warp_sum(h);
-            V = e / kAuToKcalPerMol - 0.5 * h;
-        }
-        if (lane == 0) {
-            a.v[s] = V;
-            if (!isfinite(V)) atomicAdd(a.counters + 0, 1ull);
-            if (iters > kTtmMaxIter) atomicAdd(a.counters + 1, 1ull);
-        }
-        // 4. selected modes, coalesced per sample
-        for (int m = lane; m < a.nm; m += 32) {
-            const double qm = w.q[__ldg(a.modes + m)];
-            if (a.q64) a.q64[s * a.nm + m] = qm;
-            if (a.q32) a.q32[s * a.nm + m] = (float)qm;
-        }
-        __syncwarp();
-      }
     }
 }
 
@@ -277,7 +332,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         for (int c = lane; c < 9 * nw; c += 32) w.crd[c] = crd[g * 9 * nw + c];
         __syncwarp();
         int iters = 0;
-        const double e = potential<PES, double>(w, nw, tasks, ntasks, lane, &iters);
+        const double e = potential<PES, double>(w.crd, w, nw, tasks, ntasks, lane, &iters);
         if (lane == 0) {
             E[g] = e;
             if (iters_out) iters_out[g] = iters;
@@ -356,8 +411,8 @@ int grid_for(int64_t nwarps_needed)
 template <int PES, typename T>
 int launch_samples_t(const SampleArgs& a, cudaStream_t s)
 {
-    const size_t mua_b = mua_smem_bytes(a.nw, a.nm0);
-    const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw, a.vq != nullptr) +
+    const size_t mua_b = mua_smem_bytes<T>(a.nw, a.nm0);
+    const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw, a.vq != nullptr, kGroup) +
                       (mua_b <= kMuaSmemMax ? mua_b : 0);
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_kernel<PES, T>,
                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -377,10 +432,10 @@ int launch_samples_batch_t(const SampleArgs* args_host, const SampleArgs* args_d
     for (int c = 0; c < ncl; c++) {
         nm0 = std::max(nm0, args_host[c].nm0);
         nw = std::max(nw, args_host[c].nw);
-        const size_t b = mua_smem_bytes(args_host[c].nw, args_host[c].nm0);
+        const size_t b = mua_smem_bytes<T>(args_host[c].nw, args_host[c].nm0);
         if (b <= kMuaSmemMax) mua = std::max(mua, b);
     }
-    const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, nm0, nw) + mua;
+    const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, nm0, nw, false, kGroup) + mua;
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_batch_kernel<PES, T>,
                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int per = grid_for((n + kRun - 1) / kRun);   // per cluster; the clusters share the SMs
