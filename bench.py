@@ -397,6 +397,83 @@ def run_batch(args):
         "max_rel_diff_vs_single_builds": worst_same, "max_level_err_cm1_vs_fp64": worst_lvl, "clusters": per}))
 
 
+def _ref_scp1_rate(job):
+    """One process of the CPU reference arm of --config scp1: the reference's own
+    std_normal and qTIP4P/f operator in SCP1.cpp's sample loop (single-threaded,
+    as one MPI rank)."""
+    pes, nw, q, d, iU, skip, i0, i1 = job
+    from oracle import scp1_oracle
+    t0 = time.perf_counter()
+    scp1_oracle.ref_average_sums(pes, nw, q, d, iU, skip, i0, i1, fast=True)
+    return (i1 - i0) / (time.perf_counter() - t0)
+
+
+def run_scp1(args):
+    """SCP1 averages: SCP1::average (SCP1.cpp:34-90) on the hexamer prism input --
+    per point the qTIP4P/f energy and gradient at bohr (q + isqrtM_U (y % sqrt(d))),
+    summed into <V>, <UX> and <UX dq^T> -- over 2^20 unscrambled Sobol points
+    (SCP1_main's default NSobol), harmonic density of the input Hessian at T = 0.
+    value: points/s of one scp3gpu_scp1_average call (host clock around the
+    synchronous C-ABI call, inputs and sums copied inside).  cpu_baseline: the
+    reference's own functions in the same loop, one process per host core as
+    MPI ranks would run it.  One JSON line; not the benchmark's default."""
+    import multiprocessing as mproc
+
+    import torch
+    import scp3_b200
+    from scp3_b200 import constants as C, modes, scp1
+    torch.cuda.set_device(0)
+    n = args.samples
+    species, mass, x0, H = modes.read_input(os.path.join(ROOT, "scp3_b200", "data", INPUT + ".dat"))
+    _, mass, x0, H = modes.ohhohh(mass, x0, H)
+    nw = x0.size // 9
+    w2, U = scp1.eig_sym(H)
+    omega = np.sqrt(np.abs(w2))
+    d = np.zeros_like(omega)
+    keep = omega >= 50.0 / C.autocm
+    d[keep] = 0.5 / omega[keep]
+    iU = U / np.sqrt(mass)[:, None]
+    skip = 1 << (int(np.floor(np.log2(float(n)))) + 1)
+    g = scp3_b200.SCP1Average("qtip4pf", nw)
+    for k in range(max(args.warmup, 1)):
+        g.sums(x0, d, iU, skip, 0, 1 << 14)
+    clocks = Clocks(0)
+    times = []
+    for k in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        up, UX, UXq = g.sums(x0, d, iU, skip, 0, n)
+        times.append(time.perf_counter() - t0)
+    clk = clocks.stop()
+    g.close()
+    t = float(np.median(times))
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            import oracle
+            if oracle.ref_available(fast=True):
+                procs = min(16, os.cpu_count() or 1)
+                per = 1 << 15
+                jobs = [("qtip4pf", nw, x0, d, iU, skip, r * per, (r + 1) * per) for r in range(procs)]
+                with mproc.get_context("spawn").Pool(procs) as pool:
+                    rates = pool.map(_ref_scp1_rate, jobs)
+                cpu = {"value": float(np.sum(rates)), "unit": "samples/s", "cores": procs, "kind": "reference",
+                       "sample": "%d processes x %d points each (the reference's std_normal + qTIP4P/f "
+                                 "operator in SCP1.cpp's loop, oracle/_ref release flags)" % (procs, per)}
+        except Exception as e:          # noqa: BLE001
+            cpu = {"unavailable": str(e)}
+    chunks = (n + 65535) // 65536
+    print(json.dumps({
+        "metric": "SCP1 average: Sobol points/s (hexamer, qTIP4P/f energy + gradient per point)",
+        "value": n / t, "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "hexamer prism qTIP4P/f, 54 Cartesian dims, %d unscrambled Sobol points, T = 0 "
+                               "harmonic density of the input Hessian" % n},
+        "timing": "host clock around the synchronous scp3gpu_scp1_average call (inputs and sums copied inside)",
+        "gpu_launches": 2 * chunks + 1, "clocks": clk, "cpu_baseline": cpu,
+        "check": {"mean_V_hartree": up / n, "max_abs_mean_UX": float(np.abs(UX).max() / n)}}))
+
+
 def main():
     global SAMPLES
     ap = argparse.ArgumentParser()
@@ -407,9 +484,10 @@ def main():
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16x3", "f16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--config", default="doubles", choices=["doubles", "triples", "cv", "batch"],
+    ap.add_argument("--config", default="doubles", choices=["doubles", "triples", "cv", "batch", "scp1"],
                     help="doubles: the benchmark (hexamer, Nb=1225); triples: the TTM3-F triples build; "
-                         "cv: the learned control variate; batch: 32 clusters in one batched build")
+                         "cv: the learned control variate; batch: 32 clusters in one batched build; "
+                         "scp1: the SCP1 effective-Hessian averages")
     ap.add_argument("--cv-epochs", type=int, default=100)
     ap.add_argument("--no-levels", action="store_true", help="skip the FP64 level check (profiler captures)")
     ap.add_argument("--no-dump", action="store_true", help="triples: skip the sM_*.h5 dumps")
@@ -422,6 +500,9 @@ def main():
         return
     if args.config == "batch":
         run_batch(args)
+        return
+    if args.config == "scp1":
+        run_scp1(args)
         return
     if args.config == "triples":
         if args.samples == 1 << 20:

@@ -277,6 +277,27 @@ int scp3gpu_hbuild_set_surrogate(scp3gpu_hbuild* h, scp3gpu_mlp* m, int mode);
  * data for the surrogate. */
 int scp3gpu_hbuild_sample(scp3gpu_hbuild* h, int64_t index0, int64_t n, float* q, double* v);
 
+/* ------------------------------------------------------------------ SCP1
+ * The thermal averages of the SCP1 effective-Hessian iteration: the sample
+ * loop of SCP1::average (SCP1.cpp:34-90) for one rank's share of the points.
+ * A handle holds the device buffers (pes: SCP3GPU_PES_*, 1 <= nw <= 8, chunk:
+ * samples per device pass, 0 = 65536). */
+typedef struct scp3gpu_scp1 scp3gpu_scp1;
+int scp3gpu_scp1_create(int pes, int nw, int64_t chunk, int device, scp3gpu_scp1** out);
+/* Points i0 <= i < i1 of the unscrambled Sobol sequence at offset `skip`
+ * (dimension 9*nw; the reference's current_skip = sobol_skip + i), with
+ * q[9nw] (bohr), d[9nw] (displacement variances, >= 0) and isqrtM_U (9nw x 9nw,
+ * column-major): returns the SUMS over those points of V (hartree), UX[9nw] =
+ * dV/dr (hartree/bohr) and UX_q (9nw x 9nw, column-major) = sum UX dq^T -- the
+ * per-rank partials that SCP1.cpp:71-78 all-reduces before dividing by NSobol.
+ * Host buffers.  Replaces SCP1::average's loop (SCP1.cpp:49-69). */
+int scp3gpu_scp1_average(scp3gpu_scp1* h, const double* q, const double* d, const double* isqrtM_U, int64_t skip,
+                         int64_t i0, int64_t i1, double* Upot, double* UX, double* UX_q);
+/* TTM3-F samples whose dipoles hit the 500-sweep cap so far (the reference
+ * uses their energies and gradients as they are). */
+int scp3gpu_scp1_status(const scp3gpu_scp1* h, int64_t* not_converged);
+void scp3gpu_scp1_destroy(scp3gpu_scp1* h);
+
 /* Kernel timing (no counterpart in the reference, which has no in-code timing;
  * only a VTune build profile, config/vtune.mk:1-4).  enable = 1 clears and starts
  * recording CUDA events around every kernel the handle launches on its stream;

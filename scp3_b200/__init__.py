@@ -3,5 +3,5 @@
 a C ABI (include/scp3gpu.h, libscp3gpu.so)."""
 from . import constants, modes, clusters  # noqa: F401
 from ._lib import SCP3GPUError, build  # noqa: F401
-from .api import (PES, Batch, HBuild, PESFromString, dsyevr, ScaledMatrixElements, qtip4pf, std_normal,  # noqa: F401
-                  std_normals, ttm3f)
+from .api import (PES, Batch, HBuild, PESFromString, SCP1Average, dsyevr, ScaledMatrixElements, qtip4pf,  # noqa: F401
+                  std_normal, std_normals, ttm3f)

@@ -31,6 +31,7 @@ EXPORTS = [
     "scp3gpu_batch_create", "scp3gpu_batch_destroy", "scp3gpu_batch_reset", "scp3gpu_batch_size",
     "scp3gpu_batch_basis_size", "scp3gpu_batch_sample_count", "scp3gpu_batch_stream", "scp3gpu_batch_shape",
     "scp3gpu_batch_accumulate", "scp3gpu_batch_read", "scp3gpu_batch_status",
+    "scp3gpu_scp1_create", "scp3gpu_scp1_average", "scp3gpu_scp1_status", "scp3gpu_scp1_destroy",
 ]
 
 
@@ -104,6 +105,11 @@ def lib():
     L.scp3gpu_syevr_lowest.argtypes = [dp, i64, i64, ctypes.c_int, dp, dp, i64, ctypes.c_int]
     L.scp3gpu_load_h5.argtypes = [ctypes.c_char_p, dp, ctypes.POINTER(i64), ctypes.POINTER(i64)]
     L.scp3gpu_hbuild_status.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(i64)]
+    L.scp3gpu_scp1_create.argtypes = [ctypes.c_int, ctypes.c_int, i64, ctypes.c_int, ctypes.POINTER(vp)]
+    L.scp3gpu_scp1_average.argtypes = [vp, dp, dp, dp, i64, i64, i64, dp, dp, dp]
+    L.scp3gpu_scp1_status.argtypes = [vp, ctypes.POINTER(i64)]
+    L.scp3gpu_scp1_destroy.argtypes = [vp]
+    L.scp3gpu_scp1_destroy.restype = None
     L.scp3gpu_batch_create.argtypes = [ctypes.POINTER(Config), ctypes.c_int, i64, ctypes.c_int, ctypes.POINTER(vp)]
     L.scp3gpu_batch_destroy.argtypes = [vp]
     L.scp3gpu_batch_reset.argtypes = [vp]

@@ -361,3 +361,49 @@ class Batch:
         a, b = ctypes.c_int64(), ctypes.c_int64()
         rc = _lib.lib().scp3gpu_batch_status(self._h, cluster, ctypes.byref(a), ctypes.byref(b))
         return rc, a.value, b.value
+
+
+class SCP1Average:
+    """The sample loop of SCP1::average (SCP1.cpp:34-90) on one GPU: for Sobol
+    points i0 <= i < i1 (offset `skip`, dimension 9*nw), the sums of V, dV/dr
+    and dV/dr dq^T.  The caller all-reduces the sums over ranks and divides by
+    NSobol, as SCP1.cpp:71-88 does."""
+
+    def __init__(self, pes, nw, chunk=0, device=0):
+        if pes not in C.PES_IDS:
+            raise ValueError("Unknown H2O potential: %s" % pes)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib().scp3gpu_scp1_create(C.PES_IDS[pes], nw, chunk, device, ctypes.byref(h)))
+        self._h = h
+        self.nw = nw
+        self.dim = 9 * nw
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().scp3gpu_scp1_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sums(self, q, d, isqrtM_U, skip, i0, i1):
+        """(sum V, sum UX[dim], sum UX dq^T [dim x dim]) over points i0..i1-1."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        U = np.asfortranarray(isqrtM_U, dtype=np.float64)
+        if q.size != self.dim or d.size != self.dim or U.shape != (self.dim, self.dim):
+            raise ValueError("q, d and isqrtM_U must have 9*nw rows")
+        up = ctypes.c_double()
+        UX = np.zeros(self.dim)
+        UXq = np.zeros((self.dim, self.dim), order="F")
+        _lib.check(_lib.lib().scp3gpu_scp1_average(self._h, _p(q), _p(d), U.ctypes.data_as(_dp), int(skip), int(i0),
+                                                  int(i1), ctypes.byref(up), _p(UX), UXq.ctypes.data_as(_dp)))
+        return up.value, UX, UXq
+
+    def not_converged(self):
+        n = ctypes.c_int64()
+        _lib.check(_lib.lib().scp3gpu_scp1_status(self._h, ctypes.byref(n)))
+        return n.value

@@ -173,4 +173,24 @@ int launch_unpack(const double* partial, const TileMap& tm, int nsplit, int nb, 
 // to the current device once.
 int ttm_init_device();
 
+// SCP1 per-sample stage (SCP1.cpp:52-63): for points index0 + s, s < n, of the
+// unscrambled Sobol sequence in dim = 9 nw dimensions, y = std_normal % sqrt(d),
+// dq = isqrtM_U y, V = pes(bohr (q + dq)) / autokcal, G = dV/dr bohr / autokcal;
+// writes V[n], G[n][dim], D[n][dim] = dq (and the TTM3-F sweep counts).
+struct Scp1Args {
+    int nw, dim;
+    const double* q;          // [dim] bohr
+    const double* sqd;        // [dim] sqrt(d)
+    const double* U;          // [dim x dim] isqrtM_U, column-major
+    const int64_t* vdir;      // [62][dim]
+    int64_t index0, n;
+    const uint32_t* tasks;
+    int ntasks;
+    double* V;
+    double* G;
+    double* D;
+    int* iters;               // may be null
+};
+int launch_scp1_samples(int pes, const Scp1Args& a, cudaStream_t s);
+
 }  // namespace scp3

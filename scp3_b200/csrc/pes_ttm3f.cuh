@@ -300,7 +300,7 @@ __device__ __forceinline__ void smear123(double r, double AA, double& ts1, doubl
 // Monomer at w[9]: energy e (kcal/mol), its gradient g9 (written), the charges
 // q3 and the derivatives of the scaled site charges grdq[27] (GRDQ layout of
 // ttm3f.cpp:371-393: [atom H1, H2, O][charge H1, H2, M][xyz], times CHARGECON).
-__device__ void monomer_grad(const double* w, double* f, double& e, double q3[3], double* g9, double* grdq)
+__device__ inline void monomer_grad(const double* w, double* f, double& e, double q3[3], double* g9, double* grdq)
 {
     constexpr double reoh = 0.958649, b1 = 2.0, roh = 0.9519607159623009, alphaoh = 2.587949757553683;
     constexpr double deohA = 42290.92019288289, phh2 = 12.66426998162947, f5z = 0.999677885;

@@ -371,6 +371,78 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     }
 }
 
+// SCP1 per-sample stage (SCP1.cpp:52-63): one warp per sample, contiguous
+// balanced ranges per warp with the Gray-code Sobol walk, isqrtM_U staged in
+// shared memory, the potential's energy and gradient (the gradient estimator's
+// warp code).
+constexpr int kS1Warps = 8;
+
+__host__ __device__ inline size_t scp1_slot(int pes, int nw, int dim)
+{
+    return 2 * (size_t)dim + 24 * (size_t)nw + (pes == SCP3GPU_PES_TTM3F ? ttm::scratch_elems(nw, true) : 0);
+}
+
+template <int PES>
+__global__ void __launch_bounds__(kS1Warps * 32) scp1_samples_kernel(Scp1Args a)
+{
+    extern __shared__ __align__(16) double s1[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int nw = a.nw, dim = a.dim;
+    double* U = s1;
+    for (int e = threadIdx.x; e < dim * dim; e += blockDim.x) U[e] = a.U[e];
+    double* y = s1 + (size_t)dim * dim + (size_t)wib * scp1_slot(PES, nw, dim);
+    double* dq = y + dim;
+    double* x = dq + dim;
+    double* ms = x + 9 * nw;
+    double* g = ms + 3 * nw;
+    double* gm = g + 9 * nw;
+    double* sc = gm + 3 * nw;
+    __syncthreads();
+    const int64_t nwarps = (int64_t)gridDim.x * kS1Warps;
+    const int64_t gw = (int64_t)blockIdx.x * kS1Warps + wib;
+    const int64_t s_first = a.n * gw / nwarps, s_end = a.n * (gw + 1) / nwarps;
+    constexpr int kDimsPerLane = 4;
+    uint64_t st[kDimsPerLane];
+    for (int64_t s = s_first; s < s_end; s++) {
+        const uint64_t idx = (uint64_t)(a.index0 + s);
+        // y = std_normal % sqrt(d)   (SCP1.cpp:54-58)
+#pragma unroll
+        for (int jd = 0; jd < kDimsPerLane; jd++) {
+            const int d = lane + 32 * jd;
+            if (d >= dim) break;
+            if (s == s_first) st[jd] = sobol_state(a.vdir, dim, d, idx);
+            else st[jd] ^= (uint64_t)__ldg(a.vdir + (size_t)(__ffsll((long long)idx) - 1) * dim + d);
+            y[d] = bsm(sobol_uniform(st[jd])) * __ldg(a.sqd + d);
+        }
+        for (int d = lane + 32 * kDimsPerLane; d < dim; d += 32)
+            y[d] = bsm(sobol_uniform(sobol_state(a.vdir, dim, d, idx))) * __ldg(a.sqd + d);
+        __syncwarp();
+        // dq = isqrtM_U y, r = bohr (q + dq)   (SCP1.cpp:60-61), k in order
+        for (int c = lane; c < dim; c += 32) {
+            double acc = 0.0;
+            for (int k = 0; k < dim; k++) acc += U[(size_t)k * dim + c] * y[k];
+            dq[c] = acc;
+            x[c] = kBohr * (__ldg(a.q + c) + acc);
+        }
+        __syncwarp();
+        int it = 0;
+        double e;
+        if constexpr (PES == SCP3GPU_PES_QTIP4PF)
+            e = qt::energy_grad_warp(x, ms, g, gm, nw, a.tasks, a.ntasks, lane);
+        else
+            e = ttm::energy_grad_warp(x, ms, sc, g, nw, a.tasks, a.ntasks, lane, &it);
+        if (lane == 0) {
+            a.V[s] = e / kAuToKcalPerMol;
+            if (a.iters) a.iters[s] = it;
+        }
+        for (int c = lane; c < dim; c += 32) {
+            a.G[s * dim + c] = g[c] * (kBohr / kAuToKcalPerMol);    // UX_ *= bohr/autokcalpmol
+            a.D[s * dim + c] = dq[c];
+        }
+        __syncwarp();
+    }
+}
+
 __global__ void std_normal_kernel(int dims, int64_t index0, int64_t n, const int64_t* __restrict__ vdir,
                                   const uint64_t* __restrict__ shift, double* __restrict__ out)
 {
@@ -516,6 +588,25 @@ int launch_pes_energy_grad(int pes, int nw, int64_t n, const double* crd, double
     auto kern = ttm ? pes_energy_grad_kernel<SCP3GPU_PES_TTM3F> : pes_energy_grad_kernel<SCP3GPU_PES_QTIP4PF>;
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     kern<<<grid_for(n), kWarpsPerBlock * 32, sm, s>>>(nw, n, crd, E, G, iters, tasks, ntasks);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
+int launch_scp1_samples(int pes, const Scp1Args& a, cudaStream_t s)
+{
+    if (a.n <= 0) return SCP3GPU_OK;
+    if (pes != SCP3GPU_PES_QTIP4PF && pes != SCP3GPU_PES_TTM3F) return fail(SCP3GPU_ERR_ARG, "unknown potential id");
+    const size_t sm = sizeof(double) * ((size_t)a.dim * a.dim + kS1Warps * scp1_slot(pes, a.nw, a.dim));
+    auto kern = pes == SCP3GPU_PES_QTIP4PF ? scp1_samples_kernel<SCP3GPU_PES_QTIP4PF>
+                                            : scp1_samples_kernel<SCP3GPU_PES_TTM3F>;
+    SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int dev = 0, sms = 148, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kS1Warps * 32, sm) != cudaSuccess || per < 1) per = 1;
+    const int64_t want = (a.n + 4 * kS1Warps - 1) / (4 * kS1Warps);     // >= 4 samples per warp
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per * sms));
+    kern<<<grid, kS1Warps * 32, sm, s>>>(a);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }

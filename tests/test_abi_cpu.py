@@ -111,3 +111,18 @@ def test_argument_errors_before_any_device_work():
     assert L.scp3gpu_pes_energy_grad(1, 9, 1, crd.ctypes.data_as(dp), E.ctypes.data_as(dp),
                                      G.ctypes.data_as(dp)) == _lib.ERR_ARG
     assert "TTM3-F" in L.scp3gpu_last_error().decode()
+
+
+def test_scp1_argument_errors_without_device():
+    from scp3_b200 import _lib
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    assert L.scp3gpu_scp1_create(5, 2, 0, 0, ctypes.byref(h)) == _lib.ERR_ARG
+    assert L.scp3gpu_scp1_create(0, 9, 0, 0, ctypes.byref(h)) == _lib.ERR_ARG
+    assert L.scp3gpu_scp1_create(0, 2, -1, 0, ctypes.byref(h)) == _lib.ERR_ARG
+    assert L.scp3gpu_scp1_create(0, 2, 0, 0, None) == _lib.ERR_ARG
+    # a valid request on a host without a GPU: an error status, not a crash
+    assert L.scp3gpu_scp1_create(0, 2, 0, 0, ctypes.byref(h)) == _lib.ERR_UNSUPPORTED
+    assert not h.value
+    assert L.scp3gpu_scp1_average(None, None, None, None, 0, 0, 0, None, None, None) == _lib.ERR_ARG
+    L.scp3gpu_scp1_destroy(None)
