@@ -386,6 +386,273 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// ---------------------------------------------------------------------------
+// The single build's contraction: 128 x 256 tiles, one M=128, N=256, K=16 MMA
+// per product.  An MMA costs about the same time for N = 128 and N = 256, so
+// the wider tile doubles the work per instruction.
+//
+// Operand: 32-slot boxes in the 64-byte swizzle, [row block][k-block32][hi, lo]
+// [128 x 32] (16-byte chunk c of row r at c ^ ((r >> 1) & 3)).  A stage holds
+// 32 K slots: A (one row panel, hi + lo, 16 KB) and B (two consecutive panels,
+// hi then lo, 32 KB); four stages are in flight.
+//
+// Tiles: (A panel, first B panel); every upper 128 x 128 block is owned by one
+// tile (the tiling and which half of a tile owns which block are the host's;
+// a tile may own one half only).  Work unit u = split * ntiles + tile takes the
+// tile over k-blocks [split * nkb_full / nsplit, (split + 1) * nkb_full /
+// nsplit) of the pass; CTA b runs units b, b + gridDim.x, ... .  Units of one
+// wave share k-ranges, so L2 serves the panels they have in common.
+//
+// Accumulation.  One FP32 TMEM accumulator per tile takes all three products
+// (256 columns; two alternate, so a drain overlaps the next run's MMAs).  It is
+// drained every 4 k-blocks (128 K slots, 24 MMAs) into FP32 registers of the
+// epilogue threads (one row and 128 columns each), which are added into the
+// unit's own FP64 partial every 32 drains (4096 K slots) and at the unit's end.
+// (A 128 x 256 tile's FP64 state would not fit beside the operand stages.)
+constexpr int kBK2 = 32;
+constexpr int kStages2 = 4;
+constexpr int kBox2 = kTile * kBK2 * 2;            // 8 KB: one half of one panel
+constexpr int kStageBytes2 = 6 * kBox2;            // A hi, A lo, B hi x2, B lo x2
+constexpr int kKB2PerFlush = kSlotsPerFlush / kBK2;   // 130
+constexpr int kDrain2 = 4;                          // k-blocks per FP32 TMEM run
+constexpr int kL2Drains = 32;                       // runs per FP64 flush
+constexpr int kSmemBytes2 = kStages2 * kStageBytes2 + 1024 + 256;
+constexpr int kN2 = 2 * kTile;
+constexpr uint32_t kIdesc2 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kN2 >> 3) << 17) |
+                             ((uint32_t)(kTile >> 4) << 24);
+constexpr uint32_t kIdesc2NegA = kIdesc2 | (1u << 13);
+constexpr uint32_t kIdesc2F16 = kIdesc2 & ~((7u << 7) | (7u << 10));
+constexpr uint32_t kIdesc2F16NegA = kIdesc2F16 | (1u << 13);
+
+// K-major, SWIZZLE_64B: start >> 4, LBO 16 B (unused), SBO 512 B (8 rows x 64 B),
+// version 1, layout type 4.
+__device__ __forceinline__ uint64_t smem_desc64(const void* p)
+{
+    const uint64_t addr = smem_u32(p);
+    return ((addr >> 4) & 0x3FFFull) | (1ull << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46) | (4ull << 61);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    contract_n256_kernel(const uint16_t* __restrict__ xop, long long nkb_alloc, const int2* __restrict__ tiles,
+                         int ntiles, int nsplit, int nkb_full, int nkb_pass, const int* __restrict__ neg_group,
+                         int f16, double* __restrict__ partial, int* __restrict__ err_flag)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages2 * kStageBytes2);
+    uint64_t* full = bars;
+    uint64_t* empty = bars + kStages2;
+    uint64_t* acc_full = bars + 2 * kStages2;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* drain = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nunits = ntiles * nsplit;
+    // k-blocks [lo, hi) of unit u in this pass
+    auto krange = [&](int u, int& lo, int& hi) {
+        const int split = u / ntiles;
+        lo = (int)((long long)split * nkb_full / nsplit);
+        hi = (int)((long long)(split + 1) * nkb_full / nsplit);
+        if (hi > nkb_pass) hi = nkb_pass;
+        if (hi < lo) hi = lo;
+    };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages2; s++) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(acc_full + a, 1);
+            mbar_init(acc_empty + a, kEpiWarps);
+        }
+        mbar_init(drain, 1);
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    constexpr int kBoxElems = kTile * kBK2;           // 4096 16-bit values per half box
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int issued[kStages2] = {0, 0, 0, 0};
+            uint32_t issued_phase[kStages2] = {0, 0, 0, 0};
+            bool ok = true;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                int lo, hi;
+                krange(u, lo, hi);
+                const int2 ti = tiles[u % ntiles];
+                const uint16_t* pa = xop + (size_t)(ti.x / kTile) * nkb_alloc * (2 * kBoxElems);
+                const uint16_t* pb0 = xop + (size_t)(ti.y / kTile) * nkb_alloc * (2 * kBoxElems);
+                const uint16_t* pb1 = pb0 + (size_t)nkb_alloc * (2 * kBoxElems);
+                for (int kb = lo; kb < hi; kb++) {
+                    if (!mbar_wait(empty + stage, phase ^ 1, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* st = smem + stage * kStageBytes2;
+                    mbar_expect_tx(full + stage, kStageBytes2);
+                    const size_t o = (size_t)kb * (2 * kBoxElems);
+                    bulk_load(st, pa + o, 2 * kBox2, full + stage);                      // A hi, lo
+                    bulk_load(st + 2 * kBox2, pb0 + o, kBox2, full + stage);             // B hi rows 0..127
+                    bulk_load(st + 3 * kBox2, pb1 + o, kBox2, full + stage);             // B hi rows 128..255
+                    bulk_load(st + 4 * kBox2, pb0 + o + kBoxElems, kBox2, full + stage); // B lo rows 0..127
+                    bulk_load(st + 5 * kBox2, pb1 + o + kBoxElems, kBox2, full + stage); // B lo rows 128..255
+                    issued[stage] = 1;
+                    issued_phase[stage] = phase;
+                    if (++stage == kStages2) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            if (*abort) {
+                for (int s = 0; s < kStages2; s++)
+                    if (issued[s]) {
+                        volatile int never = 0;
+                        mbar_wait(full + s, issued_phase[s], &never);
+                    }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int stage = 0, use = 0;
+            uint32_t phase = 0;
+            bool ok = true;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                int lo, hi;
+                krange(u, lo, hi);
+                for (int k0 = lo; k0 < hi && ok; k0 += kDrain2, use++) {
+                    const int a = use & 1;
+                    if (!mbar_wait(acc_empty + a, ((use >> 1) & 1) ^ 1, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t d = tmem + (uint32_t)(a * kN2);
+                    const int k1 = min(hi, k0 + kDrain2);
+                    for (int kb = k0; kb < k1; kb++) {
+                        if (!mbar_wait(full + stage, phase, abort)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        uint8_t* st = smem + stage * kStageBytes2;
+                        const uint64_t ahi = smem_desc64(st), alo = smem_desc64(st + kBox2);
+                        const uint64_t bhi = smem_desc64(st + 2 * kBox2), blo = smem_desc64(st + 4 * kBox2);
+                        const int f = kb / kKB2PerFlush;
+                        const int neg0 = neg_group[f];
+                        const int ks0 = (kb - f * kKB2PerFlush) * (kBK2 / 16);
+#pragma unroll
+                        for (int kk = 0; kk < kBK2 / 16; kk++) {
+                            const bool neg = ks0 + kk >= neg0;
+                            const uint32_t idesc =
+                                f16 ? (neg ? kIdesc2F16NegA : kIdesc2F16) : (neg ? kIdesc2NegA : kIdesc2);
+                            const uint64_t adv = (uint64_t)(kk * 2);    // 32 B along K inside the 64 B atom
+                            const uint32_t acc = (kb != k0) | (kk != 0);
+                            mma_bf16(d, ahi + adv, bhi + adv, idesc, acc);
+                            mma_bf16(d, ahi + adv, blo + adv, idesc, 1);
+                            mma_bf16(d, alo + adv, bhi + adv, idesc, 1);
+                        }
+                        mma_commit(empty + stage);
+                        if (++stage == kStages2) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+                    if (ok) mma_commit(acc_full + a);
+                }
+            }
+            mma_commit(drain);
+            volatile int never = 0;
+            mbar_wait(drain, 0, &never);
+        }
+    } else {
+        // epilogue: warp w reads TMEM lane quadrant w % 4 and column half (w - 2) / 4
+        const int quad = warp & 3, half = (warp - 2) >> 2;
+        const int row = quad * 32 + lane;
+        const double unscale = f16 ? kF16Unscale : 1.0;
+        float l2[kTile];
+#pragma unroll
+        for (int j = 0; j < kTile; j++) l2[j] = 0.f;
+        int use = 0;
+        bool ok = true;
+        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+            int lo, hi;
+            krange(u, lo, hi);
+            const int nruns = (hi - lo + kDrain2 - 1) / kDrain2;
+            double* P = partial + (size_t)u * (size_t)(kTile * kN2);
+            for (int k = 0; k < nruns; k++, use++) {
+                const int a = use & 1;
+                if (!mbar_wait(acc_full + a, (use >> 1) & 1, abort)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * kN2 + half * kTile);
+#pragma unroll
+                for (int c0 = 0; c0 < kTile; c0 += 32) {
+                    float v[32];
+                    tmem_ld32(base + c0, v);
+#pragma unroll
+                    for (int j = 0; j < 32; j++) l2[c0 + j] += v[j];
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acc_empty + a);
+                if (k % kL2Drains == kL2Drains - 1 || k == nruns - 1) {
+#pragma unroll
+                    for (int j = 0; j < kTile; j++) {
+                        P[(size_t)(half * kTile + j) * kTile + row] += (double)l2[j] * unscale;
+                        l2[j] = 0.f;
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort) atomicExch(err_flag, 1);
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+    }
+}
+
+// Dense column-major nb x nb from the 128 x 256 tiles' unit partials: element
+// (r <= c) lies in block (r / 128, c / 128), owned by tile t at column half h
+// (block_owner = 2 t + h); its value is the sum over the splits, in order, of
+// unit (split * ntiles + t) at row r % 128 and column 128 h + c % 128.
+__global__ void unpack_n256_kernel(const double* __restrict__ partial, const int* __restrict__ block_owner, int nt,
+                                   int ntiles, int nsplit, int nb, double divisor, const double* __restrict__ diag,
+                                   double zpe, double* __restrict__ M, int64_t ld)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)nb * nb) return;
+    const int j = (int)(e / nb), i = (int)(e - (int64_t)j * nb);
+    const int r = min(i, j), c = max(i, j);
+    const int ti = r / kTile, tj = c / kTile;
+    const int own = block_owner[ti * nt + tj];
+    const int t = own >> 1, h = own & 1;
+    const size_t off = (size_t)(h * kTile + (c - tj * kTile)) * kTile + (r - ti * kTile);
+    double val = 0.0;
+    for (int s = 0; s < nsplit; s++) val += partial[((size_t)s * ntiles + t) * (size_t)(kTile * kN2) + off];
+    val = val / divisor;
+    if (diag && i == j) val = (val + diag[i]) + zpe;
+    M[(size_t)j * ld + i] = val;
+}
+
 // One CTA of 1024 threads per 4096-sample block (4 samples per thread): stable
 // partition of its samples by the sign of V into K slots; writes slot -> sample
 // (-1 = zero padding) and the first negative 16-group of the block.
@@ -511,7 +778,9 @@ __host__ __device__ inline size_t expand_smem(int nm, bool staged)
     return f * sizeof(float);
 }
 
-template <bool F16>
+// SW64: the single build's operand (32-slot boxes in the 64-byte swizzle, nkb
+// counts 32-slot k-blocks); otherwise 64-slot boxes in the 128-byte swizzle.
+template <bool F16, bool SW64>
 __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandDesc* __restrict__ descs, int ncl,
                                                                     int64_t nkbp, int64_t nkb, int staged,
                                                                     uint16_t* __restrict__ xop)
@@ -675,12 +944,21 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandD
                         split2<F16>(w1.x * (a1.x * b1.x * c1.x), w1.y * (a1.y * b1.y * c1.y), hi.z, lo.z);
                         split2<F16>(w1.z * (a1.z * b1.z * c1.z), w1.w * (a1.w * b1.w * c1.w), hi.w, lo.w);
                     }
-                    // box (row block, k-block), swizzled: 16-byte chunk g8 of row rin at g8 ^ (rin & 7)
                     const int row = row0 + rr, rin = row & (kTile - 1);
-                    uint16_t* box = xkb + (size_t)(row / kTile) * nkb * (2 * kTile * kExpSlots);
-                    const int off = rin * kExpSlots + ((g8 ^ (rin & 7)) << 3);
-                    *reinterpret_cast<uint4*>(box + off) = hi;
-                    *reinterpret_cast<uint4*>(box + kTile * kExpSlots + off) = lo;
+                    if (SW64) {
+                        // 32-slot box (row block, 2 k-block + g8 / 4): chunk c of row rin at c ^ ((rin >> 1) & 3)
+                        const int c = g8 & 3;
+                        uint16_t* box = xop + ((size_t)(row / kTile) * nkb + 2 * cur.kb + (g8 >> 2)) * (2 * kTile * 32);
+                        const int off = rin * 32 + ((c ^ ((rin >> 1) & 3)) << 3);
+                        *reinterpret_cast<uint4*>(box + off) = hi;
+                        *reinterpret_cast<uint4*>(box + kTile * 32 + off) = lo;
+                    } else {
+                        // box (row block, k-block), swizzled: 16-byte chunk g8 of row rin at g8 ^ (rin & 7)
+                        uint16_t* box = xkb + (size_t)(row / kTile) * nkb * (2 * kTile * kExpSlots);
+                        const int off = rin * kExpSlots + ((g8 ^ (rin & 7)) << 3);
+                        *reinterpret_cast<uint4*>(box + off) = hi;
+                        *reinterpret_cast<uint4*>(box + kTile * kExpSlots + off) = lo;
+                    }
                 }
             }
         }
@@ -724,15 +1002,76 @@ void record(std::vector<cudaEvent_t>* pev, std::vector<int>* pkind, int kind, cu
 
 }  // namespace
 
+// The 128 x 256 tiling of the upper block triangle of an nt x nt grid of
+// 128 x 128 blocks (nt even): row panel ti takes its blocks ti..nt-1 in pairs,
+// and an odd one out as the second half of the tile on panels (nt-2, nt-1).
+// Tiles come in 12-row x 6-pair groups so that a wave of CTAs shares panels.
+// Choosing more tiles than the minimum splits pairs into two one-half tiles;
+// (tiles, splits) minimise waves / splits (the time in units of a whole-pass
+// tile) over at most 16 splits and 4 GB of partials.  owner[ti * nt + tj] =
+// 2 * tile + half for every block ti <= tj.
+void tiling_n256(int nt, int sms, std::vector<int2>& tiles, std::vector<int>& owner, int& nsplit)
+{
+    struct T2 {
+        int ti, s, halves;   // halves: bit 0 = block s, bit 1 = block s + 1
+    };
+    std::vector<T2> base;
+    const int R = 12, C = 6;
+    for (int r0 = 0; r0 < nt; r0 += R)
+        for (int c0 = 0; c0 < nt / 2; c0 += C)
+            for (int ti = r0; ti < std::min(r0 + R, nt); ti++)
+                for (int pr = c0; pr < std::min(c0 + C, nt / 2); pr++) {
+                    // pair pr covers column panels 2pr, 2pr+1 of the aligned grid; row ti needs tj >= ti
+                    const int a = 2 * pr, b = 2 * pr + 1;
+                    const bool na = a >= ti, nb_ = b >= ti;
+                    if (na && nb_) base.push_back({ti, a, 3});
+                    else if (nb_) base.push_back({ti, a, 2});
+                }
+    const int tmin = (int)base.size();
+    int pairs = 0;
+    for (const T2& t : base) pairs += t.halves == 3;
+    double best = 1e30;
+    int bestT = tmin, bestM = 1;
+    long long bestU = 0;
+    for (int m = 1; m <= 16; m++)
+        for (int T = tmin; T <= tmin + pairs; T++) {
+            const long long units = (long long)T * m;
+            if (units * (long long)(kTile * kN2) * 8 > (4ll << 30)) continue;
+            const double cost = (double)((units + sms - 1) / sms) / m;
+            if (cost < best - 1e-12 || (cost < best + 1e-12 && units < bestU)) {
+                best = cost;
+                bestT = T;
+                bestM = m;
+                bestU = units;
+            }
+        }
+    tiles.clear();
+    owner.assign((size_t)nt * nt, -1);
+    int extra = bestT - tmin;
+    for (const T2& t : base) {
+        if (t.halves == 3 && extra > 0) {
+            extra--;
+            for (int h = 0; h < 2; h++) {
+                owner[(size_t)t.ti * nt + t.s + h] = 2 * (int)tiles.size() + h;
+                tiles.push_back(make_int2(t.ti * kTile, t.s * kTile));
+            }
+            continue;
+        }
+        for (int h = 0; h < 2; h++)
+            if (t.halves & (1 << h)) owner[(size_t)t.ti * nt + t.s + h] = 2 * (int)tiles.size() + h;
+        tiles.push_back(make_int2(t.ti * kTile, t.s * kTile));
+    }
+    nsplit = bestM;
+}
+
 int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int chunk_req, int sms, bool f16)
 {
     const int nm_for_factors = nm;
     p.f16 = f16;
     p.nb = nb;
     p.nm = nm;
-    p.nt = (nb + kTile - 1) / kTile;
-    p.nb_pad = p.nt * kTile;
-    p.ntiles = p.nt * (p.nt + 1) / 2;
+    p.nb_pad = (nb + kN2 - 1) / kN2 * kN2;         // whole 256-row panel pairs
+    p.nt = p.nb_pad / kTile;
     int64_t chunk = chunk_req > 0 ? chunk_req : (int64_t)kFlush * 32;
     // the split operand of one pass stays under ~6 GB
     while (chunk > kFlush && (int64_t)p.nb_pad * (chunk / kFlush) * kSlotsPerFlush * 4 > (6ll << 30)) chunk /= 2;
@@ -740,48 +1079,35 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
     p.chunk = chunk;
     const int nflush = (int)(chunk / kFlush);
     p.slots = (int64_t)nflush * kSlotsPerFlush;
-    int nsplit = 1;
-    while (nsplit < nflush && (int64_t)p.ntiles * nsplit < 2ll * sms) nsplit *= 2;
-    p.nsplit = nsplit;
-    // Launch order: upper tiles grouped into G x G super-tiles, so the CTAs of one
-    // wave share a few row and column panels of the operand and read them from L2
-    // (row-major order would stream ~150 distinct panels per wave for the
-    // triples basis).
-    const int G = 12;
-    std::vector<WorkItem> t;
-    std::vector<int> tindex((size_t)p.nt * p.nt, -1);
-    for (int bi = 0; bi < p.nt; bi += G)
-        for (int bj = bi; bj < p.nt; bj += G)
-            for (int i = bi; i < std::min(bi + G, p.nt); i++)
-                for (int j = std::max(i, bj); j < std::min(bj + G, p.nt); j++) {
-                    tindex[(size_t)i * p.nt + j] = (int)t.size();
-                    WorkItem w{i * kTile, j * kTile, 0, 0, (long long)t.size() * kTile * kTile};
-                    t.push_back(w);
-                }
+    std::vector<int2> tiles;
+    std::vector<int> owner;
+    tiling_n256(p.nt, sms, tiles, owner, p.nsplit);
+    p.ntiles = (int)tiles.size();
+    p.grid = (int)std::min<long long>((long long)p.ntiles * p.nsplit, sms);
     for (int b = 0; b < 2; b++) {
         SCP3_CUDA(cudaMalloc(&p.x[b], sizeof(uint16_t) * 2 * (size_t)p.nb_pad * p.slots));
         SCP3_CUDA(cudaMalloc(&p.slot_of[b], sizeof(int) * (size_t)p.slots));
         SCP3_CUDA(cudaMalloc(&p.group_meta[b], sizeof(int) * nflush));
     }
-    SCP3_CUDA(cudaMalloc(&p.tiles, sizeof(WorkItem) * t.size()));
-    SCP3_CUDA(cudaMemcpy(p.tiles, t.data(), sizeof(WorkItem) * t.size(), cudaMemcpyHostToDevice));
+    SCP3_CUDA(cudaMalloc(&p.tiles2, sizeof(int2) * tiles.size()));
+    SCP3_CUDA(cudaMemcpy(p.tiles2, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
     const std::vector<uint32_t> fac = basis_factor_table(nm_for_factors, n2_for_factors, n3_for_factors);
     SCP3_CUDA(cudaMalloc(&p.factors, sizeof(uint32_t) * fac.size()));
     SCP3_CUDA(cudaMemcpy(p.factors, fac.data(), sizeof(uint32_t) * fac.size(), cudaMemcpyHostToDevice));
     SCP3_CUDA(cudaMalloc(&p.desc_dev, sizeof(ExpandDesc) * 2));
-    SCP3_CUDA(cudaMalloc(&p.tile_index, sizeof(int) * tindex.size()));
-    SCP3_CUDA(cudaMemcpy(p.tile_index, tindex.data(), sizeof(int) * tindex.size(), cudaMemcpyHostToDevice));
-    SCP3_CUDA(cudaMalloc(&p.partial, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kTile));
+    SCP3_CUDA(cudaMalloc(&p.tile_index, sizeof(int) * owner.size()));
+    SCP3_CUDA(cudaMemcpy(p.tile_index, owner.data(), sizeof(int) * owner.size(), cudaMemcpyHostToDevice));
+    SCP3_CUDA(cudaMalloc(&p.partial, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kN2));
     SCP3_CUDA(cudaMalloc(&p.err_flag, sizeof(int)));
     SCP3_CUDA(cudaMemset(p.err_flag, 0, sizeof(int)));
-    SCP3_CUDA(cudaFuncSetAttribute(contract_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    SCP3_CUDA(cudaFuncSetAttribute(contract_n256_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes2));
     return SCP3GPU_OK;
 }
 
 void destroy(Plan& p)
 {
     void* ptrs[] = {p.x[0], p.x[1], p.slot_of[0], p.slot_of[1], p.group_meta[0],
-                    p.group_meta[1], p.tiles, p.tile_index, p.factors, p.partial, p.err_flag, p.desc_dev};
+                    p.group_meta[1], p.tiles2, p.tile_index, p.factors, p.partial, p.err_flag, p.desc_dev};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     p = Plan{};
@@ -795,7 +1121,7 @@ int64_t pass_samples(const Plan& p, int64_t nvalid)
 
 int zero(Plan& p, cudaStream_t s)
 {
-    SCP3_CUDA(cudaMemsetAsync(p.partial, 0, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kTile, s));
+    SCP3_CUDA(cudaMemsetAsync(p.partial, 0, sizeof(double) * (size_t)p.nsplit * p.ntiles * kTile * kN2, s));
     SCP3_CUDA(cudaMemsetAsync(p.err_flag, 0, sizeof(int), s));
     return SCP3GPU_OK;
 }
@@ -809,12 +1135,13 @@ int launch_partition(const double* v, int64_t v_stride, int* slot_of, int64_t sl
 }
 
 int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t nkb,
-                  uint16_t* x, bool f16, cudaStream_t s)
+                  uint16_t* x, bool f16, cudaStream_t s, bool sw64)
 {
     constexpr size_t kMaxSmem = 227 * 1024;
     const bool staged = expand_smem(max_nm, true) <= kMaxSmem;
     const size_t sm = expand_smem(max_nm, staged);
-    auto kern = f16 ? expand_split_kernel<true> : expand_split_kernel<false>;
+    auto kern = sw64 ? (f16 ? expand_split_kernel<true, true> : expand_split_kernel<false, true>)
+                     : (f16 ? expand_split_kernel<true, false> : expand_split_kernel<false, false>);
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int dev = 0, sms = 148, per = 0;
     SCP3_CUDA(cudaGetDevice(&dev));
@@ -868,7 +1195,7 @@ int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v,
         SCP3_CUDA(cudaMemcpyAsync(p.desc_dev + buf, &d, sizeof(d), cudaMemcpyHostToDevice, s));
         p.desc_host[buf] = d;
     }
-    rc = launch_expand(p.desc_dev + buf, 1, p.nb_pad, nm, slots, p.slots / kBK, p.x[buf], p.f16, s);
+    rc = launch_expand(p.desc_dev + buf, 1, p.nb_pad, nm, slots, p.slots / kBK2, p.x[buf], p.f16, s, true);
     if (rc) return rc;
     record(pev, pkind, 1, s);
     return SCP3GPU_OK;
@@ -878,10 +1205,10 @@ int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_
 {
     const int nflush = (int)(n / kFlush);
     record(pev, pkind, 2, s);
-    const int nsplit = p.nsplit < nflush ? p.nsplit : nflush;
-    int rc = launch_contract(p.x[buf], p.slots / kBK, p.tiles, p.ntiles, p.group_meta[buf], nflush, nsplit,
-                             p.products, p.f16, p.partial, p.err_flag, s);
-    if (rc) return rc;
+    contract_n256_kernel<<<p.grid, kThreads, kSmemBytes2, s>>>(
+        p.x[buf], (long long)(p.slots / kBK2), p.tiles2, p.ntiles, p.nsplit, (int)(p.slots / kBK2),
+        nflush * kKB2PerFlush, p.group_meta[buf], (int)p.f16, p.partial, p.err_flag);
+    SCP3_CUDA(cudaGetLastError());
     record(pev, pkind, 2, s);
     return SCP3GPU_OK;
 }
@@ -901,8 +1228,10 @@ int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, doub
     SCP3_CUDA(cudaStreamSynchronize(s));
     if (err) return fail(SCP3GPU_ERR_TIMEOUT, "tensor-core contraction: a bounded pipeline wait expired");
     const int64_t total = (int64_t)nb * nb;
-    (void)total;
-    return launch_unpack(p.partial, p.tile_index, p.nt, p.ntiles, p.nsplit, 0, nb, divisor, diag, zpe, M, ld, s);
+    unpack_n256_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p.partial, p.tile_index, p.nt, p.ntiles,
+                                                                      p.nsplit, nb, divisor, diag, zpe, M, ld);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
 }
 
 }  // namespace tc

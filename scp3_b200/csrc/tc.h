@@ -26,10 +26,12 @@ struct ExpandDesc {
     const int* slot_of;        // [slots] K slot -> sample
 };
 
+// The single build's contraction (128 x 256 tiles, contract_tc.cu).
 struct Plan {
-    int nb = 0, nb_pad = 0, nm = 0;
-    int nt = 0, ntiles = 0;       // 128-row tiles per side, upper tiles
-    int nsplit = 1;               // sample ranges per pass (each owns an FP64 partial per tile)
+    int nb = 0, nb_pad = 0, nm = 0;   // nb_pad: whole 256-row panel pairs
+    int nt = 0, ntiles = 0;       // 128-row panels per side; 128 x 256 tiles
+    int nsplit = 1;               // sample ranges per pass (each unit (split, tile) owns an FP64 partial)
+    int grid = 0;                 // CTAs of the contraction (one per SM at most)
     int64_t chunk = 0;            // samples per pass (multiple of kFlush)
     int products = 3;             // 3: hi*hi + hi*lo + lo*hi; 4: + lo*lo
     bool f16 = false;             // halves in FP16 (operand scaled by 2^6) instead of BF16
@@ -40,12 +42,12 @@ struct Plan {
     uint16_t* x[2] = {nullptr, nullptr};
     int* slot_of[2] = {nullptr, nullptr};    // [slots] K slot -> sample (-1: zero padding)
     int* group_meta[2] = {nullptr, nullptr}; // per 4096-sample block: first negative 16-group
-    WorkItem* tiles = nullptr;    // [ntiles] work items, in launch order
-    int* tile_index = nullptr;    // [nt*nt] position of tile (ti, tj) in `tiles`
+    int2* tiles2 = nullptr;       // [ntiles] (first A row, first B row) of each 128 x 256 tile
+    int* tile_index = nullptr;    // [nt*nt] owner of block (ti, tj): 2 * tile + column half
     uint32_t* factors = nullptr;  // [nb] basis functions as products of Hermite-table entries
     ExpandDesc* desc_dev = nullptr;   // [2] expansion descriptors of the two pass buffers
     ExpandDesc desc_host[2] = {};     // what desc_dev holds (uploaded again only when it changes)
-    double* partial = nullptr;    // [nsplit][ntiles][128*128] FP64
+    double* partial = nullptr;    // [nsplit][ntiles][128 x 256] FP64, tile-local column-major
     int* err_flag = nullptr;      // bounded-wait failures
 };
 
@@ -73,8 +75,10 @@ int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, doub
 int launch_partition(const double* v, int64_t v_stride, int* slot_of, int64_t slot_stride, int* neg, int neg_stride,
                      int nflush, int nclusters, cudaStream_t s);
 // slots: K slots of this pass (k-blocks of 64); nkb: k-blocks per row block in the operand's allocation
+// sw64: 32-slot boxes in the 64-byte swizzle (the single build's 128 x 256 contraction;
+// nkb then counts 32-slot k-blocks); otherwise 64-slot boxes in the 128-byte swizzle.
 int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t nkb,
-                  uint16_t* x, bool f16, cudaStream_t s);
+                  uint16_t* x, bool f16, cudaStream_t s, bool sw64 = false);
 // max_ctas > 0: at most that many CTAs, each looping over work units (persistent); 0: one CTA per unit.
 int launch_contract(const uint16_t* x, int64_t nkb, const WorkItem* items, int nitems, const int* neg, int nflush,
                     int nsplit, int products, bool f16, double* partial, int* err_flag, cudaStream_t s,

@@ -2,12 +2,13 @@
 
 Clusters of uneven size and basis built in one batch give, cluster by
 cluster, the matrix that a single split-form build of the same config gives:
-both run the same per-sample, partition, expansion and contraction code, and
-only the grouping of the FP64 partial sums differs (pass size and sample-range
-split), so they agree to 1e-11 of max|M|.  Graph replay equals direct launches
-bit for bit, several accumulate calls equal one call over the same points, and
-the batch stays within the split form's tolerance of the reference's golden
-matrices."""
+both run the same per-sample, partition and expansion code on the same BF16 (or
+FP16) operand values; the batch contracts 128 x 128 tiles with separate FP32
+accumulators for hi*hi and the cross terms, the single build 128 x 256 tiles
+with one FP32 accumulator, so they agree to the FP32 accumulation error
+(1e-5 of max|M|).  Graph replay equals direct launches bit for bit, several
+accumulate calls equal one call over the same points, and the batch stays
+within the split form's tolerance of the reference's golden matrices."""
 import numpy as np
 import pytest
 
@@ -64,9 +65,9 @@ def test_batch_matches_single_builds(scp3, prec):
         M = b.read(i, 0)
         assert M.shape == ref.shape
         scale = np.abs(ref).max()
-        assert np.abs(M - ref).max() <= 1e-11 * scale, (i, np.abs(M - ref).max() / scale)
+        assert np.abs(M - ref).max() <= 1e-5 * scale, (i, np.abs(M - ref).max() / scale)
         M1, R1 = b.read(i, 1), hb.read(1)
-        assert np.abs(M1 - R1).max() <= 1e-11 * np.abs(R1).max()
+        assert np.abs(M1 - R1).max() <= 1e-5 * np.abs(R1).max()
         assert b.status(i)[0] == 0
         hb.close()
     assert b.sample_count() == n
@@ -133,7 +134,7 @@ def test_batch_ttm3f(scp3):
         hb = _single(scp3, d, "ttm3f", "bf16x3")
         hb.accumulate(7, 4096)
         ref = hb.read(0)
-        assert np.abs(b.read(i, 0) - ref).max() <= 1e-11 * np.abs(ref).max()
+        assert np.abs(b.read(i, 0) - ref).max() <= 1e-5 * np.abs(ref).max()
         assert b.status(i)[0] == 0
         hb.close()
 
