@@ -4,17 +4,17 @@
 // kernel (grid.y = cluster, each cluster with its own geometry, modes and Sobol
 // tables), the sign partition (grid.y = cluster), the split-operand expansion
 // (grid.z = cluster) into one operand whose rows hold the clusters' bases one
-// after another (each padded to 128 rows), and one tensor-core contraction
-// over the concatenated list of every cluster's upper 128x128 tiles.  The
+// after another (each padded to 256 rows), and one tensor-core contraction
+// over the concatenated list of every cluster's 128 x 256 tiles.  The
 // passes of an accumulate call are captured once into a CUDA graph (the
 // prepare stream fills pass buffer p&1 while the main stream contracts the
 // other) and replayed; per-pass arguments (Sobol offsets) live in device
 // memory and are refreshed by one copy before each replay.
 //
-// The work shape of the contraction (how many sample ranges each tile's pass
-// is split into, and whether one CTA runs per work unit or a persistent grid
-// of one CTA per SM loops over them) is chosen at creation by timing every
-// candidate on a pass of the batch's own operand.
+// The work shape of the contraction: the number of tiles and of sample ranges
+// per tile come from the tiling (the fewest waves per unit of work); whether one
+// CTA runs per work unit or a persistent grid of one CTA per SM loops over them
+// is chosen at creation by timing both on a pass of the batch's own operand.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -30,7 +30,7 @@ struct Cluster {
     scp3gpu_config cfg{};              // host copy, pointers cleared
     int nb = 0, nb_pad = 0, nt = 0, row0 = 0;
     int64_t qoff = 0;                  // offset of the cluster's q in a pass buffer (floats)
-    int tindex_off = 0;                // offset of its tile index table
+    int tindex_off = 0;                // offset of its block-owner table
     std::vector<double> omega_sel;
     double zpe_inactive = 0.0;
     // device tables
@@ -54,11 +54,11 @@ struct scp3gpu_batch {
     int64_t chunk = 0, slots = 0;     // samples and K slots per pass
     int nflush = 0;
     // contraction work
-    int nitems = 0, nsplit_max = 1;
-    int nsplit = 1, ctas = 0;          // chosen work shape (ctas 0: one CTA per unit)
+    int ntiles = 0, nsplit = 1;        // 128 x 256 tiles of all clusters; sample ranges per pass
+    int ctas = 0;                      // chosen grid (one per unit, or one per SM looping over units)
     double tuned_ms = 0.0;
-    tc::WorkItem* items = nullptr;
-    int* tile_index = nullptr;
+    int4* tiles = nullptr;
+    int* tile_index = nullptr;         // per cluster, owner of block (ti, tj): 2 * tile + column half
     double* partial = nullptr;
     int* err_flag = nullptr;
     // pass buffers
@@ -66,7 +66,7 @@ struct scp3gpu_batch {
     double* v[kBuffers] = {};
     int* slot_of[kBuffers] = {};
     int* neg[kBuffers] = {};
-    uint16_t* x[kBuffers] = {};        // the operand (box layout of contract_tc.cu), rows x slots x 2 halves
+    uint16_t* x[kBuffers] = {};        // the operand (32-slot box layout of contract_tc.cu), rows x slots x 2 halves
     tc::ExpandDesc* desc_dev[kBuffers] = {};
     // per-pass sample arguments [pass][cluster]
     SampleArgs* args_dev = nullptr;
@@ -158,13 +158,14 @@ int enqueue(scp3gpu_batch* b, int64_t passes, int64_t last)
                                       b->args_dev + (size_t)p * b->ncl, b->ncl, npad, b->prep);
         if (!rc) rc = tc::launch_partition(b->v[buf], b->chunk, b->slot_of[buf], b->slots, b->neg[buf], b->nflush,
                                            nflush, b->ncl, b->prep);
-        if (!rc) rc = tc::launch_expand(b->desc_dev[buf], b->ncl, round_up(b->max_nb, tc::kTile), b->max_nm, slots, b->slots / 64,
-                                        b->x[buf], b->f16, b->prep);
+        if (!rc) rc = tc::launch_expand(b->desc_dev[buf], b->ncl, round_up(b->max_nb, 2 * tc::kTile), b->max_nm, slots,
+                                        b->slots / tc::kKBlock2, b->x[buf], b->f16, b->prep);
         if (rc) return rc;
         SCP3_CUDA(cudaEventRecord(b->prepared[buf], b->prep));
         SCP3_CUDA(cudaStreamWaitEvent(b->stream, b->prepared[buf], 0));
-        rc = tc::launch_contract(b->x[buf], b->slots / 64, b->items, b->nitems, b->neg[buf], nflush,
-                                 std::min(b->nsplit, nflush), 3, b->f16, b->partial, b->err_flag, b->stream, b->ctas);
+        rc = tc::launch_contract(b->x[buf], b->slots / tc::kKBlock2, b->tiles, b->ntiles, b->nsplit,
+                                  (int)(b->slots / tc::kKBlock2), (int)(slots / tc::kKBlock2), b->neg[buf], b->f16,
+                                  b->partial, b->err_flag, b->ctas, b->stream);
         if (rc) return rc;
         SCP3_CUDA(cudaEventRecord(b->contracted[buf], b->stream));
     }
@@ -223,53 +224,51 @@ int run_passes(scp3gpu_batch* b, int64_t passes, int64_t last)
 
 int zero_sums(scp3gpu_batch* b)
 {
-    SCP3_CUDA(cudaMemsetAsync(b->partial, 0, sizeof(double) * (size_t)b->nsplit_max * b->nitems * tc::kTile * tc::kTile,
+    SCP3_CUDA(cudaMemsetAsync(b->partial, 0, sizeof(double) * (size_t)b->nsplit * b->ntiles * tc::kTile * 2 * tc::kTile,
                               b->stream));
     SCP3_CUDA(cudaMemsetAsync(b->err_flag, 0, sizeof(int), b->stream));
     SCP3_CUDA(cudaMemsetAsync(b->counters, 0, sizeof(unsigned long long) * 2 * b->ncl, b->stream));
     return SCP3GPU_OK;
 }
 
-// Times every contraction work shape on one prepared pass (buffer 0) and keeps
-// the fastest.  The trial sums are discarded afterwards.
+// Times both grid forms of the contraction (one CTA per work unit; one CTA per
+// SM looping over the units) on one prepared pass (buffer 0) and keeps the
+// faster.  The trial sums are discarded afterwards.
 int autotune(scp3gpu_batch* b)
 {
     int rc = stage_args(b, 1ll << 30, b->chunk, 1);   // trial points from the reference's default skip
     if (rc) return rc;
+    const int units = b->ntiles * b->nsplit;
     // one direct pass prepares buffer 0 (and sets the kernels' attributes before any capture)
-    const int keep_split = b->nsplit, keep_ctas = b->ctas;
-    b->nsplit = 1;
-    b->ctas = b->sms;
+    b->ctas = std::min(units, b->sms);
     if ((rc = enqueue(b, 1, b->chunk))) return rc;
     cudaEvent_t e0, e1;
     SCP3_CUDA(cudaEventCreate(&e0));
     SCP3_CUDA(cudaEventCreate(&e1));
     double best = 1e30;
-    int best_split = keep_split, best_ctas = keep_ctas;
-    for (int ns = 1; ns <= b->nsplit_max && rc == 0; ns *= 2)
-        for (int persistent = 0; persistent < 2 && rc == 0; persistent++) {
-            const int ctas = persistent ? b->sms : 0;
-            float ms_best = 1e30f;
-            for (int rep = 0; rep < 3 && rc == 0; rep++) {
-                cudaEventRecord(e0, b->stream);
-                rc = tc::launch_contract(b->x[0], b->slots / 64, b->items, b->nitems, b->neg[0], b->nflush, ns, 3,
-                                         b->f16, b->partial, b->err_flag, b->stream, ctas);
-                cudaEventRecord(e1, b->stream);
-                if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(SCP3GPU_ERR_CUDA, "batch: autotune sync");
-                float ms = 0;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (rep > 0) ms_best = std::min(ms_best, ms);   // first run warms the caches
-            }
-            if (rc == 0 && ms_best < best) {
-                best = ms_best;
-                best_split = ns;
-                best_ctas = ctas;
-            }
+    int best_ctas = b->ctas;
+    const int cand[2] = {std::min(units, b->sms), units};
+    for (int ci = 0; ci < 2 && rc == 0; ci++) {
+        float ms_best = 1e30f;
+        for (int rep = 0; rep < 3 && rc == 0; rep++) {
+            cudaEventRecord(e0, b->stream);
+            rc = tc::launch_contract(b->x[0], b->slots / tc::kKBlock2, b->tiles, b->ntiles, b->nsplit,
+                                      (int)(b->slots / tc::kKBlock2), (int)(b->slots / tc::kKBlock2), b->neg[0], b->f16,
+                                      b->partial, b->err_flag, cand[ci], b->stream);
+            cudaEventRecord(e1, b->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(SCP3GPU_ERR_CUDA, "batch: autotune sync");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) ms_best = std::min(ms_best, ms);   // first run warms the caches
         }
+        if (rc == 0 && ms_best < best) {
+            best = ms_best;
+            best_ctas = cand[ci];
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    b->nsplit = best_split;
     b->ctas = best_ctas;
     b->tuned_ms = best;
     int err = 0;
@@ -336,7 +335,7 @@ int scp3gpu_batch_destroy(scp3gpu_batch* b)
         if (b->prepared[i]) cudaEventDestroy(b->prepared[i]);
         if (b->contracted[i]) cudaEventDestroy(b->contracted[i]);
     }
-    void* ptrs[] = {b->items, b->tile_index, b->partial, b->err_flag, b->args_dev, b->dense, b->counters};
+    void* ptrs[] = {b->tiles, b->tile_index, b->partial, b->err_flag, b->args_dev, b->dense, b->counters};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (b->args_pinned) cudaFreeHost(b->args_pinned);
@@ -404,8 +403,8 @@ int scp3gpu_batch_create(const scp3gpu_config* cfgs, int ncl, int64_t chunk, int
         k.cfg.x0 = k.cfg.MUa = k.cfg.omega = nullptr;
         k.cfg.modes = nullptr;
         k.nb = (int)scp3gpu_basis_size(cf.nmodes, cf.n2, cf.n3);
-        k.nt = (k.nb + tc::kTile - 1) / tc::kTile;
-        k.nb_pad = k.nt * tc::kTile;
+        k.nb_pad = (int)round_up(k.nb, 2 * tc::kTile);    // whole 256-row panel pairs
+        k.nt = k.nb_pad / tc::kTile;
         k.row0 = b->rows;
         b->rows += k.nb_pad;
         b->max_nb = std::max(b->max_nb, k.nb);
@@ -421,9 +420,10 @@ int scp3gpu_batch_create(const scp3gpu_config* cfgs, int ncl, int64_t chunk, int
         k.zpe_inactive = 0.5 * (sum_all - sum_sel);
         if ((rc = upload_cluster(k, &cf))) return bail(rc);
     }
-    // samples per pass: the two split operands of a pass buffer stay under ~3 GB
-    int64_t ch = chunk > 0 ? chunk : (int64_t)tc::kFlush * 16;
-    while (ch > tc::kFlush && (int64_t)b->rows * (ch / tc::kFlush) * tc::kSlotsPerFlush * 4 > (3ll << 30)) ch /= 2;
+    // samples per pass: up to 2^17 (long work units amortise each unit's pipeline
+    // fill and FP64 write-back), with each pass buffer's split operand under ~8 GB
+    int64_t ch = chunk > 0 ? chunk : (int64_t)tc::kFlush * 32;
+    while (ch > tc::kFlush && (int64_t)b->rows * (ch / tc::kFlush) * tc::kSlotsPerFlush * 4 > (8ll << 30)) ch /= 2;
     b->chunk = ch / tc::kFlush * tc::kFlush;
     b->nflush = (int)(b->chunk / tc::kFlush);
     b->slots = (int64_t)b->nflush * tc::kSlotsPerFlush;
@@ -434,28 +434,26 @@ int scp3gpu_batch_create(const scp3gpu_config* cfgs, int ncl, int64_t chunk, int
             off += b->chunk * k.cfg.nmodes;
         }
     }
-    // work items: every cluster's upper tiles, cluster by cluster, row-major
-    std::vector<tc::WorkItem> items;
+    // 128 x 256 tiles of every cluster, cluster by cluster
+    std::vector<tc::BaseTile> base;
+    std::vector<int> cnt;
+    for (int c = 0; c < ncl; c++) {
+        const Cluster& k = b->cl[c];
+        tc::add_cluster_tiles(base, c, k.nt, (k.nb + tc::kTile - 1) / tc::kTile, k.row0, c * b->nflush);
+        cnt.push_back(k.nt);
+    }
+    std::vector<int4> tiles;
+    std::vector<std::vector<int>> owners;
+    tc::finish_tiling(base, cnt, b->sms, tiles, owners, b->nsplit);
+    b->ntiles = (int)tiles.size();
     std::vector<int> tindex;
     for (int c = 0; c < ncl; c++) {
-        Cluster& k = b->cl[c];
-        k.tindex_off = (int)tindex.size();
-        tindex.resize(tindex.size() + (size_t)k.nt * k.nt, -1);
-        for (int i = 0; i < k.nt; i++)
-            for (int j = i; j < k.nt; j++) {
-                tindex[k.tindex_off + (size_t)i * k.nt + j] = (int)items.size();
-                tc::WorkItem w{k.row0 + i * tc::kTile, k.row0 + j * tc::kTile, c * b->nflush, 0,
-                               (long long)items.size() * tc::kTile * tc::kTile};
-                items.push_back(w);
-            }
+        b->cl[c].tindex_off = (int)tindex.size();
+        tindex.insert(tindex.end(), owners[c].begin(), owners[c].end());
     }
-    b->nitems = (int)items.size();
-    b->nsplit_max = 1;
-    while (b->nsplit_max < 8 && b->nsplit_max * 2 <= b->nflush) b->nsplit_max *= 2;
-    b->nsplit = 1;
-    b->ctas = b->sms;
-    if ((rc = upload(&b->items, items.data(), items.size())) || (rc = upload(&b->tile_index, tindex.data(), tindex.size())) ||
-        (rc = dalloc(&b->partial, (size_t)b->nsplit_max * b->nitems * tc::kTile * tc::kTile)) ||
+    b->ctas = std::min(b->ntiles * b->nsplit, b->sms);
+    if ((rc = upload(&b->tiles, tiles.data(), tiles.size())) || (rc = upload(&b->tile_index, tindex.data(), tindex.size())) ||
+        (rc = dalloc(&b->partial, (size_t)b->nsplit * b->ntiles * tc::kTile * 2 * tc::kTile)) ||
         (rc = dalloc(&b->err_flag, 1)) || (rc = dalloc(&b->counters, (size_t)2 * ncl)))
         return bail(rc);
     for (int i = 0; i < kBuffers; i++) {
@@ -544,9 +542,9 @@ int scp3gpu_batch_read(scp3gpu_batch* b, int c, double* M, int64_t ld, int mode)
     SCP3_CUDA(cudaMemcpyAsync(&err, b->err_flag, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
     SCP3_CUDA(cudaStreamSynchronize(b->stream));
     if (err) return fail(SCP3GPU_ERR_TIMEOUT, "tensor-core contraction: a bounded pipeline wait expired");
-    rc = tc::launch_unpack(b->partial, b->tile_index + k.tindex_off, k.nt, b->nitems, b->nsplit_max, 0, k.nb,
-                           mode == 1 ? (double)b->count : 1.0, mode == 1 ? k.hodiag : nullptr,
-                           mode == 1 ? k.zpe_inactive : 0.0, b->dense, k.nb, b->stream);
+    rc = tc::launch_unpack(b->partial, b->tile_index + k.tindex_off, k.nt, b->ntiles, b->nsplit, k.nb,
+                            mode == 1 ? (double)b->count : 1.0, mode == 1 ? k.hodiag : nullptr,
+                            mode == 1 ? k.zpe_inactive : 0.0, b->dense, k.nb, b->stream);
     if (rc) return rc;
     SCP3_CUDA(cudaMemcpy2DAsync(M, sizeof(double) * ld, b->dense, sizeof(double) * k.nb, sizeof(double) * k.nb, k.nb,
                                 cudaMemcpyDeviceToHost, b->stream));

@@ -4,39 +4,33 @@
 //                                              ScaledMatrixElements.cpp:951-971)
 //
 // Operand.  X_i(s) = sqrt|V_s| Phi_i(s), so that X_i X_j = |V_s| Phi_i Phi_j and
-// one operand array serves as both A (rows of tile ti) and B (rows of tile tj).
-// Within every 4096-sample block the samples are stably partitioned by the
-// sign of V (positive first), each sign group padded to a multiple of 16, so a
-// whole K=16 MMA step has one sign; negative steps set the negate-A bit of the
-// instruction descriptor.  X is stored split, X = hi + lo in BF16 (hi = bf16(x),
-// lo = bf16(x - hi)), and every product is formed as hi*hi + hi*lo + lo*hi
-// (three kind::f16 MMAs into one FP32 TMEM accumulator).
+// one operand array serves as both A (a 128-row panel) and B (two consecutive
+// panels).  Within every 4096-sample block the samples are stably partitioned
+// by the sign of V (positive first), each sign group padded to a multiple of
+// 16, so a whole K=16 MMA step has one sign; negative steps set the negate-A
+// bit of the instruction descriptor.  X is stored split, X = hi + lo in BF16
+// (hi = bf16(x), lo = bf16(x - hi)) or FP16 (scaled by 2^6), and every product
+// is formed as hi*hi + hi*lo + lo*hi: three kind::f16 MMAs of M = 128, N = 256,
+// K = 16 into one FP32 TMEM accumulator.
 //
-// Accumulation.  Each CTA owns one 128x128 upper tile (ti <= tj) and one range
-// of 4096-sample blocks of the pass.  FP32 accumulators live in TMEM: one for
-// the hi*hi products and one for the (2^8 times smaller) cross products, so the
-// large accumulator takes a third of the additions.  After every 4 k-blocks
-// (256 K slots) the epilogue warps drain both into FP64 accumulators held in
-// their registers (one row and 64 columns per thread); the FP64 tile is added
-// into the CTA's partial in global memory once, at the end of its range.  Two
-// TMEM buffers alternate so a drain overlaps the next segment's MMAs.  Why so
-// often: the tensor core's FP32 accumulation error grows with the number of
-// additions into one accumulator, and V carries the cluster's binding energy
-// (~ -0.07 Eh) into every element; on the hexamer, 4096-sample FP32 runs in one
-// accumulator put ~0.45 cm^-1 into the levels, 1024-slot runs in split
-// accumulators ~0.08, 512-slot runs ~0.06 (BF16) / 0.04 (FP16 halves).
+// Operand layout.  The expansion writes X in boxes of 128 rows x 32 K slots
+// (8 KB), each already in the 64-byte-swizzled order the MMA descriptors read
+// (16-byte chunk c of row r at chunk c ^ ((r >> 1) & 3)), the hi and lo boxes
+// of a (row block, k-block) next to each other: [row block][k-block][hi, lo].
+// A pipeline stage is five bulk copies (A hi+lo, then B hi and lo of each of
+// the two panels), and the expansion's stores are sequential.
 //
-// Operand layout.  The expansion writes X in boxes of 128 rows x 64 K slots
-// (16 KB), each already in the 128-byte-swizzled order the MMA descriptors
-// read (16-byte chunk c of row r at chunk c ^ (r & 7)), the hi and lo boxes of
-// a (row block, k-block) next to each other: [row block][k-block][hi, lo][16 KB].
-// A stage is then two contiguous 32 KB bulk copies (A and B), and the
-// expansion's stores are sequential.
+// Accumulation: see the 128 x 256 kernel below.  Why the FP32 runs are short:
+// the tensor core's FP32 accumulation error grows with the number of additions
+// into one accumulator, and V carries the cluster's binding energy (~ -0.07 Eh)
+// into every element; on the hexamer, 4096-sample FP32 runs in one accumulator
+// put ~0.45 cm^-1 into the levels.
 //
-// Warp roles (320 threads): warp 0 lane 0 issues the bulk copies, warp 1 owns TMEM (512 columns) and lane 0
-// issues the MMAs and commits, warps 2..9 drain the accumulators.  Every mbarrier wait is
-// bounded (4 s of %globaltimer); on expiry the CTA records an error, stops
-// issuing, waits (bounded) for its own loads and MMAs, frees TMEM and returns.
+// Warp roles (320 threads): warp 0 lane 0 issues the bulk copies, warp 1 owns
+// TMEM (512 columns) and lane 0 issues the MMAs and commits, warps 2..9 drain
+// the accumulator.  Every mbarrier wait is bounded (4 s of %globaltimer); on
+// expiry the CTA records an error, stops issuing, waits (bounded) for its own
+// loads and MMAs, frees TMEM and returns.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -52,26 +46,10 @@ namespace tc {
 
 namespace {
 
-constexpr int kBK = 64;                      // K slots per stage (128 B of bf16: one swizzle atom)
-constexpr int kStages = 3;
-constexpr int kTileBytes = kTile * kBK * 2;  // 16 KB per operand box
-constexpr int kStageBytes = 4 * kTileBytes;  // A_hi A_lo B_hi B_lo
-constexpr int kKBlocks = kSlotsPerFlush / kBK;   // 65 k-blocks per 4096-sample block
-constexpr int kDrainKB = 4;                      // k-blocks per FP32 accumulation run (256 K slots)
-constexpr int kSegments = (kKBlocks + kDrainKB - 1) / kDrainKB;   // runs per block
 constexpr int kThreads = 320;
 constexpr int kEpiWarps = 8;
-constexpr int kSmemBytes = kStages * kStageBytes + 1024 /* align */ + 256 /* barriers */;
 constexpr unsigned long long kWaitNs = 4000000000ull;
 
-// instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A/B BF16 (bits 7-9,
-// 10-12 = 1), both K-major (bits 15/16 = 0), N>>3 at bits 17-22, M>>4 at 24-28.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTile >> 3) << 17) |
-                            ((uint32_t)(kTile >> 4) << 24);
-constexpr uint32_t kIdescNegA = kIdesc | (1u << 13);
-// FP16 inputs: A/B format 0
-constexpr uint32_t kIdescF16 = kIdesc & ~((7u << 7) | (7u << 10));
-constexpr uint32_t kIdescF16NegA = kIdescF16 | (1u << 13);
 // FP16 operands are stored as 2^6 x; products carry 2^12
 constexpr float kF16Scale = 64.0f;
 constexpr double kF16Unscale = 1.0 / 4096.0;
@@ -138,15 +116,6 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                  : "memory");
 }
 
-// K-major, SWIZZLE_128B shared-memory matrix descriptor: start address >> 4,
-// LBO 16 B (unused for swizzled K-major), SBO 1024 B (8 rows x 128 B), version 1
-// (bits 46-47), layout type 2 = SWIZZLE_128B (bits 61-63).
-__device__ __forceinline__ uint64_t smem_desc(const void* p)
-{
-    const uint64_t addr = smem_u32(p);
-    return ((addr >> 4) & 0x3FFFull) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
-}
-
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
 {
     asm volatile(
@@ -180,212 +149,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
     for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[j]);
 }
 
-// Work units: unit u = split * nitems + item takes work item `item` over flush
-// blocks [split*nflush/nsplit, (split+1)*nflush/nsplit).  CTA b runs units b,
-// b + gridDim.x, ...: with one CTA per unit this is the plain launch, with fewer
-// CTAs (one per SM) it is persistent, and the loads and MMAs of a CTA's next
-// unit overlap the FP64 write-back of the previous one.  Pipeline counters
-// (stage, phase, accumulator use) run on across units.
-__global__ void __launch_bounds__(kThreads, 1)
-    contract_bf16x3_kernel(const uint16_t* __restrict__ xop, long long nkb,
-                           const WorkItem* __restrict__ items, const int* __restrict__ neg_group, int nflush,
-                           int nitems, int nsplit, int products, int f16, double* __restrict__ partial,
-                           int* __restrict__ err_flag)
-{
-    extern __shared__ uint8_t smem_raw[];
-    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
-    uint64_t* full = bars;                    // [kStages]
-    uint64_t* empty = bars + kStages;         // [kStages]
-    uint64_t* acc_full = bars + 2 * kStages;  // [2]
-    uint64_t* acc_empty = acc_full + 2;       // [2]
-    uint64_t* drain = acc_empty + 2;          // [1]
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
-    volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nunits = nitems * nsplit;
-    auto flush_range = [&](int split, int& f0, int& f1) {
-        f0 = (int)((int64_t)split * nflush / nsplit);
-        f1 = (int)((int64_t)(split + 1) * nflush / nsplit);
-    };
-
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; s++) {
-            mbar_init(full + s, 1);
-            mbar_init(empty + s, 1);
-        }
-        for (int a = 0; a < 2; a++) {
-            mbar_init(acc_full + a, 1);
-            mbar_init(acc_empty + a, kEpiWarps);
-        }
-        mbar_init(drain, 1);
-        *abort = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
-
-    if (warp == 0) {
-        if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
-            int issued[kStages] = {0, 0, 0};
-            uint32_t issued_phase[kStages] = {0, 0, 0};
-            bool ok = true;
-            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
-                const WorkItem wi = items[u % nitems];
-                const bool diag = wi.arow == wi.brow;
-                const uint32_t bytes = diag ? 2 * kTileBytes : 4 * kTileBytes;
-                int f0, f1;
-                flush_range(u / nitems, f0, f1);
-                for (int f = f0; f < f1 && ok; f++) {
-                    for (int kb = 0; kb < kKBlocks; kb++) {
-                        if (!mbar_wait(empty + stage, phase ^ 1, abort)) {
-                            ok = false;
-                            break;
-                        }
-                        uint8_t* st = smem + stage * kStageBytes;
-                        mbar_expect_tx(full + stage, bytes);
-                        const long long kbi = (long long)f * kKBlocks + kb;
-                        bulk_load(st, xop + ((wi.arow / kTile) * nkb + kbi) * (2 * kTile * kBK), 2 * kTileBytes,
-                                  full + stage);
-                        if (!diag)
-                            bulk_load(st + 2 * kTileBytes, xop + ((wi.brow / kTile) * nkb + kbi) * (2 * kTile * kBK),
-                                      2 * kTileBytes, full + stage);
-                        issued[stage] = 1;
-                        issued_phase[stage] = phase;
-                        if (++stage == kStages) {
-                            stage = 0;
-                            phase ^= 1;
-                        }
-                    }
-                }
-            }
-            if (*abort) {   // let our own loads land before the CTA leaves
-                for (int s = 0; s < kStages; s++)
-                    if (issued[s]) {
-                        volatile int never = 0;
-                        mbar_wait(full + s, issued_phase[s], &never);
-                    }
-            }
-        }
-    } else if (warp == 1) {
-        if (lane == 0) {
-            int stage = 0, use = 0;
-            uint32_t phase = 0;
-            bool ok = true;
-            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
-                const WorkItem wi = items[u % nitems];
-                const bool diag = wi.arow == wi.brow;
-                int f0, f1;
-                flush_range(u / nitems, f0, f1);
-                for (int f = f0; f < f1 && ok; f++) {
-                    const int neg0 = neg_group[wi.neg_off + f];
-                    for (int seg = 0; seg < kSegments && ok; seg++, use++) {
-                        const int a = use & 1;
-                        if (!mbar_wait(acc_empty + a, ((use >> 1) & 1) ^ 1, abort)) {
-                            ok = false;
-                            break;
-                        }
-                        tc_fence_after();
-                        const uint32_t dhh = tmem + (uint32_t)(a * 2 * kTile), dx = dhh + kTile;
-                        const int kb1 = min(kKBlocks, (seg + 1) * kDrainKB);
-                        for (int kb = seg * kDrainKB; kb < kb1; kb++) {
-                            if (!mbar_wait(full + stage, phase, abort)) {
-                                ok = false;
-                                break;
-                            }
-                            tc_fence_after();
-                            uint8_t* st = smem + stage * kStageBytes;
-                            const uint64_t ahi = smem_desc(st), alo = smem_desc(st + kTileBytes);
-                            const uint64_t bhi = diag ? ahi : smem_desc(st + 2 * kTileBytes);
-                            const uint64_t blo = diag ? alo : smem_desc(st + 3 * kTileBytes);
-#pragma unroll
-                            for (int kk = 0; kk < kBK / 16; kk++) {
-                                const bool neg = kb * 4 + kk >= neg0;
-                                const uint32_t idesc =
-                                    f16 ? (neg ? kIdescF16NegA : kIdescF16) : (neg ? kIdescNegA : kIdesc);
-                                const uint64_t adv = (uint64_t)(kk * 2);    // 32 B along K inside the swizzle atom
-                                const uint32_t acc = (kb != seg * kDrainKB) | (kk != 0);
-                                mma_bf16(dhh, ahi + adv, bhi + adv, idesc, acc);
-                                mma_bf16(dx, ahi + adv, blo + adv, idesc, acc);
-                                mma_bf16(dx, alo + adv, bhi + adv, idesc, 1);
-                                if (products == 4) mma_bf16(dx, alo + adv, blo + adv, idesc, 1);
-                            }
-                            mma_commit(empty + stage);      // frees the stage once these MMAs have read it
-                            if (++stage == kStages) {
-                                stage = 0;
-                                phase ^= 1;
-                            }
-                        }
-                        if (ok) mma_commit(acc_full + a);
-                    }
-                }
-            }
-            mma_commit(drain);                     // completes when every MMA above has
-            volatile int never = 0;
-            mbar_wait(drain, 0, &never);
-        }
-    } else {
-        // epilogue: warps 2..9; warp w reads TMEM lane quadrant w%4 and column half (w-2)/4
-        const int quad = warp & 3, half = (warp - 2) >> 2;
-        const int row = quad * 32 + lane;
-        const double unscale = f16 ? kF16Unscale : 1.0;
-        int use = 0;
-        bool ok = true;
-        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
-            const WorkItem wi = items[u % nitems];
-            const int split = u / nitems;
-            int f0, f1;
-            flush_range(split, f0, f1);
-            double acc[64];
-#pragma unroll
-            for (int j = 0; j < 64; j++) acc[j] = 0.0;
-            const int nseg = (f1 - f0) * kSegments;
-            for (int k = 0; k < nseg; k++, use++) {
-                const int a = use & 1;
-                if (!mbar_wait(acc_full + a, (use >> 1) & 1, abort)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * 2 * kTile + half * 64);
-#pragma unroll
-                for (int c0 = 0; c0 < 64; c0 += 32) {
-#pragma unroll
-                    for (int part = 0; part < 2; part++) {     // hi*hi, then the cross terms
-                        float t[32];
-                        tmem_ld32(base + part * kTile + c0, t);
-#pragma unroll
-                        for (int j = 0; j < 32; j++) acc[c0 + j] += (double)t[j];
-                    }
-                }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(acc_empty + a);
-            }
-            if (!ok) break;
-            double* P = partial + (size_t)split * nitems * (kTile * kTile) + wi.poff;
-#pragma unroll
-            for (int j = 0; j < 64; j++) P[(size_t)(half * 64 + j) * kTile + row] += acc[j] * unscale;
-        }
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (threadIdx.x == 0 && *abort) atomicExch(err_flag, 1);
-    if (warp == 1) {
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
-    }
-}
-
 // ---------------------------------------------------------------------------
 // The single build's contraction: 128 x 256 tiles, one M=128, N=256, K=16 MMA
 // per product.  An MMA costs about the same time for N = 128 and N = 256, so
@@ -396,9 +159,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 // 32 K slots: A (one row panel, hi + lo, 16 KB) and B (two consecutive panels,
 // hi then lo, 32 KB); four stages are in flight.
 //
-// Tiles: (A panel, first B panel); every upper 128 x 128 block is owned by one
-// tile (the tiling and which half of a tile owns which block are the host's;
-// a tile may own one half only).  Work unit u = split * ntiles + tile takes the
+// Tiles: (first A row, first B row, offset of the cluster's sign-group table);
+// every needed upper 128 x 128 block is owned by one tile (the tiling and which
+// half of a tile owns which block are the host's; a tile may own one half only).  Work unit u = split * ntiles + tile takes the
 // tile over k-blocks [split * nkb_full / nsplit, (split + 1) * nkb_full /
 // nsplit) of the pass; CTA b runs units b, b + gridDim.x, ... .  Units of one
 // wave share k-ranges, so L2 serves the panels they have in common.
@@ -433,7 +196,7 @@ __device__ __forceinline__ uint64_t smem_desc64(const void* p)
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
-    contract_n256_kernel(const uint16_t* __restrict__ xop, long long nkb_alloc, const int2* __restrict__ tiles,
+    contract_n256_kernel(const uint16_t* __restrict__ xop, long long nkb_alloc, const int4* __restrict__ tiles,
                          int ntiles, int nsplit, int nkb_full, int nkb_pass, const int* __restrict__ neg_group,
                          int f16, double* __restrict__ partial, int* __restrict__ err_flag)
 {
@@ -492,7 +255,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
                 int lo, hi;
                 krange(u, lo, hi);
-                const int2 ti = tiles[u % ntiles];
+                const int4 ti = tiles[u % ntiles];
                 const uint16_t* pa = xop + (size_t)(ti.x / kTile) * nkb_alloc * (2 * kBoxElems);
                 const uint16_t* pb0 = xop + (size_t)(ti.y / kTile) * nkb_alloc * (2 * kBoxElems);
                 const uint16_t* pb1 = pb0 + (size_t)nkb_alloc * (2 * kBoxElems);
@@ -533,6 +296,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
                 int lo, hi;
                 krange(u, lo, hi);
+                const int neg_off = tiles[u % ntiles].z;
                 for (int k0 = lo; k0 < hi && ok; k0 += kDrain2, use++) {
                     const int a = use & 1;
                     if (!mbar_wait(acc_empty + a, ((use >> 1) & 1) ^ 1, abort)) {
@@ -552,7 +316,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const uint64_t ahi = smem_desc64(st), alo = smem_desc64(st + kBox2);
                         const uint64_t bhi = smem_desc64(st + 2 * kBox2), blo = smem_desc64(st + 4 * kBox2);
                         const int f = kb / kKB2PerFlush;
-                        const int neg0 = neg_group[f];
+                        const int neg0 = neg_group[neg_off + f];
                         const int ks0 = (kb - f * kKB2PerFlush) * (kBK2 / 16);
 #pragma unroll
                         for (int kk = 0; kk < kBK2 / 16; kk++) {
@@ -778,9 +542,9 @@ __host__ __device__ inline size_t expand_smem(int nm, bool staged)
     return f * sizeof(float);
 }
 
-// SW64: the single build's operand (32-slot boxes in the 64-byte swizzle, nkb
-// counts 32-slot k-blocks); otherwise 64-slot boxes in the 128-byte swizzle.
-template <bool F16, bool SW64>
+// The operand is written as 32-slot boxes in the 64-byte swizzle (nkb counts
+// 32-slot k-blocks per row block).
+template <bool F16>
 __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandDesc* __restrict__ descs, int ncl,
                                                                     int64_t nkbp, int64_t nkb, int staged,
                                                                     uint16_t* __restrict__ xop)
@@ -917,7 +681,6 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandD
             const float4* tab4 = reinterpret_cast<const float4*>(tab);
             const float4 w0 = reinterpret_cast<const float4*>(sv)[g8];
             const float4 w1 = reinterpret_cast<const float4*>(sv)[g8 + 8];
-            uint16_t* xkb = xop + (size_t)cur.kb * (2 * kTile * kExpSlots);
             for (int r = cur.r0 + rl; r < cur.r1; r += 4 * kStep) {
                 uint32_t f[4];
 #pragma unroll
@@ -944,21 +707,12 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandD
                         split2<F16>(w1.x * (a1.x * b1.x * c1.x), w1.y * (a1.y * b1.y * c1.y), hi.z, lo.z);
                         split2<F16>(w1.z * (a1.z * b1.z * c1.z), w1.w * (a1.w * b1.w * c1.w), hi.w, lo.w);
                     }
-                    const int row = row0 + rr, rin = row & (kTile - 1);
-                    if (SW64) {
-                        // 32-slot box (row block, 2 k-block + g8 / 4): chunk c of row rin at c ^ ((rin >> 1) & 3)
-                        const int c = g8 & 3;
-                        uint16_t* box = xop + ((size_t)(row / kTile) * nkb + 2 * cur.kb + (g8 >> 2)) * (2 * kTile * 32);
-                        const int off = rin * 32 + ((c ^ ((rin >> 1) & 3)) << 3);
-                        *reinterpret_cast<uint4*>(box + off) = hi;
-                        *reinterpret_cast<uint4*>(box + kTile * 32 + off) = lo;
-                    } else {
-                        // box (row block, k-block), swizzled: 16-byte chunk g8 of row rin at g8 ^ (rin & 7)
-                        uint16_t* box = xkb + (size_t)(row / kTile) * nkb * (2 * kTile * kExpSlots);
-                        const int off = rin * kExpSlots + ((g8 ^ (rin & 7)) << 3);
-                        *reinterpret_cast<uint4*>(box + off) = hi;
-                        *reinterpret_cast<uint4*>(box + kTile * kExpSlots + off) = lo;
-                    }
+                    // 32-slot box (row block, 2 k-block + g8 / 4): chunk c of row rin at c ^ ((rin >> 1) & 3)
+                    const int row = row0 + rr, rin = row & (kTile - 1), c = g8 & 3;
+                    uint16_t* box = xop + ((size_t)(row / kTile) * nkb + 2 * cur.kb + (g8 >> 2)) * (2 * kTile * kBK2);
+                    const int off = rin * kBK2 + ((c ^ ((rin >> 1) & 3)) << 3);
+                    *reinterpret_cast<uint4*>(box + off) = hi;
+                    *reinterpret_cast<uint4*>(box + kTile * kBK2 + off) = lo;
                 }
             }
         }
@@ -969,25 +723,6 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandD
         __syncthreads();
         cur = nxt;
     }
-}
-
-// Dense column-major nb x nb from the tile partials (tile-local column-major).
-__global__ void unpack_tc_kernel(const double* __restrict__ partial, const int* __restrict__ tile_index, int nt,
-                                 int ntiles, int nsplit, int nb, double divisor, const double* __restrict__ diag,
-                                 double zpe, double* __restrict__ M, int64_t ld, int64_t item0)
-{
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (int64_t)nb * nb) return;
-    const int j = (int)(e / nb), i = (int)(e - (int64_t)j * nb);
-    const int r = min(i, j), c = max(i, j);
-    const int ti = r / kTile, tj = c / kTile;
-    const int64_t t = item0 + tile_index[(size_t)ti * nt + tj];
-    const size_t off = (size_t)t * kTile * kTile + (size_t)(c - tj * kTile) * kTile + (r - ti * kTile);
-    double val = 0.0;
-    for (int s = 0; s < nsplit; s++) val += partial[(size_t)s * ntiles * kTile * kTile + off];
-    val = val / divisor;
-    if (diag && i == j) val = (val + diag[i]) + zpe;
-    M[(size_t)j * ld + i] = val;
 }
 
 void record(std::vector<cudaEvent_t>* pev, std::vector<int>* pkind, int kind, cudaStream_t s)
@@ -1002,34 +737,34 @@ void record(std::vector<cudaEvent_t>* pev, std::vector<int>* pkind, int kind, cu
 
 }  // namespace
 
-// The 128 x 256 tiling of the upper block triangle of an nt x nt grid of
-// 128 x 128 blocks (nt even): row panel ti takes its blocks ti..nt-1 in pairs,
-// and an odd one out as the second half of the tile on panels (nt-2, nt-1).
-// Tiles come in 12-row x 6-pair groups so that a wave of CTAs shares panels.
-// Choosing more tiles than the minimum splits pairs into two one-half tiles;
-// (tiles, splits) minimise waves / splits (the time in units of a whole-pass
-// tile) over at most 16 splits and 4 GB of partials.  owner[ti * nt + tj] =
-// 2 * tile + half for every block ti <= tj.
-void tiling_n256(int nt, int sms, std::vector<int2>& tiles, std::vector<int>& owner, int& nsplit)
+// The 128 x 256 tiling of a cluster's upper block triangle (nt x nt grid of
+// 128 x 128 blocks, nt even; blocks ti <= tj < nt_need hold basis rows): row
+// panel ti takes the aligned column pairs (2q, 2q+1) that hold a needed block,
+// owning both halves or one.  Tiles come in 12-row x 6-pair groups so that a
+// wave of CTAs shares panels.
+void add_cluster_tiles(std::vector<BaseTile>& base, int cluster, int nt, int nt_need, int row0, int neg_off)
 {
-    struct T2 {
-        int ti, s, halves;   // halves: bit 0 = block s, bit 1 = block s + 1
-    };
-    std::vector<T2> base;
     const int R = 12, C = 6;
-    for (int r0 = 0; r0 < nt; r0 += R)
+    for (int r0 = 0; r0 < nt_need; r0 += R)
         for (int c0 = 0; c0 < nt / 2; c0 += C)
-            for (int ti = r0; ti < std::min(r0 + R, nt); ti++)
-                for (int pr = c0; pr < std::min(c0 + C, nt / 2); pr++) {
-                    // pair pr covers column panels 2pr, 2pr+1 of the aligned grid; row ti needs tj >= ti
-                    const int a = 2 * pr, b = 2 * pr + 1;
-                    const bool na = a >= ti, nb_ = b >= ti;
-                    if (na && nb_) base.push_back({ti, a, 3});
-                    else if (nb_) base.push_back({ti, a, 2});
+            for (int ti = r0; ti < std::min(r0 + R, nt_need); ti++)
+                for (int q = c0; q < std::min(c0 + C, nt / 2); q++) {
+                    const int a = 2 * q, b = 2 * q + 1;
+                    const int halves = (a >= ti && a < nt_need ? 1 : 0) | (b >= ti && b < nt_need ? 2 : 0);
+                    if (halves) base.push_back(BaseTile{cluster, ti, a, halves, row0, neg_off});
                 }
+}
+
+// Chooses the number of tiles (the base tiling, with some pairs split into two
+// one-half tiles) and of splits, minimising waves / splits -- the contraction
+// time in units of one whole-pass tile -- over at most 16 splits and 4 GB of
+// partials; emits the tiles and, per cluster, owner[ti * nt + tj] = 2 tile + half.
+void finish_tiling(const std::vector<BaseTile>& base, const std::vector<int>& cluster_nt, int sms,
+                   std::vector<int4>& tiles, std::vector<std::vector<int>>& owner, int& nsplit)
+{
     const int tmin = (int)base.size();
     int pairs = 0;
-    for (const T2& t : base) pairs += t.halves == 3;
+    for (const BaseTile& t : base) pairs += t.halves == 3;
     double best = 1e30;
     int bestT = tmin, bestM = 1;
     long long bestU = 0;
@@ -1046,22 +781,47 @@ void tiling_n256(int nt, int sms, std::vector<int2>& tiles, std::vector<int>& ow
             }
         }
     tiles.clear();
-    owner.assign((size_t)nt * nt, -1);
+    owner.assign(cluster_nt.size(), {});
+    for (size_t c = 0; c < cluster_nt.size(); c++) owner[c].assign((size_t)cluster_nt[c] * cluster_nt[c], -1);
     int extra = bestT - tmin;
-    for (const T2& t : base) {
+    for (const BaseTile& t : base) {
+        const int nt = cluster_nt[t.cluster];
+        const int4 tile = make_int4(t.row0 + t.ti * kTile, t.row0 + t.s * kTile, t.neg_off, t.cluster);
         if (t.halves == 3 && extra > 0) {
             extra--;
             for (int h = 0; h < 2; h++) {
-                owner[(size_t)t.ti * nt + t.s + h] = 2 * (int)tiles.size() + h;
-                tiles.push_back(make_int2(t.ti * kTile, t.s * kTile));
+                owner[t.cluster][(size_t)t.ti * nt + t.s + h] = 2 * (int)tiles.size() + h;
+                tiles.push_back(tile);
             }
             continue;
         }
         for (int h = 0; h < 2; h++)
-            if (t.halves & (1 << h)) owner[(size_t)t.ti * nt + t.s + h] = 2 * (int)tiles.size() + h;
-        tiles.push_back(make_int2(t.ti * kTile, t.s * kTile));
+            if (t.halves & (1 << h)) owner[t.cluster][(size_t)t.ti * nt + t.s + h] = 2 * (int)tiles.size() + h;
+        tiles.push_back(tile);
     }
     nsplit = bestM;
+}
+
+int launch_contract(const uint16_t* x, int64_t nkb_alloc, const int4* tiles, int ntiles, int nsplit, int nkb_full,
+                     int nkb_pass, const int* neg, bool f16, double* partial, int* err_flag, int grid, cudaStream_t s)
+{
+    if (ntiles <= 0 || nsplit <= 0 || grid <= 0) return SCP3GPU_OK;
+    SCP3_CUDA(cudaFuncSetAttribute(contract_n256_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes2));
+    contract_n256_kernel<<<grid, kThreads, kSmemBytes2, s>>>(x, (long long)nkb_alloc, tiles, ntiles, nsplit, nkb_full,
+                                                             nkb_pass, neg, (int)f16, partial, err_flag);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
+
+int launch_unpack(const double* partial, const int* owner, int nt, int ntiles, int nsplit, int nb, double divisor,
+                   const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s)
+{
+    const int64_t total = (int64_t)nb * nb;
+    if (total <= 0) return SCP3GPU_OK;
+    unpack_n256_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(partial, owner, nt, ntiles, nsplit, nb, divisor,
+                                                                      diag, zpe, M, ld);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
 }
 
 int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int chunk_req, int sms, bool f16)
@@ -1079,9 +839,12 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
     p.chunk = chunk;
     const int nflush = (int)(chunk / kFlush);
     p.slots = (int64_t)nflush * kSlotsPerFlush;
-    std::vector<int2> tiles;
-    std::vector<int> owner;
-    tiling_n256(p.nt, sms, tiles, owner, p.nsplit);
+    std::vector<BaseTile> base;
+    add_cluster_tiles(base, 0, p.nt, (nb + kTile - 1) / kTile, 0, 0);
+    std::vector<int4> tiles;
+    std::vector<std::vector<int>> owners;
+    finish_tiling(base, std::vector<int>{p.nt}, sms, tiles, owners, p.nsplit);
+    const std::vector<int>& owner = owners[0];
     p.ntiles = (int)tiles.size();
     p.grid = (int)std::min<long long>((long long)p.ntiles * p.nsplit, sms);
     for (int b = 0; b < 2; b++) {
@@ -1089,8 +852,8 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
         SCP3_CUDA(cudaMalloc(&p.slot_of[b], sizeof(int) * (size_t)p.slots));
         SCP3_CUDA(cudaMalloc(&p.group_meta[b], sizeof(int) * nflush));
     }
-    SCP3_CUDA(cudaMalloc(&p.tiles2, sizeof(int2) * tiles.size()));
-    SCP3_CUDA(cudaMemcpy(p.tiles2, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
+    SCP3_CUDA(cudaMalloc(&p.tiles2, sizeof(int4) * tiles.size()));
+    SCP3_CUDA(cudaMemcpy(p.tiles2, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice));
     const std::vector<uint32_t> fac = basis_factor_table(nm_for_factors, n2_for_factors, n3_for_factors);
     SCP3_CUDA(cudaMalloc(&p.factors, sizeof(uint32_t) * fac.size()));
     SCP3_CUDA(cudaMemcpy(p.factors, fac.data(), sizeof(uint32_t) * fac.size(), cudaMemcpyHostToDevice));
@@ -1135,13 +898,12 @@ int launch_partition(const double* v, int64_t v_stride, int* slot_of, int64_t sl
 }
 
 int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t nkb,
-                  uint16_t* x, bool f16, cudaStream_t s, bool sw64)
+                  uint16_t* x, bool f16, cudaStream_t s)
 {
     constexpr size_t kMaxSmem = 227 * 1024;
     const bool staged = expand_smem(max_nm, true) <= kMaxSmem;
     const size_t sm = expand_smem(max_nm, staged);
-    auto kern = sw64 ? (f16 ? expand_split_kernel<true, true> : expand_split_kernel<false, true>)
-                     : (f16 ? expand_split_kernel<true, false> : expand_split_kernel<false, false>);
+    auto kern = f16 ? expand_split_kernel<true> : expand_split_kernel<false>;
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int dev = 0, sms = 148, per = 0;
     SCP3_CUDA(cudaGetDevice(&dev));
@@ -1154,30 +916,6 @@ int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, in
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }
-
-int launch_contract(const uint16_t* x, int64_t nkb, const WorkItem* items, int nitems, const int* neg, int nflush,
-                    int nsplit, int products, bool f16, double* partial, int* err_flag, cudaStream_t s, int max_ctas)
-{
-    if (nitems <= 0 || nsplit <= 0) return SCP3GPU_OK;
-    SCP3_CUDA(cudaFuncSetAttribute(contract_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-    const int64_t units = (int64_t)nitems * nsplit;
-    const int grid = (int)(max_ctas > 0 ? std::min<int64_t>(units, max_ctas) : units);
-    contract_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(x, (long long)nkb, items, neg, nflush, nitems, nsplit,
-                                                              products, (int)f16, partial, err_flag);
-    SCP3_CUDA(cudaGetLastError());
-    return SCP3GPU_OK;
-}
-
-int launch_unpack(const double* partial, const int* tile_index, int nt, int nitems_total, int nsplit, int64_t item0,
-                  int nb, double divisor, const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s)
-{
-    const int64_t total = (int64_t)nb * nb;
-    unpack_tc_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(partial, tile_index, nt, nitems_total, nsplit, nb,
-                                                                      divisor, diag, zpe, M, ld, item0);
-    SCP3_CUDA(cudaGetLastError());
-    return SCP3GPU_OK;
-}
-
 
 int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v, int64_t n, cudaStream_t s,
             std::vector<cudaEvent_t>* pev, std::vector<int>* pkind)
@@ -1195,7 +933,7 @@ int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v,
         SCP3_CUDA(cudaMemcpyAsync(p.desc_dev + buf, &d, sizeof(d), cudaMemcpyHostToDevice, s));
         p.desc_host[buf] = d;
     }
-    rc = launch_expand(p.desc_dev + buf, 1, p.nb_pad, nm, slots, p.slots / kBK2, p.x[buf], p.f16, s, true);
+    rc = launch_expand(p.desc_dev + buf, 1, p.nb_pad, nm, slots, p.slots / kBK2, p.x[buf], p.f16, s);
     if (rc) return rc;
     record(pev, pkind, 1, s);
     return SCP3GPU_OK;
@@ -1205,10 +943,9 @@ int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_
 {
     const int nflush = (int)(n / kFlush);
     record(pev, pkind, 2, s);
-    contract_n256_kernel<<<p.grid, kThreads, kSmemBytes2, s>>>(
-        p.x[buf], (long long)(p.slots / kBK2), p.tiles2, p.ntiles, p.nsplit, (int)(p.slots / kBK2),
-        nflush * kKB2PerFlush, p.group_meta[buf], (int)p.f16, p.partial, p.err_flag);
-    SCP3_CUDA(cudaGetLastError());
+    const int rc = launch_contract(p.x[buf], p.slots / kBK2, p.tiles2, p.ntiles, p.nsplit, (int)(p.slots / kBK2),
+                                    nflush * kKB2PerFlush, p.group_meta[buf], p.f16, p.partial, p.err_flag, p.grid, s);
+    if (rc) return rc;
     record(pev, pkind, 2, s);
     return SCP3GPU_OK;
 }
@@ -1227,11 +964,7 @@ int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, doub
     SCP3_CUDA(cudaMemcpyAsync(&err, p.err_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     SCP3_CUDA(cudaStreamSynchronize(s));
     if (err) return fail(SCP3GPU_ERR_TIMEOUT, "tensor-core contraction: a bounded pipeline wait expired");
-    const int64_t total = (int64_t)nb * nb;
-    unpack_n256_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(p.partial, p.tile_index, p.nt, p.ntiles,
-                                                                      p.nsplit, nb, divisor, diag, zpe, M, ld);
-    SCP3_CUDA(cudaGetLastError());
-    return SCP3GPU_OK;
+    return launch_unpack(p.partial, p.tile_index, p.nt, p.ntiles, p.nsplit, nb, divisor, diag, zpe, M, ld, s);
 }
 
 }  // namespace tc

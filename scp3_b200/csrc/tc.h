@@ -1,20 +1,9 @@
-// Split-precision (BF16x3) contraction on the tcgen05 tensor cores.
+// Split-precision (BF16x3 / FP16x3) contraction on the tcgen05 tensor cores.
 #pragma once
 #include "internal.h"
 
 namespace scp3 {
 namespace tc {
-
-// One CTA's share of the contraction: the A and B row bases (128-row panels of
-// the operand, which may hold several clusters' bases one after another), the
-// offset of its cluster's per-block sign-group table, and the offset of its
-// FP64 partial tile (per sample-range split, after split * nitems tiles).
-struct WorkItem {
-    int arow, brow;     // first operand rows of the tile's A and B panels
-    int neg_off;        // index of the cluster's first entry in the sign-group table
-    int pad;
-    long long poff;     // partial offset in doubles (tile index * 128 * 128)
-};
 
 // Per-cluster inputs of the split-operand expansion.
 struct ExpandDesc {
@@ -33,16 +22,15 @@ struct Plan {
     int nsplit = 1;               // sample ranges per pass (each unit (split, tile) owns an FP64 partial)
     int grid = 0;                 // CTAs of the contraction (one per SM at most)
     int64_t chunk = 0;            // samples per pass (multiple of kFlush)
-    int products = 3;             // 3: hi*hi + hi*lo + lo*hi; 4: + lo*lo
     bool f16 = false;             // halves in FP16 (operand scaled by 2^6) instead of BF16
     int64_t slots = 0;            // K slots per pass after sign partition and padding
     // device buffers
     // two pass buffers, so one pass can be prepared while the previous contracts
-    // [row block][k-block][hi, lo][128 x 64] 16-bit sqrt|V| Phi, each box in the swizzled MMA order
+    // [row block][32-slot k-block][hi, lo][128 x 32] 16-bit sqrt|V| Phi, each box in the swizzled MMA order
     uint16_t* x[2] = {nullptr, nullptr};
     int* slot_of[2] = {nullptr, nullptr};    // [slots] K slot -> sample (-1: zero padding)
     int* group_meta[2] = {nullptr, nullptr}; // per 4096-sample block: first negative 16-group
-    int2* tiles2 = nullptr;       // [ntiles] (first A row, first B row) of each 128 x 256 tile
+    int4* tiles2 = nullptr;       // [ntiles] (first A row, first B row, sign-table offset, cluster) of each 128 x 256 tile
     int* tile_index = nullptr;    // [nt*nt] owner of block (ti, tj): 2 * tile + column half
     uint32_t* factors = nullptr;  // [nb] basis functions as products of Hermite-table entries
     ExpandDesc* desc_dev = nullptr;   // [2] expansion descriptors of the two pass buffers
@@ -51,7 +39,7 @@ struct Plan {
     int* err_flag = nullptr;      // bounded-wait failures
 };
 
-constexpr int kTile = 128;        // UMMA M = N = 128
+constexpr int kTile = 128;        // UMMA M; a tile is 128 x 256 (two panels of B)
 constexpr int kFlush = 4096;      // samples per sign-partition block (the FP64 flush is finer, see contract_tc.cu)
 constexpr int kSlotsPerFlush = kFlush + 64;  // sign partition pads each sign group to 16
 
@@ -74,17 +62,24 @@ int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, doub
 // Launchers shared by the single build and the batch (several clusters in one launch).
 int launch_partition(const double* v, int64_t v_stride, int* slot_of, int64_t slot_stride, int* neg, int neg_stride,
                      int nflush, int nclusters, cudaStream_t s);
-// slots: K slots of this pass (k-blocks of 64); nkb: k-blocks per row block in the operand's allocation
-// sw64: 32-slot boxes in the 64-byte swizzle (the single build's 128 x 256 contraction;
-// nkb then counts 32-slot k-blocks); otherwise 64-slot boxes in the 128-byte swizzle.
+// slots: K slots of this pass; nkb: 32-slot k-blocks per row block in the operand's allocation
 int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, int max_nm, int64_t slots, int64_t nkb,
-                  uint16_t* x, bool f16, cudaStream_t s, bool sw64 = false);
-// max_ctas > 0: at most that many CTAs, each looping over work units (persistent); 0: one CTA per unit.
-int launch_contract(const uint16_t* x, int64_t nkb, const WorkItem* items, int nitems, const int* neg, int nflush,
-                    int nsplit, int products, bool f16, double* partial, int* err_flag, cudaStream_t s,
-                    int max_ctas = 0);
-int launch_unpack(const double* partial, const int* tile_index, int nt, int nitems_total, int nsplit, int64_t item0,
-                  int nb, double divisor, const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s);
+                  uint16_t* x, bool f16, cudaStream_t s);
+// 128 x 256 tiling shared by the single build and the batch (contract_tc.cu).
+struct BaseTile {
+    int cluster, ti, s, halves;   // row panel, first column panel (even), owned halves (bit 0: s, bit 1: s + 1)
+    int row0, neg_off;            // the cluster's first operand row and sign-group table offset
+};
+void add_cluster_tiles(std::vector<BaseTile>& base, int cluster, int nt, int nt_need, int row0, int neg_off);
+void finish_tiling(const std::vector<BaseTile>& base, const std::vector<int>& cluster_nt, int sms,
+                   std::vector<int4>& tiles, std::vector<std::vector<int>>& owner, int& nsplit);
+// grid CTAs loop over units (split, tile); nkb_* count 32-slot k-blocks
+int launch_contract(const uint16_t* x, int64_t nkb_alloc, const int4* tiles, int ntiles, int nsplit, int nkb_full,
+                    int nkb_pass, const int* neg, bool f16, double* partial, int* err_flag, int grid, cudaStream_t s);
+// dense column-major nb x nb of one cluster (its block-owner table) from the unit partials
+int launch_unpack(const double* partial, const int* owner, int nt, int ntiles, int nsplit, int nb, double divisor,
+                  const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s);
+constexpr int kKBlock2 = 32;      // K slots per k-block of the 128 x 256 contraction's operand
 
 }  // namespace tc
 }  // namespace scp3

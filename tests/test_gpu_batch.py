@@ -3,10 +3,10 @@
 Clusters of uneven size and basis built in one batch give, cluster by
 cluster, the matrix that a single split-form build of the same config gives:
 both run the same per-sample, partition and expansion code on the same BF16 (or
-FP16) operand values; the batch contracts 128 x 128 tiles with separate FP32
-accumulators for hi*hi and the cross terms, the single build 128 x 256 tiles
-with one FP32 accumulator, so they agree to the FP32 accumulation error
-(1e-5 of max|M|).  Graph replay equals direct launches bit for bit, several
+FP16) operand values; both contract 128 x 256 tiles, but the batch splits
+its passes by the tiling of all clusters and a single build by its own, so the
+FP32 runs end at different samples and they agree to the FP32 accumulation
+error (1e-5 of max|M|).  Graph replay equals direct launches bit for bit, several
 accumulate calls equal one call over the same points, and the batch stays
 within the split form's tolerance of the reference's golden matrices."""
 import numpy as np
@@ -92,8 +92,8 @@ def test_batch_autotuned_shape_is_valid(scp3):
     cl = _qt_clusters()
     b = scp3.Batch(cl, precision="bf16x3", chunk=16384)
     nsplit, ctas, chunk, ms = b.shape()
-    assert chunk == 16384 and nsplit in (1, 2, 4) and ms > 0
-    assert ctas >= 0
+    assert chunk == 16384 and 1 <= nsplit <= 16 and ms > 0
+    assert ctas >= 1
     # tuning trials leave no trace in the sums
     b.accumulate(7, 4096)
     ref = scp3.Batch(cl, precision="bf16x3", chunk=16384, autotune=False)
