@@ -34,9 +34,9 @@ WORKLOAD = "hexamer prism qTIP4P/f, 48 modes, doubles basis Nb=1225, 2^20 scramb
 METRIC = "Sobol samples/s (hexamer H-build) at <=0.1 cm^-1 on 10 lowest levels vs FP64"
 FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (vector and tensor) nominal; no measured FP64 peak on this pool
 # DRAM bytes (read + write) of one BF16x3 contraction launch of 2^17 samples on the hexamer doubles
-# basis, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum = 859.5 + 51.6 MB); the
+# basis, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum = 959.4 + 230.0 MB); the
 # traffic grows with the samples per launch
-CONTRACT_DRAM_BYTES_PER_SAMPLE = (859.509504e6 + 51.570432e6) / 131072
+CONTRACT_DRAM_BYTES_PER_SAMPLE = (959.430912e6 + 230.024448e6) / 131072
 
 
 def load_peaks():
