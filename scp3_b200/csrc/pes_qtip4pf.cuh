@@ -59,6 +59,37 @@ __device__ __forceinline__ T pair(uint32_t task, const T* crd, const T* ms)
     }
 }
 
+// Energies of ng <= 4 geometries crd + j * stride (shared memory, T) at once,
+// ms a [4][3nw] shared scratch: lane l works for geometry l % 4 only (M sites and
+// monomers as items (water, geometry), pair terms as items (task, geometry)), so
+// a warp keeps all lanes busy on the per-water terms and the pair tasks of one
+// type run together; lane l returns the sum of geometry l % 4.
+template <typename T>
+__device__ double energy_warp4(const T* crd, int stride, T* ms, int nw, int ng, const uint32_t* __restrict__ tasks,
+                               int ntasks, int lane)
+{
+    const int j = lane & 3;
+    const bool on = j < ng;
+    const T* cj = crd + j * stride;
+    T* mj = ms + j * 3 * nw;
+    if (on)
+        for (int i = lane >> 2; i < nw; i += 8) {
+            const T* w = cj + 9 * i;
+#pragma unroll
+            for (int k = 0; k < 3; k++) mj[3 * i + k] = T(kGammaM) * w[k] + T(kGamma1) * (w[3 + k] + w[6 + k]);
+        }
+    __syncwarp();
+    double part = 0;    // terms in T, their sums in FP64
+    if (on) {
+        for (int i = lane >> 2; i < nw; i += 8) part += (double)monomer(cj + 9 * i);
+        for (int t = lane >> 2; t < ntasks; t += 8) part += (double)pair(__ldg(tasks + t), cj, mj);
+    }
+    part += __shfl_xor_sync(0xffffffffu, part, 4);
+    part += __shfl_xor_sync(0xffffffffu, part, 8);
+    part += __shfl_xor_sync(0xffffffffu, part, 16);
+    return part;
+}
+
 // Energy of the geometry crd[9nw] (shared memory, T), all lanes return the sum.
 // ms is a 3nw shared scratch for the M sites.
 template <typename T>

@@ -31,7 +31,7 @@ template <typename T>
 struct WarpSlot {
     T* q;           // [group][qs] normal coordinates (the form's precision)
     T* crd;         // [group][9nw] geometries
-    T* ms;          // 3nw
+    T* ms;          // [group][3nw] M sites
     T* ttm;         // TTM3-F scratch
     double* g;      // 9nw gradient (gradient path)
     double* gm;     // 3nw forces on the M sites
@@ -41,7 +41,7 @@ struct WarpSlot {
 template <typename T>
 __host__ __device__ inline size_t slot_bytes(int pes, int nm0, int nw, bool grad = false, int group = 1)
 {
-    size_t b = sizeof(T) * ((size_t)group * ((nm0 + 1) & ~1) + (size_t)(9 * nw * group + 3 * nw));
+    size_t b = sizeof(T) * ((size_t)group * ((nm0 + 1) & ~1) + (size_t)(12 * nw * group));
     if (pes == SCP3GPU_PES_TTM3F) b += sizeof(T) * ttm::scratch_elems(nw, grad);
     b = (b + 7) & ~(size_t)7;
     if (grad) b += sizeof(double) * (size_t)(12 * nw);
@@ -56,8 +56,8 @@ __device__ inline WarpSlot<T> warp_slot(char* base, int pes, int nm0, int nw, bo
     s.q = reinterpret_cast<T*>(base);
     s.crd = s.q + (size_t)group * s.qs;
     s.ms = s.crd + 9 * nw * group;
-    s.ttm = s.ms + 3 * nw;
-    size_t off = sizeof(T) * ((size_t)group * s.qs + (size_t)(9 * nw * group + 3 * nw));
+    s.ttm = s.ms + 3 * nw * group;
+    size_t off = sizeof(T) * ((size_t)group * s.qs + (size_t)(12 * nw * group));
     if (pes == SCP3GPU_PES_TTM3F) off += sizeof(T) * ttm::scratch_elems(nw, grad);
     off = (off + 7) & ~(size_t)7;
     s.g = grad ? reinterpret_cast<double*>(base + off) : nullptr;
@@ -255,10 +255,16 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
             }
         }
         __syncwarp();
+        // qTIP4P/f energies of the whole group in one warp pass
+        double e4 = 0.0;
+        if constexpr (PES == SCP3GPU_PES_QTIP4PF) {
+            if (!a.skip_pes && !grad) e4 = qt::energy_warp4<T>(w.crd, N3, w.ms, nw, gn, a.tasks, a.ntasks, lane);
+        }
         for (int j = 0; j < gn; j++) {
             const int64_t s = s0 + j;
             const T* q = w.q + j * w.qs;
             const T* crd = w.crd + j * N3;
+            const double e4j = __shfl_sync(0xffffffffu, e4, j);
             if (s >= a.nvalid) {
                 if (lane == 0) a.v[s] = 0.0;
                 for (int m = lane; m < a.nm; m += 32) {
@@ -297,7 +303,8 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
                 }
             }
             if (!a.skip_pes && !grad) {
-                const double e = potential<PES, T>(crd, w, nw, a.tasks, a.ntasks, lane, &iters);
+                const double e = PES == SCP3GPU_PES_QTIP4PF ? e4j
+                                                             : potential<PES, T>(crd, w, nw, a.tasks, a.ntasks, lane, &iters);
                 double h = 0.0;
                 for (int d = lane; d < nm0; d += 32) h += (double)q[d] * (__ldg(a.omega + d) * (double)q[d]);
                 h = warp_sum(h);
