@@ -461,6 +461,9 @@ int scp3gpu_batch_create(const scp3gpu_config* cfgs, int ncl, int64_t chunk, int
             (rc = dalloc(&b->slot_of[i], (size_t)b->slots * ncl)) || (rc = dalloc(&b->neg[i], (size_t)b->nflush * ncl)) ||
             (rc = dalloc(&b->x[i], (size_t)2 * b->rows * b->slots)))
             return bail(rc);
+        // each cluster's padding rows are never written by the expansion: zero once
+        if (cudaMemset(b->x[i], 0, sizeof(uint16_t) * 2 * (size_t)b->rows * b->slots) != cudaSuccess)
+            return bail(fail(SCP3GPU_ERR_CUDA, "batch: operand zeroing failed"));
         std::vector<tc::ExpandDesc> d(ncl);
         for (int c = 0; c < ncl; c++) {
             const Cluster& k = b->cl[c];

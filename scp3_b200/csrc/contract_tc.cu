@@ -681,17 +681,19 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandD
             const float4* tab4 = reinterpret_cast<const float4*>(tab);
             const float4 w0 = reinterpret_cast<const float4*>(sv)[g8];
             const float4 w1 = reinterpret_cast<const float4*>(sv)[g8 + 8];
-            for (int r = cur.r0 + rl; r < cur.r1; r += 4 * kStep) {
+            // rows past nb stay as the operand's allocation zeroed them
+            const int rend = min(cur.r1, nb);
+            for (int r = cur.r0 + rl; r < rend; r += 4 * kStep) {
                 uint32_t f[4];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     const int rr = r + u * kStep;
-                    f[u] = (rr < nb && rr < cur.r1) ? __ldg(factors + rr) : kNone;
+                    f[u] = rr < rend ? __ldg(factors + rr) : kNone;
                 }
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     const int rr = r + u * kStep;
-                    if (rr >= cur.r1) break;
+                    if (rr >= rend) break;
                     uint4 hi = make_uint4(0, 0, 0, 0), lo = hi;
                     if (f[u] != kNone) {
                         // factor 0 is the constant 1: not read (most rows have one or two)
@@ -849,6 +851,8 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
     p.grid = (int)std::min<long long>((long long)p.ntiles * p.nsplit, sms);
     for (int b = 0; b < 2; b++) {
         SCP3_CUDA(cudaMalloc(&p.x[b], sizeof(uint16_t) * 2 * (size_t)p.nb_pad * p.slots));
+        // padding rows (nb..nb_pad) are never written by the expansion: zero once
+        SCP3_CUDA(cudaMemset(p.x[b], 0, sizeof(uint16_t) * 2 * (size_t)p.nb_pad * p.slots));
         SCP3_CUDA(cudaMalloc(&p.slot_of[b], sizeof(int) * (size_t)p.slots));
         SCP3_CUDA(cudaMalloc(&p.group_meta[b], sizeof(int) * nflush));
     }
