@@ -115,7 +115,11 @@ template <int PES, typename T>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_batch_kernel(const SampleArgs* __restrict__ args)
 {
     extern __shared__ __align__(16) char smem[];
-    const SampleArgs a = args[blockIdx.y];
+    // the cluster's arguments in shared memory, read where used (a register copy
+    // of the whole block costs occupancy)
+    __shared__ SampleArgs a;
+    if (threadIdx.x == 0) a = args[blockIdx.y];
+    __syncthreads();
     samples_body<PES, T>(a, smem);
 }
 
