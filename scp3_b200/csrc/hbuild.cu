@@ -40,7 +40,7 @@ struct scp3gpu_hbuild {
     scp3gpu_config cfg{};
     std::vector<double> omega_sel;
     double zpe_inactive = 0.0;
-    int dev = 0;
+    int dev = 0, sms = 148;
     cudaStream_t stream = nullptr, copy_stream = nullptr, prep_stream = nullptr;
     cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
     cudaEvent_t prepared[2] = {nullptr, nullptr}, contracted[2] = {nullptr, nullptr};
@@ -136,8 +136,9 @@ namespace {
 
 // One pass.  Plain form: everything on the handle's stream.  Split form: the
 // per-sample kernel, sign partition and expansion run on the prepare stream into
-// pass buffer (pass & 1) while the previous pass contracts on the main stream;
-// events order buffer reuse.  `copied` (may be null): event the normals copy of
+// pass buffer (pass & 1), alongside the previous pass's contraction on the main
+// stream when that contraction leaves SMs free (otherwise after it); events
+// order buffer reuse.  `copied` (may be null): event the normals copy of
 // this pass completes; the pass records `consumed` once it has read them.
 int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double* normals_dev,
                  cudaEvent_t copied = nullptr, cudaEvent_t consumed = nullptr)
@@ -170,6 +171,10 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     if (h->split_form) {
         cudaStream_t ps = h->prep_stream;
         SCP3_CUDA(cudaStreamWaitEvent(ps, h->contracted[b], 0));   // buffer b free again
+        // A contraction with a CTA on every SM leaves no room for the preparation
+        // kernels (they would only delay its CTAs): prepare after it.  Smaller
+        // contractions share the GPU with the next pass's preparation.
+        if (h->tcp.grid >= h->sms) SCP3_CUDA(cudaStreamWaitEvent(ps, h->contracted[b ^ 1], 0));
         if (copied) SCP3_CUDA(cudaStreamWaitEvent(ps, copied, 0));
         {
             Timed t(h, 0, ps);
@@ -484,6 +489,7 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     h->zpe_inactive = 0.5 * (sum_all - sum_sel);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    h->sms = sms;
 
     auto bail = [&](int code) {
         scp3gpu_hbuild_destroy(h);
