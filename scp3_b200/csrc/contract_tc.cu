@@ -163,7 +163,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
 // every needed upper 128 x 128 block is owned by one tile (the tiling and which
 // half of a tile owns which block are the host's; a tile may own one half only).  Work unit u = split * ntiles + tile takes the
 // tile over k-blocks [split * nkb_full / nsplit, (split + 1) * nkb_full /
-// nsplit) of the pass; CTA b runs units b, b + gridDim.x, ... .  Units of one
+// nsplit) of the pass; a launch covers units [u_begin, u_end), CTA b running
+// u_begin + b, u_begin + b + gridDim.x, ... .  Units of one
 // wave share k-ranges, so L2 serves the panels they have in common.
 //
 // Accumulation.  One FP32 TMEM accumulator per tile takes all three products
@@ -197,7 +198,8 @@ __device__ __forceinline__ uint64_t smem_desc64(const void* p)
 
 __global__ void __launch_bounds__(kThreads, 1)
     contract_n256_kernel(const uint16_t* __restrict__ xop, long long nkb_alloc, const int4* __restrict__ tiles,
-                         int ntiles, int nsplit, int nkb_full, int nkb_pass, const int* __restrict__ neg_group,
+                         int ntiles, int nsplit, int nkb_full, int nkb_pass, int u_begin, int u_end,
+                         const int* __restrict__ neg_group,
                          int f16, double* __restrict__ partial, int* __restrict__ err_flag)
 {
     extern __shared__ uint8_t smem_raw[];
@@ -212,7 +214,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nunits = ntiles * nsplit;
     // k-blocks [lo, hi) of unit u in this pass
     auto krange = [&](int u, int& lo, int& hi) {
         const int split = u / ntiles;
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             int issued[kStages2] = {0, 0, 0, 0};
             uint32_t issued_phase[kStages2] = {0, 0, 0, 0};
             bool ok = true;
-            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+            for (int u = u_begin + blockIdx.x; u < u_end && ok; u += gridDim.x) {
                 int lo, hi;
                 krange(u, lo, hi);
                 const int4 ti = tiles[u % ntiles];
@@ -293,7 +294,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             int stage = 0, use = 0;
             uint32_t phase = 0;
             bool ok = true;
-            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+            for (int u = u_begin + blockIdx.x; u < u_end && ok; u += gridDim.x) {
                 int lo, hi;
                 krange(u, lo, hi);
                 const int neg_off = tiles[u % ntiles].z;
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int j = 0; j < kTile; j++) l2[j] = 0.f;
         int use = 0;
         bool ok = true;
-        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        for (int u = u_begin + blockIdx.x; u < u_end && ok; u += gridDim.x) {
             int lo, hi;
             krange(u, lo, hi);
             const int nruns = (hi - lo + kDrain2 - 1) / kDrain2;
@@ -805,12 +806,15 @@ void finish_tiling(const std::vector<BaseTile>& base, const std::vector<int>& cl
 }
 
 int launch_contract(const uint16_t* x, int64_t nkb_alloc, const int4* tiles, int ntiles, int nsplit, int nkb_full,
-                     int nkb_pass, const int* neg, bool f16, double* partial, int* err_flag, int grid, cudaStream_t s)
+                    int nkb_pass, const int* neg, bool f16, double* partial, int* err_flag, int grid, cudaStream_t s,
+                    int u_begin, int u_end)
 {
-    if (ntiles <= 0 || nsplit <= 0 || grid <= 0) return SCP3GPU_OK;
+    if (u_end < 0) u_end = ntiles * nsplit;
+    if (ntiles <= 0 || nsplit <= 0 || grid <= 0 || u_end <= u_begin) return SCP3GPU_OK;
     SCP3_CUDA(cudaFuncSetAttribute(contract_n256_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes2));
     contract_n256_kernel<<<grid, kThreads, kSmemBytes2, s>>>(x, (long long)nkb_alloc, tiles, ntiles, nsplit, nkb_full,
-                                                             nkb_pass, neg, (int)f16, partial, err_flag);
+                                                             nkb_pass, u_begin, u_end, neg, (int)f16, partial,
+                                                             err_flag);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }
@@ -943,14 +947,25 @@ int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v,
     return SCP3GPU_OK;
 }
 
-int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind)
+int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind,
+             cudaEvent_t head_done)
 {
     const int nflush = (int)(n / kFlush);
-    record(pev, pkind, 2, s);
-    const int rc = launch_contract(p.x[buf], p.slots / kBK2, p.tiles2, p.ntiles, p.nsplit, (int)(p.slots / kBK2),
-                                    nflush * kKB2PerFlush, p.group_meta[buf], p.f16, p.partial, p.err_flag, p.grid, s);
-    if (rc) return rc;
-    record(pev, pkind, 2, s);
+    const int units = p.ntiles * p.nsplit;
+    // whole waves first, then the partial last wave as its own launch, so that
+    // work queued behind head_done can use the SMs that last wave leaves idle
+    const int head = units > p.grid && units % p.grid ? units / p.grid * p.grid : units;
+    for (int part = 0; part < 2; part++) {
+        const int u0 = part ? head : 0, u1 = part ? units : head;
+        if (u1 <= u0) continue;
+        record(pev, pkind, 2, s);
+        const int rc = launch_contract(p.x[buf], p.slots / kBK2, p.tiles2, p.ntiles, p.nsplit, (int)(p.slots / kBK2),
+                                       nflush * kKB2PerFlush, p.group_meta[buf], p.f16, p.partial, p.err_flag,
+                                       std::min(p.grid, u1 - u0), s, u0, u1);
+        if (rc) return rc;
+        record(pev, pkind, 2, s);
+        if (part == 0 && head_done) SCP3_CUDA(cudaEventRecord(head_done, s));
+    }
     return SCP3GPU_OK;
 }
 

@@ -44,6 +44,7 @@ struct scp3gpu_hbuild {
     cudaStream_t stream = nullptr, copy_stream = nullptr, prep_stream = nullptr;
     cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
     cudaEvent_t prepared[2] = {nullptr, nullptr}, contracted[2] = {nullptr, nullptr};
+    cudaEvent_t head_done[2] = {nullptr, nullptr};   // a pass's whole waves of contraction units done
     int64_t pass = 0;                 // split form: passes launched (buffer = pass & 1)
     int nb = 0, nb_pad = 0, ntasks = 0, nsplit = 1;
     int64_t chunk = 0;
@@ -172,9 +173,10 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
         cudaStream_t ps = h->prep_stream;
         SCP3_CUDA(cudaStreamWaitEvent(ps, h->contracted[b], 0));   // buffer b free again
         // A contraction with a CTA on every SM leaves no room for the preparation
-        // kernels (they would only delay its CTAs): prepare after it.  Smaller
+        // kernels (they would only delay its CTAs): prepare once its whole waves
+        // are done, on the SMs its last, partial wave leaves idle.  Smaller
         // contractions share the GPU with the next pass's preparation.
-        if (h->tcp.grid >= h->sms) SCP3_CUDA(cudaStreamWaitEvent(ps, h->contracted[b ^ 1], 0));
+        if (h->tcp.grid >= h->sms) SCP3_CUDA(cudaStreamWaitEvent(ps, h->head_done[b ^ 1], 0));
         if (copied) SCP3_CUDA(cudaStreamWaitEvent(ps, copied, 0));
         {
             Timed t(h, 0, ps);
@@ -197,7 +199,8 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
         if (rc) return rc;
         SCP3_CUDA(cudaEventRecord(h->prepared[b], ps));
         SCP3_CUDA(cudaStreamWaitEvent(h->stream, h->prepared[b], 0));
-        rc = tc::contract(h->tcp, b, a.n, h->stream, h->prof ? &h->pev : nullptr, h->prof ? &h->pkind : nullptr);
+        rc = tc::contract(h->tcp, b, a.n, h->stream, h->prof ? &h->pev : nullptr, h->prof ? &h->pkind : nullptr,
+                          h->head_done[b]);
         if (rc) return rc;
         SCP3_CUDA(cudaEventRecord(h->contracted[b], h->stream));
         h->pass++;
@@ -431,6 +434,7 @@ int scp3gpu_hbuild_destroy(scp3gpu_hbuild* h)
         if (h->consumed[b]) cudaEventDestroy(h->consumed[b]);
         if (h->prepared[b]) cudaEventDestroy(h->prepared[b]);
         if (h->contracted[b]) cudaEventDestroy(h->contracted[b]);
+        if (h->head_done[b]) cudaEventDestroy(h->head_done[b]);
     }
     if (h->prep_stream) cudaStreamDestroy(h->prep_stream);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -503,7 +507,8 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
         if (cudaEventCreateWithFlags(&h->copied[b], cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&h->consumed[b], cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&h->prepared[b], cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&h->contracted[b], cudaEventDisableTiming) != cudaSuccess)
+            cudaEventCreateWithFlags(&h->contracted[b], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->head_done[b], cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(SCP3GPU_ERR_CUDA, "event creation failed"));
 
     std::vector<int64_t> vd;

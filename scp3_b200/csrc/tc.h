@@ -52,8 +52,10 @@ int zero(Plan& p, cudaStream_t s);
 // prepare: sign partition + expansion of n samples (q32, v) into pass buffer buf.
 int prepare(Plan& p, int buf, int nb, int nm, const float* q32, const double* v, int64_t n, cudaStream_t s,
             std::vector<cudaEvent_t>* pev, std::vector<int>* pkind);
-// contract: the tensor-core accumulation of pass buffer buf into the partials.
-int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind);
+// contract: the tensor-core accumulation of pass buffer buf into the partials;
+// head_done (may be null) is recorded once every whole wave of work units is queued.
+int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind,
+             cudaEvent_t head_done = nullptr);
 // both, on one stream, buffer 0
 int accumulate_pass(Plan& p, const uint32_t* desc, int nb, int nm, const float* q32, const double* v, int64_t n,
                     cudaStream_t s, std::vector<cudaEvent_t>* pev, std::vector<int>* pkind);
@@ -74,8 +76,10 @@ void add_cluster_tiles(std::vector<BaseTile>& base, int cluster, int nt, int nt_
 void finish_tiling(const std::vector<BaseTile>& base, const std::vector<int>& cluster_nt, int sms,
                    std::vector<int4>& tiles, std::vector<std::vector<int>>& owner, int& nsplit);
 // grid CTAs loop over units (split, tile); nkb_* count 32-slot k-blocks
+// units [u_begin, u_end) (u_end < 0: all)
 int launch_contract(const uint16_t* x, int64_t nkb_alloc, const int4* tiles, int ntiles, int nsplit, int nkb_full,
-                    int nkb_pass, const int* neg, bool f16, double* partial, int* err_flag, int grid, cudaStream_t s);
+                    int nkb_pass, const int* neg, bool f16, double* partial, int* err_flag, int grid, cudaStream_t s,
+                    int u_begin = 0, int u_end = -1);
 // dense column-major nb x nb of one cluster (its block-owner table) from the unit partials
 int launch_unpack(const double* partial, const int* owner, int nt, int ntiles, int nsplit, int nb, double divisor,
                   const double* diag, double zpe, double* M, int64_t ld, cudaStream_t s);
