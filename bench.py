@@ -623,6 +623,9 @@ def main():
         # back to host; the slowest rank's time is the job's
         normals = torch.from_numpy(scp3_b200.std_normals(nm0, (1 << 41) + rank * SAMPLES, SAMPLES,
                                                           scramble_seed=SCRAMBLE_SEED))
+        if args.precision != "fp64":
+            # the split forms compute q in FP32: their normals go in as FP32, half the bytes
+            normals = normals.float()
         normals = normals.pin_memory().numpy()
         Mh = np.asfortranarray(torch.empty((nb, nb), dtype=torch.float64).pin_memory().numpy().T)
         hb.reset()
@@ -644,8 +647,8 @@ def main():
             e2e_s = float(t.item())
         line["e2e"] = {"value": world * SAMPLES / e2e_s, "unit": "samples/s",
                        "h2d_bytes_per_step": int(normals.nbytes), "d2h_bytes_per_step": int(nb * nb * 8),
-                       "path": "scp3gpu_hbuild_accumulate_normals + scp3gpu_hbuild_read(mode 1), host buffers, "
-                               "every rank; bytes per rank"}
+                       "path": ("scp3gpu_hbuild_accumulate_normals" + ("" if args.precision == "fp64" else "_f32") +
+                                " + scp3gpu_hbuild_read(mode 1), host buffers, every rank; bytes per rank")}
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         normals = scp3_b200.std_normals(nm0, 0, 1 << 17, scramble_seed=SCRAMBLE_SEED)
         line["cpu_baseline"] = cpu_reference(nw, x0, MUa, omega, np.arange(nm0, dtype=np.int32), 48, 0, normals)

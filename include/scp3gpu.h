@@ -141,6 +141,11 @@ int scp3gpu_hbuild_accumulate(scp3gpu_hbuild* h, int64_t index0, int64_t n);
  * in host memory (copied in, overlapped with compute).  Blocks until the host
  * buffer may be reused. */
 int scp3gpu_hbuild_accumulate_normals(scp3gpu_hbuild* h, const double* normals, int64_t n);
+/* As scp3gpu_hbuild_accumulate_normals with the normals in FP32 (half the
+ * host-to-device bytes): the build equals scp3gpu_hbuild_accumulate_normals on
+ * the same values widened to double.  The split forms compute q in FP32, so
+ * for them the FP32 input loses nothing but the normals' own rounding. */
+int scp3gpu_hbuild_accumulate_normals_f32(scp3gpu_hbuild* h, const float* normals, int64_t n);
 
 /* addEpot(q, V, M) of the -G path on caller data (ScaledMatrixElements.cpp:951-971):
  * q is n x nmodes (selected modes, sample-major), V is n; both host buffers. */

@@ -21,8 +21,8 @@ EXPORTS = [
     "scp3gpu_last_error", "scp3gpu_version", "scp3gpu_pes_energy", "scp3gpu_pes_energy_dev", "scp3gpu_pes_energy_grad",
     "scp3gpu_sobol_std_normal", "scp3gpu_basis_size", "scp3gpu_sub_basis_size", "scp3gpu_hbuild_create",
     "scp3gpu_hbuild_destroy", "scp3gpu_hbuild_reset", "scp3gpu_hbuild_basis_size", "scp3gpu_hbuild_stream",
-    "scp3gpu_hbuild_accumulate", "scp3gpu_hbuild_accumulate_normals", "scp3gpu_hbuild_add_epot",
-    "scp3gpu_hbuild_sample_count", "scp3gpu_hbuild_read", "scp3gpu_hbuild_read_dev", "scp3gpu_hbuild_eigvals", "scp3gpu_hbuild_status",
+    "scp3gpu_hbuild_accumulate", "scp3gpu_hbuild_accumulate_normals", "scp3gpu_hbuild_accumulate_normals_f32",
+    "scp3gpu_hbuild_add_epot", "scp3gpu_hbuild_sample_count", "scp3gpu_hbuild_read", "scp3gpu_hbuild_read_dev", "scp3gpu_hbuild_eigvals", "scp3gpu_hbuild_status",
     "scp3gpu_hbuild_profile", "scp3gpu_add_epot_static", "scp3gpu_save_h5", "scp3gpu_save_h5_layout",
     "scp3gpu_load_h5", "scp3gpu_syevr_lowest",
     "scp3gpu_mlp_create", "scp3gpu_mlp_destroy", "scp3gpu_mlp_num_params", "scp3gpu_mlp_get_params",
@@ -91,6 +91,7 @@ def lib():
     L.scp3gpu_hbuild_stream.argtypes = [vp]
     L.scp3gpu_hbuild_accumulate.argtypes = [vp, i64, i64]
     L.scp3gpu_hbuild_accumulate_normals.argtypes = [vp, dp, i64]
+    L.scp3gpu_hbuild_accumulate_normals_f32.argtypes = [vp, ctypes.POINTER(ctypes.c_float), i64]
     L.scp3gpu_hbuild_add_epot.argtypes = [vp, dp, dp, i64]
     L.scp3gpu_hbuild_add_epot_grad.argtypes = [vp, dp, dp, dp, i64]
     L.scp3gpu_hbuild_sample_count.restype = i64

@@ -182,6 +182,14 @@ class HBuild:
         _lib.check(_lib.lib().scp3gpu_hbuild_accumulate(self._h, index0, n))
 
     def accumulate_normals(self, normals):
+        """The -r path: n x nmodes0 standard normals, sample-major.  A float32 array
+        goes in as FP32 (scp3gpu_hbuild_accumulate_normals_f32, half the copy);
+        anything else as FP64."""
+        if isinstance(normals, np.ndarray) and normals.dtype == np.float32:
+            normals = np.ascontiguousarray(normals)
+            _lib.check(_lib.lib().scp3gpu_hbuild_accumulate_normals_f32(
+                self._h, normals.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), normals.shape[0]))
+            return
         normals = np.ascontiguousarray(normals, dtype=np.float64)
         _lib.check(_lib.lib().scp3gpu_hbuild_accumulate_normals(self._h, _p(normals), normals.shape[0]))
 

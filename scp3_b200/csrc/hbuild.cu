@@ -142,7 +142,7 @@ namespace {
 // order buffer reuse.  `copied` (may be null): event the normals copy of
 // this pass completes; the pass records `consumed` once it has read them.
 int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double* normals_dev,
-                 cudaEvent_t copied = nullptr, cudaEvent_t consumed = nullptr)
+                 const float* normals32_dev = nullptr, cudaEvent_t copied = nullptr, cudaEvent_t consumed = nullptr)
 {
     const bool fp32 = h->pes_fp32;
     const int b = (int)(h->pass & 1);
@@ -159,6 +159,7 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     a.tasks = h->tasks;
     a.ntasks = h->ntasks;
     a.normals = normals_dev;
+    a.normals32 = normals32_dev;
     a.index0 = index0;
     a.n = h->split_form ? tc::pass_samples(h->tcp, nvalid) : round_up(nvalid, 16ll * h->nsplit);
     a.nvalid = nvalid;
@@ -265,6 +266,41 @@ int zero_sums(scp3gpu_hbuild* h)
     return SCP3GPU_OK;
 }
 
+
+// The -r path for normals of type T (double, or float for the FP32 entry): the
+// host buffer goes in piece by piece into two device buffers (FP64-sized, so
+// either type fits), each copy on the copy stream overlapped with the previous
+// piece's pass.  The first copy overlaps nothing, so the pieces ramp up: a
+// quarter, a quarter and a half of a chunk, then whole chunks.
+template <typename T>
+int accumulate_host_normals(scp3gpu_hbuild* h, const T* normals, int64_t n, const char* who)
+{
+    if (!h || n < 0 || (n > 0 && !normals)) return fail(SCP3GPU_ERR_ARG, who);
+    DeviceGuard g(h->dev);
+    (void)cudaGetLastError();
+    const int nm0 = h->cfg.nmodes0;
+    int rc = SCP3GPU_OK;
+    for (int b = 0; b < 2 && !h->normals[b]; b++)
+        if ((rc = dalloc(&h->normals[b], (size_t)h->chunk * nm0))) return rc;
+    int k = 0;
+    for (int64_t off = 0, c = 0; off < n; off += c, k++) {
+        const int b = k & 1;
+        const int64_t part = k < 2 ? h->chunk / 4 : k == 2 ? h->chunk / 2 : h->chunk;
+        c = std::min(std::min(h->chunk, (part + 4095) / 4096 * 4096), n - off);
+        T* dst = reinterpret_cast<T*>(h->normals[b]);
+        // the copy into buffer b may start once the pass that last read it is done
+        SCP3_CUDA(cudaStreamWaitEvent(h->copy_stream, h->consumed[b], 0));
+        SCP3_CUDA(cudaMemcpyAsync(dst, normals + off * nm0, sizeof(T) * c * nm0, cudaMemcpyHostToDevice,
+                                  h->copy_stream));
+        SCP3_CUDA(cudaEventRecord(h->copied[b], h->copy_stream));
+        const double* d64 = sizeof(T) == 8 ? reinterpret_cast<const double*>(dst) : nullptr;
+        const float* d32 = sizeof(T) == 4 ? reinterpret_cast<const float*>(dst) : nullptr;
+        if ((rc = launch_chunk(h, 0, c, d64, d32, h->copied[b], h->consumed[b]))) return rc;
+        h->count += c;
+    }
+    SCP3_CUDA(cudaStreamSynchronize(h->copy_stream));
+    return SCP3GPU_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -589,27 +625,12 @@ int scp3gpu_hbuild_accumulate(scp3gpu_hbuild* h, int64_t index0, int64_t n)
 
 int scp3gpu_hbuild_accumulate_normals(scp3gpu_hbuild* h, const double* normals, int64_t n)
 {
-    if (!h || n < 0 || (n > 0 && !normals)) return fail(SCP3GPU_ERR_ARG, "accumulate_normals: bad arguments");
-    DeviceGuard g(h->dev);
-    (void)cudaGetLastError();
-    const int nm0 = h->cfg.nmodes0;
-    int rc = SCP3GPU_OK;
-    for (int b = 0; b < 2 && !h->normals[b]; b++)
-        if ((rc = dalloc(&h->normals[b], (size_t)h->chunk * nm0))) return rc;
-    int k = 0;
-    for (int64_t off = 0; off < n; off += h->chunk, k++) {
-        const int b = k & 1;
-        const int64_t c = std::min(h->chunk, n - off);
-        // the copy into buffer b may start once the pass that last read it is done
-        SCP3_CUDA(cudaStreamWaitEvent(h->copy_stream, h->consumed[b], 0));
-        SCP3_CUDA(cudaMemcpyAsync(h->normals[b], normals + off * nm0, sizeof(double) * c * nm0,
-                                  cudaMemcpyHostToDevice, h->copy_stream));
-        SCP3_CUDA(cudaEventRecord(h->copied[b], h->copy_stream));
-        if ((rc = launch_chunk(h, 0, c, h->normals[b], h->copied[b], h->consumed[b]))) return rc;
-        h->count += c;
-    }
-    SCP3_CUDA(cudaStreamSynchronize(h->copy_stream));
-    return SCP3GPU_OK;
+    return accumulate_host_normals(h, normals, n, "accumulate_normals: bad arguments");
+}
+
+int scp3gpu_hbuild_accumulate_normals_f32(scp3gpu_hbuild* h, const float* normals, int64_t n)
+{
+    return accumulate_host_normals(h, normals, n, "accumulate_normals_f32: bad arguments");
 }
 
 int scp3gpu_hbuild_add_epot(scp3gpu_hbuild* h, const double* q, const double* V, int64_t n)

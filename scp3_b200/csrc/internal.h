@@ -113,6 +113,7 @@ struct SampleArgs {
     const uint32_t* tasks;        // pair tasks
     int ntasks;
     const double* normals;        // [n x nm0] sample-major, or nullptr to draw Sobol points
+    const float* normals32;       // the same in FP32 (read when normals is nullptr), or nullptr
     int64_t index0;               // first Sobol index
     int64_t n;                    // samples this launch
     int64_t nvalid;               // samples beyond this are padding (q = 0, V = 0)

@@ -159,7 +159,7 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
     constexpr int kDimsPerLane = 4;           // dimensions up to 128 keep their state in registers
     uint64_t st[kDimsPerLane];
     const int64_t s_first = a.n * gw / nwarps, s_end = a.n * (gw + 1) / nwarps;
-    const bool sobol = a.normals == nullptr;
+    const bool sobol = a.normals == nullptr && a.normals32 == nullptr;
     for (int64_t s0 = s_first; s0 < s_end; s0 += kGroup) {
         const int gn = (int)(s_end - s0 < kGroup ? s_end - s0 : kGroup);
         // 1. standard normals -> q   (SCP3.cpp:196-201)
@@ -177,7 +177,7 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
                 if (d >= nm0) break;
                 double y;
                 if (!sobol) {
-                    y = a.normals[s * nm0 + d];
+                    y = a.normals ? a.normals[s * nm0 + d] : (double)a.normals32[s * nm0 + d];
                 } else {
                     if (s == s_first) st[jd] = sobol_state(a.vdir, nm0, d, idx);
                     else st[jd] ^= (uint64_t)__ldg(a.vdir + (size_t)(__ffsll((long long)idx) - 1) * nm0 + d);
@@ -193,7 +193,7 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
             for (int d = lane + 32 * kDimsPerLane; d < nm0; d += 32) {   // beyond 128 dimensions
                 double y = sobol ? bsm(sobol_uniform((a.shift ? __ldg(a.shift + d) : 0ull) ^
                                                      sobol_state(a.vdir, nm0, d, idx)))
-                                 : a.normals[s * nm0 + d];
+                                 : a.normals ? a.normals[s * nm0 + d] : (double)a.normals32[s * nm0 + d];
                 q[d] = (T)(y / 1.4142135623730951);
             }
         }

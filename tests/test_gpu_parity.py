@@ -114,6 +114,26 @@ def test_hbuild_normals_path_and_chunking(scp3, oracle_mod, name):
     assert np.all(np.abs(M2 - ref) <= 1e-12 * A + 1e-300)
 
 
+
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_hbuild_normals_f32_entry(scp3, oracle_mod, precision):
+    """scp3gpu_hbuild_accumulate_normals_f32 equals the FP64 entry on the same
+    values widened to double, bit for bit, over several chunks."""
+    c = load_hbuild_case("hexamer_qtip4pf")
+    normals, q, v, A = _scale(oracle_mod, c)
+    n32 = np.ascontiguousarray(normals, dtype=np.float32)
+    hb = _build(scp3, c, precision=precision, chunk=1 << 12)
+    hb.accumulate_normals(n32)
+    M32 = hb.read(0)
+    hb2 = _build(scp3, c, precision=precision, chunk=1 << 12)
+    hb2.accumulate_normals(n32.astype(np.float64))
+    M64 = hb2.read(0)
+    assert np.array_equal(M32, M64)
+    assert hb.sample_count() == normals.shape[0]
+    assert hb.status() == (0, 0, 0)
+    hb.close(), hb2.close()
+
+
 def test_add_epot_matches_oracle(scp3, oracle_mod):
     rng = np.random.default_rng(3)
     nm, n2, n3 = 9, 7, 5
