@@ -54,23 +54,35 @@ __device__ __forceinline__ double bsm(double u)
     return (y < 0) ? -t : t;
 }
 
-// The same inverse CDF in FP32 for the FP32 form, from the 62-bit Sobol state x
-// (u = x 2^-62, one rounding to FP32): the upper tail takes 1 - u = (2^62 - x)
-// 2^-62 from the integer state instead of subtracting rounded floats.  The
-// central branch's rational function divides with __fdividef (the denominator
-// lies in [0.11, 1]; within 2 ulp).
-__device__ __forceinline__ float bsm_f32(uint64_t x)
+// The same inverse CDF in FP32 for the FP32 form, split at its branch so that
+// a warp can run the central branch over all its items and the rarer tail
+// branch (|u - 0.5| >= 0.42, 16 % of the points) over a compacted list of them.
+// From the 62-bit Sobol state x (u = x 2^-62):
+// * bsm_centred_f32: y = u - 0.5 from the top 32 bits of x as a centred signed
+//   integer (truncation below 2^-32, then one rounding to FP32);
+// * bsm_central_f32: the rational function of the central branch, divided with
+//   __fdividef (the denominator lies in [0.11, 1]; within 2 ulp);
+// * bsm_tail_f32: the tail branch, from min(u, 1 - u) formed exactly from the
+//   integer state (the upper tail as (2^62 - x) 2^-62); the two logarithms are
+//   the __logf intrinsic (3 ulp here: both arguments lie outside [0.5, 2]).
+__device__ __forceinline__ float bsm_centred_f32(uint64_t x)
 {
-    const float u = (float)(int64_t)x * 0x1p-62f;
-    const float y = u - 0.5f;
-    if (fabsf(y) < 0.42f) {
-        const float r = y * y;
-        return __fdividef(
-            y * (((-25.44106049637f * r + 41.39119773534f) * r + -18.61500062529f) * r + 2.50662823884f),
-            (((3.13082909833f * r + -21.06224101826f) * r + 23.08336743743f) * r + -8.47351093090f) * r + 1.0f);
-    }
-    const float tail = (y > 0) ? (float)(int64_t)((1ull << 62) - x) * 0x1p-62f : u;
-    const float r = logf(-logf(tail));
+    return (float)(int32_t)((uint32_t)(x >> 30) ^ 0x80000000u) * 0x1p-32f;
+}
+
+__device__ __forceinline__ float bsm_central_f32(float y)
+{
+    const float r = y * y;
+    return __fdividef(
+        y * (((-25.44106049637f * r + 41.39119773534f) * r + -18.61500062529f) * r + 2.50662823884f),
+        (((3.13082909833f * r + -21.06224101826f) * r + 23.08336743743f) * r + -8.47351093090f) * r + 1.0f);
+}
+
+__device__ __forceinline__ float bsm_tail_f32(uint64_t x)
+{
+    const bool upper = x >= (1ull << 61);
+    const float p = (float)(int64_t)(upper ? (1ull << 62) - x : x) * 0x1p-62f;
+    const float r = __logf(-__logf(p));
     const float t = 0.3374754822726147f +
                     r * (0.9761690190917186f +
                          r * (0.1607979714918209f +
@@ -79,7 +91,7 @@ __device__ __forceinline__ float bsm_f32(uint64_t x)
                                         r * (0.0003951896511919f +
                                              r * (0.0000321767881768f + r * (0.0000002888167364f +
                                                                              r * 0.0000003960315187f)))))));
-    return (y < 0) ? -t : t;
+    return upper ? t : -t;
 }
 
 // The 62-bit Sobol state of point `index` of dimension d: XOR of the direction

@@ -35,6 +35,8 @@ struct WarpSlot {
     T* ttm;         // TTM3-F scratch
     double* g;      // 9nw gradient (gradient path)
     double* gm;     // 3nw forces on the M sites
+    uint64_t* xs;   // FP32 form: [group][nm0] Sobol states of the group
+    uint16_t* tl;   // FP32 form: [group * nm0] items that take the inverse CDF's tail branch
     int qs;         // q stride: nm0 rounded up to even (16-byte aligned rows)
 };
 
@@ -45,6 +47,7 @@ __host__ __device__ inline size_t slot_bytes(int pes, int nm0, int nw, bool grad
     if (pes == SCP3GPU_PES_TTM3F) b += sizeof(T) * ttm::scratch_elems(nw, grad);
     b = (b + 7) & ~(size_t)7;
     if (grad) b += sizeof(double) * (size_t)(12 * nw);
+    if (sizeof(T) == 4) b += (size_t)group * nm0 * (sizeof(uint64_t) + sizeof(uint16_t));
     return (b + 15) & ~(size_t)15;
 }
 
@@ -62,6 +65,9 @@ __device__ inline WarpSlot<T> warp_slot(char* base, int pes, int nm0, int nw, bo
     off = (off + 7) & ~(size_t)7;
     s.g = grad ? reinterpret_cast<double*>(base + off) : nullptr;
     s.gm = grad ? s.g + 9 * nw : nullptr;
+    if (grad) off += sizeof(double) * (size_t)(12 * nw);
+    s.xs = sizeof(T) == 4 ? reinterpret_cast<uint64_t*>(base + off) : nullptr;
+    s.tl = sizeof(T) == 4 ? reinterpret_cast<uint16_t*>(base + off + sizeof(uint64_t) * (size_t)group * nm0) : nullptr;
     return s;
 }
 
@@ -163,7 +169,62 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
     for (int64_t s0 = s_first; s0 < s_end; s0 += kGroup) {
         const int gn = (int)(s_end - s0 < kGroup ? s_end - s0 : kGroup);
         // 1. standard normals -> q   (SCP3.cpp:196-201)
-        for (int j = 0; j < gn; j++) {
+        bool done = false;
+        if constexpr (sizeof(T) == 4) {
+            if (sobol) {
+                // FP32 form: (a) the group's Sobol states, lane-owned by dimension,
+                // staged as [sample][dimension] (padding samples get u = 0.5, so
+                // q = 0); (b) the central branch over all gn * nm0 items, the warp's
+                // lanes strided over them, the tail items listed; (c) the tail
+                // branch over the list.
+                for (int j = 0; j < gn; j++) {
+                    const int64_t s = s0 + j;
+                    const uint64_t idx = (uint64_t)(a.index0 + s);
+                    uint64_t* xj = w.xs + j * nm0;
+                    if (s >= a.nvalid) {
+                        for (int d = lane; d < nm0; d += 32) xj[d] = 1ull << 61;
+                        continue;
+                    }
+#pragma unroll
+                    for (int jd = 0; jd < kDimsPerLane; jd++) {
+                        const int d = lane + 32 * jd;
+                        if (d >= nm0) break;
+                        if (s == s_first) st[jd] = sobol_state(a.vdir, nm0, d, idx);
+                        else st[jd] ^= (uint64_t)__ldg(a.vdir + (size_t)(__ffsll((long long)idx) - 1) * nm0 + d);
+                        xj[d] = a.shift ? st[jd] ^ __ldg(a.shift + d) : st[jd];
+                    }
+                    for (int d = lane + 32 * kDimsPerLane; d < nm0; d += 32)
+                        xj[d] = (a.shift ? __ldg(a.shift + d) : 0ull) ^ sobol_state(a.vdir, nm0, d, idx);
+                }
+                __syncwarp();
+                const int items = gn * nm0;
+                const float inv_nm0 = 1.0f / (float)nm0;   // item i is (i / nm0, i % nm0); exact for i < 2^16
+                int ntail = 0;
+                for (int i0 = 0; i0 < items; i0 += 32) {
+                    const int i = i0 + lane;
+                    bool tail = false;
+                    if (i < items) {
+                        const float y = bsm_centred_f32(w.xs[i]);
+                        tail = !(fabsf(y) < 0.42f);
+                        if (!tail) {
+                            const int j = (int)(((float)i + 0.5f) * inv_nm0);
+                            w.q[j * w.qs + (i - j * nm0)] = (T)(bsm_central_f32(y) * 0.70710678f);
+                        }
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, tail);
+                    if (tail) w.tl[ntail + __popc(m & ((1u << lane) - 1u))] = (uint16_t)i;
+                    ntail += __popc(m);
+                }
+                __syncwarp();
+                for (int t = lane; t < ntail; t += 32) {
+                    const int i = w.tl[t];
+                    const int j = (int)(((float)i + 0.5f) * inv_nm0);
+                    w.q[j * w.qs + (i - j * nm0)] = (T)(bsm_tail_f32(w.xs[i]) * 0.70710678f);
+                }
+                done = true;
+            }
+        }
+        for (int j = 0; j < gn && !done; j++) {
             const int64_t s = s0 + j;
             T* q = w.q + j * w.qs;
             if (s >= a.nvalid) {        // padding sample (the range's tail): contributes nothing
@@ -182,10 +243,6 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
                     if (s == s_first) st[jd] = sobol_state(a.vdir, nm0, d, idx);
                     else st[jd] ^= (uint64_t)__ldg(a.vdir + (size_t)(__ffsll((long long)idx) - 1) * nm0 + d);
                     const uint64_t x = a.shift ? st[jd] ^ __ldg(a.shift + d) : st[jd];
-                    if (sizeof(T) == 4) {              // FP32 form: inverse CDF in FP32
-                        q[d] = (T)(bsm_f32(x) * 0.70710678f);
-                        continue;
-                    }
                     y = bsm(sobol_uniform(x));
                 }
                 q[d] = (T)(y / 1.4142135623730951);   // by /= sqrt(2.0)
