@@ -199,21 +199,32 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
                 __syncwarp();
                 const int items = gn * nm0;
                 const float inv_nm0 = 1.0f / (float)nm0;   // item i is (i / nm0, i % nm0); exact for i < 2^16
+                // two items per lane and round (i, i + 32): two independent chains;
+                // every item runs the central formula, the tail items' values are
+                // dropped (their denominator may vanish; nothing reads the quotient)
                 int ntail = 0;
-                for (int i0 = 0; i0 < items; i0 += 32) {
-                    const int i = i0 + lane;
-                    bool tail = false;
-                    if (i < items) {
-                        const float y = bsm_centred_f32(w.xs[i]);
-                        tail = !(fabsf(y) < 0.42f);
-                        if (!tail) {
-                            const int j = (int)(((float)i + 0.5f) * inv_nm0);
-                            w.q[j * w.qs + (i - j * nm0)] = (T)(bsm_central_f32(y) * 0.70710678f);
-                        }
+                const unsigned below = (1u << lane) - 1u;
+                for (int i0 = 0; i0 < items; i0 += 64) {
+                    const int ia = i0 + lane, ib = ia + 32;
+                    const float ya = ia < items ? bsm_centred_f32(w.xs[ia]) : 0.0f;
+                    const float yb = ib < items ? bsm_centred_f32(w.xs[ib]) : 0.0f;
+                    const float va = bsm_central_f32(ya), vb = bsm_central_f32(yb);
+                    const bool ta = ia < items && !(fabsf(ya) < 0.42f);
+                    const bool tb = ib < items && !(fabsf(yb) < 0.42f);
+                    if (ia < items && !ta) {
+                        const int j = (int)(((float)ia + 0.5f) * inv_nm0);
+                        w.q[j * w.qs + (ia - j * nm0)] = (T)(va * 0.70710678f);
                     }
-                    const unsigned m = __ballot_sync(0xffffffffu, tail);
-                    if (tail) w.tl[ntail + __popc(m & ((1u << lane) - 1u))] = (uint16_t)i;
-                    ntail += __popc(m);
+                    if (ib < items && !tb) {
+                        const int j = (int)(((float)ib + 0.5f) * inv_nm0);
+                        w.q[j * w.qs + (ib - j * nm0)] = (T)(vb * 0.70710678f);
+                    }
+                    const unsigned ma = __ballot_sync(0xffffffffu, ta);
+                    if (ta) w.tl[ntail + __popc(ma & below)] = (uint16_t)ia;
+                    ntail += __popc(ma);
+                    const unsigned mb = __ballot_sync(0xffffffffu, tb);
+                    if (tb) w.tl[ntail + __popc(mb & below)] = (uint16_t)ib;
+                    ntail += __popc(mb);
                 }
                 __syncwarp();
                 for (int t = lane; t < ntail; t += 32) {
