@@ -33,10 +33,10 @@ SCRAMBLE_SEED = 0x5C3
 WORKLOAD = "hexamer prism qTIP4P/f, 48 modes, doubles basis Nb=1225, 2^20 scrambled Sobol points per GPU per step"
 METRIC = "Sobol samples/s (hexamer H-build) at <=0.1 cm^-1 on 10 lowest levels vs FP64"
 FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (vector and tensor) nominal; no measured FP64 peak on this pool
-# DRAM bytes (read + write) of one BF16x3 contraction launch of 2^17 samples on the hexamer doubles
-# basis, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum = 959.4 + 230.0 MB); the
-# traffic grows with the samples per launch
-CONTRACT_DRAM_BYTES_PER_SAMPLE = (959.430912e6 + 230.024448e6) / 131072
+# DRAM bytes (read + write) of the BF16x3 contraction on the hexamer doubles basis, from an ncu
+# capture of one 2^18-sample pass (its two launches: dram__bytes_read.sum + dram__bytes_write.sum =
+# 1349.0 + 335.2 MB and 566.8 + 112.8 MB); per launch it grows with the samples the launch covers
+CONTRACT_DRAM_BYTES_PER_SAMPLE = (1349.039872e6 + 335.236864e6 + 566.846464e6 + 112.826624e6) / 262144
 
 
 def load_peaks():
@@ -251,7 +251,7 @@ def run_cv(args):
     q, v = surrogate.sample(hb, 1 << 44, 1 << 18)
     t_sample = time.perf_counter() - t0
     hb.close()
-    net = surrogate.MLP(48, hidden=256, max_batch=1 << 17, seed=11)
+    net = surrogate.MLP(48, hidden=256, max_batch=1 << 18, seed=11)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     loss = net.fit(q, v.astype(np.float32), epochs=args.cv_epochs, batch=4096, lr=2e-3)

@@ -838,7 +838,9 @@ int create(Plan& p, int nb, int nm, int n2_for_factors, int n3_for_factors, int 
     p.nm = nm;
     p.nb_pad = (nb + kN2 - 1) / kN2 * kN2;         // whole 256-row panel pairs
     p.nt = p.nb_pad / kTile;
-    int64_t chunk = chunk_req > 0 ? chunk_req : (int64_t)kFlush * 32;
+    // 2^18 samples per pass by default: each work unit ends with a read-modify-write
+    // of its FP64 partial, so longer passes spread that over more samples
+    int64_t chunk = chunk_req > 0 ? chunk_req : (int64_t)kFlush * 64;
     // the split operand of one pass stays under ~6 GB
     while (chunk > kFlush && (int64_t)p.nb_pad * (chunk / kFlush) * kSlotsPerFlush * 4 > (6ll << 30)) chunk /= 2;
     chunk = chunk / kFlush * kFlush;

@@ -270,8 +270,9 @@ int zero_sums(scp3gpu_hbuild* h)
 // The -r path for normals of type T (double, or float for the FP32 entry): the
 // host buffer goes in piece by piece into two device buffers (FP64-sized, so
 // either type fits), each copy on the copy stream overlapped with the previous
-// piece's pass.  The first copy overlaps nothing, so the pieces ramp up: a
-// quarter, a quarter and a half of a chunk, then whole chunks.
+// piece's pass.  The first copy overlaps nothing, so the pieces ramp up from
+// 2^15 samples, doubling after the second piece, to whole chunks (each copy
+// then takes about as long as the previous piece's pass).
 template <typename T>
 int accumulate_host_normals(scp3gpu_hbuild* h, const T* normals, int64_t n, const char* who)
 {
@@ -285,8 +286,8 @@ int accumulate_host_normals(scp3gpu_hbuild* h, const T* normals, int64_t n, cons
     int k = 0;
     for (int64_t off = 0, c = 0; off < n; off += c, k++) {
         const int b = k & 1;
-        const int64_t part = k < 2 ? h->chunk / 4 : k == 2 ? h->chunk / 2 : h->chunk;
-        c = std::min(std::min(h->chunk, (part + 4095) / 4096 * 4096), n - off);
+        const int64_t part = k < 20 ? (int64_t)1 << (15 + (k > 0 ? k - 1 : 0)) : h->chunk;
+        c = std::min(std::min(h->chunk, part), n - off);
         T* dst = reinterpret_cast<T*>(h->normals[b]);
         // the copy into buffer b may start once the pass that last read it is done
         SCP3_CUDA(cudaStreamWaitEvent(h->copy_stream, h->consumed[b], 0));

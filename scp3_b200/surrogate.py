@@ -49,7 +49,7 @@ SURROGATE_NONE, SURROGATE_REPLACE, SURROGATE_RESIDUAL = 0, 1, 2
 
 
 class MLP:
-    def __init__(self, n_in, hidden=256, max_batch=1 << 17, seed=1, device=0):
+    def __init__(self, n_in, hidden=256, max_batch=1 << 18, seed=1, device=0):
         L = _bind()
         h = ctypes.c_void_p()
         _lib.check(L.scp3gpu_mlp_create(n_in, hidden, max_batch, seed, device, ctypes.byref(h)))

@@ -74,7 +74,7 @@ def test_control_variate_gains_over_plain(sur):
 
     hb = make()
     qtr, vtr = sur.sample(hb, 1 << 30, 1 << 13)
-    net = sur.MLP(12, hidden=256, max_batch=1 << 17, seed=9)
+    net = sur.MLP(12, hidden=256, max_batch=1 << 18, seed=9)
     net.fit(qtr, vtr.astype(np.float32), epochs=60, batch=1024, lr=2e-3)
     ref = make()
     ref.accumulate(0, 1 << 20)
@@ -101,7 +101,7 @@ def test_builds_sharing_a_network_run_concurrently(sur):
         return scp3_b200.HBuild(2, c["x0"], c["MUa"], c["omega"], n2=12, n3=0, precision="bf16x3",
                                 scramble_seed=0x5C3)
 
-    net = sur.MLP(12, hidden=256, max_batch=1 << 17, seed=5)
+    net = sur.MLP(12, hidden=256, max_batch=1 << 18, seed=5)
     net.set_output(0.01, -0.01)
     seq = []
     for mode, i0 in ((sur.SURROGATE_REPLACE, 1 << 40), (sur.SURROGATE_RESIDUAL, 0)):
