@@ -164,7 +164,7 @@ int enqueue(scp3gpu_batch* b, int64_t passes, int64_t last)
         SCP3_CUDA(cudaEventRecord(b->prepared[buf], b->prep));
         SCP3_CUDA(cudaStreamWaitEvent(b->stream, b->prepared[buf], 0));
         rc = tc::launch_contract(b->x[buf], b->slots / tc::kKBlock2, b->tiles, b->ntiles, b->nsplit,
-                                  (int)(b->slots / tc::kKBlock2), (int)(slots / tc::kKBlock2), b->neg[buf], b->f16,
+                                  (int)(slots / tc::kKBlock2), b->neg[buf], b->f16,
                                   b->partial, b->err_flag, b->ctas, b->stream);
         if (rc) return rc;
         SCP3_CUDA(cudaEventRecord(b->contracted[buf], b->stream));
@@ -253,7 +253,7 @@ int autotune(scp3gpu_batch* b)
         for (int rep = 0; rep < 3 && rc == 0; rep++) {
             cudaEventRecord(e0, b->stream);
             rc = tc::launch_contract(b->x[0], b->slots / tc::kKBlock2, b->tiles, b->ntiles, b->nsplit,
-                                      (int)(b->slots / tc::kKBlock2), (int)(b->slots / tc::kKBlock2), b->neg[0], b->f16,
+                                      (int)(b->slots / tc::kKBlock2), b->neg[0], b->f16,
                                       b->partial, b->err_flag, cand[ci], b->stream);
             cudaEventRecord(e1, b->stream);
             if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(SCP3GPU_ERR_CUDA, "batch: autotune sync");

@@ -162,8 +162,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
 // Tiles: (first A row, first B row, offset of the cluster's sign-group table);
 // every needed upper 128 x 128 block is owned by one tile (the tiling and which
 // half of a tile owns which block are the host's; a tile may own one half only).  Work unit u = split * ntiles + tile takes the
-// tile over k-blocks [split * nkb_full / nsplit, (split + 1) * nkb_full /
-// nsplit) of the pass; a launch covers units [u_begin, u_end), CTA b running
+// tile over k-blocks [split * nkb_pass / nsplit, (split + 1) * nkb_pass /
+// nsplit) of the pass (so a shorter pass has shorter units, not fewer); a
+// launch covers units [u_begin, u_end), CTA b running
 // u_begin + b, u_begin + b + gridDim.x, ... .  Units of one
 // wave share k-ranges, so L2 serves the panels they have in common.
 //
@@ -198,7 +199,7 @@ __device__ __forceinline__ uint64_t smem_desc64(const void* p)
 
 __global__ void __launch_bounds__(kThreads, 1)
     contract_n256_kernel(const uint16_t* __restrict__ xop, long long nkb_alloc, const int4* __restrict__ tiles,
-                         int ntiles, int nsplit, int nkb_full, int nkb_pass, int u_begin, int u_end,
+                         int ntiles, int nsplit, int nkb_pass, int u_begin, int u_end,
                          const int* __restrict__ neg_group,
                          int f16, double* __restrict__ partial, int* __restrict__ err_flag)
 {
@@ -217,10 +218,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     // k-blocks [lo, hi) of unit u in this pass
     auto krange = [&](int u, int& lo, int& hi) {
         const int split = u / ntiles;
-        lo = (int)((long long)split * nkb_full / nsplit);
-        hi = (int)((long long)(split + 1) * nkb_full / nsplit);
-        if (hi > nkb_pass) hi = nkb_pass;
-        if (hi < lo) hi = lo;
+        lo = (int)((long long)split * nkb_pass / nsplit);
+        hi = (int)((long long)(split + 1) * nkb_pass / nsplit);
     };
 
     if (threadIdx.x == 0) {
@@ -805,15 +804,15 @@ void finish_tiling(const std::vector<BaseTile>& base, const std::vector<int>& cl
     nsplit = bestM;
 }
 
-int launch_contract(const uint16_t* x, int64_t nkb_alloc, const int4* tiles, int ntiles, int nsplit, int nkb_full,
-                    int nkb_pass, const int* neg, bool f16, double* partial, int* err_flag, int grid, cudaStream_t s,
+int launch_contract(const uint16_t* x, int64_t nkb_alloc, const int4* tiles, int ntiles, int nsplit, int nkb_pass,
+                    const int* neg, bool f16, double* partial, int* err_flag, int grid, cudaStream_t s,
                     int u_begin, int u_end)
 {
     if (u_end < 0) u_end = ntiles * nsplit;
     if (ntiles <= 0 || nsplit <= 0 || grid <= 0 || u_end <= u_begin) return SCP3GPU_OK;
     SCP3_CUDA(cudaFuncSetAttribute(contract_n256_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes2));
-    contract_n256_kernel<<<grid, kThreads, kSmemBytes2, s>>>(x, (long long)nkb_alloc, tiles, ntiles, nsplit, nkb_full,
-                                                             nkb_pass, u_begin, u_end, neg, (int)f16, partial,
+    contract_n256_kernel<<<grid, kThreads, kSmemBytes2, s>>>(x, (long long)nkb_alloc, tiles, ntiles, nsplit, nkb_pass,
+                                                             u_begin, u_end, neg, (int)f16, partial,
                                                              err_flag);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
@@ -961,8 +960,8 @@ int contract(Plan& p, int buf, int64_t n, cudaStream_t s, std::vector<cudaEvent_
         const int u0 = part ? head : 0, u1 = part ? units : head;
         if (u1 <= u0) continue;
         record(pev, pkind, 2, s);
-        const int rc = launch_contract(p.x[buf], p.slots / kBK2, p.tiles2, p.ntiles, p.nsplit, (int)(p.slots / kBK2),
-                                       nflush * kKB2PerFlush, p.group_meta[buf], p.f16, p.partial, p.err_flag,
+        const int rc = launch_contract(p.x[buf], p.slots / kBK2, p.tiles2, p.ntiles, p.nsplit, nflush * kKB2PerFlush,
+                                       p.group_meta[buf], p.f16, p.partial, p.err_flag,
                                        std::min(p.grid, u1 - u0), s, u0, u1);
         if (rc) return rc;
         record(pev, pkind, 2, s);

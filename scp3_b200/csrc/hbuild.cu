@@ -271,8 +271,9 @@ int zero_sums(scp3gpu_hbuild* h)
 // host buffer goes in piece by piece into two device buffers (FP64-sized, so
 // either type fits), each copy on the copy stream overlapped with the previous
 // piece's pass.  The first copy overlaps nothing, so the pieces ramp up from
-// 2^15 samples, doubling after the second piece, to whole chunks (each copy
-// then takes about as long as the previous piece's pass).
+// 2^15 samples, doubling after the second piece, to 2^17 samples (at ~50 GB/s
+// a piece's FP32 normals then copy in about half its pass, and the last pass,
+// which follows its copy, stays short).
 template <typename T>
 int accumulate_host_normals(scp3gpu_hbuild* h, const T* normals, int64_t n, const char* who)
 {
@@ -286,7 +287,7 @@ int accumulate_host_normals(scp3gpu_hbuild* h, const T* normals, int64_t n, cons
     int k = 0;
     for (int64_t off = 0, c = 0; off < n; off += c, k++) {
         const int b = k & 1;
-        const int64_t part = k < 20 ? (int64_t)1 << (15 + (k > 0 ? k - 1 : 0)) : h->chunk;
+        const int64_t part = (int64_t)1 << std::min(17, 15 + (k > 0 ? k - 1 : 0));
         c = std::min(std::min(h->chunk, part), n - off);
         T* dst = reinterpret_cast<T*>(h->normals[b]);
         // the copy into buffer b may start once the pass that last read it is done

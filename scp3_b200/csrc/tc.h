@@ -77,8 +77,8 @@ void finish_tiling(const std::vector<BaseTile>& base, const std::vector<int>& cl
                    std::vector<int4>& tiles, std::vector<std::vector<int>>& owner, int& nsplit);
 // grid CTAs loop over units (split, tile); nkb_* count 32-slot k-blocks
 // units [u_begin, u_end) (u_end < 0: all)
-int launch_contract(const uint16_t* x, int64_t nkb_alloc, const int4* tiles, int ntiles, int nsplit, int nkb_full,
-                    int nkb_pass, const int* neg, bool f16, double* partial, int* err_flag, int grid, cudaStream_t s,
+int launch_contract(const uint16_t* x, int64_t nkb_alloc, const int4* tiles, int ntiles, int nsplit, int nkb_pass,
+                    const int* neg, bool f16, double* partial, int* err_flag, int grid, cudaStream_t s,
                     int u_begin = 0, int u_end = -1);
 // dense column-major nb x nb of one cluster (its block-owner table) from the unit partials
 int launch_unpack(const double* partial, const int* owner, int nt, int ntiles, int nsplit, int nb, double divisor,
