@@ -79,3 +79,36 @@ def test_split_hexamer_doubles_levels(scp3, prec):
     (M32, e32), (M64, e64) = out[prec], out["fp64"]
     assert np.abs(e32 - e64).max() * AUTOCM <= 0.1, (e32 - e64) * AUTOCM
     assert np.linalg.norm(M32 - M64) <= 1e-4 * np.linalg.norm(M64)
+
+
+def test_split_uneven_passes_and_host_normals(scp3):
+    """The same 2^17 hexamer points through the BF16x3 form three ways: one call
+    (one pass, shorter than the 2^18-sample plan), uneven calls (passes of 3, 9
+    and 20 flush blocks of 4096), and the FP32 host-normals entry (its pieces
+    ramp 2^15, 2^15, 2^16).  Every pass cuts its work units' k-block ranges from
+    its own length; a missing or repeated k-block range would move the sums by
+    ~1/14 of a pass, far beyond the FP32 regrouping and the normals' FP32
+    rounding that the three builds differ by."""
+    from scp3_b200 import inputs
+    nw, x0, MUa, omega = inputs.load("prism_qtip4pf", build_if_missing=False)
+    ns = 1 << 17
+
+    def make():
+        return scp3.HBuild(nw, x0, MUa, omega, n2=48, n3=0, precision="bf16x3", scramble_seed=0x5C3)
+
+    hb = make()
+    hb.accumulate(0, ns)
+    M1 = hb.read(0)
+    hb2 = make()
+    for a, b in ((0, 3 * 4096), (3 * 4096, 12 * 4096), (12 * 4096, ns)):
+        hb2.accumulate(a, b - a)
+    M2 = hb2.read(0)
+    hb3 = make()
+    hb3.accumulate_normals(scp3.std_normals(omega.size, 0, ns, scramble_seed=0x5C3).astype(np.float32))
+    M3 = hb3.read(0)
+    for h in (hb, hb2, hb3):
+        assert h.sample_count() == ns and h.status() == (0, 0, 0)
+        h.close()
+    n1 = np.linalg.norm(M1)
+    assert np.linalg.norm(M2 - M1) <= 1e-5 * n1, np.linalg.norm(M2 - M1) / n1
+    assert np.linalg.norm(M3 - M1) <= 1e-4 * n1, np.linalg.norm(M3 - M1) / n1
