@@ -110,8 +110,8 @@ typedef struct scp3gpu_config {
     int precision;          /* SCP3GPU_PREC_*                                          */
     int scramble;           /* SCP3GPU_SOBOL_*                                         */
     uint64_t scramble_seed;
-    int chunk;              /* samples per device pass; multiple of 4096, 0 = auto:     
-                               2^18 for the split forms (halved while one pass's      
+    int chunk;              /* samples per device pass; multiple of 4096, 0 = auto:
+                               2^18 for the split forms (halved while one pass's
                                operand would exceed ~6 GB), 4096 for the FP64 form    */
     int device;             /* CUDA device ordinal                                     */
     int estimator;          /* SCP3GPU_ESTIMATOR_*                                     */
