@@ -111,6 +111,13 @@ def test_argument_errors_before_any_device_work():
     assert L.scp3gpu_pes_energy_grad(1, 9, 1, crd.ctypes.data_as(dp), E.ctypes.data_as(dp),
                                      G.ctypes.data_as(dp)) == _lib.ERR_ARG
     assert "TTM3-F" in L.scp3gpu_last_error().decode()
+    # the -r path's two entries: no handle, negative count, no buffer
+    fp = ctypes.POINTER(ctypes.c_float)
+    n32 = np.zeros(48, dtype=np.float32)
+    assert L.scp3gpu_hbuild_accumulate_normals(None, x0.ctypes.data_as(dp), 1) == _lib.ERR_ARG
+    assert L.scp3gpu_hbuild_accumulate_normals_f32(None, n32.ctypes.data_as(fp), 1) == _lib.ERR_ARG
+    assert L.scp3gpu_hbuild_accumulate_normals_f32(None, None, -1) == _lib.ERR_ARG
+    assert "accumulate_normals_f32" in L.scp3gpu_last_error().decode()
 
 
 def test_scp1_argument_errors_without_device():
