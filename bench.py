@@ -51,7 +51,9 @@ class Clocks:
     """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
 
     def __init__(self, gpu):
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%d.csv" % os.getpid())
+        # the raw samples stay beside the summary (BENCH_CLOCKS_DIR, default bench_out/)
+        out = os.environ.get("BENCH_CLOCKS_DIR", os.path.join(ROOT, "bench_out"))
+        self.path = os.path.join(out, "clocks_%d.csv" % os.getpid())
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"

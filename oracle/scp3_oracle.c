@@ -598,7 +598,7 @@ void or_accumulate(int nm, int n2, int n3, const double* q_sel, const double* v,
 }
 
 /* |bra_i| |V| |bra_j| summed over samples: the scale against which an
- * element's rounding error is judged (near-cancelling elements). */
+ * element's rounding error is measured (near-cancelling elements). */
 void or_accumulate_abs(int nm, int n2, int n3, const double* q_sel, const double* v, int64_t n, double* M)
 {
     size_t nb = or_basis_size(nm, n2, n3);

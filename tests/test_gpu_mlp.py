@@ -60,7 +60,7 @@ def test_control_variate_gains_over_plain(sur):
     """Dimer doubles basis: the surrogate trained on 2^13 exact samples, then
     M_cv with 2^17 surrogate points + 2^12 exact residual points against the plain
     estimator with the same 2^12 exact points; errors of the 10 lowest levels
-    judged against a 2^20-point plain build."""
+    compared with a 2^20-point plain build."""
     import scp3_b200
     c = load_hbuild_case("dimer_qtip4pf")
 

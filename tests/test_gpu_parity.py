@@ -4,7 +4,7 @@ vectors (tests/golden) and the oracle (oracle/scp3_oracle.c), FP64 plain form.
 Tolerances: Sobol integer states and uniforms bit-exact; normals <= 1e-14
 relative (device log vs glibc log); potentials <= 1e-12 relative; matrix
 elements <= 1e-12 of sum_s |Phi_i||V||Phi_j| (the scale a near-cancelling
-element is judged on)."""
+element is measured against)."""
 import os
 
 import numpy as np
