@@ -133,3 +133,16 @@ def test_scp1_argument_errors_without_device():
     assert not h.value
     assert L.scp3gpu_scp1_average(None, None, None, None, 0, 0, 0, None, None, None) == _lib.ERR_ARG
     L.scp3gpu_scp1_destroy(None)
+
+
+def test_inverse_cdf_item_split_is_exact():
+    """The FP32 per-sample kernel (sampling.cu) splits item i of a sample group
+    into (sample, dimension) as j = (int)((i + 0.5f) * (1.0f / nm0)) instead of an
+    integer division; restated here in IEEE float32, it equals i // nm0 for every
+    mode count the library admits (nm0 <= 144: at most 16 waters) and every
+    i < 2^16, a bound far above the 4 * nm0 items of a group."""
+    for nm0 in range(1, 145):
+        inv = np.float32(1.0) / np.float32(nm0)
+        i = np.arange(1 << 16, dtype=np.int64)
+        j = ((i.astype(np.float32) + np.float32(0.5)) * inv).astype(np.int32)
+        assert np.array_equal(j, i // nm0), nm0
