@@ -22,12 +22,22 @@ import subprocess
 import sys
 import time
 
-import numpy as np
+# Thread pools of the reference's CPU build (cpu_baseline and --impl reference):
+# OpenBLAS and OpenMP threads sleep when idle instead of spinning against each
+# other's phase of the block loop.  Set before numpy and torch load their BLAS
+# and OpenMP runtimes, which read these once; the reference's build shares the
+# OpenMP runtime torch loads.
+REF_THREAD_ENV = {"OPENBLAS_THREAD_TIMEOUT": "4", "OMP_WAIT_POLICY": "PASSIVE"}
+for _k, _v in REF_THREAD_ENV.items():
+    os.environ.setdefault(_k, _v)
+
+import numpy as np  # noqa: E402
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SAMPLES = 1 << 20
+TRIPLES_SAMPLES = 1 << 18       # the default line's triples sub-record: two 2^17 chunks, a dump after each
 INPUT = "prism_qtip4pf"
 SCRAMBLE_SEED = 0x5C3
 WORKLOAD = "hexamer prism qTIP4P/f, 48 modes, doubles basis Nb=1225, 2^20 scrambled Sobol points per GPU per step"
@@ -88,16 +98,90 @@ class Clocks:
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons)}
 
 
-def dist_setup(n_gpus):
+def launch_ranks(n, argv, limit_s=1800):
+    """`--gpus N` started without a launcher: run N local ranks of this script
+    under torch.distributed.run (one per GPU, rendezvous on 127.0.0.1) and
+    return their exit code.  `timeout -k 60` bounds the whole job well above the
+    process group's own timeout, so ranks that wait for one another end."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = ["timeout", "-k", "60", str(limit_s), sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node", str(n), "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.abspath(__file__)] + list(argv)
+    return subprocess.call(cmd)
+
+
+def dist_setup(n_gpus, backend="nccl"):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != n_gpus:
+        raise SystemExit("bench.py: --gpus %d but the launcher started %d ranks" % (n_gpus, world))
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=None)
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
+
+
+def exchange(hb, Mdev, stream):
+    """The ranks' one exchange (sample-range sharding): the rank's matrix is
+    written into Mdev on the build's stream, the current stream waits for that
+    write, then Mdev is summed over the ranks in place.  `stream` is None for
+    the host stand-in, whose read is synchronous."""
+    from scp3_b200 import shard
+    hb.read_dev(Mdev.data_ptr(), Mdev.shape[0], 0)
+    if stream is not None:
+        import torch
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        torch.cuda.current_stream().wait_event(ev)
+    shard.reduce_matrix(Mdev)
+
+
+class HostStandIn:
+    """`--standin`: a small numpy build on the host that takes the calls the
+    benchmark step makes of a build (accumulate, read_dev, reset, status,
+    close), so the CPU tests can run the rank launcher, the sample-range split
+    and the exchange without a GPU.  Sample s contributes phi(s) v(s) phi(s)^T
+    with phi and v fixed functions of the Sobol index, so any split of the
+    indices over ranks sums to the same matrix.  Not a Hamiltonian build."""
+
+    def __init__(self, nb=6):
+        self.nb = nb
+        self.M = np.zeros((nb, nb))
+        self.n = 0
+
+    @staticmethod
+    def terms(index0, n, nb):
+        s = (index0 + np.arange(n, dtype=np.float64))[None, :]
+        k = np.arange(1, nb + 1, dtype=np.float64)[:, None]
+        return np.cos(1e-3 * k * s + 0.1 * k), np.sin(7e-4 * s[0]) - 0.25
+
+    def accumulate(self, index0, n):
+        phi, v = self.terms(index0, n, self.nb)
+        self.M += (phi * v) @ phi.T
+        self.n += n
+
+    def read_dev(self, ptr, ld, mode=0):
+        import ctypes
+        out = np.ctypeslib.as_array((ctypes.c_double * (ld * self.nb)).from_address(ptr)).reshape(self.nb, ld)
+        out[:, :self.nb] = self.M      # symmetric: row- and column-major agree
+
+    def reset(self):
+        self.M[:] = 0.0
+        self.n = 0
+
+    def status(self):
+        return 0, 0, 0
+
+    def close(self):
+        pass
 
 
 def cpu_reference(nw, x0, MUa, omega, modes, n2, n3, normals, target_s=12.0, max_samples=None):
@@ -118,10 +202,62 @@ def cpu_reference(nw, x0, MUa, omega, modes, n2, n3, normals, target_s=12.0, max
     return {"value": n / wall, "unit": "samples/s", "cores": os.cpu_count(), "kind": "reference" if fast else "port",
             "sample": "%d of the %d samples (blocks of %d, -r normals path: PES + get_bra + dsyr2k, OpenMP/OpenBLAS on "
                       "all host threads); Sobol skip walk excluded" % (n, SAMPLES, block),
-            "split_s": {"pes": float(t[0]), "bra": float(t[1]), "dsyr2k": float(t[2])}}
+            "split_s": {"pes": float(t[0]), "bra": float(t[1]), "dsyr2k": float(t[2])},
+            "threads": oracle.ref_thread_env()}
 
 
-def run_reference(args, world, rank):
+def run_standin(args, world, rank):
+    """The benchmark's rank logic with HostStandIn as the build (CPU tests):
+    the same sample ranges, warm-up, reset, barrier, exchange and max-over-ranks
+    timing as the GPU step, host-clocked.  --dump-matrix writes rank 0's
+    reduced matrix after the timed steps."""
+    import torch
+    import torch.distributed as dist
+    from scp3_b200 import shard
+    hb = HostStandIn()
+    Mdev = torch.zeros((hb.nb, hb.nb), dtype=torch.float64)
+    base, _ = shard.sample_range(rank, world, 0, SAMPLES, "weak")
+
+    def step(k):
+        hb.accumulate(base + k * SAMPLES, SAMPLES)
+        if world > 1:
+            exchange(hb, Mdev, None)
+
+    for k in range(args.warmup):
+        step(k)
+    hb.reset()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        step(args.warmup + k)
+    total_ms = 1e3 * (time.perf_counter() - t0)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    else:
+        exchange(hb, Mdev, None)
+    if rank == 0:
+        if args.dump_matrix:
+            np.save(args.dump_matrix, Mdev.numpy())
+        print(json.dumps({"metric": "stand-in build rank exchange (host)", "value": world * SAMPLES * args.steps /
+                          (total_ms / 1e3), "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "data": "stand-in",
+                          "config": {"workload": "HostStandIn nb=%d, %d samples per rank per step" % (hb.nb, SAMPLES),
+                                     "parallelism": "dp%d (sample ranges)" % world, "base": base}}))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def bench_config(precision, nb, world):
+    """The `config` of the benchmark line, the same in both arms."""
+    return {"workload": WORKLOAD, "precision": precision, "nb": nb, "samples_per_step": SAMPLES,
+            "l2": "flushed between steps (256 MB write)", "parallelism": "dp%d (sample ranges)" % world}
+
+
+def run_reference(args, rank):
     if rank != 0:
         return
     from scp3_b200 import inputs, std_normals
@@ -142,70 +278,119 @@ def run_reference(args, world, rank):
         if k >= args.warmup:
             times.append(time.perf_counter() - t0)
     v = per_step * len(times) / sum(times)
+    nb = oracle.basis_size(omega.size, 48, 0)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "samples/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD + " (each reference step: a bounded 2^14-sample slice)",
-                       "samples_per_step": per_step},
+            "config": bench_config(args.precision, nb, args.gpus),
+            "reference_step": "a bounded 2^14-sample slice of the workload per step (samples/s is a rate)",
             "cpu_baseline": {"value": v, "unit": "samples/s", "cores": os.cpu_count(),
                              "kind": "reference" if fast else "port",
-                             "sample": "2^14 samples per step of the same workload, -r normals path"},
+                             "sample": "2^14 samples per step of the same workload, -r normals path",
+                             "threads": oracle.ref_thread_env()},
             "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-def run_triples(args):
+def timed_accumulate(hb, index0, n):
+    """Device time (ms) of one accumulate call: CUDA events on the build's stream,
+    which every pass of the call joins before it returns."""
+    import torch
+    st = torch.cuda.ExternalStream(hb.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    hb.accumulate(index0, n)
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def triples_record(total, precision, dump=True, deflate=6):
     """The triples configuration: TTM3-F hexamer prism, N2 = N3 = 48 (20825 basis
-    functions), 2^21 scrambled points in 2^17-sample chunks with an sM_*.h5 dump
-    after each chunk, the 10 lowest levels of the split form against the FP64
-    form on the same points.  One JSON line; not the benchmark's default."""
+    functions), `total` scrambled points in 2^17-sample chunks, after each chunk
+    Mout read back and written as sM_<n>.h5 in the reference's layout (chunked,
+    deflate 6; SCP3.cpp:252-255, DiskIO.cpp:201-227) for the split form; the 10
+    lowest levels (FP64 eigensolve) of the split form against the FP64 form on
+    the same points.  samples_per_s is device-timed over the accumulate calls;
+    the dumps and the eigensolve are timed apart."""
     import tempfile
 
     import torch
     import scp3_b200
     from scp3_b200 import h5, inputs
-    torch.cuda.set_device(0)
     nw, x0, MUa, omega = inputs.load("prism_ttm3f")
-    total, chunk = args.samples, 1 << 17
+    chunk = 1 << 17
     res = {}
     outdir = tempfile.mkdtemp(prefix="scp3_triples_")
     autocm = scp3_b200.constants.autocm
-    for prec in (args.precision, "fp64"):
+    for prec in (precision, "fp64"):
         hb = scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=48, pes="ttm3f", precision=prec,
                               scramble_seed=SCRAMBLE_SEED)
         nb = hb.nb
-        hb.accumulate(0, 4096)           # warm-up, then start clean
+        hb.accumulate(1 << 45, 4096)           # warm-up, then start clean
         hb.reset()
         torch.cuda.synchronize()
-        t_compute, t_dump = 0.0, 0.0
-        Mh = np.zeros((nb, nb), order="F") if prec != "fp64" else None
+        ms, t_dump, dumps = 0.0, 0.0, []
+        Mh = np.zeros((nb, nb), order="F") if prec != "fp64" and dump else None
         for c0 in range(0, total, chunk):
-            t0 = time.perf_counter()
-            hb.accumulate(c0, min(chunk, total - c0))
-            torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            t_compute += t1 - t0
-            if Mh is not None and not args.no_dump:
+            ms += timed_accumulate(hb, c0, min(chunk, total - c0))
+            if Mh is not None:
+                t1 = time.perf_counter()
                 hb.read(1, out=Mh)
                 path = os.path.join(outdir, "sM_%07d.h5" % (c0 + chunk))
-                h5.save(path, Mh)
+                h5.save(path, Mh, deflate=deflate)
                 t_dump += time.perf_counter() - t1
-                if c0 > 0:          # keep only the newest dump on disk (1.7 GB each)
-                    os.remove(os.path.join(outdir, "sM_%07d.h5" % c0))
+                dumps.append({"file": os.path.basename(path), "bytes": os.path.getsize(path)})
+                os.remove(path)           # 1.7 GB of float32 before compression
         t0 = time.perf_counter()
         ev = hb.eigvals(10)
         t_eig = time.perf_counter() - t0
         rc, nonfinite, notconv = hb.status()
-        res[prec] = dict(samples_per_s=total / t_compute, compute_s=t_compute, dump_s=t_dump, eig_s=t_eig,
-                         levels_cm1=[float(x * autocm) for x in ev], nonfinite=nonfinite, not_converged=notconv)
+        res[prec] = dict(samples_per_s=total / (ms * 1e-3), compute_ms=ms, dump_s=t_dump, dumps=dumps,
+                         eig_s=t_eig, levels_cm1=[float(x * autocm) for x in ev], rc=rc, nonfinite=nonfinite,
+                         not_converged=notconv)
         hb.close()
-    sp, dp = res[args.precision], res["fp64"]
+    os.rmdir(outdir)
+    sp, dp = res[precision], res["fp64"]
     err = float(np.abs(np.array(sp["levels_cm1"]) - np.array(dp["levels_cm1"])).max())
-    print(json.dumps({"config": {"workload": "hexamer prism TTM3-F, 48 modes, triples basis Nb=20825, %d scrambled "
-                                             "Sobol points in 2^17 chunks with an sM_*.h5 dump after each" % total,
-                                 "precision": args.precision, "nb": 20825},
-                      "split": sp, "fp64": dp, "speedup_vs_fp64": sp["samples_per_s"] / dp["samples_per_s"],
-                      "max_abs_err_cm1_vs_fp64": err, "h5_dir": outdir}))
+    return {"config": {"workload": "hexamer prism TTM3-F, 48 modes, triples basis Nb=20825, %d scrambled Sobol "
+                                   "points in 2^17 chunks, an sM_*.h5 (chunked, deflate %d) after each chunk of the "
+                                   "split form" % (total, deflate), "precision": precision, "nb": 20825},
+            "split": sp, "fp64": dp, "speedup_vs_fp64": sp["samples_per_s"] / dp["samples_per_s"],
+            "max_abs_err_cm1_vs_fp64": err,
+            "note": "levels of a %d-point build are dominated by Monte Carlo noise (the plain estimator collapses "
+                    "at these sizes); the error compares two arithmetic forms on the same points" % total}
+
+
+def run_triples(args):
+    """--config triples: triples_record at 2^21 points (one JSON line)."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(triples_record(args.samples, args.precision, dump=not args.no_dump)))
+
+
+def fp64_record(nw, x0, MUa, omega, steps, device):
+    """The plain FP64 form on the benchmark's workload (the hexamer doubles
+    build, 2^20 points per step): device-timed samples/s and the contraction's
+    algorithmic FP64 rate against the B200's nominal FP64 peak."""
+    import scp3_b200
+    hb = scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=0, pes="qtip4pf", precision="fp64",
+                          scramble_seed=SCRAMBLE_SEED, device=device)
+    nb = hb.nb
+    timed_accumulate(hb, 1 << 44, SAMPLES)        # warm-up
+    hb.reset()
+    hb.profile(True)
+    ms = [timed_accumulate(hb, k * SAMPLES, SAMPLES) for k in range(steps)]
+    kms, launches = hb.profile(False)
+    hb.close()
+    achieved = nb * (nb + 1) * SAMPLES * steps / (kms[2] * 1e-3) / 1e12
+    return {"value": SAMPLES * steps / (sum(ms) * 1e-3), "unit": "samples/s", "steps": steps,
+            "ms_per_step": sum(ms) / steps,
+            "kernel_ms": {"per_sample": kms[0], "expand": kms[1], "contract": kms[2]},
+            "contraction": {"achieved": achieved, "unit": "TFLOP/s", "peak": FP64_NOMINAL_TFLOPS,
+                            "frac": achieved / FP64_NOMINAL_TFLOPS,
+                            "peak_source": "nominal B200 FP64 (no measured FP64 peak)",
+                            "work": "Nb(Nb+1) FLOP per sample, upper triangle"}}
 
 
 def run_cv(args):
@@ -495,6 +680,11 @@ def main():
     ap.add_argument("--no-dump", action="store_true", help="triples: skip the sM_*.h5 dumps")
     ap.add_argument("--samples", type=int, default=SAMPLES,
                     help="samples per step (the benchmark is 2^20; smaller only for profiler captures)")
+    ap.add_argument("--no-subrecords", action="store_true",
+                    help="skip the fp64 and triples sub-records of the default line")
+    ap.add_argument("--standin", action="store_true",
+                    help="CPU tests: ranks over gloo with a host stand-in build (no GPU, not a benchmark)")
+    ap.add_argument("--dump-matrix", default=None, help="--standin: save rank 0's reduced matrix (.npy)")
     args = ap.parse_args()
     SAMPLES = args.samples
     if args.config == "cv":
@@ -511,9 +701,15 @@ def main():
             args.samples = 1 << 21
         run_triples(args)
         return
-    world, rank, local = dist_setup(args.gpus)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args.gpus, sys.argv[1:]))
     if args.impl == "reference":
-        run_reference(args, world, rank)
+        # rank 0 alone times the CPU build; the other ranks exit without work
+        run_reference(args, int(os.environ.get("RANK", "0")))
+        return
+    world, rank, local = dist_setup(args.gpus, "gloo" if args.standin else "nccl")
+    if args.standin:
+        run_standin(args, world, rank)
         return
 
     import torch
@@ -534,12 +730,7 @@ def main():
     def step(k):
         hb.accumulate(base + k * SAMPLES, SAMPLES)
         if world > 1:
-            import torch.distributed as dist
-            hb.read_dev(Mdev.data_ptr(), nb, 0)
-            ev = torch.cuda.Event()
-            ev.record(stream)
-            torch.cuda.current_stream().wait_event(ev)
-            shard.reduce_matrix(Mdev)
+            exchange(hb, Mdev, stream)
 
     for k in range(args.warmup):
         step(k)
@@ -590,14 +781,15 @@ def main():
         roof = {"bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
                 "traffic": traffic, "note": "algorithmic Nb(Nb+1) flops/sample; BF16x3 issues 3 tensor products each "
                                             "(ceiling 1/3); peak " + peak_src + "; traffic: ncu DRAM bytes per "
-                                            "launch (read + write; operand 5200 B/sample)"}
+                                            "launch (read + write; operand 5200 B/sample)",
+                "traffic_source": "not measured in this run: a constant per sample from one ncu capture of the "
+                                  "contraction (profiles/), scaled to the samples of an average launch"}
 
     line = {"metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3/f32/f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "precision": args.precision, "nb": nb, "samples_per_step": SAMPLES,
-                       "l2": "flushed between steps (256 MB write)", "parallelism": "dp%d (sample ranges)" % world},
+            "config": bench_config(args.precision, nb, world),
             "roofline": roof,
             # the handle's timing counts a split-form preparation (sign partition + expansion) as one
             # launch of kind 1; it is two kernels
@@ -637,7 +829,7 @@ def main():
             import torch.distributed as dist
             dist.barrier()
         t0 = time.perf_counter()
-        ne = max(2, min(args.steps, 5))
+        ne = args.steps
         for k in range(ne):
             hb.accumulate_normals(normals)
             hb.read(1, out=Mh)
@@ -651,6 +843,16 @@ def main():
                        "h2d_bytes_per_step": int(normals.nbytes), "d2h_bytes_per_step": int(nb * nb * 8),
                        "path": ("scp3gpu_hbuild_accumulate_normals" + ("" if args.precision == "fp64" else "_f32") +
                                 " + scp3gpu_hbuild_read(mode 1), host buffers, every rank; bytes per rank")}
+    if rank == 0 and world == 1 and args.precision != "fp64" and not args.no_subrecords:
+        # the plain form on the same workload, and the triples configuration with its
+        # split-vs-FP64 ratio: the two other numbers the metric's target is read from
+        hb.close()
+        line["fp64"] = fp64_record(nw, x0, MUa, omega, 3, local)
+        line["triples"] = triples_record(TRIPLES_SAMPLES, args.precision)
+        t = line["triples"]
+        line["target"] = {"triples_speedup_vs_fp64": t["speedup_vs_fp64"], "wanted": ">= 10",
+                          "triples_max_level_err_cm1": t["max_abs_err_cm1_vs_fp64"], "wanted_cm1": "<= 0.1",
+                          "doubles_speedup_vs_fp64": value / line["fp64"]["value"]}
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         normals = scp3_b200.std_normals(nm0, 0, 1 << 17, scramble_seed=SCRAMBLE_SEED)
         line["cpu_baseline"] = cpu_reference(nw, x0, MUa, omega, np.arange(nm0, dtype=np.int32), 48, 0, normals)

@@ -29,11 +29,12 @@ def _dp(a):
 
 
 def build(reference=None):
-    """Compile the restatement (and, when the reference tree exists, oracle/_ref)."""
+    """Compile the restatement, and oracle/_ref when a reference tree is given
+    (the argument, else $SCP3_REFERENCE) and exists."""
     import subprocess
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    ref = reference or "/root/reference"
-    if os.path.isdir(ref):
+    ref = reference or os.environ.get("SCP3_REFERENCE")
+    if ref and os.path.isdir(ref):
         subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + ref], check=True)
 
 
@@ -240,10 +241,30 @@ def ref_available(fast=False):
     return os.path.exists(os.path.join(HERE, "_ref", "libscp3ref_fast.so" if fast else "libscp3ref.so"))
 
 
+# Threading of the reference's CPU build.  Its block loop alternates an OpenMP
+# region (get_bra and the ket, ScaledMatrixElements.cpp:956-968) with a threaded
+# BLAS dsyr2k (:970).  With the libraries' defaults both thread pools busy-wait
+# after their work (OpenBLAS for 2^28 cycles, libgomp for its spin count), so
+# each phase ran against the other's spinning threads on the same cores: the
+# get_bra phase took 3x as long as dsyr2k for a tenth of its work.  The
+# reference's production build shares one OpenMP pool between its loop and
+# MKL; here the two pools are told to sleep when idle instead.  Both variables
+# are read when the libraries load, so they are set before the first load;
+# values the caller exported win.
+REF_THREAD_ENV = {"OPENBLAS_THREAD_TIMEOUT": "4", "OMP_WAIT_POLICY": "PASSIVE"}
+
+
+def ref_thread_env():
+    """The thread settings in force for the reference's CPU build."""
+    return {k: os.environ.get(k) for k in REF_THREAD_ENV}
+
+
 def ref_lib(fast=False):
     """The reference's own sources compiled by oracle/Makefile (parity or release flags)."""
     key = "fast" if fast else "parity"
     if key not in _ref:
+        for k, v in REF_THREAD_ENV.items():
+            os.environ.setdefault(k, v)
         L = ctypes.CDLL(os.path.join(HERE, "_ref", "libscp3ref_fast.so" if fast else "libscp3ref.so"))
         for fn in ("ref_qtip4pf_energy", "ref_ttm3f_energy"):
             getattr(L, fn).restype = ctypes.c_double

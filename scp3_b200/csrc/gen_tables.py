@@ -4,7 +4,7 @@
   numbers of the 62-bit Sobol generator, dimensions 1..1111.  They are the data
   that ``i8_sobol`` fills in before its Bratley-Fox recurrence
   (sobol.cpp:14308-14420 ``poly[]``, sobol.cpp:14440-27670 ``v[i][j] = ...``).
-  The recurrence itself is restated in our own code (``sobol_table.cpp``).
+  The recurrence itself is restated in our own code (``tables.cpp``).
 * ``ps_coeffs.h``: the Partridge-Schwenke monomer expansion (245 terms, four
   coefficient sets combined at start-up, ps.cpp:18-458) and the 84-term dipole
   moment surface (ps.cpp:417-466) used by TTM3-F.
@@ -14,8 +14,9 @@ a potential with different numbers is a different sequence or potential, so the
 numbers are kept exactly as the reference writes them (the decimal literals are
 re-emitted verbatim so the compiler parses identical doubles).
 
-Usage (only where the reference tree is mounted):
-    python scp3_b200/csrc/gen_tables.py /root/reference
+Usage (only where the reference tree is present; its root is the argument, or
+$SCP3_REFERENCE when no argument is given):
+    python scp3_b200/csrc/gen_tables.py <reference tree>
 """
 import os
 import re
@@ -109,4 +110,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SCP3_REFERENCE")
+    if not ref:
+        sys.exit("usage: gen_tables.py <reference tree>  (or set SCP3_REFERENCE)")
+    main(ref)

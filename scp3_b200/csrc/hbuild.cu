@@ -284,11 +284,11 @@ int accumulate_host_normals(scp3gpu_hbuild* h, const T* normals, int64_t n, cons
     int rc = SCP3GPU_OK;
     for (int b = 0; b < 2 && !h->normals[b]; b++)
         if ((rc = dalloc(&h->normals[b], (size_t)h->chunk * nm0))) return rc;
-    int k = 0;
-    for (int64_t off = 0, c = 0; off < n; off += c, k++) {
-        const int b = k & 1;
-        const int64_t part = (int64_t)1 << std::min(17, 15 + (k > 0 ? k - 1 : 0));
-        c = std::min(std::min(h->chunk, part), n - off);
+    // A failed step ends the loop but not the function: copies already queued
+    // from the caller's buffer are waited for before returning, so the caller
+    // may free or reuse that buffer as soon as the call returns, error or not.
+    // h->count then holds the samples whose passes were queued.
+    auto step = [&](int64_t off, int64_t c, int b) -> int {
         T* dst = reinterpret_cast<T*>(h->normals[b]);
         // the copy into buffer b may start once the pass that last read it is done
         SCP3_CUDA(cudaStreamWaitEvent(h->copy_stream, h->consumed[b], 0));
@@ -297,10 +297,17 @@ int accumulate_host_normals(scp3gpu_hbuild* h, const T* normals, int64_t n, cons
         SCP3_CUDA(cudaEventRecord(h->copied[b], h->copy_stream));
         const double* d64 = sizeof(T) == 8 ? reinterpret_cast<const double*>(dst) : nullptr;
         const float* d32 = sizeof(T) == 4 ? reinterpret_cast<const float*>(dst) : nullptr;
-        if ((rc = launch_chunk(h, 0, c, d64, d32, h->copied[b], h->consumed[b]))) return rc;
-        h->count += c;
+        return launch_chunk(h, 0, c, d64, d32, h->copied[b], h->consumed[b]);
+    };
+    int k = 0;
+    for (int64_t off = 0, c = 0; off < n && rc == SCP3GPU_OK; off += c, k++) {
+        const int64_t part = (int64_t)1 << std::min(17, 15 + (k > 0 ? k - 1 : 0));
+        c = std::min(std::min(h->chunk, part), n - off);
+        if ((rc = step(off, c, k & 1)) == SCP3GPU_OK) h->count += c;
     }
-    SCP3_CUDA(cudaStreamSynchronize(h->copy_stream));
+    const cudaError_t e = cudaStreamSynchronize(h->copy_stream);
+    if (rc != SCP3GPU_OK) return rc;
+    if (e != cudaSuccess) return scp3::cuda_fail(e, "accumulate_host_normals: copy stream");
     return SCP3GPU_OK;
 }
 }  // namespace

@@ -3,7 +3,9 @@
 // Same command line as the reference (SCP3.cpp:33-44, 92-151):
 //   scp3 [-N p] [-S p] [-r file] [-2 N2] [-3 N3] [-p pes] [-m modes] [-G] [-B block] input.dat
 // plus --precision fp64|bf16x3|f16x3, --scramble-seed S (seeded scramble of the
-// device Sobol points), --device d.  Reads the input file (load_from_vladimir,
+// device Sobol points), --device d, --write-modes file (x0 and the normal modes
+// the run samples: the eigenvector signs are the eigensolver's choice, so the
+// file is what another program needs to reproduce the run's points).  Reads the input file (load_from_vladimir,
 // DiskIO.cpp:72-116), reorders O H H (DiskIO.cpp:142-195), builds the normal
 // modes (SCP3.cpp:296-314), and runs the sample loop of SCP3_a (SCP3.cpp:154-272)
 // on the GPU: E0_sd.dat every 2^14 samples (SCP3.cpp:234-250), sM_%07d.h5 every
@@ -38,7 +40,7 @@ const double kOmass = kCmass * 15.9994 / 12.0107;
 struct Options {
     int64_t nsobol = 1 << 20;
     int64_t skip = 1 << 30;
-    string rng_file, input, pes = "qtip4pf", precision = "fp64";
+    string rng_file, input, pes = "qtip4pf", precision = "fp64", modes_file;
     int n2 = 0, n3 = 0, block = 1024, device = 0;
     bool use_gradient = true, scramble = false;
     uint64_t scramble_seed = 0;
@@ -83,6 +85,7 @@ Options parse(int argc, char** argv)
                                    {"precision", required_argument, nullptr, 1000},
                                    {"scramble-seed", required_argument, nullptr, 1001},
                                    {"device", required_argument, nullptr, 1002},
+                                   {"write-modes", required_argument, nullptr, 1003},
                                    {nullptr, 0, nullptr, 0}};
     Options o;
     int ch;
@@ -113,6 +116,7 @@ Options parse(int argc, char** argv)
                 o.scramble_seed = strtoull(optarg, nullptr, 0);
                 break;
             case 1002: o.device = atoi(optarg); break;
+            case 1003: o.modes_file = optarg; break;
             default: die("Unknown option: " + to_string(ch));
         }
     }
@@ -264,6 +268,18 @@ int main(int argc, char** argv)
         const double alpha = sqrt(omega[k]);
         for (int i = 0; i < n; i++) MUa[(size_t)k * n + i] = U[(size_t)(6 + k) * n + i] / (sqrt(mass[i]) * alpha);
     }
+    if (!o.modes_file.empty()) {
+        // line 1: x0 (bohr, O H H order); line 2 + k: omega_k, then column k of MUa
+        FILE* f = fopen(o.modes_file.c_str(), "w");
+        if (!f) die("cannot write " + o.modes_file);
+        for (int i = 0; i < n; i++) fprintf(f, "%.17g%c", x0[i], i + 1 < n ? ' ' : '\n');
+        for (int k = 0; k < nm0; k++) {
+            fprintf(f, "%.17g", omega[k]);
+            for (int i = 0; i < n; i++) fprintf(f, " %.17g", MUa[(size_t)k * n + i]);
+            fprintf(f, "\n");
+        }
+        fclose(f);
+    }
     if (o.modes.empty())
         for (int k = 0; k < nm0; k++) o.modes.push_back(k);
     if (o.n2 > (int)o.modes.size() || o.n3 > (int)o.modes.size())
@@ -326,6 +342,11 @@ int main(int argc, char** argv)
             if ((i + o.block) % (1 << 17) == 0) {      // SCP3.cpp:252-255
                 Mout.resize((size_t)nb * nb);
                 check(scp3gpu_hbuild_read(h, Mout.data(), nb, 1), "read");
+                // The reference's M holds the upper triangle only (dsyr2k 'U' into a zero
+                // matrix, ScaledMatrixElements.cpp:970; the gradient path fills upper
+                // elements, :709-725), so its sM files hold zeros below the diagonal.
+                for (int64_t j = 0; j < nb; j++)
+                    for (int64_t r = j + 1; r < nb; r++) Mout[(size_t)j * nb + r] = 0.0;
                 char s[128];
                 snprintf(s, sizeof s, "sM_%07lld.h5", (long long)(i + o.block));
                 check(scp3gpu_save_h5(s, Mout.data(), nb, nb), "save_h5");

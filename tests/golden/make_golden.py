@@ -39,7 +39,7 @@ import oracle  # noqa: E402
 from scp3_b200 import clusters, constants as C, modes  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("SCP3_REFERENCE", "/root/reference")
+REF = os.environ.get("SCP3_REFERENCE")
 
 # test-potentials.cpp:14-33, O H H order, Angstrom
 PRISM_TP = np.array([
@@ -301,6 +301,8 @@ def stein_matrix(Ls, names, params, egrad, x0, MUa, omega, n2, n3, ns, sseed):
 
 
 def main():
+    if not REF:
+        sys.exit("set SCP3_REFERENCE to the reference tree's root")
     oracle.build(REF)
     L = oracle.ref_lib()
     if sys.argv[1:] == ["stein"]:

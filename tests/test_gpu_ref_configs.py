@@ -1,0 +1,182 @@
+"""The benchmarked configurations against the reference's own build, element by
+element.
+
+The reference side is oracle/_ref's ref_hbuild: the -G sample loop of SCP3_a
+(SCP3.cpp:154-232) over the reference's own potentials and Hermite functions
+(compiled unchanged from its sources), get_bra (ScaledMatrixElements.cpp:870-930)
+and dsyr2k (ScaledMatrixElements.cpp:942-971) from OpenBLAS, fed the same
+scrambled Sobol normals through its -r path (SCP3.cpp:188-194).  The GPU side is
+the build the benchmark runs: device Sobol, the per-sample kernel and the
+contraction, through the C ABI.
+
+  C1  dimer, qTIP4P/f, 12 modes, N2 = 12 (Nb = 91), 2^16 points: the whole config
+  C2  hexamer prism, qTIP4P/f, N2 = 48 (Nb = 1225), 2^13 points: the benchmark's basis
+      and tiling (ten 128-row panels, multi-tile, half-owned diagonal tiles)
+  C3  hexamer prism, TTM3-F, N2 = N3 = 48 (Nb = 20825), 1024 points: the triples basis
+
+Tolerances.  FP64 form: every upper element within 1e-12 of
+A_ij = sum_s |Phi_i||V||Phi_j| (the scale a near-cancelling element is measured
+against), and the 10 lowest levels of Mout = M/n + HO diagonal within 1e-6 cm^-1
+of the reference's.  Split forms (BF16x3, FP16x3): per element within 5e-4 of
+A_ij, median within 2e-5; levels within 0.1 cm^-1 of the reference's (C1, C2).
+Each test prints its measured error distribution; with SCP3_PARITY_OUT set it
+also writes it there as JSON."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+AUTOCM = 2.194746313e5
+SEED = 0x5C3
+
+CONFIGS = {
+    "C1": dict(input="dimer_qtip4pf", pes=0, n2=12, n3=0, n=1 << 16),
+    "C2": dict(input="prism_qtip4pf", pes=0, n2=48, n3=0, n=1 << 13),
+    "C3": dict(input="prism_ttm3f", pes=1, n2=48, n3=48, n=1 << 10),
+}
+
+
+@pytest.fixture(scope="module")
+def scp3():
+    import torch
+    assert torch.cuda.is_available()
+    import scp3_b200
+    scp3_b200._lib.lib()
+    return scp3_b200
+
+
+def _record(name, stats):
+    print("\n%s %s" % (name, json.dumps(stats)))
+    out = os.environ.get("SCP3_PARITY_OUT")
+    if out:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, name + ".json"), "w") as f:
+            json.dump(stats, f, indent=1)
+
+
+_cache = {}
+
+
+def reference(cfg_name):
+    """The reference's build of config `cfg_name`: (inputs, M upper from dsyr2k,
+    |Phi| and |V| for the scale, lowest 10 levels of its Mout or None)."""
+    if cfg_name in _cache:
+        return _cache[cfg_name]
+    import oracle
+    from scp3_b200 import inputs
+    if not oracle.ref_available():
+        pytest.fail("oracle/_ref (the reference built from its sources) is missing: build it where the "
+                    "reference tree is present")
+    cfg = CONFIGS[cfg_name]
+    nw, x0, MUa, omega = inputs.load(cfg["input"], build_if_missing=False)
+    nm = omega.size
+    modes = np.arange(nm, dtype=np.int32)
+    n = cfg["n"]
+    normals = oracle.std_normals(nm, 0, n, scramble_seed=SEED)
+    M, _, _ = oracle.ref_hbuild(cfg["pes"], nw, x0, MUa, omega, modes, cfg["n2"], cfg["n3"], n, 1024,
+                                normals=normals)
+    q, v = oracle.samples(cfg["pes"], nw, x0, MUa, omega, normals)
+    nb = M.shape[0]
+    absphi = np.empty((n, nb))
+    for s in range(n):
+        absphi[s] = np.abs(oracle.get_bra(q[s], cfg["n2"], cfg["n3"]))
+    levels = None
+    if nb <= 2048:
+        Mout = np.asfortranarray(np.triu(M) + np.triu(M, 1).T) / n
+        oracle.add_ho_diagonal(Mout, omega, cfg["n2"], cfg["n3"], 0.0)
+        levels = np.linalg.eigvalsh(Mout)[:10]
+    _cache[cfg_name] = dict(nw=nw, x0=x0, MUa=MUa, omega=omega, M=M, absphi=absphi, absv=np.abs(v),
+                            levels=levels, cfg=cfg)
+    return _cache[cfg_name]
+
+
+def scaled_errors(Mgpu, ref, block=2048):
+    """|M_gpu - M_ref| / A over the upper triangle, column block by column block
+    (A = |Phi|^T diag|V| |Phi| is formed one block at a time: at Nb = 20825 each
+    full matrix is 3.5 GB).  Returns the flat errors and the max per 128 x 128
+    block of the upper triangle."""
+    M = ref["M"]
+    nb = M.shape[0]
+    W = ref["absphi"] * ref["absv"][:, None]
+    errs, nblk = [], (nb + 127) // 128
+    per = np.zeros((nblk, nblk))
+    for j0 in range(0, nb, block):
+        j1 = min(nb, j0 + block)
+        A = W.T @ ref["absphi"][:, j0:j1]
+        rows = np.arange(nb)[:, None]
+        cols = np.arange(j0, j1)[None, :]
+        upper = rows <= cols
+        e = np.abs(Mgpu[:, j0:j1] - M[:, j0:j1]) / np.maximum(A, 1e-300)
+        e[~upper] = 0.0
+        errs.append(e[upper])
+        for bj in range(j0 // 128, (j1 - 1) // 128 + 1):
+            c0, c1 = max(bj * 128, j0) - j0, min((bj + 1) * 128, j1) - j0
+            if c1 <= c0:
+                continue
+            colmax = e[:, c0:c1].max(axis=1)
+            for bi in range(0, bj + 1):
+                per[bi, bj] = max(per[bi, bj], colmax[bi * 128:(bi + 1) * 128].max())
+    return np.concatenate(errs), per
+
+
+def gpu_build(scp3, ref, precision):
+    cfg = ref["cfg"]
+    hb = scp3.HBuild(ref["nw"], ref["x0"], ref["MUa"], ref["omega"], n2=cfg["n2"], n3=cfg["n3"],
+                     pes=cfg["pes"], precision=precision, scramble_seed=SEED)
+    hb.accumulate(0, cfg["n"])
+    assert hb.sample_count() == cfg["n"]
+    assert hb.status() == (0, 0, 0), hb.status()
+    return hb
+
+
+@pytest.mark.parametrize("cfg_name", ["C1", "C2", "C3"])
+def test_fp64_matches_reference_build(scp3, cfg_name):
+    ref = reference(cfg_name)
+    hb = gpu_build(scp3, ref, "fp64")
+    M = hb.read(0)
+    levels = hb.eigvals(10) if ref["levels"] is not None else None
+    hb.close()
+    e, per = scaled_errors(M, ref)
+    del M
+    stats = {"config": cfg_name, "form": "fp64", "nb": int(ref["M"].shape[0]), "samples": ref["cfg"]["n"],
+             "max_scaled": float(e.max()), "median_scaled": float(np.median(e)),
+             "p99_scaled": float(np.quantile(e, 0.99))}
+    if levels is not None:
+        d = np.abs(levels - ref["levels"]) * AUTOCM
+        stats.update(max_level_err_cm1=float(d.max()), lowest10_cm1_ref=[float(x * AUTOCM) for x in ref["levels"]])
+    _record("parity_%s_fp64" % cfg_name, stats)
+    assert e.max() <= 1e-12, stats
+    if levels is not None:
+        assert stats["max_level_err_cm1"] <= 1e-6, stats
+
+
+@pytest.mark.parametrize("prec", ["bf16x3", "f16x3"])
+@pytest.mark.parametrize("cfg_name", ["C1", "C2", "C3"])
+def test_split_against_reference_build(scp3, cfg_name, prec):
+    if cfg_name == "C3" and prec == "f16x3":
+        pytest.skip("C3 runs the benchmark's BF16x3 form only (one 20825-function pass per form)")
+    ref = reference(cfg_name)
+    hb = gpu_build(scp3, ref, prec)
+    M = hb.read(0)
+    levels = hb.eigvals(10) if ref["levels"] is not None else None
+    hb.close()
+    e, per = scaled_errors(M, ref)
+    del M
+    nblk = per.shape[0]
+    iu = np.triu_indices(nblk)
+    stats = {"config": cfg_name, "form": prec, "nb": int(ref["M"].shape[0]), "samples": ref["cfg"]["n"],
+             "max_scaled": float(e.max()), "median_scaled": float(np.median(e)),
+             "p99_scaled": float(np.quantile(e, 0.99)),
+             "per_128_block_max": {"blocks": int(iu[0].size), "min": float(per[iu].min()),
+                                   "median": float(np.median(per[iu])), "max": float(per[iu].max()),
+                                   "diagonal_blocks_max": float(np.diag(per).max())}}
+    if levels is not None:
+        d = (levels - ref["levels"]) * AUTOCM
+        stats.update(level_err_cm1=[float(x) for x in d], max_level_err_cm1=float(np.abs(d).max()))
+    _record("parity_%s_%s" % (cfg_name, prec), stats)
+    assert e.max() <= 5e-4, stats
+    assert np.median(e) <= 2e-5, stats
+    if levels is not None:
+        assert stats["max_level_err_cm1"] <= 0.1, stats
