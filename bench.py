@@ -332,8 +332,11 @@ def triples_record(total, precision, dump=True, deflate=6):
         torch.cuda.synchronize()
         ms, t_dump, dumps = 0.0, 0.0, []
         Mh = np.zeros((nb, nb), order="F") if prec != "fp64" and dump else None
+        kms = np.zeros(4)
         for c0 in range(0, total, chunk):
+            hb.profile(True)
             ms += timed_accumulate(hb, c0, min(chunk, total - c0))
+            kms += hb.profile(False)[0]
             if Mh is not None:
                 t1 = time.perf_counter()
                 hb.read(1, out=Mh)
@@ -346,7 +349,9 @@ def triples_record(total, precision, dump=True, deflate=6):
         ev = hb.eigvals(10)
         t_eig = time.perf_counter() - t0
         rc, nonfinite, notconv = hb.status()
-        res[prec] = dict(samples_per_s=total / (ms * 1e-3), compute_ms=ms, dump_s=t_dump, dumps=dumps,
+        res[prec] = dict(samples_per_s=total / (ms * 1e-3), compute_ms=ms,
+                         kernel_ms={"per_sample": kms[0], "expand": kms[1], "contract": kms[2]},
+                         dump_s=t_dump, dumps=dumps,
                          eig_s=t_eig, levels_cm1=[float(x * autocm) for x in ev], rc=rc, nonfinite=nonfinite,
                          not_converged=notconv)
         hb.close()
@@ -584,6 +589,43 @@ def run_batch(args):
         "max_rel_diff_vs_single_builds": worst_same, "max_level_err_cm1_vs_fp64": worst_lvl, "clusters": per}))
 
 
+def run_gradient(args):
+    """The reference's default estimator (no -G): the Stein estimator of every
+    upper element from V and dV/dq (ScaledMatrixElements.cpp:102-725,
+    TripleExcitations.h) on the hexamer prism doubles basis (Nb = 1225, 48 modes,
+    qTIP4P/f energy and gradient per sample), FP64.  value: samples/s,
+    device-timed; the kernel split from the build's timing.  One JSON line; not
+    the benchmark's default."""
+    import torch
+    import scp3_b200
+    from scp3_b200 import inputs
+    torch.cuda.set_device(0)
+    nw, x0, MUa, omega = inputs.load(INPUT)
+    n = args.samples
+    hb = scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=0, pes="qtip4pf", precision="fp64",
+                          scramble_seed=SCRAMBLE_SEED, estimator="gradient")
+    for k in range(max(args.warmup, 1)):
+        timed_accumulate(hb, (1 << 44) + k * n, n)
+    hb.reset()
+    clocks = Clocks(0)
+    hb.profile(True)
+    ms = [timed_accumulate(hb, k * n, n) for k in range(args.steps)]
+    kms, launches = hb.profile(False)
+    clk = clocks.stop()
+    rc, nonfinite, notconv = hb.status()
+    nb = hb.nb
+    hb.close()
+    t = sum(ms) / len(ms)
+    print(json.dumps({
+        "metric": "gradient-estimator build: Sobol samples/s (hexamer doubles, FP64)", "value": n / (t * 1e-3),
+        "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "hexamer prism qTIP4P/f, 48 modes, doubles basis Nb=%d, %d scrambled Sobol points per "
+                               "step, the Stein estimator of SCP3's default path" % (nb, n)},
+        "kernel_ms": {"per_sample": kms[0] / args.steps, "stein": kms[2] / args.steps},
+        "clocks": clk, "status": {"rc": rc, "nonfinite": nonfinite, "not_converged": notconv}}))
+
+
 def _ref_scp1_rate(job):
     """One process of the CPU reference arm of --config scp1: the reference's own
     std_normal and qTIP4P/f operator in SCP1.cpp's sample loop (single-threaded,
@@ -671,10 +713,10 @@ def main():
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16x3", "f16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--config", default="doubles", choices=["doubles", "triples", "cv", "batch", "scp1"],
+    ap.add_argument("--config", default="doubles", choices=["doubles", "triples", "cv", "batch", "scp1", "gradient"],
                     help="doubles: the benchmark (hexamer, Nb=1225); triples: the TTM3-F triples build; "
                          "cv: the learned control variate; batch: 32 clusters in one batched build; "
-                         "scp1: the SCP1 effective-Hessian averages")
+                         "scp1: the SCP1 effective-Hessian averages; gradient: the default (Stein) estimator")
     ap.add_argument("--cv-epochs", type=int, default=100)
     ap.add_argument("--no-levels", action="store_true", help="skip the FP64 level check (profiler captures)")
     ap.add_argument("--no-dump", action="store_true", help="triples: skip the sM_*.h5 dumps")
@@ -695,6 +737,9 @@ def main():
         return
     if args.config == "scp1":
         run_scp1(args)
+        return
+    if args.config == "gradient":
+        run_gradient(args)
         return
     if args.config == "triples":
         if args.samples == 1 << 20:

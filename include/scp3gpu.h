@@ -112,7 +112,9 @@ typedef struct scp3gpu_config {
     uint64_t scramble_seed;
     int chunk;              /* samples per device pass; multiple of 4096, 0 = auto:
                                2^18 for the split forms (halved while one pass's
-                               operand would exceed ~6 GB), 4096 for the FP64 form    */
+                               operand would exceed ~6 GB); 2^14 for the FP64 form
+                               (halved while its Phi and W would exceed ~4 GB), 4096
+                               for the gradient estimator                             */
     int device;             /* CUDA device ordinal                                     */
     int estimator;          /* SCP3GPU_ESTIMATOR_*                                     */
 } scp3gpu_config;
@@ -229,9 +231,14 @@ int scp3gpu_batch_status(scp3gpu_batch* b, int cluster, int64_t* nonfinite, int6
  * sum_s Phi(q_s) V_s Phi(q_s)^T into M_dev (both triangles), FP64, ordered on
  * `stream` (a cudaStream_t; NULL = the legacy default stream).  Working space
  * comes from one static 64 MiB device array; bases over 4032 functions are
- * rejected with SCP3GPU_ERR_ARG.  The first call on a device looks up that
- * array's address (make it before any stream capture); all calls share the
- * array, so calls that overlap on the GPU race -- order them on one stream. */
+ * rejected with SCP3GPU_ERR_ARG.  Throughput falls as the basis nears that
+ * limit: samples go through in chunks of 4096 up to 832 functions, and the
+ * chunk halves as the tile sums take more of the array (1024 at 1217-1536
+ * functions, 512 at 1985-2368, 16 from 3969), each chunk costing two kernel
+ * launches.  The first call
+ * on a device looks up that array's address (make it before any stream
+ * capture); all calls share the array, so calls that overlap on the GPU race --
+ * order them on one stream. */
 int scp3gpu_add_epot_static(int nmodes, int n2, int n3, const double* q_dev, const double* V_dev, int64_t n,
                             double* M_dev, int64_t ld, void* stream);
 

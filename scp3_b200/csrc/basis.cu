@@ -58,7 +58,49 @@ __global__ void __launch_bounds__(kExpSamples) expand_fp64_kernel(const uint32_t
     }
 }
 
+// Sample-major form for the 128 x 128 FP64 contraction: phi/w [n][ld], rows
+// contiguous.  grid: x = sample blocks of 64, y = row blocks of 128; a thread
+// owns one row and walks the block's samples, so each sample's 128 rows are one
+// coalesced 1 KB store.
+__global__ void __launch_bounds__(kExpRows) expand_fp64_sm_kernel(const uint32_t* __restrict__ desc, int nb,
+                                                                  int nm, const double* __restrict__ q,
+                                                                  const double* __restrict__ v, int64_t n,
+                                                                  int64_t ld, double* __restrict__ phi,
+                                                                  double* __restrict__ w)
+{
+    extern __shared__ double qs[];   // [nm][64]
+    const int t = threadIdx.x;
+    const int64_t s0 = (int64_t)blockIdx.x * kExpSamples;
+    for (int e = t; e < nm * kExpSamples; e += kExpRows) {
+        const int ss = e / nm, m = e - ss * nm;          // coalesced read of q[s0+ss][m]
+        qs[m * kExpSamples + ss] = (s0 + ss < n) ? q[(s0 + ss) * nm + m] : 0.0;
+    }
+    __syncthreads();
+    const int i = blockIdx.y * kExpRows + t;            // < ld: ld is a whole number of row blocks
+    const uint32_t d = i < nb ? __ldg(desc + i) : 0u;
+    const int ns = (int)min((int64_t)kExpSamples, n - s0);
+    for (int ss = 0; ss < ns; ss++) {
+        const double val = (i < nb) ? basis_value(d, qs, ss) : 0.0;
+        phi[(size_t)(s0 + ss) * ld + i] = val;
+        w[(size_t)(s0 + ss) * ld + i] = val * v[s0 + ss];   // ket = bra * V (ScaledMatrixElements.cpp:964-967)
+    }
+}
+
 }  // namespace
+
+int launch_expand_fp64_sm(const uint32_t* desc, int nb, int nm, const double* q, const double* v, int64_t n,
+                          int64_t ld, double* phi, double* w, cudaStream_t s)
+{
+    if (n <= 0) return SCP3GPU_OK;
+    if (ld % kExpRows != 0) return fail(SCP3GPU_ERR_ARG, "expand_fp64_sm: ld is not a whole number of row blocks");
+    const size_t sm = sizeof(double) * nm * kExpSamples;
+    if (sm > 48 * 1024)
+        SCP3_CUDA(cudaFuncSetAttribute(expand_fp64_sm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    dim3 grid((unsigned)((n + kExpSamples - 1) / kExpSamples), (unsigned)(ld / kExpRows));
+    expand_fp64_sm_kernel<<<grid, kExpRows, sm, s>>>(desc, nb, nm, q, v, n, ld, phi, w);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
+}
 
 int launch_expand_fp64(const uint32_t* desc, int nb, int nb_pad, int nm, const double* q, const double* v, int64_t n,
                        int64_t ldk, double* phi, double* w, cudaStream_t s)

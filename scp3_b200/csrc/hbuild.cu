@@ -67,6 +67,7 @@ struct scp3gpu_hbuild {
     double *phi = nullptr, *w = nullptr;
     double* vq = nullptr;             // gradient path: dV_anh/dq of the selected modes, [chunk][nmodes]
     bool gradient = false;
+    SteinPlan sp{};                   // gradient path: tables, operands and sums
     double* partial = nullptr;
     tc::Plan tcp{};
     // read-out
@@ -111,19 +112,31 @@ struct Timed {
     }
 };
 
-// Samples per device pass and the split of each pass over CTAs of a tile.
+// Samples per device pass and the split of each pass over CTAs of a tile, plain
+// FP64 form with the direct estimator: 128 x 128 tiles with one CTA per SM
+// (contract_fp64_t128_kernel), in passes of 2^14 samples by default (fewer where
+// Phi and W of a pass would pass ~4 GB).  Sample ranges per tile (nsplit, a
+// power of two, each range at least 2048 samples) minimise the waves of units
+// per unit of work: the units of a pass run in ceil(units / sms) waves.  (The
+// gradient estimator plans its own passes: stein_create.)
 void plan_fp64(scp3gpu_hbuild* h, int sms)
 {
-    h->tm.tile = 64;
-    h->tm.nt = (h->nb + 63) / 64;
+    const int T = 128;
+    h->tm.tile = T;
+    h->tm.nt = (h->nb + T - 1) / T;
     h->tm.ntiles = h->tm.nt * (h->tm.nt + 1) / 2;
-    h->nb_pad = h->tm.nt * 64;
-    int64_t chunk = h->cfg.chunk > 0 ? h->cfg.chunk : 4096;
+    h->nb_pad = h->tm.nt * T;
+    int64_t chunk = h->cfg.chunk > 0 ? h->cfg.chunk : 16384;
     // keep Phi and W of one pass under ~4 GB
     while (chunk > 4096 && (int64_t)h->nb_pad * chunk * 16 > (4ll << 30)) chunk /= 2;
     h->chunk = chunk;
     int nsplit = 1;
-    while ((int64_t)h->tm.ntiles * nsplit < 2ll * sms && chunk / (nsplit * 2) >= 64) nsplit *= 2;
+    double best = 1e300;
+    for (int ns = 1; chunk / ns >= 2048 && chunk % (16ll * ns) == 0; ns *= 2) {
+        const int64_t units = (int64_t)h->tm.ntiles * ns;
+        const double cost = (double)((units + sms - 1) / sms) / ns;   // waves per unit of work
+        if (cost < best - 1e-9) best = cost, nsplit = ns;
+    }
     h->nsplit = nsplit;
 }
 
@@ -216,17 +229,16 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     if (consumed) SCP3_CUDA(cudaEventRecord(consumed, h->stream));
     if (h->gradient) {
         Timed t(h, 2);
-        return launch_stein_fp64(h->desc, h->nb, h->cfg.nmodes, h->q64, h->v, h->vq, a.n, h->tm, h->nsplit,
-                                 h->partial, h->stream);
+        return stein_pass(h->sp, h->desc, h->q64, h->v, h->vq, a.n, h->stream);
     }
     {
         Timed t(h, 1);
-        rc = launch_expand_fp64(h->desc, h->nb, h->nb_pad, h->cfg.nmodes, h->q64, h->v, a.n, h->chunk, h->phi, h->w,
-                                h->stream);
+        rc = launch_expand_fp64_sm(h->desc, h->nb, h->cfg.nmodes, h->q64, h->v, a.n, h->nb_pad, h->phi, h->w,
+                                   h->stream);
     }
     if (rc) return rc;
     Timed t(h, 2);
-    return launch_contract_fp64(h->phi, h->w, h->chunk, a.n, h->nb_pad, h->tm, h->nsplit, h->partial, h->stream);
+    return launch_contract_fp64_t128(h->phi, h->w, h->nb_pad, a.n, h->tm, h->nsplit, h->partial, h->stream);
 }
 
 }  // namespace
@@ -262,7 +274,9 @@ int drain_prep(scp3gpu_hbuild* h)
 int zero_sums(scp3gpu_hbuild* h)
 {
     if (h->split_form) return tc::zero(h->tcp, h->stream);
-    SCP3_CUDA(cudaMemsetAsync(h->partial, 0, sizeof(double) * (size_t)h->nsplit * h->tm.ntiles * 64 * 64, h->stream));
+    if (h->gradient) return stein_zero(h->sp, h->stream);
+    SCP3_CUDA(cudaMemsetAsync(h->partial, 0, sizeof(double) * (size_t)h->nsplit * h->tm.ntiles * h->tm.tile *
+                                                 h->tm.tile, h->stream));
     return SCP3GPU_OK;
 }
 
@@ -474,6 +488,7 @@ int scp3gpu_hbuild_destroy(scp3gpu_hbuild* h)
     for (void* p : ptrs)
         if (p) cudaFree(p);
     tc::destroy(h->tcp);
+    stein_destroy(h->sp);
     for (int b = 0; b < 2; b++) {
         if (h->copied[b]) cudaEventDestroy(h->copied[b]);
         if (h->consumed[b]) cudaEventDestroy(h->consumed[b]);
@@ -583,15 +598,20 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
         h->v = h->vb[0];
     } else {
         h->gradient = c->estimator == SCP3GPU_ESTIMATOR_GRADIENT;
-        plan_fp64(h, sms);
-        if ((rc = dalloc(&h->q64, (size_t)h->chunk * c->nmodes)) || (rc = dalloc(&h->v, (size_t)h->chunk)) ||
-            (rc = dalloc(&h->partial, (size_t)h->nsplit * h->tm.ntiles * 64 * 64)))
-            return bail(rc);
         if (h->gradient) {
-            if ((rc = dalloc(&h->vq, (size_t)h->chunk * c->nmodes))) return bail(rc);
-        } else if ((rc = dalloc(&h->phi, (size_t)h->nb_pad * h->chunk)) ||
-                   (rc = dalloc(&h->w, (size_t)h->nb_pad * h->chunk))) {
-            return bail(rc);
+            if ((rc = stein_create(h->sp, desc, c->nmodes, c->chunk, sms))) return bail(rc);
+            h->chunk = h->sp.chunk;
+            h->nsplit = h->sp.nsplit;
+            h->nb_pad = h->sp.nb_pad;
+            if ((rc = dalloc(&h->q64, (size_t)h->chunk * c->nmodes)) || (rc = dalloc(&h->v, (size_t)h->chunk)) ||
+                (rc = dalloc(&h->vq, (size_t)h->chunk * c->nmodes)))
+                return bail(rc);
+        } else {
+            plan_fp64(h, sms);
+            if ((rc = dalloc(&h->q64, (size_t)h->chunk * c->nmodes)) || (rc = dalloc(&h->v, (size_t)h->chunk)) ||
+                (rc = dalloc(&h->partial, (size_t)h->nsplit * h->tm.ntiles * h->tm.tile * h->tm.tile)) ||
+                (rc = dalloc(&h->phi, (size_t)h->nb_pad * h->chunk)) || (rc = dalloc(&h->w, (size_t)h->nb_pad * h->chunk)))
+                return bail(rc);
         }
     }
     if ((rc = zero_sums(h))) return bail(rc);
@@ -666,9 +686,9 @@ int scp3gpu_hbuild_add_epot(scp3gpu_hbuild* h, const double* q, const double* V,
         } else {
             SCP3_CUDA(cudaMemsetAsync(h->q64, 0, sizeof(double) * kn * nm, h->stream));
             SCP3_CUDA(cudaMemcpyAsync(h->q64, q + off * nm, sizeof(double) * c * nm, cudaMemcpyHostToDevice, h->stream));
-            rc = launch_expand_fp64(h->desc, h->nb, h->nb_pad, nm, h->q64, h->v, kn, h->chunk, h->phi, h->w, h->stream);
-            if (!rc) rc = launch_contract_fp64(h->phi, h->w, h->chunk, kn, h->nb_pad, h->tm, h->nsplit, h->partial,
-                                               h->stream);
+            rc = launch_expand_fp64_sm(h->desc, h->nb, nm, h->q64, h->v, kn, h->nb_pad, h->phi, h->w, h->stream);
+            if (!rc) rc = launch_contract_fp64_t128(h->phi, h->w, h->nb_pad, kn, h->tm, h->nsplit, h->partial,
+                                                    h->stream);
             SCP3_CUDA(cudaStreamSynchronize(h->stream));
         }
         if (rc) return rc;
@@ -695,8 +715,7 @@ int scp3gpu_hbuild_add_epot_grad(scp3gpu_hbuild* h, const double* q, const doubl
         SCP3_CUDA(cudaMemcpyAsync(h->v, V + off, sizeof(double) * c, cudaMemcpyHostToDevice, h->stream));
         SCP3_CUDA(cudaMemcpyAsync(h->q64, q + off * nm, sizeof(double) * c * nm, cudaMemcpyHostToDevice, h->stream));
         SCP3_CUDA(cudaMemcpyAsync(h->vq, Vq + off * nm, sizeof(double) * c * nm, cudaMemcpyHostToDevice, h->stream));
-        int rc = launch_stein_fp64(h->desc, h->nb, nm, h->q64, h->v, h->vq, kn, h->tm, h->nsplit, h->partial,
-                                   h->stream);
+        int rc = stein_pass(h->sp, h->desc, h->q64, h->v, h->vq, kn, h->stream);
         SCP3_CUDA(cudaStreamSynchronize(h->stream));
         if (rc) return rc;
         h->count += c;
@@ -722,6 +741,7 @@ static int build_dense(scp3gpu_hbuild* h, int mode)
     }
     Timed t(h, 3);
     if (h->split_form) return tc::unpack(h->tcp, h->nb, divisor, diag, zpe, h->dense, h->nb, h->stream);
+    if (h->gradient) return stein_unpack(h->sp, h->desc, divisor, diag, zpe, h->dense, h->nb, h->stream);
     return launch_unpack(h->partial, h->tm, h->nsplit, h->nb, divisor, diag, zpe, h->dense, h->nb, h->stream);
 }
 

@@ -149,11 +149,37 @@ int launch_std_normal(int dims, int64_t index0, int64_t n, const int64_t* vdir, 
 int launch_expand_fp64(const uint32_t* desc, int nb, int nb_pad, int nm, const double* q, const double* v,
                        int64_t n, int64_t ldk, double* phi, double* w, cudaStream_t s);
 
-struct TileMap;
-// Gradient (Stein) estimator, FP64: partial[split][tile] += sum over this split's
-// samples of the estimate of every upper element (q, vq: [k][nm], v: [k]).
-int launch_stein_fp64(const uint32_t* desc, int nb, int nm, const double* q, const double* v, const double* vq,
-                      int64_t k, const TileMap& tm, int nsplit, double* partial, cudaStream_t s);
+// Gradient (Stein) estimator, FP64, as products of reduced basis functions
+// (stein.cu).  Virtual rows (m, i): basis function i that excites mode m, ordered
+// by m then i, plus one last row for <0|V|0>.
+struct SteinPlan {
+    int nb = 0, nb_pad = 0, nm = 0;
+    int nv = 0, nv_pad = 0;          // virtual rows (with the ground row), padded to 128
+    int rt = 0, ct = 0;              // 128-row tiles of the virtual rows and of the basis
+    int nsplit = 1;
+    int64_t chunk = 0;               // samples per pass
+    int64_t dsize = 0;               // doubles of the same-mode pair sums per split
+    int ndtasks = 0;
+    uint32_t* vrdesc = nullptr;      // [nv] mode, level, the other factors of the row's function
+    int* rank3 = nullptr;            // [nb * 3] rank of function i in E_m for its k-th mode
+    int* voff = nullptr;             // [nm + 1] first virtual row of mode m
+    int64_t* doff = nullptr;         // [nm] first same-mode pair sum of mode m
+    int4* dtasks = nullptr;          // [ndtasks] (m, row tile, column tile) of the pair kernel
+    double* W = nullptr;             // [chunk][nv_pad]  reduced function x Stein weight
+    double* Phi = nullptr;           // [chunk][nb_pad]  basis functions
+    double* C = nullptr;             // [nsplit][rt * ct][128 * 128]
+    double* D = nullptr;             // [nsplit][dsize]
+};
+int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_t chunk, int sms);
+void stein_destroy(SteinPlan& p);
+int stein_zero(const SteinPlan& p, cudaStream_t s);
+// One pass of k samples (k a multiple of 16 * nsplit; q, vq: [k][nm], v: [k]).
+int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const double* v, const double* vq,
+               int64_t k, cudaStream_t s);
+// The dense column-major nb x nb estimate (both triangles), divided by `divisor`;
+// with `diag` the diagonal becomes (v + diag[i]) + zpe, as launch_unpack.
+int stein_unpack(const SteinPlan& p, const uint32_t* desc, double divisor, const double* diag, double zpe,
+                 double* M, int64_t ld, cudaStream_t s);
 
 struct TileMap {
     int tile;          // tile edge (64 FP64, 128 tensor-core)
@@ -163,6 +189,19 @@ struct TileMap {
 // P[split][tile][tile*tile] += sum over this split's sample range of Phi_i W_j.
 int launch_contract_fp64(const double* phi, const double* w, int64_t ldk, int64_t k, int nb_pad,
                          const TileMap& tm, int nsplit, double* partial, cudaStream_t s);
+
+// The plain build's form: Phi and W sample-major ([k][ld], ld = tm.nt * 128),
+// P[split][tile][128*128] += sum over this split's sample range of Phi_i W_j.
+int launch_expand_fp64_sm(const uint32_t* desc, int nb, int nm, const double* q, const double* v, int64_t n,
+                          int64_t ld, double* phi, double* w, cudaStream_t s);
+int launch_contract_fp64_t128(const double* phi, const double* w, int64_t ld, int64_t k, const TileMap& tm,
+                              int nsplit, double* partial, cudaStream_t s);
+
+// P[split][ti * ct + tj][128*128] += sum over this split's sample range of
+// A[k][ti*128 + r] B[k][tj*128 + c] (sample-major operands, every tile of the
+// rt x ct rectangle).
+int launch_gemm_fp64_rect(const double* A, int64_t lda, const double* B, int64_t ldb, int64_t k, int rt, int ct,
+                          int nsplit, double* partial, cudaStream_t s);
 
 // Sum the splits of P into a dense column-major nb x nb matrix (upper triangle
 // mirrored to the lower), divided by `divisor`; with `diag` (length nb) the

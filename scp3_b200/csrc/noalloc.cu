@@ -10,8 +10,10 @@
 // file-scope __device__ array of kStaticScratchBytes (64 MiB), which every GPU
 // that loads the library keeps until the process exits.
 //
-// It computes exactly what scp3gpu_hbuild_add_epot computes (the same expansion
-// and FP64 tile kernels), adding sum_s Phi(q_s) V_s Phi(q_s)^T into M.
+// It computes what scp3gpu_hbuild_add_epot computes, sum_s Phi(q_s) V_s
+// Phi(q_s)^T added into M, in FP64 with the same basis expansion; its
+// contraction is the 64 x 64 tile kernel, whose partial sums take a quarter of
+// the space of the build's 128 x 128 tiles.
 //
 // Rules of use:
 //  * The first call on a device looks up the array's device address

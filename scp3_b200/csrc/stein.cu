@@ -1,6 +1,6 @@
 // The gradient (default) estimator of SCP3: addEpot(q, V, Vq, M)
 // (ScaledMatrixElements.cpp:102-725 with the formulas of TripleExcitations.h),
-// FP64, on the upper-triangle 64x64 tiles of the plain form.
+// FP64, as dense products on the FP64 pipe.
 //
 // Every formula of the reference follows one rule.  For the pair (i, j) let S be
 // the modes either function excites and p_m(q_m) = h_a(q_m) h_b(q_m) the
@@ -14,17 +14,22 @@
 // rule and is reproduced as written: <3_m|V|3_m> (TripleExcitations.h:763-773)
 // carries (q^2 - 3) V where the identity gives (10 q^2 - 3) V.
 //
-// Layout: a CTA owns one upper 64x64 tile and one range of samples (split);
-// 256 threads hold a 4x4 fragment each.  Every factor above depends on one
-// mode, its two levels and the sample, so the samples are taken in small
-// chunks and, per sample and mode, a table of the 16 level pairs (a, b) holds
-// p_ab and t_ab = (p_ab(0) + r_ab'/2) V + (r_ab/2) dV/dq_m.  An element is
-// then up to six table slots (its mode set; spare slots point at an entry with
-// p = 1, t = 0, and <0|V|0> at one with t = V), and its estimate is
-// (1/|S|) sum_u t_u prod_{u' != u} p_u' from prefix and suffix products.  The
-// slot indices of the thread's 16 elements are formed once and kept in
-// registers.  Partials: [split][tile][64 x 64] row-major within the tile, as
-// the plain -G form, so the same read-out applies.
+// As products.  prod_{m' != m} p_m' = R_i^m R_j^m, where R_i^m is function i
+// without its mode-m factor, and the bracket is K^m_ab = u_ab(q_m) V + w_ab(q_m)
+// dV/dq_m, which depends on the pair only through the levels (a, b) of i and j
+// in mode m.  When j does not excite m (b = 0), R_j^m = Phi_j, so
+//     T^m_ij = sum_s [R_i^m K^m_a0](s) Phi_j(s)
+// is one row of a product W Phi^T, with one "virtual row" W_(m,i) = R_i^m K^m_a0
+// per (mode, function exciting it): 2352 rows against 1225 columns for the
+// hexamer doubles basis, an FP64 GEMM (contract_fp64.cu, rectangular form).
+// When both excite m, T^m_ij = sum_s R_i^m R_j^m K^m_ab is a pair sum over the
+// functions exciting m, kept per mode (stein_pairs_kernel; 48 x 49^2 pairs for
+// the hexamer doubles basis against 48 x 49 x 1225 products in the GEMM).  The
+// read-out forms each element from its |S| <= 6 terms and divides by |S|;
+// <0|V|0> comes from one more virtual row, W = V, against Phi_0 = 1.
+//
+// Every sum runs over samples in a fixed order per (split, tile) and the splits
+// are added in order at read-out, so results are deterministic.
 #include <algorithm>
 
 #include "internal.h"
@@ -33,11 +38,8 @@ namespace scp3 {
 
 namespace {
 
-constexpr int kT = 64;
-constexpr int kMaxS = 6;
-
 // (mode, level) list of a basis descriptor (kind | m << 3 | n << 11 | p << 19)
-__device__ __forceinline__ int decode(uint32_t d, int* m, int* l)
+__host__ __device__ __forceinline__ int decode(uint32_t d, int* m, int* l)
 {
     const int kind = (int)(d & 7u), a = (int)((d >> 3) & 255u), b = (int)((d >> 11) & 255u), c = (int)(d >> 19);
     switch (kind) {
@@ -52,8 +54,18 @@ __device__ __forceinline__ int decode(uint32_t d, int* m, int* l)
     }
 }
 
+// h_l(q) (HarmonicOscillatorBasis.cpp: 1, sqrt2 q, (2q^2 - 1)/sqrt2, (2q^3 - 3q)/sqrt3)
+__device__ __forceinline__ double ho(int l, double q)
+{
+    switch (l) {
+        case 0: return 1.0;
+        case 1: return 1.4142135623730951 * q;
+        case 2: return (2.0 * q * q - 1.0) * 0.70710678118654752;
+        default: return (2.0 * q * q - 3.0) * q * 0.57735026918962576;
+    }
+}
+
 // h_a(q), h_a(0), h_a'(q), d_a(q), d_a'(q) for the oscillator functions h_0..h_3
-// (HarmonicOscillatorBasis.cpp: sqrt2 q, (2q^2 - 1)/sqrt2, (2q^3 - 3q)/sqrt3)
 __device__ __forceinline__ void ho_parts(int a, double q, double& h, double& h0, double& dh, double& d, double& dd)
 {
     constexpr double s2 = 1.4142135623730951, is2 = 0.70710678118654752, is3 = 0.57735026918962576;
@@ -66,152 +78,360 @@ __device__ __forceinline__ void ho_parts(int a, double q, double& h, double& h0,
     }
 }
 
-// Table entry of mode m, levels (a, b) at q = x: p and the two Stein coefficients.
-__device__ __forceinline__ void stein_entry(int a, int b, double x, double& p, double& u, double& w)
+// K_ab = u V + w dV/dq_m for mode m at q_m = x, levels (a, b)
+__device__ __forceinline__ double stein_weight(int a, int b, double x, double V, double Vm)
 {
     double ha, ha0, dha, da, dda, hb, hb0, dhb, db, ddb;
     ho_parts(a, x, ha, ha0, dha, da, dda);
     ho_parts(b, x, hb, hb0, dhb, db, ddb);
     const double r = da * hb + ha0 * db;
     const double dr = dda * hb + da * dhb + ha0 * ddb;
-    p = ha * hb;
-    u = ha0 * hb0 + 0.5 * dr;
-    w = 0.5 * r;
+    double u = ha0 * hb0 + 0.5 * dr;
+    const double w = 0.5 * r;
     if (a == 3 && b == 3) u = (2 * x * x - 3) * (x * x - 3) * (1.0 / 6.0);   // TripleExcitations.h:763-773
+    return u * V + w * Vm;
 }
 
-constexpr int kSlots = 6;
-__constant__ double kInvNs[kSlots + 1] = {0.0, 1.0, 1.0 / 2, 1.0 / 3, 1.0 / 4, 1.0 / 5, 1.0 / 6};
+// Virtual row descriptor: m | a << 8 | m1 << 10 | l1 << 18 | m2 << 20 | l2 << 28,
+// (m1, l1), (m2, l2) the function's other factors (level 0: none); bit 30: the
+// ground row (W = V).
+constexpr uint32_t kGroundRow = 1u << 30;
 
-__global__ void __launch_bounds__(256, 2) stein_fp64_kernel(const uint32_t* __restrict__ desc, int nb, int nm,
-                                                             const double* __restrict__ q,
-                                                             const double* __restrict__ v,
-                                                             const double* __restrict__ vq, int64_t kps, int chunk,
-                                                             int nt, int ntiles, double* __restrict__ partial)
+__device__ __forceinline__ double reduced(uint32_t vd, const double* qs, int stride, int j)
 {
-    extern __shared__ __align__(16) double2 tab[];   // [chunk][nm * 16 + 2] (p, t), then the slot words
-    const int per = nm * 16 + 2;                     // + the p = 1, t = 0 entry and the t = V entry
-    uint32_t* slw = reinterpret_cast<uint32_t*>(tab + (size_t)chunk * per);   // [16 x 3 words][thread]
-    const int kOne = nm * 16, kV = nm * 16 + 1;
-    int t = blockIdx.x, ti = 0;
-    while (t >= nt - ti) {
-        t -= nt - ti;
-        ti++;
-    }
-    const int tj = ti + t;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int m1 = (vd >> 10) & 255, l1 = (vd >> 18) & 3, m2 = (vd >> 20) & 255, l2 = (vd >> 28) & 3;
+    double r = 1.0;
+    if (l1) r *= ho(l1, qs[m1 * stride + j]);
+    if (l2) r *= ho(l2, qs[m2 * stride + j]);
+    return r;
+}
 
-    // slot indices of the thread's 16 elements, two 16-bit indices per word; the
-    // element's |S| rides in bits 12-15 of word 0 (|S| <= 6; 0 = skip).  Kept in
-    // shared memory, [word][thread], so the registers stay with the arithmetic.
-    auto SL = [&](int e, int wd) -> uint32_t& { return slw[(size_t)(3 * e + wd) * 256 + tid]; };
-#pragma unroll 1
-    for (int e = 0; e < 16; e++) {
-        const int gi = ti * kT + ty + 16 * (e >> 2), gj = tj * kT + tx + 16 * (e & 3);
-        int idx[kSlots];
-#pragma unroll
-        for (int u = 0; u < kSlots; u++) idx[u] = kOne;
-        int ns = 0;
-        if (gi <= gj && gj < nb) {
-            int mi[3], li[3], mj[3], lj[3];
-            const int ni = decode(__ldg(desc + gi), mi, li), nj = decode(__ldg(desc + gj), mj, lj);
-            int S[kSlots], A[kSlots], B[kSlots];
-            for (int k = 0; k < ni; k++) S[ns] = mi[k], A[ns] = li[k], B[ns] = 0, ns++;
-            for (int k = 0; k < nj; k++) {
-                int f = -1;
-                for (int u = 0; u < ns; u++)
-                    if (S[u] == mj[k]) f = u;
-                if (f >= 0) B[f] = lj[k];
-                else S[ns] = mj[k], A[ns] = 0, B[ns] = lj[k], ns++;
-            }
-#pragma unroll
-            for (int u = 0; u < kSlots; u++)
-                if (u < ns) idx[u] = S[u] * 16 + A[u] * 4 + B[u];
-            if (ns == 0) {                 // <0|V|0> = V
-                idx[0] = kV;
-                ns = 1;
-            }
+constexpr int kExpS = 64, kExpR = 128;
+
+// Phi [s][j] (ld nb_pad) and W [s][r] (ld nv_pad) for 64 samples; one thread per
+// row of the stacked [Phi rows | W rows], coalesced 1 KB stores per sample.
+__global__ void __launch_bounds__(kExpR) stein_expand_kernel(const uint32_t* __restrict__ desc, int nb, int nb_pad,
+                                                             const uint32_t* __restrict__ vrdesc, int nv,
+                                                             int nv_pad, int nm, const double* __restrict__ q,
+                                                             const double* __restrict__ v,
+                                                             const double* __restrict__ vq, int64_t n,
+                                                             double* __restrict__ Phi, double* __restrict__ W)
+{
+    extern __shared__ double st[];          // q [nm][64], vq [nm][64], V [64]
+    double* qs = st;
+    double* vqs = st + (size_t)nm * kExpS;
+    double* vs = vqs + (size_t)nm * kExpS;
+    const int t = threadIdx.x;
+    const int64_t s0 = (int64_t)blockIdx.x * kExpS;
+    for (int e = t; e < nm * kExpS; e += kExpR) {
+        const int ss = e / nm, m = e - ss * nm;          // coalesced reads of row s0 + ss
+        const bool ok = s0 + ss < n;
+        qs[m * kExpS + ss] = ok ? q[(s0 + ss) * nm + m] : 0.0;
+        vqs[m * kExpS + ss] = ok ? vq[(s0 + ss) * nm + m] : 0.0;
+    }
+    for (int ss = t; ss < kExpS; ss += kExpR) vs[ss] = s0 + ss < n ? v[s0 + ss] : 0.0;
+    __syncthreads();
+    const int ns = (int)min((int64_t)kExpS, n - s0);
+    const int row = blockIdx.y * kExpR + t;
+    if (row < nb_pad) {
+        int mm[3], ll[3], k = 0;
+        if (row < nb) k = decode(__ldg(desc + row), mm, ll);
+        for (int j = 0; j < ns; j++) {
+            double x = row < nb ? 1.0 : 0.0;
+            for (int u = 0; u < k; u++) x *= ho(ll[u], qs[mm[u] * kExpS + j]);
+            Phi[(size_t)(s0 + j) * nb_pad + row] = x;
         }
-        SL(e, 0) = (uint32_t)idx[0] | ((uint32_t)ns << 12) | ((uint32_t)idx[1] << 16);
-        SL(e, 1) = (uint32_t)idx[2] | ((uint32_t)idx[3] << 16);
-        SL(e, 2) = (uint32_t)idx[4] | ((uint32_t)idx[5] << 16);
-    }
-    double acc[16];
-#pragma unroll
-    for (int e = 0; e < 16; e++) acc[e] = 0.0;
-
-    const int64_t s0 = (int64_t)blockIdx.y * kps;
-    for (int64_t c0 = 0; c0 < kps; c0 += chunk) {
-        const int nc = (int)(kps - c0 < chunk ? kps - c0 : chunk);
-        __syncthreads();
-        for (int k = tid; k < nc * per; k += blockDim.x) {
-            const int j = k / per, id = k - j * per;
-            const int64_t smp = s0 + c0 + j;
-            double2 ent;
-            if (id >= kOne) {
-                ent = make_double2(1.0, id == kV ? v[smp] : 0.0);
-            } else {
-                const int m = id >> 4, a = (id >> 2) & 3, b = id & 3;
-                double p, u, w;
-                stein_entry(a, b, q[smp * nm + m], p, u, w);
-                ent = make_double2(p, u * v[smp] + w * vq[smp * nm + m]);
+    } else {
+        const int r = row - nb_pad;
+        const uint32_t vd = r < nv ? __ldg(vrdesc + r) : 0u;
+        const int m = vd & 255, a = (vd >> 8) & 3;
+        for (int j = 0; j < ns; j++) {
+            double x = 0.0;
+            if (r < nv) {
+                if (vd & kGroundRow) x = vs[j];
+                else x = reduced(vd, qs, kExpS, j) * stein_weight(a, 0, qs[m * kExpS + j], vs[j], vqs[m * kExpS + j]);
             }
-            tab[k] = ent;
+            W[(size_t)(s0 + j) * nv_pad + r] = x;
+        }
+    }
+}
+
+// Same-mode pair sums D^m[ri][rj] += sum_s R_i^m R_j^m K^m_{a_i b_j} over the
+// functions exciting m (ranks ri <= rj), one 64 x 64 tile of ranks per CTA,
+// 4 x 4 elements per thread; samples in chunks of kPS staged in shared memory.
+constexpr int kPS = 16, kPT = 64;
+
+__global__ void __launch_bounds__(256) stein_pairs_kernel(const int4* __restrict__ tasks,
+                                                          const uint32_t* __restrict__ vrdesc,
+                                                          const int* __restrict__ voff,
+                                                          const int64_t* __restrict__ doff, int nm,
+                                                          const double* __restrict__ q,
+                                                          const double* __restrict__ v,
+                                                          const double* __restrict__ vq, int64_t kps,
+                                                          int64_t dsize, double* __restrict__ D)
+{
+    extern __shared__ double ps[];   // q [kPS][nm], V [kPS], Vm [kPS], Rr [kPS][64], Rc [kPS][64], K [kPS][16]
+    double* qs = ps;
+    double* vs = qs + (size_t)kPS * nm;
+    double* vms = vs + kPS;
+    double* Rr = vms + kPS;
+    double* Rc = Rr + kPS * kPT;
+    double* K = Rc + kPS * kPT;
+    const int4 task = tasks[blockIdx.x];
+    const int m = task.x, ti = task.y, tj = task.z;
+    const int v0 = voff[m], e = voff[m + 1] - v0;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    int arow[4], bcol[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const int rr = ti * kPT + ty + 16 * r, rc = tj * kPT + tx + 16 * r;
+        arow[r] = rr < e ? (int)((vrdesc[v0 + rr] >> 8) & 3u) : 0;
+        bcol[r] = rc < e ? (int)((vrdesc[v0 + rc] >> 8) & 3u) : 0;
+    }
+    double acc[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[r][c] = 0.0;
+    const int64_t s0 = (int64_t)blockIdx.y * kps;
+    for (int64_t c0 = 0; c0 < kps; c0 += kPS) {
+        const int nc = (int)min((int64_t)kPS, kps - c0);
+        __syncthreads();
+        for (int x = tid; x < nc * nm; x += 256) qs[x] = q[(s0 + c0) * nm + x];
+        for (int j = tid; j < nc; j += 256) {
+            vs[j] = v[s0 + c0 + j];
+            vms[j] = vq[(s0 + c0 + j) * nm + m];
+        }
+        __syncthreads();
+        for (int x = tid; x < nc * (2 * kPT + 16); x += 256) {
+            const int j = x / (2 * kPT + 16), y = x - j * (2 * kPT + 16);
+            if (y < 2 * kPT) {
+                const int rk = (y < kPT ? ti : tj) * kPT + (y & (kPT - 1));
+                double val = 0.0;
+                if (rk < e) val = reduced(vrdesc[v0 + rk], qs + (size_t)j * nm, 1, 0);
+                (y < kPT ? Rr : Rc)[j * kPT + (y & (kPT - 1))] = val;
+            } else {
+                const int ab = y - 2 * kPT, a = ab >> 2, b = ab & 3;
+                K[j * 16 + ab] = (a && b) ? stein_weight(a, b, qs[(size_t)j * nm + m], vs[j], vms[j]) : 0.0;
+            }
         }
         __syncthreads();
         for (int j = 0; j < nc; j++) {
-            const double2* T = tab + (size_t)j * per;
+            double rr[4], rc[4];
 #pragma unroll
-            for (int e = 0; e < 16; e++) {
-                const uint32_t w0 = SL(e, 0);
-                const int ns = (int)((w0 >> 12) & 15u);
-                if (ns == 0) continue;
-                const uint32_t w1 = SL(e, 1), w2 = SL(e, 2);
-                double2 x[kSlots];
-                x[0] = T[w0 & 0xfffu];
-                x[1] = T[w0 >> 16];
-                x[2] = T[w1 & 0xffffu];
-                x[3] = T[w1 >> 16];
-                x[4] = T[w2 & 0xffffu];
-                x[5] = T[w2 >> 16];
-                // sum_u t_u prod_{u' != u} p_u' over the six slots (spare ones p = 1, t = 0)
-                double pre = 1.0, tot = 0.0;
-                double suf[kSlots];
-                suf[kSlots - 1] = 1.0;
+            for (int r = 0; r < 4; r++) rr[r] = Rr[j * kPT + ty + 16 * r], rc[r] = Rc[j * kPT + tx + 16 * r];
 #pragma unroll
-                for (int u = kSlots - 1; u > 0; u--) suf[u - 1] = suf[u] * x[u].x;
+            for (int r = 0; r < 4; r++)
 #pragma unroll
-                for (int u = 0; u < kSlots; u++) {
-                    tot += x[u].y * (pre * suf[u]);
-                    pre *= x[u].x;
-                }
-                acc[e] += tot * kInvNs[ns];
-            }
+                for (int c = 0; c < 4; c++) acc[r][c] = fma(rr[r], rc[c] * K[j * 16 + arow[r] * 4 + bcol[c]], acc[r][c]);
         }
     }
-    double* P = partial + ((size_t)blockIdx.y * ntiles + blockIdx.x) * (kT * kT);
+    double* Dp = D + (size_t)blockIdx.y * dsize + doff[m];
 #pragma unroll
-    for (int e = 0; e < 16; e++) {
-        const int lr = ty + 16 * (e >> 2), lc = tx + 16 * (e & 3);
-        P[lr * kT + lc] += acc[e];
-    }
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int rr = ti * kPT + ty + 16 * r, rc = tj * kPT + tx + 16 * c;
+            if (rr < e && rc < e && rr <= rc) Dp[(size_t)rr * e + rc] += acc[r][c];
+        }
 }
+
+// Element (i, j) of the dense matrix from its terms: for each mode m that r =
+// min(i, j) or c = max(i, j) excites, C at virtual row (m, r) column c, or at
+// (m, c) column r, or the pair sum D^m when both excite m; the mean over those
+// modes; <0|V|0> from the ground row.
+__global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int* __restrict__ rank3,
+                                    const int* __restrict__ voff, const int64_t* __restrict__ doff, int nb, int nv,
+                                    int ct, int nsplit, const double* __restrict__ C, const double* __restrict__ D,
+                                    int64_t csize, int64_t dsize, double divisor, const double* __restrict__ diag,
+                                    double zpe, double* __restrict__ M, int64_t ld)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)nb * nb) return;
+    const int j = (int)(e / nb), i = (int)(e - (int64_t)j * nb);
+    const int r = min(i, j), c = max(i, j);
+    auto cidx = [&](int vr, int col) -> int64_t {
+        return ((int64_t)(vr >> 7) * ct + (col >> 7)) * (128 * 128) + (int64_t)(vr & 127) * 128 + (col & 127);
+    };
+    int mr[3], lr[3], mc[3], lc[3];
+    const int nr = decode(desc[r], mr, lr), ncn = decode(desc[c], mc, lc);
+    double val = 0.0;
+    if (nr + ncn == 0) {   // <0|V|0>
+        const int64_t x = cidx(nv - 1, 0);
+        for (int s = 0; s < nsplit; s++) val += C[s * csize + x];
+    } else {
+        int ns = 0;
+        for (int a = 0; a < nr; a++) {
+            int b = -1;
+            for (int k = 0; k < ncn; k++)
+                if (mc[k] == mr[a]) b = k;
+            const int m = mr[a];
+            double t = 0.0;
+            if (b < 0) {
+                const int64_t x = cidx(voff[m] + rank3[3 * r + a], c);
+                for (int s = 0; s < nsplit; s++) t += C[s * csize + x];
+            } else {
+                const int en = voff[m + 1] - voff[m];
+                const int64_t x = doff[m] + (int64_t)rank3[3 * r + a] * en + rank3[3 * c + b];
+                for (int s = 0; s < nsplit; s++) t += D[s * dsize + x];
+            }
+            val += t;
+            ns++;
+        }
+        for (int b = 0; b < ncn; b++) {
+            bool shared = false;
+            for (int a = 0; a < nr; a++) shared |= mr[a] == mc[b];
+            if (shared) continue;
+            const int64_t x = cidx(voff[mc[b]] + rank3[3 * c + b], r);
+            double t = 0.0;
+            for (int s = 0; s < nsplit; s++) t += C[s * csize + x];
+            val += t;
+            ns++;
+        }
+        val /= (double)ns;
+    }
+    val = val / divisor;
+    if (diag && i == j) val = (val + diag[i]) + zpe;
+    M[(size_t)j * ld + i] = val;
+}
+
+int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
 }  // namespace
 
-int launch_stein_fp64(const uint32_t* desc, int nb, int nm, const double* q, const double* v, const double* vq,
-                      int64_t k, const TileMap& tm, int nsplit, double* partial, cudaStream_t s)
+int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_t chunk_cfg, int sms)
 {
-    if (tm.tile != kT || k % nsplit != 0) return fail(SCP3GPU_ERR_ARG, "stein: shapes not tiled");
-    if (nm * 16 + 2 > 0xfff) return fail(SCP3GPU_ERR_ARG, "stein: too many modes for the slot encoding");
+    p = SteinPlan{};
+    p.nb = (int)desc.size();
+    p.nm = nm;
+    p.nb_pad = (int)round_up(p.nb, 128);
+    if (sizeof(double) * (2 * (size_t)nm * kExpS + kExpS) > 227 * 1024)
+        return fail(SCP3GPU_ERR_ARG, "stein: too many modes for the expansion's shared memory (at most 220)");
+    // functions exciting each mode, in basis order; rank of each in its mode's list
+    std::vector<std::vector<int>> E(nm);
+    std::vector<std::vector<int>> lev(nm);
+    std::vector<int> rank3((size_t)p.nb * 3, 0);
+    std::vector<uint32_t> vr_of_rank;
+    for (int i = 0; i < p.nb; i++) {
+        int mm[3], ll[3];
+        const int k = decode(desc[i], mm, ll);
+        for (int a = 0; a < k; a++) {
+            if (mm[a] >= nm) return fail(SCP3GPU_ERR_ARG, "stein: basis mode out of range");
+            rank3[(size_t)3 * i + a] = (int)E[mm[a]].size();
+            E[mm[a]].push_back(i);
+            lev[mm[a]].push_back(ll[a]);
+        }
+    }
+    std::vector<int> voff(nm + 1, 0);
+    std::vector<int64_t> doff(nm, 0);
+    std::vector<uint32_t> vrdesc;
+    std::vector<int4> tasks;
+    int64_t dsz = 0;
+    for (int m = 0; m < nm; m++) {
+        voff[m] = (int)vrdesc.size();
+        doff[m] = dsz;
+        const int en = (int)E[m].size();
+        dsz += (int64_t)en * en;
+        for (int r = 0; r < en; r++) {
+            int mm[3], ll[3];
+            const int k = decode(desc[E[m][r]], mm, ll);
+            uint32_t d = (uint32_t)m | ((uint32_t)lev[m][r] << 8);
+            int o = 0;
+            for (int a = 0; a < k; a++) {
+                if (mm[a] == m) continue;
+                d |= o == 0 ? ((uint32_t)mm[a] << 10) | ((uint32_t)ll[a] << 18)
+                            : ((uint32_t)mm[a] << 20) | ((uint32_t)ll[a] << 28);
+                o++;
+            }
+            vrdesc.push_back(d);
+        }
+        const int nt = (en + kPT - 1) / kPT;
+        for (int a = 0; a < nt; a++)
+            for (int b = a; b < nt; b++) tasks.push_back(make_int4(m, a, b, 0));
+    }
+    voff[nm] = (int)vrdesc.size();
+    vrdesc.push_back(kGroundRow);
+    p.nv = (int)vrdesc.size();
+    p.nv_pad = (int)round_up(p.nv, 128);
+    p.rt = p.nv_pad / 128;
+    p.ct = p.nb_pad / 128;
+    p.dsize = std::max<int64_t>(dsz, 1);
+    p.ndtasks = (int)tasks.size();
+    // passes of 2^14 samples (fewer while W and Phi of a pass would pass ~4 GB);
+    // sample ranges per tile as the plain form chooses them, the C partials of
+    // all ranges held under ~8 GB (one range if a single one is larger)
+    int64_t chunk = chunk_cfg > 0 ? chunk_cfg : 16384;
+    while (chunk > 4096 && (int64_t)(p.nv_pad + p.nb_pad) * chunk * 8 > (4ll << 30)) chunk /= 2;
+    p.chunk = chunk;
+    const int64_t csize = (int64_t)p.rt * p.ct * 128 * 128;
+    double best = 1e300;
+    p.nsplit = 1;
+    for (int ns = 1; chunk / ns >= 2048 && chunk % (16ll * ns) == 0; ns *= 2) {
+        if (ns > 1 && (csize + p.dsize) * 8 * ns > (8ll << 30)) break;
+        const int64_t units = (int64_t)p.rt * p.ct * ns;
+        const double cost = (double)((units + sms - 1) / sms) / ns;
+        if (cost < best - 1e-9) best = cost, p.nsplit = ns;
+    }
+    int rc;
+    if ((rc = upload(&p.vrdesc, vrdesc.data(), vrdesc.size())) || (rc = upload(&p.rank3, rank3.data(), rank3.size())) ||
+        (rc = upload(&p.voff, voff.data(), voff.size())) || (rc = upload(&p.doff, doff.data(), doff.size())) ||
+        (p.ndtasks && (rc = upload(&p.dtasks, tasks.data(), tasks.size()))) ||
+        (rc = dalloc(&p.W, (size_t)p.chunk * p.nv_pad)) || (rc = dalloc(&p.Phi, (size_t)p.chunk * p.nb_pad)) ||
+        (rc = dalloc(&p.C, (size_t)csize * p.nsplit)) || (rc = dalloc(&p.D, (size_t)p.dsize * p.nsplit))) {
+        stein_destroy(p);
+        return rc;
+    }
+    return SCP3GPU_OK;
+}
+
+void stein_destroy(SteinPlan& p)
+{
+    cudaFree(p.vrdesc), cudaFree(p.rank3), cudaFree(p.voff), cudaFree(p.doff), cudaFree(p.dtasks);
+    cudaFree(p.W), cudaFree(p.Phi), cudaFree(p.C), cudaFree(p.D);
+    p.vrdesc = nullptr, p.rank3 = nullptr, p.voff = nullptr, p.doff = nullptr, p.dtasks = nullptr;
+    p.W = p.Phi = p.C = p.D = nullptr;
+}
+
+int stein_zero(const SteinPlan& p, cudaStream_t s)
+{
+    SCP3_CUDA(cudaMemsetAsync(p.C, 0, sizeof(double) * (size_t)p.rt * p.ct * 128 * 128 * p.nsplit, s));
+    SCP3_CUDA(cudaMemsetAsync(p.D, 0, sizeof(double) * (size_t)p.dsize * p.nsplit, s));
+    return SCP3GPU_OK;
+}
+
+int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const double* v, const double* vq,
+               int64_t k, cudaStream_t s)
+{
     if (k == 0) return SCP3GPU_OK;
-    const size_t per = (size_t)(nm * 16 + 2) * sizeof(double2);
-    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(4, (48 * 1024) / per));
-    const size_t sm = per * chunk + sizeof(uint32_t) * 48 * 256;   // table chunk + slot words
-    if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(stein_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)sm));
-    dim3 grid(tm.ntiles, nsplit);
-    stein_fp64_kernel<<<grid, 256, sm, s>>>(desc, nb, nm, q, v, vq, k / nsplit, chunk, tm.nt, tm.ntiles, partial);
+    if (k > p.chunk || k % (16ll * p.nsplit) != 0) return fail(SCP3GPU_ERR_ARG, "stein: pass not tiled");
+    const size_t es = sizeof(double) * (2 * (size_t)p.nm * kExpS + kExpS);
+    if (es > 48 * 1024)
+        SCP3_CUDA(cudaFuncSetAttribute(stein_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)es));
+    dim3 eg((unsigned)((k + kExpS - 1) / kExpS), (unsigned)((p.nb_pad + p.nv_pad) / kExpR));
+    stein_expand_kernel<<<eg, kExpR, es, s>>>(desc, p.nb, p.nb_pad, p.vrdesc, p.nv, p.nv_pad, p.nm, q, v, vq, k,
+                                              p.Phi, p.W);
+    SCP3_CUDA(cudaGetLastError());
+    int rc = launch_gemm_fp64_rect(p.W, p.nv_pad, p.Phi, p.nb_pad, k, p.rt, p.ct, p.nsplit, p.C, s);
+    if (rc) return rc;
+    if (p.ndtasks) {
+        const size_t ps = sizeof(double) * ((size_t)kPS * p.nm + 2 * kPS + 2 * kPS * kPT + 16 * kPS);
+        if (ps > 48 * 1024)
+            SCP3_CUDA(cudaFuncSetAttribute(stein_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
+        dim3 pg((unsigned)p.ndtasks, (unsigned)p.nsplit);
+        stein_pairs_kernel<<<pg, 256, ps, s>>>(p.dtasks, p.vrdesc, p.voff, p.doff, p.nm, q, v, vq, k / p.nsplit,
+                                               p.dsize, p.D);
+        SCP3_CUDA(cudaGetLastError());
+    }
+    return SCP3GPU_OK;
+}
+
+int stein_unpack(const SteinPlan& p, const uint32_t* desc, double divisor, const double* diag, double zpe,
+                 double* M, int64_t ld, cudaStream_t s)
+{
+    const int64_t total = (int64_t)p.nb * p.nb;
+    stein_unpack_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
+        desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.ct, p.nsplit, p.C, p.D, (int64_t)p.rt * p.ct * 128 * 128,
+        p.dsize, divisor, diag, zpe, M, ld);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }

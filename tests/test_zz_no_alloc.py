@@ -50,12 +50,64 @@ def test_static_scratch_matches_allocating_path():
         assert np.abs(M - ref).max() <= 1e-12 * scale, (call, np.abs(M - ref).max() / scale)
 
 
+def _plan(nb):
+    """The entry point's chunk and sample-range split for a basis of nb functions
+    (the size rule of noalloc.cu restated): nsplit 4 halving while the tile
+    partials crowd the array out, then the chunk halving from 4096."""
+    nt = (nb + 63) // 64
+    a256 = lambda b: (b + 255) // 256 * 256
+    need = lambda k, s: a256(4 * nb) + 2 * a256(8 * nt * 64 * k) + 8 * 64 * 64 * nt * (nt + 1) // 2 * s
+    cap, nsplit, chunk = 64 << 20, 4, 4096
+    while nsplit > 1 and need(16 * nsplit, nsplit) > cap:
+        nsplit //= 2
+    while chunk > 16 * nsplit and need(chunk, nsplit) > cap:
+        chunk //= 2
+    return nsplit, chunk, need(chunk, nsplit) <= cap
+
+
+@pytest.mark.parametrize("nm,n2,n,pad", [(62, 62, 1500, 3), (88, 88, 40, 0)])
+def test_static_scratch_large_bases(nm, n2, n, pad):
+    """Bases where the array forces smaller pieces: 2016 functions (two sample
+    ranges per tile, 512-sample chunks, a ragged last chunk, M with a leading
+    dimension 3 past the basis) and 4005 functions (63 tiles a side, the most
+    the array holds: one range, 16-sample chunks)."""
+    import torch
+    import scp3_b200
+    from scp3_b200 import _lib
+    L = _lib.lib()
+    nb = int(L.scp3gpu_basis_size(nm, n2, 0))
+    nsplit, chunk, fits = _plan(nb)
+    assert fits and (nsplit, chunk) == ((2, 512) if nb == 2016 else (1, 16))
+    rng = np.random.default_rng(nb)
+    omega = np.linspace(0.002, 0.02, nm)
+    ld = nb + pad
+    for call in range(2):
+        q = rng.normal(scale=np.sqrt(0.5), size=(n, nm))
+        V = rng.normal(scale=1e-3, size=n)
+        ref = _reference(scp3_b200, omega, n2, 0, q, V)
+        qd = torch.tensor(q, dtype=torch.float64, device="cuda")
+        Vd = torch.tensor(V, dtype=torch.float64, device="cuda")
+        Md = torch.full((nb, ld), 7.0, dtype=torch.float64, device="cuda")   # column-major nb x nb, ld rows
+        Md[:, :nb] = 0.0
+        rc = L.scp3gpu_add_epot_static(nm, n2, 0, qd.data_ptr(), Vd.data_ptr(), n, Md.data_ptr(), ld,
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == 0, L.scp3gpu_last_error()
+        torch.cuda.synchronize()
+        A = Md.cpu().numpy()
+        assert np.all(A[:, nb:] == 7.0)                 # rows past the basis are not written
+        M = A[:, :nb].T
+        scale = np.abs(ref).max()
+        assert np.abs(M - ref).max() <= 1e-12 * scale, (call, np.abs(M - ref).max() / scale)
+
+
 def test_static_scratch_rejects_oversized_basis():
     import torch
     from scp3_b200 import _lib
     L = _lib.lib()
     x = torch.zeros(8, dtype=torch.float64, device="cuda")
-    nb = int(L.scp3gpu_basis_size(100, 100, 0))     # 5151 functions, over the 4032 limit
-    rc = L.scp3gpu_add_epot_static(100, 100, 0, x.data_ptr(), x.data_ptr(), 1, x.data_ptr(), nb, None)
-    assert rc == _lib.ERR_ARG
-    assert b"static scratch" in L.scp3gpu_last_error()
+    for nm in (100, 89):      # 5151 functions, and 4095: the first size past 63 tiles a side (4032 rows)
+        nb = int(L.scp3gpu_basis_size(nm, nm, 0))
+        assert not _plan(nb)[2]
+        rc = L.scp3gpu_add_epot_static(nm, nm, 0, x.data_ptr(), x.data_ptr(), 1, x.data_ptr(), nb, None)
+        assert rc == _lib.ERR_ARG
+        assert b"static scratch" in L.scp3gpu_last_error()
