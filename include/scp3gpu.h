@@ -112,7 +112,7 @@ typedef struct scp3gpu_config {
     uint64_t scramble_seed;
     int chunk;              /* samples per device pass; multiple of 4096, 0 = auto:
                                2^18 for the split forms (halved while one pass's
-                               operand would exceed ~6 GB); 2^14 for the FP64 form
+                               operand would exceed ~6 GB); 2^16 for the FP64 form
                                (halved while its Phi and W would exceed ~4 GB), 4096
                                for the gradient estimator                             */
     int device;             /* CUDA device ordinal                                     */

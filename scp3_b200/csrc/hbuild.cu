@@ -114,8 +114,9 @@ struct Timed {
 
 // Samples per device pass and the split of each pass over CTAs of a tile, plain
 // FP64 form with the direct estimator: 128 x 128 tiles with one CTA per SM
-// (contract_fp64_t128_kernel), in passes of 2^14 samples by default (fewer where
-// Phi and W of a pass would pass ~4 GB).  Sample ranges per tile (nsplit, a
+// (contract_fp64_t128_kernel), in passes of 2^16 samples by default (fewer where
+// Phi and W of a pass would pass ~4 GB), so a unit's partial write-back is spread
+// over at least 8192 samples at the usual split.  Sample ranges per tile (nsplit, a
 // power of two, each range at least 2048 samples) minimise the waves of units
 // per unit of work: the units of a pass run in ceil(units / sms) waves.  (The
 // gradient estimator plans its own passes: stein_create.)
@@ -126,7 +127,7 @@ void plan_fp64(scp3gpu_hbuild* h, int sms)
     h->tm.nt = (h->nb + T - 1) / T;
     h->tm.ntiles = h->tm.nt * (h->tm.nt + 1) / 2;
     h->nb_pad = h->tm.nt * T;
-    int64_t chunk = h->cfg.chunk > 0 ? h->cfg.chunk : 16384;
+    int64_t chunk = h->cfg.chunk > 0 ? h->cfg.chunk : 65536;
     // keep Phi and W of one pass under ~4 GB
     while (chunk > 4096 && (int64_t)h->nb_pad * chunk * 16 > (4ll << 30)) chunk /= 2;
     h->chunk = chunk;

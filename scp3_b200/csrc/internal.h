@@ -164,7 +164,9 @@ struct SteinPlan {
     int* rank3 = nullptr;            // [nb * 3] rank of function i in E_m for its k-th mode
     int* voff = nullptr;             // [nm + 1] first virtual row of mode m
     int64_t* doff = nullptr;         // [nm] first same-mode pair sum of mode m
-    int4* dtasks = nullptr;          // [ndtasks] (m, row tile, column tile) of the pair kernel
+    int4* dtasks = nullptr;          // [ndtasks] (m, row tile, column tile) of the tiled pair kernel
+    int nftasks = 0;
+    int2* ftasks = nullptr;          // [nftasks] (m, first pair) of the flat pair kernel
     double* W = nullptr;             // [chunk][nv_pad]  reduced function x Stein weight
     double* Phi = nullptr;           // [chunk][nb_pad]  basis functions
     double* C = nullptr;             // [nsplit][rt * ct][128 * 128]

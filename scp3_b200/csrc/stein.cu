@@ -107,6 +107,7 @@ __device__ __forceinline__ double reduced(uint32_t vd, const double* qs, int str
 }
 
 constexpr int kExpS = 64, kExpR = 128;
+constexpr int kExpLd = kExpS + 1;   // odd row stride of the staged q: a warp's rows read different modes conflict-free
 
 // Phi [s][j] (ld nb_pad) and W [s][r] (ld nv_pad) for 64 samples; one thread per
 // row of the stacked [Phi rows | W rows], coalesced 1 KB stores per sample.
@@ -117,17 +118,17 @@ __global__ void __launch_bounds__(kExpR) stein_expand_kernel(const uint32_t* __r
                                                              const double* __restrict__ vq, int64_t n,
                                                              double* __restrict__ Phi, double* __restrict__ W)
 {
-    extern __shared__ double st[];          // q [nm][64], vq [nm][64], V [64]
+    extern __shared__ double st[];          // q [nm][65], vq [nm][65], V [64]
     double* qs = st;
-    double* vqs = st + (size_t)nm * kExpS;
-    double* vs = vqs + (size_t)nm * kExpS;
+    double* vqs = st + (size_t)nm * kExpLd;
+    double* vs = vqs + (size_t)nm * kExpLd;
     const int t = threadIdx.x;
     const int64_t s0 = (int64_t)blockIdx.x * kExpS;
     for (int e = t; e < nm * kExpS; e += kExpR) {
         const int ss = e / nm, m = e - ss * nm;          // coalesced reads of row s0 + ss
         const bool ok = s0 + ss < n;
-        qs[m * kExpS + ss] = ok ? q[(s0 + ss) * nm + m] : 0.0;
-        vqs[m * kExpS + ss] = ok ? vq[(s0 + ss) * nm + m] : 0.0;
+        qs[m * kExpLd + ss] = ok ? q[(s0 + ss) * nm + m] : 0.0;
+        vqs[m * kExpLd + ss] = ok ? vq[(s0 + ss) * nm + m] : 0.0;
     }
     for (int ss = t; ss < kExpS; ss += kExpR) vs[ss] = s0 + ss < n ? v[s0 + ss] : 0.0;
     __syncthreads();
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(kExpR) stein_expand_kernel(const uint32_t* __r
         if (row < nb) k = decode(__ldg(desc + row), mm, ll);
         for (int j = 0; j < ns; j++) {
             double x = row < nb ? 1.0 : 0.0;
-            for (int u = 0; u < k; u++) x *= ho(ll[u], qs[mm[u] * kExpS + j]);
+            for (int u = 0; u < k; u++) x *= ho(ll[u], qs[mm[u] * kExpLd + j]);
             Phi[(size_t)(s0 + j) * nb_pad + row] = x;
         }
     } else {
@@ -149,7 +150,8 @@ __global__ void __launch_bounds__(kExpR) stein_expand_kernel(const uint32_t* __r
             double x = 0.0;
             if (r < nv) {
                 if (vd & kGroundRow) x = vs[j];
-                else x = reduced(vd, qs, kExpS, j) * stein_weight(a, 0, qs[m * kExpS + j], vs[j], vqs[m * kExpS + j]);
+                else x = reduced(vd, qs, kExpLd, j) *
+                         stein_weight(a, 0, qs[m * kExpLd + j], vs[j], vqs[m * kExpLd + j]);
             }
             W[(size_t)(s0 + j) * nv_pad + r] = x;
         }
@@ -236,6 +238,82 @@ __global__ void __launch_bounds__(256) stein_pairs_kernel(const int4* __restrict
         }
 }
 
+// The same sums for modes with few exciting functions (e <= kFlatMax, 49 for
+// every mode of the hexamer doubles basis), where most of a 64 x 64 tile would be
+// idle: a CTA takes up to kFlatPairs pairs (ri <= rj) of one mode in row-major
+// upper-triangle order, 8 per thread, with the R values of all e functions and the
+// level-pair weights of a sample chunk staged in shared memory.
+constexpr int kFlatMax = 96, kFlatPairs = 2048, kFS = 16;
+
+__global__ void __launch_bounds__(256) stein_pairs_flat_kernel(const int2* __restrict__ tasks,
+                                                               const uint32_t* __restrict__ vrdesc,
+                                                               const int* __restrict__ voff,
+                                                               const int64_t* __restrict__ doff, int nm,
+                                                               const double* __restrict__ q,
+                                                               const double* __restrict__ v,
+                                                               const double* __restrict__ vq, int64_t kps,
+                                                               int64_t dsize, double* __restrict__ D)
+{
+    extern __shared__ double fs[];   // q [kFS][nm], V [kFS], Vm [kFS], R [kFS][kFlatMax], K [kFS][16]
+    double* qs = fs;
+    double* vs = qs + (size_t)kFS * nm;
+    double* vms = vs + kFS;
+    double* R = vms + kFS;
+    double* K = R + kFS * kFlatMax;
+    const int2 task = tasks[blockIdx.x];
+    const int m = task.x, p0 = task.y;
+    const int v0 = voff[m], e = voff[m + 1] - v0;
+    const int np = e * (e + 1) / 2, tid = threadIdx.x;
+    constexpr int kPer = kFlatPairs / 256;
+    int ri[kPer], rj[kPer], ab[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {
+        int p = p0 + tid + 256 * u;
+        ri[u] = -1, rj[u] = 0, ab[u] = 0;
+        if (p < np && p < p0 + kFlatPairs) {
+            int r = 0;
+            while (p >= e - r) p -= e - r, r++;
+            ri[u] = r, rj[u] = r + p;
+            ab[u] = (int)(((vrdesc[v0 + r] >> 8) & 3u) * 4 + ((vrdesc[v0 + r + p] >> 8) & 3u));
+        }
+    }
+    double acc[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; u++) acc[u] = 0.0;
+    const int64_t s0 = (int64_t)blockIdx.y * kps;
+    for (int64_t c0 = 0; c0 < kps; c0 += kFS) {
+        const int nc = (int)min((int64_t)kFS, kps - c0);
+        __syncthreads();
+        for (int x = tid; x < nc * nm; x += 256) qs[x] = q[(s0 + c0) * nm + x];
+        for (int j = tid; j < nc; j += 256) {
+            vs[j] = v[s0 + c0 + j];
+            vms[j] = vq[(s0 + c0 + j) * nm + m];
+        }
+        __syncthreads();
+        for (int x = tid; x < nc * (e + 16); x += 256) {
+            const int j = x / (e + 16), y = x - j * (e + 16);
+            if (y < e) {
+                R[j * kFlatMax + y] = reduced(vrdesc[v0 + y], qs + (size_t)j * nm, 1, 0);
+            } else {
+                const int k = y - e, a = k >> 2, b = k & 3;
+                K[j * 16 + k] = (a && b) ? stein_weight(a, b, qs[(size_t)j * nm + m], vs[j], vms[j]) : 0.0;
+            }
+        }
+        __syncthreads();
+        for (int j = 0; j < nc; j++) {
+            const double* Rj = R + j * kFlatMax;
+            const double* Kj = K + j * 16;
+#pragma unroll
+            for (int u = 0; u < kPer; u++)
+                if (ri[u] >= 0) acc[u] = fma(Rj[ri[u]], Rj[rj[u]] * Kj[ab[u]], acc[u]);
+        }
+    }
+    double* Dp = D + (size_t)blockIdx.y * dsize + doff[m];
+#pragma unroll
+    for (int u = 0; u < kPer; u++)
+        if (ri[u] >= 0) Dp[(size_t)ri[u] * e + rj[u]] += acc[u];
+}
+
 // Element (i, j) of the dense matrix from its terms: for each mode m that r =
 // min(i, j) or c = max(i, j) excites, C at virtual row (m, r) column c, or at
 // (m, c) column r, or the pair sum D^m when both excite m; the mean over those
@@ -305,7 +383,7 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
     p.nb = (int)desc.size();
     p.nm = nm;
     p.nb_pad = (int)round_up(p.nb, 128);
-    if (sizeof(double) * (2 * (size_t)nm * kExpS + kExpS) > 227 * 1024)
+    if (sizeof(double) * (2 * (size_t)nm * kExpLd + kExpS) > 227 * 1024)
         return fail(SCP3GPU_ERR_ARG, "stein: too many modes for the expansion's shared memory (at most 220)");
     // functions exciting each mode, in basis order; rank of each in its mode's list
     std::vector<std::vector<int>> E(nm);
@@ -325,7 +403,8 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
     std::vector<int> voff(nm + 1, 0);
     std::vector<int64_t> doff(nm, 0);
     std::vector<uint32_t> vrdesc;
-    std::vector<int4> tasks;
+    std::vector<int4> tasks;      // 64 x 64 rank tiles of modes with many exciting functions
+    std::vector<int2> ftasks;     // pair ranges of modes with few
     int64_t dsz = 0;
     for (int m = 0; m < nm; m++) {
         voff[m] = (int)vrdesc.size();
@@ -345,9 +424,13 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
             }
             vrdesc.push_back(d);
         }
-        const int nt = (en + kPT - 1) / kPT;
-        for (int a = 0; a < nt; a++)
-            for (int b = a; b < nt; b++) tasks.push_back(make_int4(m, a, b, 0));
+        if (en <= kFlatMax) {
+            for (int p0 = 0; p0 < en * (en + 1) / 2; p0 += kFlatPairs) ftasks.push_back(make_int2(m, p0));
+        } else {
+            const int nt = (en + kPT - 1) / kPT;
+            for (int a = 0; a < nt; a++)
+                for (int b = a; b < nt; b++) tasks.push_back(make_int4(m, a, b, 0));
+        }
     }
     voff[nm] = (int)vrdesc.size();
     vrdesc.push_back(kGroundRow);
@@ -357,6 +440,7 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
     p.ct = p.nb_pad / 128;
     p.dsize = std::max<int64_t>(dsz, 1);
     p.ndtasks = (int)tasks.size();
+    p.nftasks = (int)ftasks.size();
     // passes of 2^14 samples (fewer while W and Phi of a pass would pass ~4 GB);
     // sample ranges per tile as the plain form chooses them, the C partials of
     // all ranges held under ~8 GB (one range if a single one is larger)
@@ -376,6 +460,7 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
     if ((rc = upload(&p.vrdesc, vrdesc.data(), vrdesc.size())) || (rc = upload(&p.rank3, rank3.data(), rank3.size())) ||
         (rc = upload(&p.voff, voff.data(), voff.size())) || (rc = upload(&p.doff, doff.data(), doff.size())) ||
         (p.ndtasks && (rc = upload(&p.dtasks, tasks.data(), tasks.size()))) ||
+        (p.nftasks && (rc = upload(&p.ftasks, ftasks.data(), ftasks.size()))) ||
         (rc = dalloc(&p.W, (size_t)p.chunk * p.nv_pad)) || (rc = dalloc(&p.Phi, (size_t)p.chunk * p.nb_pad)) ||
         (rc = dalloc(&p.C, (size_t)csize * p.nsplit)) || (rc = dalloc(&p.D, (size_t)p.dsize * p.nsplit))) {
         stein_destroy(p);
@@ -386,9 +471,9 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
 
 void stein_destroy(SteinPlan& p)
 {
-    cudaFree(p.vrdesc), cudaFree(p.rank3), cudaFree(p.voff), cudaFree(p.doff), cudaFree(p.dtasks);
+    cudaFree(p.vrdesc), cudaFree(p.rank3), cudaFree(p.voff), cudaFree(p.doff), cudaFree(p.dtasks), cudaFree(p.ftasks);
     cudaFree(p.W), cudaFree(p.Phi), cudaFree(p.C), cudaFree(p.D);
-    p.vrdesc = nullptr, p.rank3 = nullptr, p.voff = nullptr, p.doff = nullptr, p.dtasks = nullptr;
+    p.vrdesc = nullptr, p.rank3 = nullptr, p.voff = nullptr, p.doff = nullptr, p.dtasks = nullptr, p.ftasks = nullptr;
     p.W = p.Phi = p.C = p.D = nullptr;
 }
 
@@ -404,7 +489,7 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
 {
     if (k == 0) return SCP3GPU_OK;
     if (k > p.chunk || k % (16ll * p.nsplit) != 0) return fail(SCP3GPU_ERR_ARG, "stein: pass not tiled");
-    const size_t es = sizeof(double) * (2 * (size_t)p.nm * kExpS + kExpS);
+    const size_t es = sizeof(double) * (2 * (size_t)p.nm * kExpLd + kExpS);
     if (es > 48 * 1024)
         SCP3_CUDA(cudaFuncSetAttribute(stein_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)es));
     dim3 eg((unsigned)((k + kExpS - 1) / kExpS), (unsigned)((p.nb_pad + p.nv_pad) / kExpR));
@@ -420,6 +505,16 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
         dim3 pg((unsigned)p.ndtasks, (unsigned)p.nsplit);
         stein_pairs_kernel<<<pg, 256, ps, s>>>(p.dtasks, p.vrdesc, p.voff, p.doff, p.nm, q, v, vq, k / p.nsplit,
                                                p.dsize, p.D);
+        SCP3_CUDA(cudaGetLastError());
+    }
+    if (p.nftasks) {
+        const size_t fsm = sizeof(double) * ((size_t)kFS * p.nm + 2 * kFS + (size_t)kFS * kFlatMax + 16 * kFS);
+        if (fsm > 48 * 1024)
+            SCP3_CUDA(cudaFuncSetAttribute(stein_pairs_flat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)fsm));
+        dim3 fg((unsigned)p.nftasks, (unsigned)p.nsplit);
+        stein_pairs_flat_kernel<<<fg, 256, fsm, s>>>(p.ftasks, p.vrdesc, p.voff, p.doff, p.nm, q, v, vq,
+                                                     k / p.nsplit, p.dsize, p.D);
         SCP3_CUDA(cudaGetLastError());
     }
     return SCP3GPU_OK;
