@@ -261,8 +261,9 @@ int scp3gpu_load_h5(const char* path, double* M, int64_t* n_rows, int64_t* n_col
  * The learned control variate (no counterpart in the reference, which always
  * evaluates the exact potential, SCP3.cpp:205-225): an n_in -> hidden -> hidden
  * -> hidden -> 1 GELU network with BF16 weights and FP32 accumulation, trained
- * and evaluated by this library's kernels.  Host buffers; q is n x n_in
- * (sample-major), t and y are n targets/outputs in the units of V_anh. */
+ * and evaluated by this library's kernels (the forward layers on the tcgen05
+ * tensor cores: n_in 1..256, hidden 64, 128, 192 or 256).  Host buffers; q is
+ * n x n_in (sample-major), t and y are n targets/outputs in the units of V_anh. */
 typedef struct scp3gpu_mlp scp3gpu_mlp;
 int scp3gpu_mlp_create(int n_in, int hidden, int max_batch, uint64_t seed, int device, scp3gpu_mlp** out);
 int scp3gpu_mlp_destroy(scp3gpu_mlp* m);

@@ -166,7 +166,7 @@ struct SteinPlan {
     int64_t* doff = nullptr;         // [nm] first same-mode pair sum of mode m
     int4* dtasks = nullptr;          // [ndtasks] (m, row tile, column tile) of the tiled pair kernel
     int nftasks = 0;
-    int2* ftasks = nullptr;          // [nftasks] (m, first pair) of the flat pair kernel
+    int* ftasks = nullptr;           // [nftasks] modes of the triangle-blocked pair kernel
     double* W = nullptr;             // [chunk][nv_pad]  reduced function x Stein weight
     double* Phi = nullptr;           // [chunk][nb_pad]  basis functions
     double* C = nullptr;             // [nsplit][rt * ct][128 * 128]

@@ -4,9 +4,11 @@
 // kernels below (the reference has no surrogate; SCP3 evaluates the exact
 // potential at every point, SCP3.cpp:205-225).
 //
-//   forward    gemm_bias_gelu: Y = GELU(X W^T + b) with warp-level BF16 MMA
-//              (mma.sync m16n8k16, FP32 accumulators), activations stored BF16
-//              for the next layer and FP32 pre-activations kept for training;
+//   forward    gemm_bias_gelu_tc: Y = GELU(X W^T + b) on the tcgen05 tensor
+//              cores, one 128-sample tile per CTA against all outputs (M = 128,
+//              N = hidden, K = 16 MMAs into a FP32 TMEM accumulator), activations
+//              stored BF16 for the next layer and FP32 pre-activations kept for
+//              training;
 //              head_kernel: y = h3 . w4 + b4, one warp per sample
 //   backward   FP32 register-tiled GEMMs for dX = dZ W and dW = dZ^T X,
 //              gelu_backward for dZ = dH * GELU'(Z), a per-column reduction for
@@ -37,80 +39,122 @@ __device__ __forceinline__ float gelu_grad(float z)
     return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
-// Y[M][N] = act(X[M][K] W[N][K]^T + b).  X, W BF16 row-major (K contiguous,
-// K % 32 == 0, M % 64 == 0, N % 64 == 0).  CTA tile 64 x 64, 4 warps of 32 x 32,
-// K staged 32 at a time.  Writes Z (FP32, may be null) and H = GELU(Z) (BF16).
-constexpr int kGM = 64, kGN = 64, kGK = 32, kPadK = 8;
+constexpr unsigned long long kWaitNs = 4000000000ull;
+#include "tc_ptx.cuh"
 
-__global__ void __launch_bounds__(128) gemm_bias_gelu(const __nv_bfloat16* __restrict__ X,
-                                                       const __nv_bfloat16* __restrict__ W,
-                                                       const float* __restrict__ b, int M, int N, int K,
-                                                       float* __restrict__ Z, __nv_bfloat16* __restrict__ H,
-                                                       int apply_gelu)
+// 16-byte cp.async into shared memory, zero-filled (nothing read) when !valid
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid)
 {
-    __shared__ __align__(16) __nv_bfloat16 As[kGM][kGK + kPadK];
-    __shared__ __align__(16) __nv_bfloat16 Bs[kGN][kGK + kPadK];
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+// Y[M][N] = act(X[M][K] W[N][K]^T + b) on the tensor cores.  X, W BF16
+// row-major (K contiguous); N a multiple of 32 up to 256, K a multiple of 32 up
+// to 256, any M.  A CTA takes 128 rows of X: it stages them and all of W with
+// cp.async into the K-major 64-byte-swizzled layout the MMA descriptors read
+// (per 32-column K box, row r's 16-byte chunk c at c ^ ((r >> 1) & 3)), one
+// thread issues K / 16 MMAs of M = 128, N, K = 16 into a FP32 TMEM accumulator,
+// and each warp reads back its 32 rows, adds the bias and writes Z (FP32, may
+// be null) and H = GELU(Z) (BF16).  The wait for the MMAs is bounded; on expiry
+// the tile's outputs are written as NaN, which the build's non-finite counters
+// report.
+constexpr int kTM = 128, kTcThreads = 128;
+
+__host__ __device__ inline size_t tc_smem_bytes(int N, int K)
+{
+    return (size_t)(K / 32) * (kTM + N) * 64 + 64 + 1024;   // operands, barrier + TMEM slot, alignment
+}
+
+__global__ void __launch_bounds__(kTcThreads) gemm_bias_gelu_tc(const __nv_bfloat16* __restrict__ X,
+                                                                const __nv_bfloat16* __restrict__ W,
+                                                                const float* __restrict__ b, int M, int N, int K,
+                                                                float* __restrict__ Z,
+                                                                __nv_bfloat16* __restrict__ H, int apply_gelu)
+{
+    extern __shared__ uint8_t sm_raw[];
+    uint8_t* sm = (uint8_t*)(((uintptr_t)sm_raw + 1023) & ~(uintptr_t)1023);
+    const int nkb = K / 32;
+    uint8_t* As = sm;                                  // [nkb][128 rows][64 B]
+    uint8_t* Bs = sm + (size_t)nkb * kTM * 64;         // [nkb][N rows][64 B]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Bs + (size_t)nkb * N * 64);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+    volatile int* abort = reinterpret_cast<volatile int*>(tslot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * kGM, n0 = blockIdx.y * kGN;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int g = lane >> 2, tg = lane & 3;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int r = 0; r < 4; r++) acc[i][j][r] = 0.0f;
-    for (int k0 = 0; k0 < K; k0 += kGK) {
-        // 64 rows x 32 bf16 = 64 B per row: 4 x 16 B per row, 256 chunks per operand
-        for (int c = tid; c < kGM * 4; c += 128) {
-            const int r = c >> 2, q = (c & 3) * 8;
-            *reinterpret_cast<uint4*>(&As[r][q]) = *reinterpret_cast<const uint4*>(X + (size_t)(m0 + r) * K + k0 + q);
-            *reinterpret_cast<uint4*>(&Bs[r][q]) = *reinterpret_cast<const uint4*>(W + (size_t)(n0 + r) * K + k0 + q);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < kGK; kk += 16) {
-            uint32_t a[2][4], bb[4][2];
-#pragma unroll
-            for (int i = 0; i < 2; i++) {
-                const int r = wm + 16 * i + g;
-                a[i][0] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 2 * tg]);
-                a[i][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 2 * tg]);
-                a[i][2] = *reinterpret_cast<const uint32_t*>(&As[r][kk + 8 + 2 * tg]);
-                a[i][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + 8 + 2 * tg]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int n = wn + 8 * j + g;
-                bb[j][0] = *reinterpret_cast<const uint32_t*>(&Bs[n][kk + 2 * tg]);
-                bb[j][1] = *reinterpret_cast<const uint32_t*>(&Bs[n][kk + 8 + 2 * tg]);
-            }
-#pragma unroll
-            for (int i = 0; i < 2; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++)
-                    asm volatile(
-                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-                        "{%8,%9}, {%0,%1,%2,%3};"
-                        : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-                        : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(bb[j][0]), "r"(bb[j][1]));
-        }
-        __syncthreads();
+    const int m0 = blockIdx.x * kTM;
+    const uint32_t ncol = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;   // TMEM: a power of 2 >= 32
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(ncol));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    const int kc = K / 8;                              // 16-byte chunks per row
+    for (int e = tid; e < kTM * kc; e += kTcThreads) {
+        const int r = e / kc, c = e - r * kc, cc = c & 3;
+        const bool ok = m0 + r < M;
+        cp_async16(As + (size_t)(c >> 2) * kTM * 64 + r * 64 + ((cc ^ ((r >> 1) & 3)) << 4),
+                   X + (size_t)(ok ? m0 + r : 0) * K + c * 8, ok);
+    }
+    for (int e = tid; e < N * kc; e += kTcThreads) {
+        const int r = e / kc, c = e - r * kc, cc = c & 3;
+        cp_async16(Bs + (size_t)(c >> 2) * N * 64 + r * 64 + ((cc ^ ((r >> 1) & 3)) << 4), W + (size_t)r * K + c * 8,
+                   true);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the tensor core reads what the copies wrote
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    if (tid == 0) {
+        const uint32_t idesc =
+            (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
+        for (int kb = 0; kb < nkb; kb++) {
+            const uint64_t a = smem_desc64(As + (size_t)kb * kTM * 64), bd = smem_desc64(Bs + (size_t)kb * N * 64);
 #pragma unroll
-    for (int i = 0; i < 2; i++)
+            for (int kk = 0; kk < 2; kk++) mma_bf16(tmem, a + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0);
+        }
+        mma_commit(bar);
+    }
+    const bool ok = mbar_wait(bar, 0, abort);
+    tc_fence_after();
+    const int row = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < N; c0 += 32) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+        if (row >= M) continue;
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int r = m0 + wm + 16 * i + g + 8 * h;
-                const int c = n0 + wn + 8 * j + 2 * tg;
-                const float z0 = acc[i][j][2 * h] + b[c], z1 = acc[i][j][2 * h + 1] + b[c + 1];
-                if (Z) *reinterpret_cast<float2*>(Z + (size_t)r * N + c) = make_float2(z0, z1);
-                const float h0 = apply_gelu ? gelu(z0) : z0, h1 = apply_gelu ? gelu(z1) : z1;
-                *reinterpret_cast<__nv_bfloat162*>(H + (size_t)r * N + c) = __floats2bfloat162_rn(h0, h1);
-            }
+        for (int j = 0; j < 32; j += 2) {
+            const float z0 = ok ? v[j] + b[c0 + j] : __int_as_float(0x7fc00000);
+            const float z1 = ok ? v[j + 1] + b[c0 + j + 1] : __int_as_float(0x7fc00000);
+            if (Z) *reinterpret_cast<float2*>(Z + (size_t)row * N + c0 + j) = make_float2(z0, z1);
+            const float h0 = apply_gelu ? gelu(z0) : z0, h1 = apply_gelu ? gelu(z1) : z1;
+            *reinterpret_cast<__nv_bfloat162*>(H + (size_t)row * N + c0 + j) = __floats2bfloat162_rn(h0, h1);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncol));
+    }
+}
+
+int launch_layer(const __nv_bfloat16* X, const __nv_bfloat16* W, const float* b, int M, int N, int K, float* Z,
+                 __nv_bfloat16* H, cudaStream_t s)
+{
+    if (N % 32 || N > 256 || K % 32 || K > 256) return fail(SCP3GPU_ERR_ARG, "mlp layer: shape out of range");
+    const size_t sm = tc_smem_bytes(N, K);
+    SCP3_CUDA(cudaFuncSetAttribute(gemm_bias_gelu_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    gemm_bias_gelu_tc<<<(unsigned)((M + kTM - 1) / kTM), kTcThreads, sm, s>>>(X, W, b, M, N, K, Z, H, 1);
+    SCP3_CUDA(cudaGetLastError());
+    return SCP3GPU_OK;
 }
 
 // y[m] = H[m][:] . w + b, one warp per sample.
@@ -316,8 +360,7 @@ int Net::forward(const float* q, int M, float* y, cudaStream_t s)
     if (Mp > M) SCP3_CUDA(cudaMemsetAsync(X + (size_t)M * kin, 0, sizeof(__nv_bfloat16) * (size_t)(Mp - M) * kin, s));
     const __nv_bfloat16* in_act = X;
     for (int l = 0; l < 3; l++) {
-        dim3 grid(Mp / kGM, hid / kGN);
-        gemm_bias_gelu<<<grid, 128, 0, s>>>(in_act, wb[l], b[l], Mp, hid, inpad[l], Z[l], H[l], 1);
+        if (int rc = launch_layer(in_act, wb[l], b[l], Mp, hid, inpad[l], Z[l], H[l], s)) return rc;
         in_act = H[l];
     }
     head_kernel<<<blocks(M, 8), 256, 0, s>>>(H[2], w[3], 0.0f, M, hid, 1.0f, 0.0f, y);
@@ -344,8 +387,7 @@ int Net::infer(const float* q, int M, float* y, cudaStream_t s, __nv_bfloat16* X
     const __nv_bfloat16* in_act = Xw;
     __nv_bfloat16* outs[3] = {Ha, Hb, Ha};
     for (int l = 0; l < 3; l++) {
-        dim3 grid(Mp / kGM, hid / kGN);
-        gemm_bias_gelu<<<grid, 128, 0, s>>>(in_act, wb[l], b[l], Mp, hid, inpad[l], nullptr, outs[l], 1);
+        if (int rc = launch_layer(in_act, wb[l], b[l], Mp, hid, inpad[l], nullptr, outs[l], s)) return rc;
         in_act = outs[l];
     }
     head_kernel<<<blocks(M, 8), 256, 0, s>>>(in_act, w[3], 0.0f, M, hid, 1.0f, 0.0f, y);
@@ -499,8 +541,8 @@ int scp3gpu_mlp_destroy(scp3gpu_mlp* m)
 int scp3gpu_mlp_create(int n_in, int hidden, int max_batch, uint64_t seed, int device, scp3gpu_mlp** out)
 {
     (void)cudaGetLastError();
-    if (!out || n_in < 1 || n_in > 1024 || hidden < 64 || hidden % 64 != 0 || max_batch < 64)
-        return fail(SCP3GPU_ERR_ARG, "mlp_create: n_in 1..1024, hidden a multiple of 64, max_batch >= 64");
+    if (!out || n_in < 1 || n_in > 256 || hidden < 64 || hidden > 256 || hidden % 64 != 0 || max_batch < 64)
+        return fail(SCP3GPU_ERR_ARG, "mlp_create: n_in 1..256, hidden 64, 128, 192 or 256, max_batch >= 64");
     *out = nullptr;
     int nd = 0;
     if (cudaGetDeviceCount(&nd) != cudaSuccess || device < 0 || device >= nd)

@@ -238,80 +238,96 @@ __global__ void __launch_bounds__(256) stein_pairs_kernel(const int4* __restrict
         }
 }
 
-// The same sums for modes with few exciting functions (e <= kFlatMax, 49 for
-// every mode of the hexamer doubles basis), where most of a 64 x 64 tile would be
-// idle: a CTA takes up to kFlatPairs pairs (ri <= rj) of one mode in row-major
-// upper-triangle order, 8 per thread, with the R values of all e functions and the
-// level-pair weights of a sample chunk staged in shared memory.
-constexpr int kFlatMax = 96, kFlatPairs = 2048, kFS = 16;
+// The same sums for modes with few exciting functions (e <= kTriMax; 49 for
+// every mode of the hexamer doubles basis), where most of a 64 x 64 tile would
+// be idle: one CTA per mode (and sample range), thread t owning the t-th 4 x 4
+// block (bi <= bj) of the mode's upper e x e triangle, so a sample costs a
+// thread four 16-byte loads of R and 16 weight loads for 16 products.  R values
+// (zero past e) and the level-pair weights of a sample chunk are staged in
+// shared memory.
+constexpr int kTriMax = 64, kTriThreads = 160, kFS = 16;
 
-__global__ void __launch_bounds__(256) stein_pairs_flat_kernel(const int2* __restrict__ tasks,
-                                                               const uint32_t* __restrict__ vrdesc,
-                                                               const int* __restrict__ voff,
-                                                               const int64_t* __restrict__ doff, int nm,
-                                                               const double* __restrict__ q,
-                                                               const double* __restrict__ v,
-                                                               const double* __restrict__ vq, int64_t kps,
-                                                               int64_t dsize, double* __restrict__ D)
+__global__ void __launch_bounds__(kTriThreads) stein_pairs_tri_kernel(const int* __restrict__ modes,
+                                                                      const uint32_t* __restrict__ vrdesc,
+                                                                      const int* __restrict__ voff,
+                                                                      const int64_t* __restrict__ doff, int nm,
+                                                                      const double* __restrict__ q,
+                                                                      const double* __restrict__ v,
+                                                                      const double* __restrict__ vq, int64_t kps,
+                                                                      int64_t dsize, double* __restrict__ D)
 {
-    extern __shared__ double fs[];   // q [kFS][nm], V [kFS], Vm [kFS], R [kFS][kFlatMax], K [kFS][16]
+    extern __shared__ __align__(16) double fs[];   // q [kFS][nm], V [kFS], Vm [kFS], R [kFS][64], K [kFS][16]
     double* qs = fs;
     double* vs = qs + (size_t)kFS * nm;
     double* vms = vs + kFS;
-    double* R = vms + kFS;
-    double* K = R + kFS * kFlatMax;
-    const int2 task = tasks[blockIdx.x];
-    const int m = task.x, p0 = task.y;
+    double* R = vms + kFS;          // 16-byte aligned: kFS * (nm + 2) doubles is even
+    double* K = R + kFS * kTriMax;
+    const int m = modes[blockIdx.x];
     const int v0 = voff[m], e = voff[m + 1] - v0;
-    const int np = e * (e + 1) / 2, tid = threadIdx.x;
-    constexpr int kPer = kFlatPairs / 256;
-    int ri[kPer], rj[kPer], ab[kPer];
-#pragma unroll
-    for (int u = 0; u < kPer; u++) {
-        int p = p0 + tid + 256 * u;
-        ri[u] = -1, rj[u] = 0, ab[u] = 0;
-        if (p < np && p < p0 + kFlatPairs) {
-            int r = 0;
-            while (p >= e - r) p -= e - r, r++;
-            ri[u] = r, rj[u] = r + p;
-            ab[u] = (int)(((vrdesc[v0 + r] >> 8) & 3u) * 4 + ((vrdesc[v0 + r + p] >> 8) & 3u));
-        }
+    const int nbk = (e + 3) / 4, tid = threadIdx.x;
+    // this thread's block (bi, bj), row-major over bi <= bj
+    int bi = -1, bj = 0;
+    if (tid < nbk * (nbk + 1) / 2) {
+        int p = tid, r = 0;
+        while (p >= nbk - r) p -= nbk - r, r++;
+        bi = r, bj = r + p;
     }
-    double acc[kPer];
+    int ab[4][4];
 #pragma unroll
-    for (int u = 0; u < kPer; u++) acc[u] = 0.0;
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int ri = 4 * bi + r, rc = 4 * bj + c;
+            const int a = (bi >= 0 && ri < e) ? (int)((vrdesc[v0 + ri] >> 8) & 3u) : 0;
+            const int b = (bi >= 0 && rc < e) ? (int)((vrdesc[v0 + rc] >> 8) & 3u) : 0;
+            ab[r][c] = a * 4 + b;
+        }
+    double acc[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[r][c] = 0.0;
     const int64_t s0 = (int64_t)blockIdx.y * kps;
     for (int64_t c0 = 0; c0 < kps; c0 += kFS) {
         const int nc = (int)min((int64_t)kFS, kps - c0);
         __syncthreads();
-        for (int x = tid; x < nc * nm; x += 256) qs[x] = q[(s0 + c0) * nm + x];
-        for (int j = tid; j < nc; j += 256) {
+        for (int x = tid; x < nc * nm; x += kTriThreads) qs[x] = q[(s0 + c0) * nm + x];
+        for (int j = tid; j < nc; j += kTriThreads) {
             vs[j] = v[s0 + c0 + j];
             vms[j] = vq[(s0 + c0 + j) * nm + m];
         }
         __syncthreads();
-        for (int x = tid; x < nc * (e + 16); x += 256) {
-            const int j = x / (e + 16), y = x - j * (e + 16);
-            if (y < e) {
-                R[j * kFlatMax + y] = reduced(vrdesc[v0 + y], qs + (size_t)j * nm, 1, 0);
+        for (int x = tid; x < nc * (kTriMax + 16); x += kTriThreads) {
+            const int j = x / (kTriMax + 16), y = x - j * (kTriMax + 16);
+            if (y < kTriMax) {
+                R[j * kTriMax + y] = y < e ? reduced(vrdesc[v0 + y], qs + (size_t)j * nm, 1, 0) : 0.0;
             } else {
-                const int k = y - e, a = k >> 2, b = k & 3;
+                const int k = y - kTriMax, a = k >> 2, b = k & 3;
                 K[j * 16 + k] = (a && b) ? stein_weight(a, b, qs[(size_t)j * nm + m], vs[j], vms[j]) : 0.0;
             }
         }
         __syncthreads();
+        if (bi < 0) continue;
         for (int j = 0; j < nc; j++) {
-            const double* Rj = R + j * kFlatMax;
+            const double2* Rj = reinterpret_cast<const double2*>(R + j * kTriMax);
+            const double2 r01 = Rj[2 * bi], r23 = Rj[2 * bi + 1], c01 = Rj[2 * bj], c23 = Rj[2 * bj + 1];
+            const double rr[4] = {r01.x, r01.y, r23.x, r23.y}, rc[4] = {c01.x, c01.y, c23.x, c23.y};
             const double* Kj = K + j * 16;
 #pragma unroll
-            for (int u = 0; u < kPer; u++)
-                if (ri[u] >= 0) acc[u] = fma(Rj[ri[u]], Rj[rj[u]] * Kj[ab[u]], acc[u]);
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[r][c] = fma(rr[r], rc[c] * Kj[ab[r][c]], acc[r][c]);
         }
     }
+    if (bi < 0) return;
     double* Dp = D + (size_t)blockIdx.y * dsize + doff[m];
 #pragma unroll
-    for (int u = 0; u < kPer; u++)
-        if (ri[u] >= 0) Dp[(size_t)ri[u] * e + rj[u]] += acc[u];
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int ri = 4 * bi + r, rc = 4 * bj + c;
+            if (ri < e && rc < e && ri <= rc) Dp[(size_t)ri * e + rc] += acc[r][c];
+        }
 }
 
 // Element (i, j) of the dense matrix from its terms: for each mode m that r =
@@ -404,7 +420,7 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
     std::vector<int64_t> doff(nm, 0);
     std::vector<uint32_t> vrdesc;
     std::vector<int4> tasks;      // 64 x 64 rank tiles of modes with many exciting functions
-    std::vector<int2> ftasks;     // pair ranges of modes with few
+    std::vector<int> ftasks;      // modes with few (one CTA each)
     int64_t dsz = 0;
     for (int m = 0; m < nm; m++) {
         voff[m] = (int)vrdesc.size();
@@ -424,8 +440,8 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
             }
             vrdesc.push_back(d);
         }
-        if (en <= kFlatMax) {
-            for (int p0 = 0; p0 < en * (en + 1) / 2; p0 += kFlatPairs) ftasks.push_back(make_int2(m, p0));
+        if (en <= kTriMax) {
+            if (en > 0) ftasks.push_back(m);
         } else {
             const int nt = (en + kPT - 1) / kPT;
             for (int a = 0; a < nt; a++)
@@ -508,13 +524,13 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
         SCP3_CUDA(cudaGetLastError());
     }
     if (p.nftasks) {
-        const size_t fsm = sizeof(double) * ((size_t)kFS * p.nm + 2 * kFS + (size_t)kFS * kFlatMax + 16 * kFS);
+        const size_t fsm = sizeof(double) * ((size_t)kFS * p.nm + 2 * kFS + (size_t)kFS * kTriMax + 16 * kFS);
         if (fsm > 48 * 1024)
-            SCP3_CUDA(cudaFuncSetAttribute(stein_pairs_flat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            SCP3_CUDA(cudaFuncSetAttribute(stein_pairs_tri_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)fsm));
         dim3 fg((unsigned)p.nftasks, (unsigned)p.nsplit);
-        stein_pairs_flat_kernel<<<fg, 256, fsm, s>>>(p.ftasks, p.vrdesc, p.voff, p.doff, p.nm, q, v, vq,
-                                                     k / p.nsplit, p.dsize, p.D);
+        stein_pairs_tri_kernel<<<fg, kTriThreads, fsm, s>>>(p.ftasks, p.vrdesc, p.voff, p.doff, p.nm, q, v, vq,
+                                                            k / p.nsplit, p.dsize, p.D);
         SCP3_CUDA(cudaGetLastError());
     }
     return SCP3GPU_OK;

@@ -120,6 +120,17 @@ def test_argument_errors_before_any_device_work():
     assert "accumulate_normals_f32" in L.scp3gpu_last_error().decode()
 
 
+def test_mlp_shape_limits_without_device():
+    """The surrogate's forward layers run on the tensor cores with N = hidden and
+    K = padded inputs, both at most 256: larger shapes are refused at creation."""
+    from scp3_b200 import _lib
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    for n_in, hidden in ((300, 256), (48, 320), (48, 96), (0, 256)):
+        assert L.scp3gpu_mlp_create(n_in, hidden, 4096, 1, 0, ctypes.byref(h)) == _lib.ERR_ARG
+    assert b"hidden 64, 128, 192 or 256" in L.scp3gpu_last_error()
+
+
 def test_scp1_argument_errors_without_device():
     from scp3_b200 import _lib
     L = _lib.lib()
