@@ -156,7 +156,8 @@ struct SteinPlan {
     int nb = 0, nb_pad = 0, nm = 0;
     int nv = 0, nv_pad = 0;          // virtual rows (with the ground row), padded to 128
     int rt = 0, ct = 0;              // 128-row tiles of the virtual rows and of the basis
-    int nsplit = 1;
+    int nsplit = 1;                  // sample ranges of the products (C)
+    int dsplit = 1;                  // sample ranges of the same-mode pair sums (D), a multiple of nsplit
     int64_t chunk = 0;               // samples per pass
     int64_t dsize = 0;               // doubles of the same-mode pair sums per split
     int ndtasks = 0;
@@ -170,7 +171,7 @@ struct SteinPlan {
     double* W = nullptr;             // [chunk][nv_pad]  reduced function x Stein weight
     double* Phi = nullptr;           // [chunk][nb_pad]  basis functions
     double* C = nullptr;             // [nsplit][rt * ct][128 * 128]
-    double* D = nullptr;             // [nsplit][dsize]
+    double* D = nullptr;             // [dsplit][dsize]
 };
 int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_t chunk, int sms);
 void stein_destroy(SteinPlan& p);

@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(256) stein_pairs_kernel(const int4* __restrict
 // thread four 16-byte loads of R and 16 weight loads for 16 products.  R values
 // (zero past e) and the level-pair weights of a sample chunk are staged in
 // shared memory.
-constexpr int kTriMax = 64, kTriThreads = 160, kFS = 16;
+constexpr int kTriMax = 64, kTriThreads = 160, kFS = 32;
 
 __global__ void __launch_bounds__(kTriThreads) stein_pairs_tri_kernel(const int* __restrict__ modes,
                                                                       const uint32_t* __restrict__ vrdesc,
@@ -336,7 +336,8 @@ __global__ void __launch_bounds__(kTriThreads) stein_pairs_tri_kernel(const int*
 // modes; <0|V|0> from the ground row.
 __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int* __restrict__ rank3,
                                     const int* __restrict__ voff, const int64_t* __restrict__ doff, int nb, int nv,
-                                    int ct, int nsplit, const double* __restrict__ C, const double* __restrict__ D,
+                                    int ct, int nsplit, int dsplit, const double* __restrict__ C,
+                                    const double* __restrict__ D,
                                     int64_t csize, int64_t dsize, double divisor, const double* __restrict__ diag,
                                     double zpe, double* __restrict__ M, int64_t ld)
 {
@@ -367,7 +368,7 @@ __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int
             } else {
                 const int en = voff[m + 1] - voff[m];
                 const int64_t x = doff[m] + (int64_t)rank3[3 * r + a] * en + rank3[3 * c + b];
-                for (int s = 0; s < nsplit; s++) t += D[s * dsize + x];
+                for (int s = 0; s < dsplit; s++) t += D[s * dsize + x];
             }
             val += t;
             ns++;
@@ -472,13 +473,19 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         const double cost = (double)((units + sms - 1) / sms) / ns;
         if (cost < best - 1e-9) best = cost, p.nsplit = ns;
     }
+    // sample ranges of the same-mode pair sums: a multiple of the products' (so a
+    // pass of 16 * nsplit samples divides), up to 4x finer while their sums stay
+    // small -- those kernels have one CTA per mode and range, too few for the GPU
+    // at the products' split (48 x 8 for the hexamer doubles basis)
+    p.dsplit = p.nsplit;
+    while (p.dsplit < 4 * p.nsplit && p.dsplit * 2 * p.dsize * 8 <= (256ll << 20)) p.dsplit *= 2;
     int rc;
     if ((rc = upload(&p.vrdesc, vrdesc.data(), vrdesc.size())) || (rc = upload(&p.rank3, rank3.data(), rank3.size())) ||
         (rc = upload(&p.voff, voff.data(), voff.size())) || (rc = upload(&p.doff, doff.data(), doff.size())) ||
         (p.ndtasks && (rc = upload(&p.dtasks, tasks.data(), tasks.size()))) ||
         (p.nftasks && (rc = upload(&p.ftasks, ftasks.data(), ftasks.size()))) ||
         (rc = dalloc(&p.W, (size_t)p.chunk * p.nv_pad)) || (rc = dalloc(&p.Phi, (size_t)p.chunk * p.nb_pad)) ||
-        (rc = dalloc(&p.C, (size_t)csize * p.nsplit)) || (rc = dalloc(&p.D, (size_t)p.dsize * p.nsplit))) {
+        (rc = dalloc(&p.C, (size_t)csize * p.nsplit)) || (rc = dalloc(&p.D, (size_t)p.dsize * p.dsplit))) {
         stein_destroy(p);
         return rc;
     }
@@ -496,7 +503,7 @@ void stein_destroy(SteinPlan& p)
 int stein_zero(const SteinPlan& p, cudaStream_t s)
 {
     SCP3_CUDA(cudaMemsetAsync(p.C, 0, sizeof(double) * (size_t)p.rt * p.ct * 128 * 128 * p.nsplit, s));
-    SCP3_CUDA(cudaMemsetAsync(p.D, 0, sizeof(double) * (size_t)p.dsize * p.nsplit, s));
+    SCP3_CUDA(cudaMemsetAsync(p.D, 0, sizeof(double) * (size_t)p.dsize * p.dsplit, s));
     return SCP3GPU_OK;
 }
 
@@ -518,8 +525,8 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
         const size_t ps = sizeof(double) * ((size_t)kPS * p.nm + 2 * kPS + 2 * kPS * kPT + 16 * kPS);
         if (ps > 48 * 1024)
             SCP3_CUDA(cudaFuncSetAttribute(stein_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps));
-        dim3 pg((unsigned)p.ndtasks, (unsigned)p.nsplit);
-        stein_pairs_kernel<<<pg, 256, ps, s>>>(p.dtasks, p.vrdesc, p.voff, p.doff, p.nm, q, v, vq, k / p.nsplit,
+        dim3 pg((unsigned)p.ndtasks, (unsigned)p.dsplit);
+        stein_pairs_kernel<<<pg, 256, ps, s>>>(p.dtasks, p.vrdesc, p.voff, p.doff, p.nm, q, v, vq, k / p.dsplit,
                                                p.dsize, p.D);
         SCP3_CUDA(cudaGetLastError());
     }
@@ -528,9 +535,9 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
         if (fsm > 48 * 1024)
             SCP3_CUDA(cudaFuncSetAttribute(stein_pairs_tri_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)fsm));
-        dim3 fg((unsigned)p.nftasks, (unsigned)p.nsplit);
+        dim3 fg((unsigned)p.nftasks, (unsigned)p.dsplit);
         stein_pairs_tri_kernel<<<fg, kTriThreads, fsm, s>>>(p.ftasks, p.vrdesc, p.voff, p.doff, p.nm, q, v, vq,
-                                                            k / p.nsplit, p.dsize, p.D);
+                                                            k / p.dsplit, p.dsize, p.D);
         SCP3_CUDA(cudaGetLastError());
     }
     return SCP3GPU_OK;
@@ -541,7 +548,7 @@ int stein_unpack(const SteinPlan& p, const uint32_t* desc, double divisor, const
 {
     const int64_t total = (int64_t)p.nb * p.nb;
     stein_unpack_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
-        desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.ct, p.nsplit, p.C, p.D, (int64_t)p.rt * p.ct * 128 * 128,
+        desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.ct, p.nsplit, p.dsplit, p.C, p.D, (int64_t)p.rt * p.ct * 128 * 128,
         p.dsize, divisor, diag, zpe, M, ld);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
