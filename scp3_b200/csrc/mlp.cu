@@ -56,11 +56,13 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool vali
 // cp.async into the K-major 64-byte-swizzled layout the MMA descriptors read
 // (per 32-column K box, row r's 16-byte chunk c at c ^ ((r >> 1) & 3)), one
 // thread issues K / 16 MMAs of M = 128, N, K = 16 into a FP32 TMEM accumulator,
-// and each warp reads back its 32 rows, adds the bias and writes Z (FP32, may
-// be null) and H = GELU(Z) (BF16).  The wait for the MMAs is bounded; on expiry
+// and 16 warps read it back -- warp w takes rows 32 (w % 4) .. +31 (its TMEM lane
+// quadrant) and every fourth 32-column chunk from 32 (w / 4) -- add the bias and
+// write Z (FP32, may be null) and H = GELU(Z) (BF16).  The epilogue's GELU is
+// most of the work, hence the 16 warps.  The wait for the MMAs is bounded; on expiry
 // the tile's outputs are written as NaN, which the build's non-finite counters
 // report.
-constexpr int kTM = 128, kTcThreads = 128;
+constexpr int kTM = 128, kTcThreads = 512;
 
 __host__ __device__ inline size_t tc_smem_bytes(int N, int K)
 {
@@ -124,10 +126,10 @@ __global__ void __launch_bounds__(kTcThreads) gemm_bias_gelu_tc(const __nv_bfloa
     }
     const bool ok = mbar_wait(bar, 0, abort);
     tc_fence_after();
-    const int row = m0 + warp * 32 + lane;
-    for (int c0 = 0; c0 < N; c0 += 32) {
+    const int quad = warp & 3, row = m0 + quad * 32 + lane;
+    for (int c0 = (warp >> 2) * 32; c0 < N; c0 += 128) {
         float v[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+        tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
         if (row >= M) continue;
 #pragma unroll
         for (int j = 0; j < 32; j += 2) {
