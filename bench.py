@@ -374,6 +374,17 @@ def run_triples(args):
     print(json.dumps(triples_record(args.samples, args.precision, dump=not args.no_dump)))
 
 
+def guarded(fn, *a):
+    """A sub-record of the default line: its dict, or {"error": ...} if it failed,
+    so the benchmark line itself is always printed."""
+    try:
+        return fn(*a)
+    except Exception as e:            # noqa: BLE001
+        import traceback
+        traceback.print_exc()
+        return {"error": "%s: %s" % (type(e).__name__, e)}
+
+
 def fp64_record(nw, x0, MUa, omega, steps, device):
     """The plain FP64 form on the benchmark's workload (the hexamer doubles
     build, 2^20 points per step): device-timed samples/s and the contraction's
@@ -398,7 +409,7 @@ def fp64_record(nw, x0, MUa, omega, steps, device):
                             "work": "Nb(Nb+1) FLOP per sample, upper triangle"}}
 
 
-def run_cv(args):
+def cv_record(precision, epochs):
     """The learned control variate on the TTM3-F hexamer prism, doubles basis
     (1225 functions): the surrogate trained on 2^18 exact samples, then
     V_nn over 2^24 points + (V - V_nn) over 2^20 exact points, against the
@@ -408,10 +419,9 @@ def run_cv(args):
     import torch
     import scp3_b200
     from scp3_b200 import inputs, surrogate
-    torch.cuda.set_device(0)
     nw, x0, MUa, omega = inputs.load("prism_ttm3f")
     autocm = scp3_b200.constants.autocm
-    prec = args.precision
+    prec = precision
 
     def make():
         return scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=0, pes="ttm3f", precision=prec,
@@ -446,7 +456,7 @@ def run_cv(args):
     net = surrogate.MLP(48, hidden=256, max_batch=1 << 18, seed=11)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    loss = net.fit(q, v.astype(np.float32), epochs=args.cv_epochs, batch=4096, lr=2e-3)
+    loss = net.fit(q, v.astype(np.float32), epochs=epochs, batch=4096, lr=2e-3)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     y = net(q[:1 << 16])
@@ -483,38 +493,43 @@ def run_cv(args):
         M_eq, t = plain(n_eq, off)
         t_eq = max(t_eq, t)
         eq_trials.append(err(M_eq))
-    print(json.dumps({"config": {"workload": "hexamer prism TTM3-F, doubles basis Nb=1225; surrogate 48-256-256-256-1 "
+    return {"config": {"workload": "hexamer prism TTM3-F, doubles basis Nb=1225; surrogate 48-256-256-256-1 "
                                              "GELU trained on 2^18 exact samples; V_nn over 2^24 + residual over 2^20",
                                  "precision": prec, "trials": "3 independent Sobol ranges for the exact points"},
-                      "train": {"samples": 1 << 18, "epochs": args.cv_epochs, "sample_s": t_sample,
+                      "train": {"samples": 1 << 18, "epochs": epochs, "sample_s": t_sample,
                                 "train_s": t_train, "final_batch_loss": loss, "r2_heldin": r2},
                       "control_variate": {"gpu_s": t_cv, "max_level_err_cm1": cv_trials,
                                           "mean": float(np.mean(cv_trials))},
                       "plain_2^21": {"gpu_s": t_p21, "max_level_err_cm1": err(M_p21)},
                       "plain_equal_time": {"samples": n_eq, "gpu_s": t_eq, "max_level_err_cm1": eq_trials,
                                            "mean": float(np.mean(eq_trials))},
-                      "reference": {"samples": 1 << 26, "gpu_s": t_ref, "lowest10_cm1": [float(x) for x in e_ref]}}))
+                      "reference": {"samples": 1 << 26, "gpu_s": t_ref, "lowest10_cm1": [float(x) for x in e_ref]}}
 
 
-def run_batch(args):
+def run_cv(args):
+    """--config cv: cv_record (one JSON line)."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(cv_record(args.precision, args.cv_epochs)))
+
+
+def batch_record(precision, n, steps, warmup):
     """The batched build: 32 qTIP4P/f clusters of 2..8 waters (doubles bases of
-    91..946 functions, scp3_b200.inputs.batch_clusters), 2^18 scrambled points
-    per cluster, built in one batch (one CUDA graph replay per step, autotuned
+    91..946 functions, scp3_b200.inputs.batch_clusters), n scrambled points per
+    cluster, built in one batch (one CUDA graph replay per step, autotuned
     contraction work shape) against 32 sequential single builds of the same
     precision and 32 sequential plain FP64 builds.  Levels of every cluster
-    against its FP64 build.  One JSON line; not the benchmark's default."""
+    against its FP64 build."""
     import torch
     import scp3_b200
     from scp3_b200 import inputs
-    torch.cuda.set_device(0)
-    n = args.samples if args.samples != 1 << 20 else 1 << 18
     cl = inputs.batch_clusters()
     for c in cl:
         c["scramble_seed"] = SCRAMBLE_SEED
     spec = [{k: v for k, v in c.items() if k != "name"} for c in cl]
     autocm = scp3_b200.constants.autocm
     t0 = time.perf_counter()
-    b = scp3_b200.Batch(spec, precision=args.precision)
+    b = scp3_b200.Batch(spec, precision=precision)
     t_create = time.perf_counter() - t0
     nsplit, ctas, chunk, tuned_ms = b.shape()
 
@@ -535,9 +550,9 @@ def run_batch(args):
             ms.append(e0.elapsed_time(e1))
         return float(np.median(ms))
 
-    ms_graph = timed_batch(b, args.steps, args.warmup)
-    bd = scp3_b200.Batch(spec, precision=args.precision, graph=False)
-    ms_direct = timed_batch(bd, args.steps, 1)
+    ms_graph = timed_batch(b, steps, warmup)
+    bd = scp3_b200.Batch(spec, precision=precision, graph=False)
+    ms_direct = timed_batch(bd, steps, 1)
     bd.close()
 
     def sequential(prec):
@@ -555,7 +570,7 @@ def run_batch(args):
         torch.cuda.synchronize()
         return hbs, 1e3 * (time.perf_counter() - t0)
 
-    seq, ms_seq = sequential(args.precision)
+    seq, ms_seq = sequential(precision)
     seq64, ms_seq64 = sequential("fp64")
     # accuracy: the batch against the same-precision single builds (same kernels) and FP64 levels
     b.reset()
@@ -573,11 +588,13 @@ def run_batch(args):
                     "max_level_err_cm1": err})
     for hb in seq + seq64:
         hb.close()
+    basis_sizes = list(b.nb)
+    b.close()
     total = len(cl) * n
-    print(json.dumps({
+    return {
         "config": {"workload": "32 qTIP4P/f clusters, 2..8 waters, 12..42 modes, doubles bases 91..946, "
-                               "2^18 scrambled Sobol points per cluster", "precision": args.precision,
-                   "clusters": len(cl), "samples_per_cluster": n, "basis_sizes": b.nb},
+                               "%d scrambled Sobol points per cluster" % n, "precision": precision,
+                   "clusters": len(cl), "samples_per_cluster": n, "basis_sizes": basis_sizes},
         "metric": "cluster-samples/s", "unit": "samples/s",
         "batch_graph": {"ms": ms_graph, "value": total / (ms_graph * 1e-3)},
         "batch_direct": {"ms": ms_direct, "value": total / (ms_direct * 1e-3)},
@@ -586,7 +603,15 @@ def run_batch(args):
         "speedup_vs_sequential": ms_seq / ms_graph, "speedup_vs_sequential_fp64": ms_seq64 / ms_graph,
         "work_shape": {"nsplit": nsplit, "ctas": ctas, "samples_per_pass": chunk, "tuned_contract_ms": tuned_ms,
                        "create_s": t_create},
-        "max_rel_diff_vs_single_builds": worst_same, "max_level_err_cm1_vs_fp64": worst_lvl, "clusters": per}))
+        "max_rel_diff_vs_single_builds": worst_same, "max_level_err_cm1_vs_fp64": worst_lvl, "clusters": per}
+
+
+def run_batch(args):
+    """--config batch: batch_record at 2^18 points per cluster (one JSON line)."""
+    import torch
+    torch.cuda.set_device(0)
+    n = args.samples if args.samples != 1 << 20 else 1 << 18
+    print(json.dumps(batch_record(args.precision, n, args.steps, args.warmup)))
 
 
 def run_gradient(args):
@@ -892,12 +917,17 @@ def main():
         # the plain form on the same workload, and the triples configuration with its
         # split-vs-FP64 ratio: the two other numbers the metric's target is read from
         hb.close()
-        line["fp64"] = fp64_record(nw, x0, MUa, omega, 3, local)
-        line["triples"] = triples_record(TRIPLES_SAMPLES, args.precision)
-        t = line["triples"]
-        line["target"] = {"triples_speedup_vs_fp64": t["speedup_vs_fp64"], "wanted": ">= 10",
-                          "triples_max_level_err_cm1": t["max_abs_err_cm1_vs_fp64"], "wanted_cm1": "<= 0.1",
-                          "doubles_speedup_vs_fp64": value / line["fp64"]["value"]}
+        line["fp64"] = guarded(fp64_record, nw, x0, MUa, omega, 3, local)
+        line["triples"] = guarded(triples_record, TRIPLES_SAMPLES, args.precision)
+        t, f = line["triples"], line["fp64"]
+        if "error" not in t and "error" not in f:
+            line["target"] = {"triples_speedup_vs_fp64": t["speedup_vs_fp64"], "wanted": ">= 10",
+                              "triples_max_level_err_cm1": t["max_abs_err_cm1_vs_fp64"], "wanted_cm1": "<= 0.1",
+                              "doubles_speedup_vs_fp64": value / f["value"]}
+        # configs C4 and C5 in compact form (their full lines: --config batch, --config cv)
+        bt = guarded(batch_record, args.precision, 1 << 18, 3, 1)
+        line["batch"] = bt if "error" in bt else {k: v for k, v in bt.items() if k != "clusters"}
+        line["cv"] = guarded(cv_record, args.precision, 100)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         normals = scp3_b200.std_normals(nm0, 0, 1 << 17, scramble_seed=SCRAMBLE_SEED)
         line["cpu_baseline"] = cpu_reference(nw, x0, MUa, omega, np.arange(nm0, dtype=np.int32), 48, 0, normals)
