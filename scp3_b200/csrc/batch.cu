@@ -58,7 +58,7 @@ struct scp3gpu_batch {
     int ctas = 0;                      // chosen grid (one per unit, or one per SM looping over units)
     double tuned_ms = 0.0;
     int4* tiles = nullptr;
-    int* tile_index = nullptr;         // per cluster, owner of block (ti, tj): 2 * tile + column half
+    int* tile_index = nullptr;         // per cluster, owner of block (ti <= tj): 4 * tile + 2 * transposed + half
     double* partial = nullptr;
     int* err_flag = nullptr;
     // pass buffers

@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const int4 ti = tiles[u % ntiles];
                 const uint16_t* pa = xop + (size_t)(ti.x / kTile) * nkb_alloc * (2 * kBoxElems);
                 const uint16_t* pb0 = xop + (size_t)(ti.y / kTile) * nkb_alloc * (2 * kBoxElems);
-                const uint16_t* pb1 = pb0 + (size_t)nkb_alloc * (2 * kBoxElems);
+                const uint16_t* pb1 = xop + (size_t)(ti.w / kTile) * nkb_alloc * (2 * kBoxElems);
                 for (int kb = lo; kb < hi; kb++) {
                     if (!mbar_wait(empty + stage, phase ^ 1, abort)) {
                         ok = false;
@@ -299,9 +299,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // Dense column-major nb x nb from the 128 x 256 tiles' unit partials: element
-// (r <= c) lies in block (r / 128, c / 128), owned by tile t at column half h
-// (block_owner = 2 t + h); its value is the sum over the splits, in order, of
-// unit (split * ntiles + t) at row r % 128 and column 128 h + c % 128.
+// (r <= c) lies in block (r / 128, c / 128), owned by tile t at column half h,
+// as itself or transposed (block_owner = 4 t + 2 transposed + h); its value is
+// the sum over the splits, in order, of unit (split * ntiles + t) at row
+// r % 128 and column 128 h + c % 128 (transposed: row c % 128, column
+// 128 h + r % 128).
 __global__ void unpack_n256_kernel(const double* __restrict__ partial, const int* __restrict__ block_owner, int nt,
                                    int ntiles, int nsplit, int nb, double divisor, const double* __restrict__ diag,
                                    double zpe, double* __restrict__ M, int64_t ld)
@@ -312,8 +314,9 @@ __global__ void unpack_n256_kernel(const double* __restrict__ partial, const int
     const int r = min(i, j), c = max(i, j);
     const int ti = r / kTile, tj = c / kTile;
     const int own = block_owner[ti * nt + tj];
-    const int t = own >> 1, h = own & 1;
-    const size_t off = (size_t)(h * kTile + (c - tj * kTile)) * kTile + (r - ti * kTile);
+    const int t = own >> 2, h = own & 1;
+    const int rr = r - ti * kTile, cc = c - tj * kTile;
+    const size_t off = (own & 2) ? (size_t)(h * kTile + rr) * kTile + cc : (size_t)(h * kTile + cc) * kTile + rr;
     double val = 0.0;
     for (int s = 0; s < nsplit; s++) val += partial[((size_t)s * ntiles + t) * (size_t)(kTile * kN2) + off];
     val = val / divisor;
@@ -643,28 +646,73 @@ void record(std::vector<cudaEvent_t>* pev, std::vector<int>* pkind, int kind, cu
 
 }  // namespace
 
-// The 128 x 256 tiling of a cluster's upper block triangle (nt x nt grid of
-// 128 x 128 blocks, nt even; blocks ti <= tj < nt_need hold basis rows): row
-// panel ti takes the aligned column pairs (2q, 2q+1) that hold a needed block,
-// owning both halves or one.  Tiles come in 12-row x 6-pair groups so that a
-// wave of CTAs shares panels.
+// The 128 x 256 tiling of a cluster's upper block triangle: blocks
+// {ti, tj} of 128 x 128, ti <= tj < nt_need, each needed once.  A tile is one A
+// panel p against two B panels (q, r) and yields blocks (p, q) and (p, r); a
+// block (p, q) with q < p is the transpose of the needed block (q, p), so the
+// read-out takes it transposed.  Which panel plays A for block {i, j} is an
+// orientation of the complete graph on the panels (with a loop per panel):
+// panel i starts with the blocks j >= i (nt_need - i of them), panels with an
+// odd count are paired in order and each pair's block moves to the later
+// panel, so at most one panel keeps an odd count.  Each panel's blocks, in
+// column order, pair up into tiles; an odd one out makes a one-half tile (both
+// B panels the same).  That is ceil(nt_need (nt_need + 1) / 4) tiles, the
+// fewest that cover the triangle (55 blocks on 10 panels: 28 tiles, where
+// aligned column pairs need 30).  Tiles come in 12-row x 6-pair groups so that
+// a wave of CTAs shares panels.
 void add_cluster_tiles(std::vector<BaseTile>& base, int cluster, int nt, int nt_need, int row0, int neg_off)
 {
+    (void)nt;
+    const int n = nt_need;
+    std::vector<std::vector<int>> cols(n);       // B panels of A panel p; negative = transposed, ~q
+    for (int i = 0; i < n; i++)
+        for (int j = i; j < n; j++) cols[i].push_back(j);
+    int odd = -1;
+    for (int i = 0; i < n; i++) {
+        if ((n - i) % 2 == 0) continue;
+        if (odd < 0) {
+            odd = i;
+            continue;
+        }
+        // block {odd, i}: from panel odd's list to panel i's, transposed
+        std::vector<int>& a = cols[odd];
+        a.erase(std::find(a.begin(), a.end(), i));
+        std::vector<int>& b = cols[i];
+        b.insert(std::lower_bound(b.begin(), b.end(), odd,
+                                  [](int x, int v) { return (x < 0 ? ~x : x) < v; }),
+                 ~odd);
+        odd = -1;
+    }
     const int R = 12, C = 6;
-    for (int r0 = 0; r0 < nt_need; r0 += R)
-        for (int c0 = 0; c0 < nt / 2; c0 += C)
-            for (int ti = r0; ti < std::min(r0 + R, nt_need); ti++)
-                for (int q = c0; q < std::min(c0 + C, nt / 2); q++) {
-                    const int a = 2 * q, b = 2 * q + 1;
-                    const int halves = (a >= ti && a < nt_need ? 1 : 0) | (b >= ti && b < nt_need ? 2 : 0);
-                    if (halves) base.push_back(BaseTile{cluster, ti, a, halves, row0, neg_off});
+    int maxp = 0;
+    for (int i = 0; i < n; i++) maxp = std::max(maxp, (int)(cols[i].size() + 1) / 2);
+    for (int r0 = 0; r0 < n; r0 += R)
+        for (int c0 = 0; c0 < maxp; c0 += C)
+            for (int ti = r0; ti < std::min(r0 + R, n); ti++)
+                for (int k = c0; k < std::min(c0 + C, maxp); k++) {
+                    const std::vector<int>& l = cols[ti];
+                    if (2 * k >= (int)l.size()) continue;
+                    const int a = l[2 * k];
+                    const bool two = 2 * k + 1 < (int)l.size();
+                    const int b = two ? l[2 * k + 1] : a;
+                    BaseTile t;
+                    t.cluster = cluster;
+                    t.ti = ti;
+                    t.s0 = a < 0 ? ~a : a;
+                    t.s1 = b < 0 ? ~b : b;
+                    t.halves = two ? 3 : 1;
+                    t.tr = (a < 0 ? 1 : 0) | (two && b < 0 ? 2 : 0);
+                    t.row0 = row0;
+                    t.neg_off = neg_off;
+                    base.push_back(t);
                 }
 }
 
 // Chooses the number of tiles (the base tiling, with some pairs split into two
 // one-half tiles) and of splits, minimising waves / splits -- the contraction
 // time in units of one whole-pass tile -- over at most 16 splits and 4 GB of
-// partials; emits the tiles and, per cluster, owner[ti * nt + tj] = 2 tile + half.
+// partials; emits the tiles and, per cluster, owner[ti * nt + tj] (ti <= tj) =
+// 4 tile + 2 transposed + half.
 void finish_tiling(const std::vector<BaseTile>& base, const std::vector<int>& cluster_nt, int sms,
                    std::vector<int4>& tiles, std::vector<std::vector<int>>& owner, int& nsplit)
 {
@@ -689,21 +737,29 @@ void finish_tiling(const std::vector<BaseTile>& base, const std::vector<int>& cl
     tiles.clear();
     owner.assign(cluster_nt.size(), {});
     for (size_t c = 0; c < cluster_nt.size(); c++) owner[c].assign((size_t)cluster_nt[c] * cluster_nt[c], -1);
+    // the block that half h of tile `index` yields, owned by that tile
+    auto own = [&](const BaseTile& t, int h, int index, int half_in_tile) {
+        const int nt = cluster_nt[t.cluster];
+        const int s = h ? t.s1 : t.s0;
+        const int tr = (t.tr >> h) & 1;
+        const int r = tr ? s : t.ti, c = tr ? t.ti : s;
+        owner[t.cluster][(size_t)r * nt + c] = 4 * index + 2 * tr + half_in_tile;
+    };
     int extra = bestT - tmin;
     for (const BaseTile& t : base) {
-        const int nt = cluster_nt[t.cluster];
-        const int4 tile = make_int4(t.row0 + t.ti * kTile, t.row0 + t.s * kTile, t.neg_off, t.cluster);
+        const int a = t.row0 + t.ti * kTile;
         if (t.halves == 3 && extra > 0) {
             extra--;
             for (int h = 0; h < 2; h++) {
-                owner[t.cluster][(size_t)t.ti * nt + t.s + h] = 2 * (int)tiles.size() + h;
-                tiles.push_back(tile);
+                const int b = t.row0 + (h ? t.s1 : t.s0) * kTile;
+                own(t, h, (int)tiles.size(), 0);
+                tiles.push_back(make_int4(a, b, t.neg_off, b));
             }
             continue;
         }
         for (int h = 0; h < 2; h++)
-            if (t.halves & (1 << h)) owner[t.cluster][(size_t)t.ti * nt + t.s + h] = 2 * (int)tiles.size() + h;
-        tiles.push_back(tile);
+            if (t.halves & (1 << h)) own(t, h, (int)tiles.size(), h);
+        tiles.push_back(make_int4(a, t.row0 + t.s0 * kTile, t.neg_off, t.row0 + t.s1 * kTile));
     }
     nsplit = bestM;
 }
@@ -893,3 +949,31 @@ int unpack(Plan& p, int nb, double divisor, const double* diag, double zpe, doub
 
 }  // namespace tc
 }  // namespace scp3
+
+// Host-only view of the 128 x 256 tiling of one cluster with nt_need 128-row
+// panels on `sms` SMs, for tests: the tile count, splits, and per tile (A
+// panel, B panel 0, B panel 1), and owner[ti * nt + tj] for nt = nt_need
+// rounded up to even.  tiles may be null (counts only).
+extern "C" int scp3gpu_internal_tiling(int nt_need, int sms, int* ntiles, int* nsplit, int* tiles, int max_tiles,
+                                       int* owner)
+{
+    using namespace scp3::tc;
+    if (nt_need < 1 || sms < 1 || !ntiles || !nsplit) return SCP3GPU_ERR_ARG;
+    const int nt = (nt_need + 1) / 2 * 2;
+    std::vector<BaseTile> base;
+    add_cluster_tiles(base, 0, nt, nt_need, 0, 0);
+    std::vector<int4> t;
+    std::vector<std::vector<int>> own;
+    finish_tiling(base, std::vector<int>{nt}, sms, t, own, *nsplit);
+    *ntiles = (int)t.size();
+    if (tiles) {
+        if ((int)t.size() > max_tiles) return SCP3GPU_ERR_ARG;
+        for (size_t i = 0; i < t.size(); i++) {
+            tiles[3 * i] = t[i].x / kTile;
+            tiles[3 * i + 1] = t[i].y / kTile;
+            tiles[3 * i + 2] = t[i].w / kTile;
+        }
+    }
+    if (owner) std::copy(own[0].begin(), own[0].end(), owner);
+    return SCP3GPU_OK;
+}

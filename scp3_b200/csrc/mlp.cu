@@ -5,10 +5,12 @@
 // potential at every point, SCP3.cpp:205-225).
 //
 //   forward    gemm_bias_gelu_tc: Y = GELU(X W^T + b) on the tcgen05 tensor
-//              cores, one 128-sample tile per CTA against all outputs (M = 128,
-//              N = hidden, K = 16 MMAs into a FP32 TMEM accumulator), activations
-//              stored BF16 for the next layer and FP32 pre-activations kept for
-//              training;
+//              cores, persistent (one CTA per SM, the layer's weights resident
+//              in shared memory), 128-sample tiles against all outputs (M = 128,
+//              N = hidden, K = 16 MMAs into one of two FP32 TMEM accumulators,
+//              the next tile loaded and multiplied while the last is drained),
+//              activations stored BF16 for the next layer and FP32
+//              pre-activations kept for training;
 //              head_kernel: y = h3 . w4 + b4, one warp per sample
 //   backward   FP32 register-tiled GEMMs for dX = dZ W and dW = dZ^T X,
 //              gelu_backward for dZ = dH * GELU'(Z), a per-column reduction for
@@ -52,24 +54,26 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool vali
 
 // Y[M][N] = act(X[M][K] W[N][K]^T + b) on the tensor cores.  X, W BF16
 // row-major (K contiguous); N a multiple of 32 up to 256, K a multiple of 32 up
-// to 256, any M.  A CTA takes 128 rows of X: it stages them and all of W with
-// cp.async into the K-major 64-byte-swizzled layout the MMA descriptors read
-// (per 32-column K box, row r's 16-byte chunk c at c ^ ((r >> 1) & 3)), one
-// thread issues K / 16 MMAs of M = 128, N, K = 16 into a FP32 TMEM accumulator,
-// and 16 warps read it back -- warp w takes rows 32 (w % 4) .. +31 (its TMEM lane
-// quadrant) and every fourth 32-column chunk from 32 (w / 4) -- add the bias and
-// write Z (FP32, may be null) and H = GELU(Z) (BF16).  The epilogue's GELU is
-// most of the work, hence the 16 warps.  The wait for the MMAs is bounded; on expiry
-// the tile's outputs are written as NaN, which the build's non-finite counters
-// report.
-constexpr int kTM = 128, kTcThreads = 512;
+// to 256, any M.  Persistent: a CTA stages all of W once, then takes 128-row
+// tiles of X in turn (tile blockIdx.x, + gridDim.x, ...), in the K-major
+// 64-byte-swizzled layout the MMA descriptors read (per 32-column K box, row r's
+// 16-byte chunk c at c ^ ((r >> 1) & 3)).  Warps 0-3 load a tile with cp.async
+// once the previous tile's MMAs have read their buffer, and thread 0 issues its
+// K / 16 MMAs of M = 128, N, K = 16 into one of two FP32 TMEM accumulators; warps
+// 4-15 drain the other accumulator meanwhile -- warp w reads rows 32 ((w - 4) % 4)
+// .. +31 (its TMEM lane quadrant) and every third 32-column chunk from
+// 32 ((w - 4) / 4) -- add the bias and write Z (FP32, may be null) and
+// H = GELU(Z) (BF16).  Every wait is bounded; after an expiry the CTA stops
+// issuing and the tiles it could not finish are written as NaN, which the
+// build's non-finite counters report.
+constexpr int kTM = 128, kTcThreads = 512, kLoadThreads = 128, kEpiWarpsL = 12;
 
 __host__ __device__ inline size_t tc_smem_bytes(int N, int K)
 {
-    return (size_t)(K / 32) * (kTM + N) * 64 + 64 + 1024;   // operands, barrier + TMEM slot, alignment
+    return (size_t)(K / 32) * (kTM + N) * 64 + 128 + (size_t)N * 4 + 1024;   // operands, barriers, bias, alignment
 }
 
-__global__ void __launch_bounds__(kTcThreads) gemm_bias_gelu_tc(const __nv_bfloat16* __restrict__ X,
+__global__ void __launch_bounds__(kTcThreads, 1) gemm_bias_gelu_tc(const __nv_bfloat16* __restrict__ X,
                                                                 const __nv_bfloat16* __restrict__ W,
                                                                 const float* __restrict__ b, int M, int N, int K,
                                                                 float* __restrict__ Z,
@@ -80,71 +84,134 @@ __global__ void __launch_bounds__(kTcThreads) gemm_bias_gelu_tc(const __nv_bfloa
     const int nkb = K / 32;
     uint8_t* As = sm;                                  // [nkb][128 rows][64 B]
     uint8_t* Bs = sm + (size_t)nkb * kTM * 64;         // [nkb][N rows][64 B]
-    uint64_t* bar = reinterpret_cast<uint64_t*>(Bs + (size_t)nkb * N * 64);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+    uint64_t* done = reinterpret_cast<uint64_t*>(Bs + (size_t)nkb * N * 64);   // [2] MMAs of a tile complete
+    uint64_t* freed = done + 2;                        // [2] accumulator drained
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(freed + 2);
     volatile int* abort = reinterpret_cast<volatile int*>(tslot + 1);
+    volatile int* stop = abort + 1;                    // the loaders' own exit flag, written by thread 0
+    float* bias = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(done) + 128);   // [N]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * kTM;
-    const uint32_t ncol = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;   // TMEM: a power of 2 >= 32
+    const int ntiles = (M + kTM - 1) / kTM;
+    const uint32_t ncol = N <= 32 ? 32u : N <= 64 ? 64u : N <= 128 ? 128u : 256u;   // per accumulator
     if (tid == 0) {
-        mbar_init(bar, 1);
+        for (int a = 0; a < 2; a++) {
+            mbar_init(done + a, 1);
+            mbar_init(freed + a, kEpiWarpsL);
+        }
         *abort = 0;
+        *stop = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                     "r"(ncol));
+                     "r"(2 * ncol));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     const int kc = K / 8;                              // 16-byte chunks per row
-    for (int e = tid; e < kTM * kc; e += kTcThreads) {
-        const int r = e / kc, c = e - r * kc, cc = c & 3;
-        const bool ok = m0 + r < M;
-        cp_async16(As + (size_t)(c >> 2) * kTM * 64 + r * 64 + ((cc ^ ((r >> 1) & 3)) << 4),
-                   X + (size_t)(ok ? m0 + r : 0) * K + c * 8, ok);
-    }
+    for (int j = tid; j < N; j += kTcThreads) bias[j] = b[j];
     for (int e = tid; e < N * kc; e += kTcThreads) {
         const int r = e / kc, c = e - r * kc, cc = c & 3;
         cp_async16(Bs + (size_t)(c >> 2) * N * 64 + r * 64 + ((cc ^ ((r >> 1) & 3)) << 4), W + (size_t)r * K + c * 8,
                    true);
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the tensor core reads what the copies wrote
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the tensor core reads what was copied
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
-    if (tid == 0) {
+
+    if (warp < kLoadThreads / 32) {
+        // loaders and, on thread 0, the MMA issue
         const uint32_t idesc =
             (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
-        for (int kb = 0; kb < nkb; kb++) {
-            const uint64_t a = smem_desc64(As + (size_t)kb * kTM * 64), bd = smem_desc64(Bs + (size_t)kb * N * 64);
+        // Thread 0 alone waits and decides; the other loaders learn the outcome
+        // from *stop after a named barrier, so all 128 take the same path
+        int i = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
+            const int a = i & 1;
+            // the buffer is free once the previous tile's MMAs have read it
+            if (tid == 0 && i > 0 && !mbar_wait(done + ((i - 1) & 1), ((i - 1) >> 1) & 1, abort)) *stop = 1;
+            asm volatile("bar.sync 1, %0;" ::"n"(kLoadThreads) : "memory");
+            if (*stop) break;
+            const int m0 = t * kTM;
+            for (int e = tid; e < kTM * kc; e += kLoadThreads) {
+                const int r = e / kc, c = e - r * kc, cc = c & 3;
+                const bool ok = m0 + r < M;
+                cp_async16(As + (size_t)(c >> 2) * kTM * 64 + r * 64 + ((cc ^ ((r >> 1) & 3)) << 4),
+                           X + (size_t)(ok ? m0 + r : 0) * K + c * 8, ok);
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("bar.sync 1, %0;" ::"n"(kLoadThreads) : "memory");
+            if (tid == 0) {
+                if (!mbar_wait(freed + a, ((i >> 1) & 1) ^ 1, abort)) {   // the epilogue is done with it
+                    *stop = 1;
+                    *abort = 1;
+                } else {
+                    tc_fence_after();
+                    const uint32_t d = tmem + (uint32_t)a * ncol;
+                    for (int kb = 0; kb < nkb; kb++) {
+                        const uint64_t ad = smem_desc64(As + (size_t)kb * kTM * 64);
+                        const uint64_t bd = smem_desc64(Bs + (size_t)kb * N * 64);
 #pragma unroll
-            for (int kk = 0; kk < 2; kk++) mma_bf16(tmem, a + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0);
+                        for (int kk = 0; kk < 2; kk++) mma_bf16(d, ad + 2 * kk, bd + 2 * kk, idesc, (kb | kk) != 0);
+                    }
+                    mma_commit(done + a);
+                }
+            }
         }
-        mma_commit(bar);
-    }
-    const bool ok = mbar_wait(bar, 0, abort);
-    tc_fence_after();
-    const int quad = warp & 3, row = m0 + quad * 32 + lane;
-    for (int c0 = (warp >> 2) * 32; c0 < N; c0 += 128) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
-        if (row >= M) continue;
+        // the epilogue waits for the last tile's MMAs before the CTA frees TMEM
+    } else {
+        const int ew = warp - kLoadThreads / 32, quad = ew & 3, grp = ew >> 2;
+        int i = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
+            const int a = i & 1;
+            // warp-uniform outcome: the TMEM loads below are warp-collective
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(done + a, (i >> 1) & 1, abort));
+            tc_fence_after();
+            const int row = t * kTM + quad * 32 + lane;
+            for (int c0 = grp * 32; c0 < N; c0 += 32 * (kEpiWarpsL / 4)) {
+                float v[32];
+                __syncwarp();
+                if (ok) tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(a * ncol + c0), v);
+                if (row < M) {
+                    // 8 columns at a time: one 16-byte store of H, two of Z
 #pragma unroll
-        for (int j = 0; j < 32; j += 2) {
-            const float z0 = ok ? v[j] + b[c0 + j] : __int_as_float(0x7fc00000);
-            const float z1 = ok ? v[j + 1] + b[c0 + j + 1] : __int_as_float(0x7fc00000);
-            if (Z) *reinterpret_cast<float2*>(Z + (size_t)row * N + c0 + j) = make_float2(z0, z1);
-            const float h0 = apply_gelu ? gelu(z0) : z0, h1 = apply_gelu ? gelu(z1) : z1;
-            *reinterpret_cast<__nv_bfloat162*>(H + (size_t)row * N + c0 + j) = __floats2bfloat162_rn(h0, h1);
+                    for (int j = 0; j < 32; j += 8) {
+                        const float4 b0 = *reinterpret_cast<const float4*>(bias + c0 + j);
+                        const float4 b1 = *reinterpret_cast<const float4*>(bias + c0 + j + 4);
+                        const float bj[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+                        float z[8];
+#pragma unroll
+                        for (int e = 0; e < 8; e++) z[e] = ok ? v[j + e] + bj[e] : __int_as_float(0x7fc00000);
+                        if (Z) {
+                            float4* zp = reinterpret_cast<float4*>(Z + (size_t)row * N + c0 + j);
+                            zp[0] = make_float4(z[0], z[1], z[2], z[3]);
+                            zp[1] = make_float4(z[4], z[5], z[6], z[7]);
+                        }
+                        uint32_t hv[4];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) {
+                            const float h0 = apply_gelu ? gelu(z[2 * e]) : z[2 * e];
+                            const float h1 = apply_gelu ? gelu(z[2 * e + 1]) : z[2 * e + 1];
+                            const __nv_bfloat162 hb = __floats2bfloat162_rn(h0, h1);
+                            hv[e] = *reinterpret_cast<const uint32_t*>(&hb);
+                        }
+                        *reinterpret_cast<uint4*>(H + (size_t)row * N + c0 + j) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(freed + a);
         }
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncol));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * ncol));
     }
 }
 
@@ -154,7 +221,11 @@ int launch_layer(const __nv_bfloat16* X, const __nv_bfloat16* W, const float* b,
     if (N % 32 || N > 256 || K % 32 || K > 256) return fail(SCP3GPU_ERR_ARG, "mlp layer: shape out of range");
     const size_t sm = tc_smem_bytes(N, K);
     SCP3_CUDA(cudaFuncSetAttribute(gemm_bias_gelu_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    gemm_bias_gelu_tc<<<(unsigned)((M + kTM - 1) / kTM), kTcThreads, sm, s>>>(X, W, b, M, N, K, Z, H, 1);
+    int dev = 0, sms = 148;
+    SCP3_CUDA(cudaGetDevice(&dev));
+    SCP3_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int tiles = (M + kTM - 1) / kTM;
+    gemm_bias_gelu_tc<<<(unsigned)std::max(1, std::min(tiles, sms)), kTcThreads, sm, s>>>(X, W, b, M, N, K, Z, H, 1);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }

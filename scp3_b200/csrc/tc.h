@@ -30,8 +30,8 @@ struct Plan {
     uint16_t* x[2] = {nullptr, nullptr};
     int* slot_of[2] = {nullptr, nullptr};    // [slots] K slot -> sample (-1: zero padding)
     int* group_meta[2] = {nullptr, nullptr}; // per 4096-sample block: first negative 16-group
-    int4* tiles2 = nullptr;       // [ntiles] (first A row, first B row, sign-table offset, cluster) of each 128 x 256 tile
-    int* tile_index = nullptr;    // [nt*nt] owner of block (ti, tj): 2 * tile + column half
+    int4* tiles2 = nullptr;       // [ntiles] (A row, B rows 0..127, sign-table offset, B rows 128..255) of each 128 x 256 tile
+    int* tile_index = nullptr;    // [nt*nt] owner of block (ti <= tj): 4 * tile + 2 * transposed + column half
     uint32_t* factors = nullptr;  // [nb] basis functions as products of Hermite-table entries
     ExpandDesc* desc_dev = nullptr;   // [2] expansion descriptors of the two pass buffers
     ExpandDesc desc_host[2] = {};     // what desc_dev holds (uploaded again only when it changes)
@@ -69,7 +69,9 @@ int launch_expand(const ExpandDesc* descs_dev, int nclusters, int max_nb_pad, in
                   uint16_t* x, bool f16, cudaStream_t s);
 // 128 x 256 tiling shared by the single build and the batch (contract_tc.cu).
 struct BaseTile {
-    int cluster, ti, s, halves;   // row panel, first column panel (even), owned halves (bit 0: s, bit 1: s + 1)
+    int cluster, ti;              // A panel
+    int s0, s1, halves;           // B panels; halves owned (bit 0: s0, bit 1: s1)
+    int tr;                       // bit h: half h yields the transpose of needed block (s_h, ti)
     int row0, neg_off;            // the cluster's first operand row and sign-group table offset
 };
 void add_cluster_tiles(std::vector<BaseTile>& base, int cluster, int nt, int nt_need, int row0, int neg_off);

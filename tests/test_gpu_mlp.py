@@ -43,6 +43,22 @@ def test_forward_and_gradients_match_oracle(sur):
             k += n
 
 
+def test_forward_many_tiles_per_block_matches_oracle(sur):
+    """A batch that gives every resident block of the persistent layer kernel
+    several 128-row tiles (both TMEM accumulators, each reused) and ends in a
+    ragged tile."""
+    from oracle import mlp_oracle as mo
+    rng = np.random.default_rng(4)
+    m = 3 * 148 * 128 + 77
+    net = sur.MLP(48, hidden=256, max_batch=1 << 16, seed=8)
+    net.set_output(0.02, -0.06)
+    q = rng.normal(scale=np.sqrt(0.5), size=(m, 48)).astype(np.float32)
+    y = net(q)
+    y_or, _ = mo.forward(net.get_params(), q, 48, 256, 0.02, -0.06)
+    assert y.shape == (m,) and np.all(np.isfinite(y))
+    assert np.allclose(y, y_or, rtol=2e-3, atol=1e-5), np.abs(y - y_or).max()
+
+
 def test_training_fits_a_smooth_function(sur):
     rng = np.random.default_rng(1)
     q = rng.normal(scale=np.sqrt(0.5), size=(1 << 14, 48)).astype(np.float32)
