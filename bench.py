@@ -614,41 +614,64 @@ def run_batch(args):
     print(json.dumps(batch_record(args.precision, n, args.steps, args.warmup)))
 
 
+def gradient_form(prec, nw, x0, MUa, omega, n, steps, warmup):
+    """One form of the gradient-estimator build on the hexamer doubles basis:
+    device-timed samples/s over `steps` accumulate calls of n points, the kernel
+    split, and the 10 lowest levels (cm^-1) of Mout over those points."""
+    import scp3_b200
+    hb = scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=0, pes="qtip4pf", precision=prec,
+                          scramble_seed=SCRAMBLE_SEED, estimator="gradient")
+    for k in range(max(warmup, 1)):
+        timed_accumulate(hb, (1 << 44) + k * n, n)
+    hb.reset()
+    hb.profile(True)
+    ms = [timed_accumulate(hb, k * n, n) for k in range(steps)]
+    kms, launches = hb.profile(False)
+    rc, nonfinite, notconv = hb.status()
+    levels = np.sort(np.linalg.eigvalsh(hb.read(1)))[:10] * scp3_b200.constants.autocm
+    nb = hb.nb
+    hb.close()
+    t = sum(ms) / len(ms)
+    return {"value": n / (t * 1e-3), "ms_per_step": t, "nb": nb,
+            "kernel_ms": {"per_sample": kms[0] / steps, "stein": kms[2] / steps},
+            "status": {"rc": rc, "nonfinite": nonfinite, "not_converged": notconv}, "levels": levels}
+
+
 def run_gradient(args):
     """The reference's default estimator (no -G): the Stein estimator of every
     upper element from V and dV/dq (ScaledMatrixElements.cpp:102-725,
     TripleExcitations.h) on the hexamer prism doubles basis (Nb = 1225, 48 modes,
-    qTIP4P/f energy and gradient per sample), FP64.  value: samples/s,
-    device-timed; the kernel split from the build's timing.  One JSON line; not
-    the benchmark's default."""
+    qTIP4P/f energy and gradient per sample).  --precision bf16x3 (default): the
+    products W Phi^T on the tensor cores (BF16x3), the potential, its gradient
+    and the same-mode pair sums in FP64, against the FP64 form on the same
+    points (rate ratio and level error); --precision fp64: the FP64 form alone.
+    value: samples/s, device-timed.  One JSON line; not the benchmark's default."""
     import torch
-    import scp3_b200
     from scp3_b200 import inputs
     torch.cuda.set_device(0)
     nw, x0, MUa, omega = inputs.load(INPUT)
     n = args.samples
-    hb = scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=0, pes="qtip4pf", precision="fp64",
-                          scramble_seed=SCRAMBLE_SEED, estimator="gradient")
-    for k in range(max(args.warmup, 1)):
-        timed_accumulate(hb, (1 << 44) + k * n, n)
-    hb.reset()
+    prec = "fp64" if args.precision == "fp64" else "bf16x3"
     clocks = Clocks(0)
-    hb.profile(True)
-    ms = [timed_accumulate(hb, k * n, n) for k in range(args.steps)]
-    kms, launches = hb.profile(False)
+    main = gradient_form(prec, nw, x0, MUa, omega, n, args.steps, args.warmup)
     clk = clocks.stop()
-    rc, nonfinite, notconv = hb.status()
-    nb = hb.nb
-    hb.close()
-    t = sum(ms) / len(ms)
-    print(json.dumps({
-        "metric": "gradient-estimator build: Sobol samples/s (hexamer doubles, FP64)", "value": n / (t * 1e-3),
-        "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
-        "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+    line = {
+        "metric": "gradient-estimator build: Sobol samples/s (hexamer doubles)", "value": main["value"],
+        "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": main["ms_per_step"], "higher_is_better": True,
+        "dtype": "bf16x3/f64" if prec != "fp64" else "f64", "data": "synthetic",
         "config": {"workload": "hexamer prism qTIP4P/f, 48 modes, doubles basis Nb=%d, %d scrambled Sobol points per "
-                               "step, the Stein estimator of SCP3's default path" % (nb, n)},
-        "kernel_ms": {"per_sample": kms[0] / args.steps, "stein": kms[2] / args.steps},
-        "clocks": clk, "status": {"rc": rc, "nonfinite": nonfinite, "not_converged": notconv}}))
+                               "step, the Stein estimator of SCP3's default path" % (main["nb"], n),
+                   "precision": prec},
+        "kernel_ms": main["kernel_ms"], "clocks": clk, "status": main["status"]}
+    if prec != "fp64":
+        ref = gradient_form("fp64", nw, x0, MUa, omega, n, args.steps, 1)
+        line["fp64"] = {"value": ref["value"], "ms_per_step": ref["ms_per_step"], "kernel_ms": ref["kernel_ms"]}
+        line["speedup_vs_fp64"] = main["value"] / ref["value"]
+        line["levels"] = {"max_abs_err_cm1_vs_fp64": float(np.abs(main["levels"] - ref["levels"]).max()),
+                          "lowest10_cm1_fp64": [float(x) for x in ref["levels"]],
+                          "samples": n * args.steps}
+    print(json.dumps(line))
 
 
 def _ref_scp1_rate(job):

@@ -113,8 +113,10 @@ typedef struct scp3gpu_config {
     int chunk;              /* samples per device pass; multiple of 4096, 0 = auto:
                                2^18 for the split forms (halved while one pass's
                                operand would exceed ~6 GB); 2^16 for the FP64 form
-                               (halved while its Phi and W would exceed ~4 GB), 4096
-                               for the gradient estimator                             */
+                               (halved while its Phi and W would exceed ~4 GB); for
+                               the gradient estimator 2^14 (FP64 products) or 2^16
+                               (BF16x3 products), halved while a pass's operands
+                               would exceed ~4 GB                                     */
     int device;             /* CUDA device ordinal                                     */
     int estimator;          /* SCP3GPU_ESTIMATOR_*                                     */
 } scp3gpu_config;
@@ -122,8 +124,11 @@ typedef struct scp3gpu_config {
 /* matrix-element estimator (SCP3.cpp:226-231) */
 #define SCP3GPU_ESTIMATOR_DIRECT 0   /* -G: sum_s Phi V Phi^T (ScaledMatrixElements.cpp:951-971)         */
 #define SCP3GPU_ESTIMATOR_GRADIENT 1 /* the default: Stein estimator from V and dV/dq
-                                        (ScaledMatrixElements.cpp:102-725, TripleExcitations.h); plain
-                                        FP64 form (qtip4pf.cpp:252-397, ttm3f.cpp:325-720 gradients)     */
+                                        (ScaledMatrixElements.cpp:102-725, TripleExcitations.h); the
+                                        potential and its gradient in FP64 (qtip4pf.cpp:252-397,
+                                        ttm3f.cpp:325-720); its products W Phi^T in FP64
+                                        (SCP3GPU_PREC_FP64) or BF16x3 on tcgen05 (SCP3GPU_PREC_BF16X3,
+                                        _BF16X3_PES64); FP16 forms are SCP3GPU_ERR_UNSUPPORTED       */
 
 /* Replaces ScaledMatrixElements(omega(modes), N2, N3) + M.zeros (SCP3.cpp:164-169). */
 int scp3gpu_hbuild_create(const scp3gpu_config* cfg, scp3gpu_hbuild** out);

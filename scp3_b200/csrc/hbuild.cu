@@ -175,7 +175,8 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     a.normals = normals_dev;
     a.normals32 = normals32_dev;
     a.index0 = index0;
-    a.n = h->split_form ? tc::pass_samples(h->tcp, nvalid) : round_up(nvalid, 16ll * h->nsplit);
+    a.n = h->split_form ? tc::pass_samples(h->tcp, nvalid)
+                        : h->gradient ? stein_pass_samples(h->sp, nvalid) : round_up(nvalid, 16ll * h->nsplit);
     a.nvalid = nvalid;
     a.q64 = h->split_form ? nullptr : h->q64;
     a.q32 = h->split_form ? h->q32b[b] : nullptr;
@@ -526,8 +527,9 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     if (c->chunk < 0 || c->chunk % 4096 != 0) return fail(SCP3GPU_ERR_ARG, "chunk must be a multiple of 4096");
     if (c->estimator != SCP3GPU_ESTIMATOR_DIRECT && c->estimator != SCP3GPU_ESTIMATOR_GRADIENT)
         return fail(SCP3GPU_ERR_ARG, "unknown estimator");
-    if (c->estimator == SCP3GPU_ESTIMATOR_GRADIENT && c->precision != SCP3GPU_PREC_FP64)
-        return fail(SCP3GPU_ERR_UNSUPPORTED, "gradient estimator: plain FP64 form only");
+    if (c->estimator == SCP3GPU_ESTIMATOR_GRADIENT && c->precision != SCP3GPU_PREC_FP64 &&
+        c->precision != SCP3GPU_PREC_BF16X3 && c->precision != SCP3GPU_PREC_BF16X3_PES64)
+        return fail(SCP3GPU_ERR_UNSUPPORTED, "gradient estimator: plain FP64 or BF16x3 products only");
     for (int m = 0; m < c->nmodes; m++)
         if (c->modes[m] < 0 || c->modes[m] >= c->nmodes0) return fail(SCP3GPU_ERR_ARG, "mode index out of range");
     int rc = check_device(c->device);
@@ -540,8 +542,11 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     h->cfg.x0 = h->cfg.MUa = h->cfg.omega = nullptr;
     h->cfg.modes = nullptr;
     h->dev = c->device;
-    h->split_form = c->precision != SCP3GPU_PREC_FP64;
-    h->pes_fp32 = c->precision == SCP3GPU_PREC_BF16X3 || c->precision == SCP3GPU_PREC_F16X3;
+    // The gradient estimator keeps its own pass structure in every form: the
+    // potential and its gradient in FP64, its products in FP64 or BF16x3 (stein.cu).
+    const bool gradient = c->estimator == SCP3GPU_ESTIMATOR_GRADIENT;
+    h->split_form = c->precision != SCP3GPU_PREC_FP64 && !gradient;
+    h->pes_fp32 = !gradient && (c->precision == SCP3GPU_PREC_BF16X3 || c->precision == SCP3GPU_PREC_F16X3);
     const int nm0 = c->nmodes0, N3 = 9 * c->nw;
     h->nb = (int)scp3gpu_basis_size(c->nmodes, c->n2, c->n3);
     // HO diagonal of the selected modes and the inactive-mode zero point (SCP3.cpp:239)
@@ -600,7 +605,8 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     } else {
         h->gradient = c->estimator == SCP3GPU_ESTIMATOR_GRADIENT;
         if (h->gradient) {
-            if ((rc = stein_create(h->sp, desc, c->nmodes, c->chunk, sms))) return bail(rc);
+            if ((rc = stein_create(h->sp, desc, c->nmodes, c->chunk, sms, c->precision != SCP3GPU_PREC_FP64)))
+                return bail(rc);
             h->chunk = h->sp.chunk;
             h->nsplit = h->sp.nsplit;
             h->nb_pad = h->sp.nb_pad;
@@ -708,7 +714,7 @@ int scp3gpu_hbuild_add_epot_grad(scp3gpu_hbuild* h, const double* q, const doubl
     SCP3_CUDA(cudaStreamSynchronize(h->stream));
     for (int64_t off = 0; off < n; off += h->chunk) {
         const int64_t c = std::min(h->chunk, n - off);
-        const int64_t kn = round_up(c, 16ll * h->nsplit);
+        const int64_t kn = stein_pass_samples(h->sp, c);
         // padding samples carry V = 0 and dV/dq = 0 and so contribute nothing
         SCP3_CUDA(cudaMemsetAsync(h->v, 0, sizeof(double) * kn, h->stream));
         SCP3_CUDA(cudaMemsetAsync(h->q64, 0, sizeof(double) * kn * nm, h->stream));

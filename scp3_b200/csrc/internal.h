@@ -172,11 +172,27 @@ struct SteinPlan {
     double* Phi = nullptr;           // [chunk][nb_pad]  basis functions
     double* C = nullptr;             // [nsplit][rt * ct][128 * 128]
     double* D = nullptr;             // [dsplit][dsize]
+    // Split form (BF16x3 products on the tensor cores): W and Phi as one operand of
+    // 32-slot boxes, W rows [0, nv_pad), Phi rows from nv_pad; C is then the
+    // 128 x 256 tiles' unit partials P.
+    bool split = false;
+    int bpairs = 0;                  // Phi panel pairs (the last a one-panel tile when ct is odd)
+    int ntiles2 = 0;                 // tiles (W panel, Phi pair): rt * bpairs
+    int64_t slots = 0;               // K slots of a whole pass (4160 per 4096 samples)
+    uint16_t* xop = nullptr;         // [row block][k-block][hi, lo][128 x 32]
+    int4* tiles2 = nullptr;          // (W row, Phi row, 0, second Phi row)
+    int* nosign = nullptr;           // [chunk / 4096] first negative 16-group: never
+    double* P = nullptr;             // [nsplit][ntiles2][128 x 256] tile-local column-major
+    int* err = nullptr;              // a bounded wait of the contraction expired
 };
-int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_t chunk, int sms);
+// split: BF16x3 products (tcgen05) instead of FP64 ones.
+int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_t chunk, int sms,
+                 bool split = false);
+// Samples of a pass holding nvalid samples (padding samples carry V = 0 and dV/dq = 0).
+int64_t stein_pass_samples(const SteinPlan& p, int64_t nvalid);
 void stein_destroy(SteinPlan& p);
 int stein_zero(const SteinPlan& p, cudaStream_t s);
-// One pass of k samples (k a multiple of 16 * nsplit; q, vq: [k][nm], v: [k]).
+// One pass of k samples (k = stein_pass_samples(); q, vq: [k][nm], v: [k]).
 int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const double* v, const double* vq,
                int64_t k, cudaStream_t s);
 // The dense column-major nb x nb estimate (both triangles), divided by `divisor`;

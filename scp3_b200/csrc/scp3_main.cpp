@@ -12,8 +12,9 @@
 // 2^17 (SCP3.cpp:252-255), omega0.dat at start (SCP3.cpp:300-302).
 //
 // Without -G the reference's default gradient estimator runs
-// (ScaledMatrixElements.cpp:102-725): on the GPU in FP64 with the potential's
-// gradient; the split precisions need -G (ScaledMatrixElements.cpp:951-971).
+// (ScaledMatrixElements.cpp:102-725): on the GPU with the potential and its
+// gradient in FP64, its products in FP64 (--precision fp64) or BF16x3 on the
+// tensor cores (--precision bf16x3); f16x3 needs -G (ScaledMatrixElements.cpp:951-971).
 #include <getopt.h>
 
 #include <cmath>
@@ -249,8 +250,8 @@ void check(int rc, const char* what)
 int main(int argc, char** argv)
 {
     Options o = parse(argc, argv);
-    if (o.use_gradient && o.precision != "fp64")
-        die("The gradient estimator runs in FP64; run the split precisions with -G.");
+    if (o.use_gradient && o.precision == "f16x3")
+        die("The gradient estimator runs its products in FP64 or BF16x3; run f16x3 with -G.");
     vector<double> mass, x0, H;
     load_input(o.input, mass, x0, H);
     ohhohh(mass, x0, H);

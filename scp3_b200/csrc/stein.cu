@@ -30,9 +30,12 @@
 //
 // Every sum runs over samples in a fixed order per (split, tile) and the splits
 // are added in order at read-out, so results are deterministic.
+#include <cuda_bf16.h>
+
 #include <algorithm>
 
 #include "internal.h"
+#include "tc.h"
 
 namespace scp3 {
 
@@ -158,6 +161,97 @@ __global__ void __launch_bounds__(kExpR) stein_expand_kernel(const uint32_t* __r
     }
 }
 
+// Split form: x = hi + lo in BF16 for two values, each half packed in one
+// 32-bit word (the first value in the low 16 bits), round-to-nearest.
+__device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t& hi, uint32_t& lo)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+    const float2 hf = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+constexpr int kSxSlots = 64, kSxThreads = 256, kSxRows = 128;
+constexpr int kSxBlocksPerFlush = tc::kSlotsPerFlush / kSxSlots;   // 65: the last holds only padding slots
+
+// The split operand of a pass: the W rows (reduced function x Stein weight, and
+// the ground row V) from row 0 and the Phi rows from row rows_w, each value
+// computed in FP64 as stein_expand_kernel does, rounded to FP32 and stored as
+// BF16 hi + lo in the 32-slot, 64-byte-swizzled boxes the tensor-core
+// contraction reads ([row block][k-block][hi, lo][128 x 32], 16-byte chunk c
+// of row r at c ^ ((r >> 1) & 3)).  K slot l of 4096-sample block f holds sample
+// 4096 f + l (l < 4096); the block's last 64 slots, rows in [nv, rows_w) and
+// rows past the basis are never written (zero since creation).  CTA: one 64-slot
+// block x 128 rows; thread (g, r) writes slots 8g..8g+7 of rows r, r + 32,
+// r + 64, r + 96: one 16-byte chunk of the hi box and one of the lo box each.
+__global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
+    const uint32_t* __restrict__ desc, int nb, const uint32_t* __restrict__ vrdesc, int nv, int rows_w, int nm,
+    const double* __restrict__ q, const double* __restrict__ v, const double* __restrict__ vq, int64_t n,
+    int64_t nkb_alloc, uint16_t* __restrict__ xop)
+{
+    extern __shared__ double sx[];   // q [nm][64], vq [nm][64], V [64]
+    const int kb = blockIdx.x;
+    const int f = kb / kSxBlocksPerFlush, lb = kb - f * kSxBlocksPerFlush;
+    if (lb * kSxSlots >= tc::kFlush) return;
+    double* qs = sx;
+    double* vqs = qs + (size_t)nm * kSxSlots;
+    double* vs = vqs + (size_t)nm * kSxSlots;
+    const int t = threadIdx.x;
+    const int64_t s0 = (int64_t)f * tc::kFlush + (int64_t)lb * kSxSlots;
+    for (int e = t; e < nm * kSxSlots; e += kSxThreads) {
+        const int ss = e / nm, m = e - ss * nm;          // coalesced reads of sample s0 + ss
+        const bool ok = s0 + ss < n;
+        qs[m * kSxSlots + ss] = ok ? q[(s0 + ss) * nm + m] : 0.0;
+        vqs[m * kSxSlots + ss] = ok ? vq[(s0 + ss) * nm + m] : 0.0;
+    }
+    for (int ss = t; ss < kSxSlots; ss += kSxThreads) vs[ss] = s0 + ss < n ? v[s0 + ss] : 0.0;
+    __syncthreads();
+    const int g = t & 7, rl = t >> 3;
+    const int64_t slot0 = (int64_t)kb * kSxSlots + 8 * g;      // first K slot of the thread in the pass
+    const int64_t box_k = slot0 / tc::kKBlock2;                // its 32-slot box
+    const int c = (int)((slot0 / 8) & 3);                      // its 16-byte chunk of a box row
+#pragma unroll 1
+    for (int u = 0; u < kSxRows / 32; u++) {
+        const int row = blockIdx.y * kSxRows + rl + 32 * u;
+        float x[8];
+        if (row < nv) {
+            const uint32_t vd = __ldg(vrdesc + row);
+            const int m = vd & 255, a = (vd >> 8) & 3;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int ss = 8 * g + j;
+                x[j] = (vd & kGroundRow)
+                           ? (float)vs[ss]
+                           : (float)(reduced(vd, qs, kSxSlots, ss) *
+                                     stein_weight(a, 0, qs[m * kSxSlots + ss], vs[ss], vqs[m * kSxSlots + ss]));
+            }
+        } else if (row >= rows_w && row - rows_w < nb) {
+            int mm[3], ll[3];
+            const int k = decode(__ldg(desc + row - rows_w), mm, ll);
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int ss = 8 * g + j;
+                double y = 1.0;
+                for (int w = 0; w < k; w++) y *= ho(ll[w], qs[mm[w] * kSxSlots + ss]);
+                x[j] = (float)y;
+            }
+        } else {
+            continue;
+        }
+        uint4 hi, lo;
+        split_bf16x2(x[0], x[1], hi.x, lo.x);
+        split_bf16x2(x[2], x[3], hi.y, lo.y);
+        split_bf16x2(x[4], x[5], hi.z, lo.z);
+        split_bf16x2(x[6], x[7], hi.w, lo.w);
+        const int rin = row & (tc::kTile - 1);
+        uint16_t* box = xop + ((size_t)(row / tc::kTile) * nkb_alloc + box_k) * (2 * tc::kTile * tc::kKBlock2);
+        const int off = rin * tc::kKBlock2 + ((c ^ ((rin >> 1) & 3)) << 3);
+        *reinterpret_cast<uint4*>(box + off) = hi;
+        *reinterpret_cast<uint4*>(box + tc::kTile * tc::kKBlock2 + off) = lo;
+    }
+}
+
 // Same-mode pair sums D^m[ri][rj] += sum_s R_i^m R_j^m K^m_{a_i b_j} over the
 // functions exciting m (ranks ri <= rj), one 64 x 64 tile of ranks per CTA,
 // 4 x 4 elements per thread; samples in chunks of kPS staged in shared memory.
@@ -183,12 +277,22 @@ __global__ void __launch_bounds__(256) stein_pairs_kernel(const int4* __restrict
     const int m = task.x, ti = task.y, tj = task.z;
     const int v0 = voff[m], e = voff[m + 1] - v0;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    // levels of the thread's rows and columns; past e (R = 0) they take the first
+    // one's, so that a thread whose functions share one level pair reads one
+    // weight per sample (the functions are ordered by level: most threads do)
     int arow[4], bcol[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
         const int rr = ti * kPT + ty + 16 * r, rc = tj * kPT + tx + 16 * r;
-        arow[r] = rr < e ? (int)((vrdesc[v0 + rr] >> 8) & 3u) : 0;
-        bcol[r] = rc < e ? (int)((vrdesc[v0 + rc] >> 8) & 3u) : 0;
+        arow[r] = rr < e ? (int)((vrdesc[v0 + rr] >> 8) & 3u) : -1;
+        bcol[r] = rc < e ? (int)((vrdesc[v0 + rc] >> 8) & 3u) : -1;
+    }
+    bool uni = true;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        if (arow[r] < 0) arow[r] = max(arow[0], 0);
+        if (bcol[r] < 0) bcol[r] = max(bcol[0], 0);
+        uni = uni && arow[r] == arow[0] && bcol[r] == bcol[0];
     }
     double acc[4][4];
 #pragma unroll
@@ -218,6 +322,20 @@ __global__ void __launch_bounds__(256) stein_pairs_kernel(const int4* __restrict
             }
         }
         __syncthreads();
+        if (uni) {
+            const int k0 = arow[0] * 4 + bcol[0];
+            for (int j = 0; j < nc; j++) {
+                double rr[4], rc[4];
+                const double kk = K[j * 16 + k0];
+#pragma unroll
+                for (int r = 0; r < 4; r++) rr[r] = Rr[j * kPT + ty + 16 * r], rc[r] = Rc[j * kPT + tx + 16 * r] * kk;
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[r][c] = fma(rr[r], rc[c], acc[r][c]);
+            }
+            continue;
+        }
         for (int j = 0; j < nc; j++) {
             double rr[4], rc[4];
 #pragma unroll
@@ -272,16 +390,32 @@ __global__ void __launch_bounds__(kTriThreads) stein_pairs_tri_kernel(const int*
         while (p >= nbk - r) p -= nbk - r, r++;
         bi = r, bj = r + p;
     }
+    // level pairs of the block; rows and columns past e (R = 0) take the block's
+    // first level, so that a block whose functions share one level pair reads one
+    // weight per sample (the functions are ordered by level: most blocks do)
     int ab[4][4];
+    bool uni = true;
+    {
+        int la[4], lb[4];
 #pragma unroll
-    for (int r = 0; r < 4; r++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const int ri = 4 * bi + r, rc = 4 * bj + c;
-            const int a = (bi >= 0 && ri < e) ? (int)((vrdesc[v0 + ri] >> 8) & 3u) : 0;
-            const int b = (bi >= 0 && rc < e) ? (int)((vrdesc[v0 + rc] >> 8) & 3u) : 0;
-            ab[r][c] = a * 4 + b;
+        for (int r = 0; r < 4; r++) {
+            const int ri = 4 * bi + r, rc = 4 * bj + r;
+            la[r] = (bi >= 0 && ri < e) ? (int)((vrdesc[v0 + ri] >> 8) & 3u) : -1;
+            lb[r] = (bi >= 0 && rc < e) ? (int)((vrdesc[v0 + rc] >> 8) & 3u) : -1;
         }
+#pragma unroll
+        for (int r = 1; r < 4; r++) {
+            if (la[r] < 0) la[r] = la[0];
+            if (lb[r] < 0) lb[r] = lb[0];
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                ab[r][c] = max(la[r], 0) * 4 + max(lb[c], 0);
+                uni = uni && ab[r][c] == ab[0][0];
+            }
+    }
     double acc[4][4];
 #pragma unroll
     for (int r = 0; r < 4; r++)
@@ -308,6 +442,21 @@ __global__ void __launch_bounds__(kTriThreads) stein_pairs_tri_kernel(const int*
         }
         __syncthreads();
         if (bi < 0) continue;
+        if (uni) {
+            const int k0 = ab[0][0];
+            for (int j = 0; j < nc; j++) {
+                const double2* Rj = reinterpret_cast<const double2*>(R + j * kTriMax);
+                const double2 r01 = Rj[2 * bi], r23 = Rj[2 * bi + 1], c01 = Rj[2 * bj], c23 = Rj[2 * bj + 1];
+                const double kk = K[j * 16 + k0];
+                const double rr[4] = {r01.x, r01.y, r23.x, r23.y};
+                const double rc[4] = {c01.x * kk, c01.y * kk, c23.x * kk, c23.y * kk};
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[r][c] = fma(rr[r], rc[c], acc[r][c]);
+            }
+            continue;
+        }
         for (int j = 0; j < nc; j++) {
             const double2* Rj = reinterpret_cast<const double2*>(R + j * kTriMax);
             const double2 r01 = Rj[2 * bi], r23 = Rj[2 * bi + 1], c01 = Rj[2 * bj], c23 = Rj[2 * bj + 1];
@@ -333,7 +482,12 @@ __global__ void __launch_bounds__(kTriThreads) stein_pairs_tri_kernel(const int*
 // Element (i, j) of the dense matrix from its terms: for each mode m that r =
 // min(i, j) or c = max(i, j) excites, C at virtual row (m, r) column c, or at
 // (m, c) column r, or the pair sum D^m when both excite m; the mean over those
-// modes; <0|V|0> from the ground row.
+// modes; <0|V|0> from the ground row.  C: FP64 tiles of 128 x 128, row-major,
+// `ct` per tile row (N256 = false); or the split form's 128 x 256 unit partials
+// (N256 = true), tile (row panel r, column panel pair q) at index q * ct + r
+// with `ct` = row panels (pair-major, as stein_create lists them), tile-local
+// column-major.
+template <bool N256>
 __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int* __restrict__ rank3,
                                     const int* __restrict__ voff, const int64_t* __restrict__ doff, int nb, int nv,
                                     int ct, int nsplit, int dsplit, const double* __restrict__ C,
@@ -346,6 +500,9 @@ __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int
     const int j = (int)(e / nb), i = (int)(e - (int64_t)j * nb);
     const int r = min(i, j), c = max(i, j);
     auto cidx = [&](int vr, int col) -> int64_t {
+        if (N256)
+            return ((int64_t)(col >> 8) * ct + (vr >> 7)) * (128 * 256) +
+                   (int64_t)(((col >> 7) & 1) * 128 + (col & 127)) * 128 + (vr & 127);
         return ((int64_t)(vr >> 7) * ct + (col >> 7)) * (128 * 128) + (int64_t)(vr & 127) * 128 + (col & 127);
     };
     int mr[3], lr[3], mc[3], lc[3];
@@ -366,8 +523,10 @@ __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int
                 const int64_t x = cidx(voff[m] + rank3[3 * r + a], c);
                 for (int s = 0; s < nsplit; s++) t += C[s * csize + x];
             } else {
+                // D holds the upper triangle of ranks (functions ordered by level in m)
                 const int en = voff[m + 1] - voff[m];
-                const int64_t x = doff[m] + (int64_t)rank3[3 * r + a] * en + rank3[3 * c + b];
+                const int ra = rank3[3 * r + a], rb = rank3[3 * c + b];
+                const int64_t x = doff[m] + (int64_t)min(ra, rb) * en + max(ra, rb);
                 for (int s = 0; s < dsplit; s++) t += D[s * dsize + x];
             }
             val += t;
@@ -394,7 +553,7 @@ int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
 }  // namespace
 
-int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_t chunk_cfg, int sms)
+int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_t chunk_cfg, int sms, bool split)
 {
     p = SteinPlan{};
     p.nb = (int)desc.size();
@@ -407,15 +566,32 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
     std::vector<std::vector<int>> lev(nm);
     std::vector<int> rank3((size_t)p.nb * 3, 0);
     std::vector<uint32_t> vr_of_rank;
+    std::vector<std::vector<int>> slot(nm);   // factor index, within its function, of mode m
     for (int i = 0; i < p.nb; i++) {
         int mm[3], ll[3];
         const int k = decode(desc[i], mm, ll);
         for (int a = 0; a < k; a++) {
             if (mm[a] >= nm) return fail(SCP3GPU_ERR_ARG, "stein: basis mode out of range");
-            rank3[(size_t)3 * i + a] = (int)E[mm[a]].size();
             E[mm[a]].push_back(i);
             lev[mm[a]].push_back(ll[a]);
+            slot[mm[a]].push_back(a);
         }
+    }
+    // each mode's functions ordered by their level in that mode (stable), so that
+    // the pair sums' 4 x 4 blocks mostly share one level pair (one weight)
+    for (int m = 0; m < nm; m++) {
+        std::vector<int> ord(E[m].size());
+        for (size_t r = 0; r < ord.size(); r++) ord[r] = (int)r;
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return lev[m][x] < lev[m][y]; });
+        std::vector<int> e2, l2;
+        for (size_t r = 0; r < ord.size(); r++) {
+            const int i = E[m][ord[r]];
+            e2.push_back(i);
+            l2.push_back(lev[m][ord[r]]);
+            rank3[(size_t)3 * i + slot[m][ord[r]]] = (int)r;
+        }
+        E[m].swap(e2);
+        lev[m].swap(l2);
     }
     std::vector<int> voff(nm + 1, 0);
     std::vector<int64_t> doff(nm, 0);
@@ -458,51 +634,115 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
     p.dsize = std::max<int64_t>(dsz, 1);
     p.ndtasks = (int)tasks.size();
     p.nftasks = (int)ftasks.size();
-    // passes of 2^14 samples (fewer while W and Phi of a pass would pass ~4 GB);
-    // sample ranges per tile as the plain form chooses them, the C partials of
-    // all ranges held under ~8 GB (one range if a single one is larger)
-    int64_t chunk = chunk_cfg > 0 ? chunk_cfg : 16384;
-    while (chunk > 4096 && (int64_t)(p.nv_pad + p.nb_pad) * chunk * 8 > (4ll << 30)) chunk /= 2;
-    p.chunk = chunk;
-    const int64_t csize = (int64_t)p.rt * p.ct * 128 * 128;
-    double best = 1e300;
-    p.nsplit = 1;
-    for (int ns = 1; chunk / ns >= 2048 && chunk % (16ll * ns) == 0; ns *= 2) {
-        if (ns > 1 && (csize + p.dsize) * 8 * ns > (8ll << 30)) break;
-        const int64_t units = (int64_t)p.rt * p.ct * ns;
-        const double cost = (double)((units + sms - 1) / sms) / ns;
-        if (cost < best - 1e-9) best = cost, p.nsplit = ns;
-    }
-    // sample ranges of the same-mode pair sums: a multiple of the products' (so a
-    // pass of 16 * nsplit samples divides), up to 4x finer while their sums stay
-    // small -- those kernels have one CTA per mode and range, too few for the GPU
-    // at the products' split (48 x 8 for the hexamer doubles basis)
-    p.dsplit = p.nsplit;
-    while (p.dsplit < 4 * p.nsplit && p.dsplit * 2 * p.dsize * 8 <= (256ll << 20)) p.dsplit *= 2;
     int rc;
+    if (!split) {
+        // passes of 2^14 samples (fewer while W and Phi of a pass would pass ~4 GB);
+        // sample ranges per tile as the plain form chooses them, the C partials of
+        // all ranges held under ~8 GB (one range if a single one is larger)
+        int64_t chunk = chunk_cfg > 0 ? chunk_cfg : 16384;
+        while (chunk > 4096 && (int64_t)(p.nv_pad + p.nb_pad) * chunk * 8 > (4ll << 30)) chunk /= 2;
+        p.chunk = chunk;
+        const int64_t csize = (int64_t)p.rt * p.ct * 128 * 128;
+        double best = 1e300;
+        p.nsplit = 1;
+        for (int ns = 1; chunk / ns >= 2048 && chunk % (16ll * ns) == 0; ns *= 2) {
+            if (ns > 1 && (csize + p.dsize) * 8 * ns > (8ll << 30)) break;
+            const int64_t units = (int64_t)p.rt * p.ct * ns;
+            const double cost = (double)((units + sms - 1) / sms) / ns;
+            if (cost < best - 1e-9) best = cost, p.nsplit = ns;
+        }
+        // sample ranges of the same-mode pair sums: a multiple of the products' (so a
+        // pass of 16 * nsplit samples divides), up to 4x finer while their sums stay
+        // small -- those kernels have one CTA per mode and range, too few for the GPU
+        // at the products' split (48 x 8 for the hexamer doubles basis)
+        p.dsplit = p.nsplit;
+        while (p.dsplit < 4 * p.nsplit && p.dsplit * 2 * p.dsize * 8 <= (256ll << 20)) p.dsplit *= 2;
+        if ((rc = dalloc(&p.W, (size_t)p.chunk * p.nv_pad)) || (rc = dalloc(&p.Phi, (size_t)p.chunk * p.nb_pad)) ||
+            (rc = dalloc(&p.C, (size_t)csize * p.nsplit))) {
+            stein_destroy(p);
+            return rc;
+        }
+    } else {
+        // The products W Phi^T on the tensor cores: tiles of one W panel against a
+        // pair of Phi panels (one panel when ct is odd), K slots in blocks of 4160
+        // per 4096 samples (the contraction's sign groups, here all positive).
+        // Passes of 2^16 samples (fewer while the operand would pass ~4 GB); sample
+        // ranges per tile minimising waves per range, at most 16, partials under ~4 GB.
+        p.split = true;
+        p.bpairs = (p.ct + 1) / 2;
+        p.ntiles2 = p.rt * p.bpairs;
+        const int64_t rows = (int64_t)p.nv_pad + p.nb_pad;
+        auto slots_of = [](int64_t k) { return k / tc::kFlush * tc::kSlotsPerFlush; };
+        int64_t chunk = chunk_cfg > 0 ? chunk_cfg : 65536;
+        while (chunk > tc::kFlush && rows * slots_of(chunk) * 4 > (4ll << 30)) chunk /= 2;
+        chunk = std::max<int64_t>(chunk / tc::kFlush * tc::kFlush, tc::kFlush);
+        p.chunk = chunk;
+        p.slots = slots_of(chunk);
+        double best = 1e300;
+        p.nsplit = 1;
+        for (int m = 1; m <= 16; m++) {
+            const int64_t units = (int64_t)p.ntiles2 * m;
+            if (m > 1 && units * 128 * 256 * 8 > (4ll << 30)) break;
+            const double cost = (double)((units + sms - 1) / sms) / m;
+            if (cost < best - 1e-12) best = cost, p.nsplit = m;
+        }
+        p.dsplit = 1;
+        while (p.dsplit < 64 && p.dsplit * 2 * p.dsize * 8 <= (256ll << 20)) p.dsplit *= 2;
+        std::vector<int4> tl;
+        for (int q = 0; q < p.bpairs; q++)          // pair-major: a wave's tiles share their Phi pairs
+            for (int r = 0; r < p.rt; r++) {
+                const int b0 = p.nv_pad + 2 * q * 128;
+                const int b1 = 2 * q + 1 < p.ct ? b0 + 128 : b0;
+                tl.push_back(make_int4(r * 128, b0, 0, b1));
+            }
+        const std::vector<int> nosign((size_t)(chunk / tc::kFlush), tc::kSlotsPerFlush / 16);
+        const size_t xop_elems = (size_t)2 * rows * p.slots;
+        if ((rc = upload(&p.tiles2, tl.data(), tl.size())) || (rc = upload(&p.nosign, nosign.data(), nosign.size())) ||
+            (rc = dalloc(&p.xop, xop_elems)) || (rc = dalloc(&p.P, (size_t)p.nsplit * p.ntiles2 * 128 * 256)) ||
+            (rc = dalloc(&p.err, (size_t)1))) {
+            stein_destroy(p);
+            return rc;
+        }
+        // padding rows and the slots closing each 4096-sample block are never written
+        SCP3_CUDA(cudaMemset(p.xop, 0, sizeof(uint16_t) * xop_elems));
+        SCP3_CUDA(cudaMemset(p.err, 0, sizeof(int)));
+        const size_t es = sizeof(double) * (2 * (size_t)nm * kSxSlots + kSxSlots);
+        if (es > 48 * 1024)
+            SCP3_CUDA(cudaFuncSetAttribute(stein_expand_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)es));
+    }
     if ((rc = upload(&p.vrdesc, vrdesc.data(), vrdesc.size())) || (rc = upload(&p.rank3, rank3.data(), rank3.size())) ||
         (rc = upload(&p.voff, voff.data(), voff.size())) || (rc = upload(&p.doff, doff.data(), doff.size())) ||
         (p.ndtasks && (rc = upload(&p.dtasks, tasks.data(), tasks.size()))) ||
         (p.nftasks && (rc = upload(&p.ftasks, ftasks.data(), ftasks.size()))) ||
-        (rc = dalloc(&p.W, (size_t)p.chunk * p.nv_pad)) || (rc = dalloc(&p.Phi, (size_t)p.chunk * p.nb_pad)) ||
-        (rc = dalloc(&p.C, (size_t)csize * p.nsplit)) || (rc = dalloc(&p.D, (size_t)p.dsize * p.dsplit))) {
+        (rc = dalloc(&p.D, (size_t)p.dsize * p.dsplit))) {
         stein_destroy(p);
         return rc;
     }
     return SCP3GPU_OK;
 }
 
+int64_t stein_pass_samples(const SteinPlan& p, int64_t nvalid)
+{
+    return p.split ? round_up(nvalid, tc::kFlush) : round_up(nvalid, 16ll * p.nsplit);
+}
+
 void stein_destroy(SteinPlan& p)
 {
     cudaFree(p.vrdesc), cudaFree(p.rank3), cudaFree(p.voff), cudaFree(p.doff), cudaFree(p.dtasks), cudaFree(p.ftasks);
     cudaFree(p.W), cudaFree(p.Phi), cudaFree(p.C), cudaFree(p.D);
-    p.vrdesc = nullptr, p.rank3 = nullptr, p.voff = nullptr, p.doff = nullptr, p.dtasks = nullptr, p.ftasks = nullptr;
-    p.W = p.Phi = p.C = p.D = nullptr;
+    cudaFree(p.xop), cudaFree(p.tiles2), cudaFree(p.nosign), cudaFree(p.P), cudaFree(p.err);
+    p = SteinPlan{};
 }
 
 int stein_zero(const SteinPlan& p, cudaStream_t s)
 {
-    SCP3_CUDA(cudaMemsetAsync(p.C, 0, sizeof(double) * (size_t)p.rt * p.ct * 128 * 128 * p.nsplit, s));
+    if (p.split) {
+        SCP3_CUDA(cudaMemsetAsync(p.P, 0, sizeof(double) * (size_t)p.nsplit * p.ntiles2 * 128 * 256, s));
+        SCP3_CUDA(cudaMemsetAsync(p.err, 0, sizeof(int), s));
+    } else {
+        SCP3_CUDA(cudaMemsetAsync(p.C, 0, sizeof(double) * (size_t)p.rt * p.ct * 128 * 128 * p.nsplit, s));
+    }
     SCP3_CUDA(cudaMemsetAsync(p.D, 0, sizeof(double) * (size_t)p.dsize * p.dsplit, s));
     return SCP3GPU_OK;
 }
@@ -511,15 +751,32 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
                int64_t k, cudaStream_t s)
 {
     if (k == 0) return SCP3GPU_OK;
-    if (k > p.chunk || k % (16ll * p.nsplit) != 0) return fail(SCP3GPU_ERR_ARG, "stein: pass not tiled");
-    const size_t es = sizeof(double) * (2 * (size_t)p.nm * kExpLd + kExpS);
-    if (es > 48 * 1024)
-        SCP3_CUDA(cudaFuncSetAttribute(stein_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)es));
-    dim3 eg((unsigned)((k + kExpS - 1) / kExpS), (unsigned)((p.nb_pad + p.nv_pad) / kExpR));
-    stein_expand_kernel<<<eg, kExpR, es, s>>>(desc, p.nb, p.nb_pad, p.vrdesc, p.nv, p.nv_pad, p.nm, q, v, vq, k,
-                                              p.Phi, p.W);
-    SCP3_CUDA(cudaGetLastError());
-    int rc = launch_gemm_fp64_rect(p.W, p.nv_pad, p.Phi, p.nb_pad, k, p.rt, p.ct, p.nsplit, p.C, s);
+    if (k > p.chunk || k != stein_pass_samples(p, k)) return fail(SCP3GPU_ERR_ARG, "stein: pass not tiled");
+    int rc;
+    if (p.split) {
+        const int nflush = (int)(k / tc::kFlush);
+        const size_t es = sizeof(double) * (2 * (size_t)p.nm * kSxSlots + kSxSlots);
+        dim3 eg((unsigned)(nflush * kSxBlocksPerFlush), (unsigned)((p.nv_pad + p.nb_pad) / kSxRows));
+        stein_expand_split_kernel<<<eg, kSxThreads, es, s>>>(desc, p.nb, p.vrdesc, p.nv, p.nv_pad, p.nm, q, v, vq, k,
+                                                             p.slots / tc::kKBlock2, p.xop);
+        SCP3_CUDA(cudaGetLastError());
+        const int units = p.ntiles2 * p.nsplit;
+        int sms = 148, dev = 0;
+        SCP3_CUDA(cudaGetDevice(&dev));
+        SCP3_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        rc = tc::launch_contract(p.xop, p.slots / tc::kKBlock2, p.tiles2, p.ntiles2, p.nsplit,
+                                 nflush * (tc::kSlotsPerFlush / tc::kKBlock2), p.nosign, false, p.P, p.err,
+                                 std::min(units, sms), s);
+    } else {
+        const size_t es = sizeof(double) * (2 * (size_t)p.nm * kExpLd + kExpS);
+        if (es > 48 * 1024)
+            SCP3_CUDA(cudaFuncSetAttribute(stein_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)es));
+        dim3 eg((unsigned)((k + kExpS - 1) / kExpS), (unsigned)((p.nb_pad + p.nv_pad) / kExpR));
+        stein_expand_kernel<<<eg, kExpR, es, s>>>(desc, p.nb, p.nb_pad, p.vrdesc, p.nv, p.nv_pad, p.nm, q, v, vq, k,
+                                                  p.Phi, p.W);
+        SCP3_CUDA(cudaGetLastError());
+        rc = launch_gemm_fp64_rect(p.W, p.nv_pad, p.Phi, p.nb_pad, k, p.rt, p.ct, p.nsplit, p.C, s);
+    }
     if (rc) return rc;
     if (p.ndtasks) {
         const size_t ps = sizeof(double) * ((size_t)kPS * p.nm + 2 * kPS + 2 * kPS * kPT + 16 * kPS);
@@ -547,9 +804,20 @@ int stein_unpack(const SteinPlan& p, const uint32_t* desc, double divisor, const
                  double* M, int64_t ld, cudaStream_t s)
 {
     const int64_t total = (int64_t)p.nb * p.nb;
-    stein_unpack_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
-        desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.ct, p.nsplit, p.dsplit, p.C, p.D, (int64_t)p.rt * p.ct * 128 * 128,
-        p.dsize, divisor, diag, zpe, M, ld);
+    const unsigned grid = (unsigned)((total + 255) / 256);
+    if (p.split) {
+        int err = 0;
+        SCP3_CUDA(cudaMemcpyAsync(&err, p.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SCP3_CUDA(cudaStreamSynchronize(s));
+        if (err) return fail(SCP3GPU_ERR_TIMEOUT, "tensor-core contraction: a bounded pipeline wait expired");
+        stein_unpack_kernel<true><<<grid, 256, 0, s>>>(desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.rt, p.nsplit,
+                                                       p.dsplit, p.P, p.D, (int64_t)p.ntiles2 * 128 * 256, p.dsize,
+                                                       divisor, diag, zpe, M, ld);
+    } else {
+        stein_unpack_kernel<false><<<grid, 256, 0, s>>>(desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.ct, p.nsplit,
+                                                        p.dsplit, p.C, p.D, (int64_t)p.rt * p.ct * 128 * 128, p.dsize,
+                                                        divisor, diag, zpe, M, ld);
+    }
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }

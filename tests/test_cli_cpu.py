@@ -35,10 +35,10 @@ def test_omega0_matches_numpy_modes(cli, tmp_path):
 
 
 def test_cli_gradient_path_limits_and_bad_options(cli, tmp_path):
-    """Without -G the gradient estimator runs (FP64); the split precisions are
-    told to use -G."""
+    """Without -G the gradient estimator runs (products in FP64 or BF16x3); the
+    FP16 form is told to use -G."""
     inp = os.path.join(ROOT, "scp3_b200", "data", "prism_qtip4pf.dat")
-    r = subprocess.run([cli, "--precision", "bf16x3", inp], cwd=tmp_path, capture_output=True, text=True)
+    r = subprocess.run([cli, "--precision", "f16x3", inp], cwd=tmp_path, capture_output=True, text=True)
     assert r.returncode == 1 and "-G" in r.stderr
     r = subprocess.run([cli, "-G", "-N", "50", inp], cwd=tmp_path, capture_output=True, text=True)
     assert r.returncode == 1 and "too large" in r.stderr
