@@ -188,11 +188,12 @@ int launch_chunk(scp3gpu_hbuild* h, int64_t index0, int64_t nvalid, const double
     if (h->split_form) {
         cudaStream_t ps = h->prep_stream;
         SCP3_CUDA(cudaStreamWaitEvent(ps, h->contracted[b], 0));   // buffer b free again
-        // A contraction with a CTA on every SM leaves no room for the preparation
-        // kernels (they would only delay its CTAs): prepare once its whole waves
-        // are done, on the SMs its last, partial wave leaves idle.  Smaller
-        // contractions share the GPU with the next pass's preparation.
-        if (h->tcp.grid >= h->sms) SCP3_CUDA(cudaStreamWaitEvent(ps, h->head_done[b ^ 1], 0));
+        // A contraction with a CTA on (nearly) every SM leaves no room for the
+        // preparation kernels (released with it, they would take SMs its CTAs
+        // wait for): prepare once its whole waves are done, on the SMs its last,
+        // partial wave leaves idle.  Smaller contractions share the GPU with the
+        // next pass's preparation.
+        if (h->tcp.grid * 8 >= h->sms * 7) SCP3_CUDA(cudaStreamWaitEvent(ps, h->head_done[b ^ 1], 0));
         if (copied) SCP3_CUDA(cudaStreamWaitEvent(ps, copied, 0));
         {
             Timed t(h, 0, ps);

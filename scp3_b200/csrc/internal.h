@@ -180,6 +180,7 @@ struct SteinPlan {
     int ntiles2 = 0;                 // tiles (W panel, Phi pair): rt * bpairs
     int64_t slots = 0;               // K slots of a whole pass (4160 per 4096 samples)
     uint16_t* xop = nullptr;         // [row block][k-block][hi, lo][128 x 32]
+    uint32_t* xdesc = nullptr;       // [nv_pad + nb_pad] the expansion's table indices of each row
     int4* tiles2 = nullptr;          // (W row, Phi row, 0, second Phi row)
     int* nosign = nullptr;           // [chunk / 4096] first negative 16-group: never
     double* P = nullptr;             // [nsplit][ntiles2][128 x 256] tile-local column-major

@@ -172,78 +172,90 @@ __device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t& hi, u
     lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
-constexpr int kSxSlots = 64, kSxThreads = 256, kSxRows = 128;
+constexpr int kSxSlots = 64, kSxThreads = 256;
+constexpr int kSxRowsPerCta = 1024;                                 // rows of the operand one CTA writes
 constexpr int kSxBlocksPerFlush = tc::kSlotsPerFlush / kSxSlots;   // 65: the last holds only padding slots
+constexpr uint32_t kSxZeroRow = 0xffffffffu;                        // padding row: never written
 
-// The split operand of a pass: the W rows (reduced function x Stein weight, and
-// the ground row V) from row 0 and the Phi rows from row rows_w, each value
-// computed in FP64 as stein_expand_kernel does, rounded to FP32 and stored as
-// BF16 hi + lo in the 32-slot, 64-byte-swizzled boxes the tensor-core
-// contraction reads ([row block][k-block][hi, lo][128 x 32], 16-byte chunk c
-// of row r at c ^ ((r >> 1) & 3)).  K slot l of 4096-sample block f holds sample
-// 4096 f + l (l < 4096); the block's last 64 slots, rows in [nv, rows_w) and
-// rows past the basis are never written (zero since creation).  CTA: one 64-slot
-// block x 128 rows; thread (g, r) writes slots 8g..8g+7 of rows r, r + 32,
-// r + 64, r + 96: one 16-byte chunk of the hi box and one of the lo box each.
+// Table column of slot l (0..63): slots 8g..8g+3 at columns 4g..4g+3 and
+// 8g+4..8g+7 at 32+4g..32+4g+3, so the 8 threads of a row (thread g taking
+// slots 8g..8g+7) read two contiguous 128-byte spans (no bank conflict).
+__device__ __forceinline__ int sx_col(int l) { return ((l >> 3) << 2) | (l & 3) | ((l & 4) << 3); }
+
+// The split operand of a pass: the W rows (reduced function x Stein weight K^m_a0,
+// and the ground row V) from row 0 and the Phi rows from row nv_pad, as BF16
+// hi + lo in the 32-slot, 64-byte-swizzled boxes the tensor-core contraction
+// reads ([row block][k-block][hi, lo][128 x 32], 16-byte chunk c of row r at
+// c ^ ((r >> 1) & 3)).  K slot l of 4096-sample block f holds sample 4096 f + l
+// (l < 4096); the block's last 64 slots and the padding rows are never written
+// (zero since creation).
+//
+// Per 64-slot block the CTA tabulates, in FP32, T = [1, h1(q_m), h2(q_m), h3(q_m),
+// K^m_10, K^m_20, K^m_30, V] (6 nm + 2 rows x 64 slots; with b = 0 the Stein
+// weights of stein_weight reduce to K_10 = Vm / sqrt2, K_20 = q Vm / sqrt2,
+// K_30 = (2 q / sqrt3) V + (2 q^2 - 3) / (2 sqrt3) Vm); every operand row is the
+// product of three table entries (xdesc: three 10-bit indices, 0 = the constant
+// 1).  The values are rounded to FP32 before the BF16 split in any case.
+// CTA: one 64-slot block x kSxRowsPerCta rows; thread (g, r) writes slots
+// 8g..8g+7 of rows r, r + 32, ...: one 16-byte chunk of the hi box and one of
+// the lo box each.
 __global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
-    const uint32_t* __restrict__ desc, int nb, const uint32_t* __restrict__ vrdesc, int nv, int rows_w, int nm,
-    const double* __restrict__ q, const double* __restrict__ v, const double* __restrict__ vq, int64_t n,
-    int64_t nkb_alloc, uint16_t* __restrict__ xop)
+    const uint32_t* __restrict__ xdesc, int rows, int nm, const double* __restrict__ q,
+    const double* __restrict__ v, const double* __restrict__ vq, int64_t n, int64_t nkb_alloc,
+    uint16_t* __restrict__ xop)
 {
-    extern __shared__ double sx[];   // q [nm][64], vq [nm][64], V [64]
+    extern __shared__ __align__(16) float tx[];   // [6 nm + 2][64]
     const int kb = blockIdx.x;
     const int f = kb / kSxBlocksPerFlush, lb = kb - f * kSxBlocksPerFlush;
     if (lb * kSxSlots >= tc::kFlush) return;
-    double* qs = sx;
-    double* vqs = qs + (size_t)nm * kSxSlots;
-    double* vs = vqs + (size_t)nm * kSxSlots;
     const int t = threadIdx.x;
     const int64_t s0 = (int64_t)f * tc::kFlush + (int64_t)lb * kSxSlots;
-    for (int e = t; e < nm * kSxSlots; e += kSxThreads) {
-        const int ss = e / nm, m = e - ss * nm;          // coalesced reads of sample s0 + ss
-        const bool ok = s0 + ss < n;
-        qs[m * kSxSlots + ss] = ok ? q[(s0 + ss) * nm + m] : 0.0;
-        vqs[m * kSxSlots + ss] = ok ? vq[(s0 + ss) * nm + m] : 0.0;
+    float* Vt = tx + (size_t)(1 + 6 * nm) * kSxSlots;
+    for (int l = t; l < kSxSlots; l += kSxThreads) {
+        tx[sx_col(l)] = 1.0f;
+        Vt[sx_col(l)] = s0 + l < n ? (float)v[s0 + l] : 0.0f;
     }
-    for (int ss = t; ss < kSxSlots; ss += kSxThreads) vs[ss] = s0 + ss < n ? v[s0 + ss] : 0.0;
+    for (int e = t; e < nm * kSxSlots; e += kSxThreads) {
+        const int l = e / nm, m = e - l * nm;      // coalesced reads of sample s0 + l
+        const bool ok = s0 + l < n;
+        const float x = ok ? (float)q[(s0 + l) * nm + m] : 0.0f;
+        const float vm = ok ? (float)vq[(s0 + l) * nm + m] : 0.0f;
+        const float V = ok ? (float)v[s0 + l] : 0.0f;
+        const float x2 = 2.0f * x * x;
+        const int c = sx_col(l);
+        tx[(1 + m) * kSxSlots + c] = 1.41421356f * x;                                  // h1
+        tx[(1 + nm + m) * kSxSlots + c] = (x2 - 1.0f) * 0.70710678f;                   // h2
+        tx[(1 + 2 * nm + m) * kSxSlots + c] = (x2 - 3.0f) * x * 0.57735027f;           // h3
+        tx[(1 + 3 * nm + m) * kSxSlots + c] = 0.70710678f * vm;                        // K_10
+        tx[(1 + 4 * nm + m) * kSxSlots + c] = 0.70710678f * x * vm;                    // K_20
+        tx[(1 + 5 * nm + m) * kSxSlots + c] = 1.15470054f * x * V + (x2 - 3.0f) * 0.28867513f * vm;   // K_30
+    }
     __syncthreads();
     const int g = t & 7, rl = t >> 3;
-    const int64_t slot0 = (int64_t)kb * kSxSlots + 8 * g;      // first K slot of the thread in the pass
-    const int64_t box_k = slot0 / tc::kKBlock2;                // its 32-slot box
-    const int c = (int)((slot0 / 8) & 3);                      // its 16-byte chunk of a box row
-#pragma unroll 1
-    for (int u = 0; u < kSxRows / 32; u++) {
-        const int row = blockIdx.y * kSxRows + rl + 32 * u;
-        float x[8];
-        if (row < nv) {
-            const uint32_t vd = __ldg(vrdesc + row);
-            const int m = vd & 255, a = (vd >> 8) & 3;
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const int ss = 8 * g + j;
-                x[j] = (vd & kGroundRow)
-                           ? (float)vs[ss]
-                           : (float)(reduced(vd, qs, kSxSlots, ss) *
-                                     stein_weight(a, 0, qs[m * kSxSlots + ss], vs[ss], vqs[m * kSxSlots + ss]));
-            }
-        } else if (row >= rows_w && row - rows_w < nb) {
-            int mm[3], ll[3];
-            const int k = decode(__ldg(desc + row - rows_w), mm, ll);
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const int ss = 8 * g + j;
-                double y = 1.0;
-                for (int w = 0; w < k; w++) y *= ho(ll[w], qs[mm[w] * kSxSlots + ss]);
-                x[j] = (float)y;
-            }
-        } else {
-            continue;
+    const float4* tab4 = reinterpret_cast<const float4*>(tx);
+    const int64_t box_k = (int64_t)kb * 2 + (g >> 2);          // the thread's 32-slot box
+    const int c = g & 3;                                       // its 16-byte chunk of a box row
+    const int r1 = min(rows, (int)(blockIdx.y + 1) * kSxRowsPerCta);
+    for (int row = blockIdx.y * kSxRowsPerCta + rl; row < r1; row += kSxThreads / 8) {
+        const uint32_t d = __ldg(xdesc + row);
+        if (d == kSxZeroRow) continue;
+        const uint32_t ia = d & 1023u, ib = (d >> 10) & 1023u, ic = d >> 20;
+        float4 a0 = tab4[ia * (kSxSlots / 4) + g], a1 = tab4[ia * (kSxSlots / 4) + g + 8];
+        if (ib) {
+            const float4 b0 = tab4[ib * (kSxSlots / 4) + g], b1 = tab4[ib * (kSxSlots / 4) + g + 8];
+            a0.x *= b0.x, a0.y *= b0.y, a0.z *= b0.z, a0.w *= b0.w;
+            a1.x *= b1.x, a1.y *= b1.y, a1.z *= b1.z, a1.w *= b1.w;
+        }
+        if (ic) {
+            const float4 c0 = tab4[ic * (kSxSlots / 4) + g], c1 = tab4[ic * (kSxSlots / 4) + g + 8];
+            a0.x *= c0.x, a0.y *= c0.y, a0.z *= c0.z, a0.w *= c0.w;
+            a1.x *= c1.x, a1.y *= c1.y, a1.z *= c1.z, a1.w *= c1.w;
         }
         uint4 hi, lo;
-        split_bf16x2(x[0], x[1], hi.x, lo.x);
-        split_bf16x2(x[2], x[3], hi.y, lo.y);
-        split_bf16x2(x[4], x[5], hi.z, lo.z);
-        split_bf16x2(x[6], x[7], hi.w, lo.w);
+        split_bf16x2(a0.x, a0.y, hi.x, lo.x);
+        split_bf16x2(a0.z, a0.w, hi.y, lo.y);
+        split_bf16x2(a1.x, a1.y, hi.z, lo.z);
+        split_bf16x2(a1.z, a1.w, hi.w, lo.w);
         const int rin = row & (tc::kTile - 1);
         uint16_t* box = xop + ((size_t)(row / tc::kTile) * nkb_alloc + box_k) * (2 * tc::kTile * tc::kKBlock2);
         const int off = rin * tc::kKBlock2 + ((c ^ ((rin >> 1) & 3)) << 3);
@@ -561,6 +573,8 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
     p.nb_pad = (int)round_up(p.nb, 128);
     if (sizeof(double) * (2 * (size_t)nm * kExpLd + kExpS) > 227 * 1024)
         return fail(SCP3GPU_ERR_ARG, "stein: too many modes for the expansion's shared memory (at most 220)");
+    if (split && sizeof(float) * (6 * (size_t)nm + 2) * kSxSlots > 227 * 1024)
+        return fail(SCP3GPU_ERR_ARG, "stein: too many modes for the split expansion's table (at most 147)");
     // functions exciting each mode, in basis order; rank of each in its mode's list
     std::vector<std::vector<int>> E(nm);
     std::vector<std::vector<int>> lev(nm);
@@ -697,7 +711,26 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
             }
         const std::vector<int> nosign((size_t)(chunk / tc::kFlush), tc::kSlotsPerFlush / 16);
         const size_t xop_elems = (size_t)2 * rows * p.slots;
-        if ((rc = upload(&p.tiles2, tl.data(), tl.size())) || (rc = upload(&p.nosign, nosign.data(), nosign.size())) ||
+        // per operand row, three indices into the expansion's table (0 = the constant 1)
+        auto hidx = [&](int m, int l) { return l ? (uint32_t)(1 + (l - 1) * nm + m) : 0u; };
+        std::vector<uint32_t> xd((size_t)rows, kSxZeroRow);
+        for (int r = 0; r < p.nv; r++) {
+            const uint32_t vd = vrdesc[r];
+            if (vd & kGroundRow) {
+                xd[r] = (uint32_t)(1 + 6 * nm);
+                continue;
+            }
+            const int m = vd & 255, a = (vd >> 8) & 3;
+            xd[r] = (uint32_t)(1 + (2 + a) * nm + m) | hidx((vd >> 10) & 255, (vd >> 18) & 3) << 10 |
+                    hidx((vd >> 20) & 255, (vd >> 28) & 3) << 20;
+        }
+        for (int j = 0; j < p.nb; j++) {
+            int mm[3] = {0, 0, 0}, ll[3] = {0, 0, 0};
+            decode(desc[j], mm, ll);
+            xd[(size_t)p.nv_pad + j] = hidx(mm[0], ll[0]) | hidx(mm[1], ll[1]) << 10 | hidx(mm[2], ll[2]) << 20;
+        }
+        if ((rc = upload(&p.xdesc, xd.data(), xd.size())) || (rc = upload(&p.tiles2, tl.data(), tl.size())) ||
+            (rc = upload(&p.nosign, nosign.data(), nosign.size())) ||
             (rc = dalloc(&p.xop, xop_elems)) || (rc = dalloc(&p.P, (size_t)p.nsplit * p.ntiles2 * 128 * 256)) ||
             (rc = dalloc(&p.err, (size_t)1))) {
             stein_destroy(p);
@@ -706,7 +739,7 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         // padding rows and the slots closing each 4096-sample block are never written
         SCP3_CUDA(cudaMemset(p.xop, 0, sizeof(uint16_t) * xop_elems));
         SCP3_CUDA(cudaMemset(p.err, 0, sizeof(int)));
-        const size_t es = sizeof(double) * (2 * (size_t)nm * kSxSlots + kSxSlots);
+        const size_t es = sizeof(float) * (6 * (size_t)nm + 2) * kSxSlots;
         if (es > 48 * 1024)
             SCP3_CUDA(cudaFuncSetAttribute(stein_expand_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)es));
@@ -731,7 +764,7 @@ void stein_destroy(SteinPlan& p)
 {
     cudaFree(p.vrdesc), cudaFree(p.rank3), cudaFree(p.voff), cudaFree(p.doff), cudaFree(p.dtasks), cudaFree(p.ftasks);
     cudaFree(p.W), cudaFree(p.Phi), cudaFree(p.C), cudaFree(p.D);
-    cudaFree(p.xop), cudaFree(p.tiles2), cudaFree(p.nosign), cudaFree(p.P), cudaFree(p.err);
+    cudaFree(p.xop), cudaFree(p.xdesc), cudaFree(p.tiles2), cudaFree(p.nosign), cudaFree(p.P), cudaFree(p.err);
     p = SteinPlan{};
 }
 
@@ -755,10 +788,11 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
     int rc;
     if (p.split) {
         const int nflush = (int)(k / tc::kFlush);
-        const size_t es = sizeof(double) * (2 * (size_t)p.nm * kSxSlots + kSxSlots);
-        dim3 eg((unsigned)(nflush * kSxBlocksPerFlush), (unsigned)((p.nv_pad + p.nb_pad) / kSxRows));
-        stein_expand_split_kernel<<<eg, kSxThreads, es, s>>>(desc, p.nb, p.vrdesc, p.nv, p.nv_pad, p.nm, q, v, vq, k,
-                                                             p.slots / tc::kKBlock2, p.xop);
+        const int rows = p.nv_pad + p.nb_pad;
+        const size_t es = sizeof(float) * (6 * (size_t)p.nm + 2) * kSxSlots;
+        dim3 eg((unsigned)(nflush * kSxBlocksPerFlush), (unsigned)((rows + kSxRowsPerCta - 1) / kSxRowsPerCta));
+        stein_expand_split_kernel<<<eg, kSxThreads, es, s>>>(p.xdesc, rows, p.nm, q, v, vq, k, p.slots / tc::kKBlock2,
+                                                             p.xop);
         SCP3_CUDA(cudaGetLastError());
         const int units = p.ntiles2 * p.nsplit;
         int sms = 148, dev = 0;
