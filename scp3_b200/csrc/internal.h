@@ -180,7 +180,17 @@ struct SteinPlan {
     int ntiles2 = 0;                 // tiles (W panel, Phi pair): rt * bpairs
     int64_t slots = 0;               // K slots of a whole pass (4160 per 4096 samples)
     uint16_t* xop = nullptr;         // [row block][k-block][hi, lo][128 x 32]
-    uint32_t* xdesc = nullptr;       // [nv_pad + nb_pad] the expansion's table indices of each row
+    uint32_t* xdesc = nullptr;       // [rows] the expansion's table indices of each row
+    // Same-mode pair sums on the tensor cores too (when every function without
+    // one of its factors is again a basis function): rows W_b(m, i) =
+    // R_i^m K^m_{a_i b} from row nv_pad, one block of e_m rows per (mode m, level
+    // b present in m), against the Phi columns of the reduced functions.
+    bool tcpairs = false;
+    int nwb_pad = 0;                 // W_b rows, padded to 128; Phi rows start at nv_pad + nwb_pad
+    int pmask = 0;                   // level pairs (a <= b) whose weights K_ab the table holds
+    int* tile_of = nullptr;          // [row panels][bpairs] tile of (W panel, Phi pair), -1 = none
+    int* red3 = nullptr;             // [nb * 3] function i without its k-th factor (basis index)
+    int* wb_off = nullptr;           // [nm * 4] first operand row of block (m, b)
     int4* tiles2 = nullptr;          // (W row, Phi row, 0, second Phi row)
     int* nosign = nullptr;           // [chunk / 4096] first negative 16-group: never
     double* P = nullptr;             // [nsplit][ntiles2][128 x 256] tile-local column-major

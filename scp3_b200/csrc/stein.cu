@@ -33,6 +33,8 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
 
 #include "internal.h"
 #include "tc.h"
@@ -173,9 +175,43 @@ __device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t& hi, u
 }
 
 constexpr int kSxSlots = 64, kSxThreads = 256;
-constexpr int kSxRowsPerCta = 1024;                                 // rows of the operand one CTA writes
+constexpr int kSxRowsPerCta = 2048;                                 // rows of the operand one CTA writes
 constexpr int kSxBlocksPerFlush = tc::kSlotsPerFlush / kSxSlots;   // 65: the last holds only padding slots
 constexpr uint32_t kSxZeroRow = 0xffffffffu;                        // padding row: never written
+
+// h_a(q), h_a(0), h_a'(q), d_a(q), d_a'(q) in FP32 (as ho_parts)
+__device__ __forceinline__ void ho_parts_f(int a, float q, float& h, float& h0, float& dh, float& d, float& dd)
+{
+    constexpr float s2 = 1.41421356f, is2 = 0.70710678f, is3 = 0.57735027f;
+    switch (a) {
+        case 0: h = 1, h0 = 1, dh = 0, d = 0, dd = 0; break;
+        case 1: h = s2 * q, h0 = 0, dh = s2, d = s2, dd = 0; break;
+        case 2: h = (2 * q * q - 1) * is2, h0 = -is2, dh = 2 * s2 * q, d = s2 * q, dd = s2; break;
+        default: h = (2 * q * q - 3) * q * is3, h0 = 0, dh = (6 * q * q - 3) * is3, d = (2 * q * q - 3) * is3,
+                 dd = 4 * q * is3; break;
+    }
+}
+
+// K_ab in FP32 (as stein_weight, including the reference's <3|V|3> form)
+__device__ __forceinline__ float stein_weight_f(int a, int b, float x, float V, float Vm)
+{
+    float ha, ha0, dha, da, dda, hb, hb0, dhb, db, ddb;
+    ho_parts_f(a, x, ha, ha0, dha, da, dda);
+    ho_parts_f(b, x, hb, hb0, dhb, db, ddb);
+    const float r = da * hb + ha0 * db;
+    const float dr = dda * hb + da * dhb + ha0 * ddb;
+    float u = ha0 * hb0 + 0.5f * dr;
+    const float w = 0.5f * r;
+    if (a == 3 && b == 3) u = (2 * x * x - 3) * (x * x - 3) * (1.0f / 6.0f);   // TripleExcitations.h:763-773
+    return u * V + w * Vm;
+}
+
+// level pair (a <= b, levels 1..3) -> 0..5: 11, 12, 13, 22, 23, 33
+__host__ __device__ __forceinline__ int level_pair(int a, int b)
+{
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    return lo == 1 ? hi - 1 : lo == 2 ? hi + 1 : 5;
+}
 
 // Table column of slot l (0..63): slots 8g..8g+3 at columns 4g..4g+3 and
 // 8g+4..8g+7 at 32+4g..32+4g+3, so the 8 threads of a row (thread g taking
@@ -193,18 +229,20 @@ __device__ __forceinline__ int sx_col(int l) { return ((l >> 3) << 2) | (l & 3) 
 // Per 64-slot block the CTA tabulates, in FP32, T = [1, h1(q_m), h2(q_m), h3(q_m),
 // K^m_10, K^m_20, K^m_30, V] (6 nm + 2 rows x 64 slots; with b = 0 the Stein
 // weights of stein_weight reduce to K_10 = Vm / sqrt2, K_20 = q Vm / sqrt2,
-// K_30 = (2 q / sqrt3) V + (2 q^2 - 3) / (2 sqrt3) Vm); every operand row is the
-// product of three table entries (xdesc: three 10-bit indices, 0 = the constant
-// 1).  The values are rounded to FP32 before the BF16 split in any case.
+// K_30 = (2 q / sqrt3) V + (2 q^2 - 3) / (2 sqrt3) Vm), followed, when the pair
+// sums run on the tensor cores, by K^m_ab for each level pair a <= b in pmask
+// (in the order 11, 12, 13, 22, 23, 33); every operand row is the product of
+// three table entries (xdesc: three 10-bit indices, 0 = the constant 1).  The
+// values are rounded to FP32 before the BF16 split in any case.
 // CTA: one 64-slot block x kSxRowsPerCta rows; thread (g, r) writes slots
 // 8g..8g+7 of rows r, r + 32, ...: one 16-byte chunk of the hi box and one of
 // the lo box each.
 __global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
-    const uint32_t* __restrict__ xdesc, int rows, int nm, const double* __restrict__ q,
+    const uint32_t* __restrict__ xdesc, int rows, int nm, int pmask, const double* __restrict__ q,
     const double* __restrict__ v, const double* __restrict__ vq, int64_t n, int64_t nkb_alloc,
     uint16_t* __restrict__ xop)
 {
-    extern __shared__ __align__(16) float tx[];   // [6 nm + 2][64]
+    extern __shared__ __align__(16) float tx[];   // [6 nm + 2 + pairs nm][64]
     const int kb = blockIdx.x;
     const int f = kb / kSxBlocksPerFlush, lb = kb - f * kSxBlocksPerFlush;
     if (lb * kSxSlots >= tc::kFlush) return;
@@ -229,6 +267,11 @@ __global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
         tx[(1 + 3 * nm + m) * kSxSlots + c] = 0.70710678f * vm;                        // K_10
         tx[(1 + 4 * nm + m) * kSxSlots + c] = 0.70710678f * x * vm;                    // K_20
         tx[(1 + 5 * nm + m) * kSxSlots + c] = 1.15470054f * x * V + (x2 - 3.0f) * 0.28867513f * vm;   // K_30
+        int k = 0;
+        for (int a = 1; a <= 3; a++)
+            for (int b = a; b <= 3; b++)
+                if ((pmask >> level_pair(a, b)) & 1)
+                    tx[(2 + 6 * nm + (k++) * nm + m) * kSxSlots + c] = stein_weight_f(a, b, x, V, vm);
     }
     __syncthreads();
     const int g = t & 7, rl = t >> 3;
@@ -496,16 +539,20 @@ __global__ void __launch_bounds__(kTriThreads) stein_pairs_tri_kernel(const int*
 // (m, c) column r, or the pair sum D^m when both excite m; the mean over those
 // modes; <0|V|0> from the ground row.  C: FP64 tiles of 128 x 128, row-major,
 // `ct` per tile row (N256 = false); or the split form's 128 x 256 unit partials
-// (N256 = true), tile (row panel r, column panel pair q) at index q * ct + r
-// with `ct` = row panels (pair-major, as stein_create lists them), tile-local
-// column-major.
+// (N256 = true), tile (row panel r, column panel pair q) at tile_of[r * ct + q]
+// with `ct` = column panel pairs, tile-local column-major.  With wb_off (the
+// split form's pair sums as products) the term of a pair exciting m in both
+// functions is C at W_b row (m, rank of r, level of c in m), column
+// red3(c without its mode-m factor).
 template <bool N256>
 __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int* __restrict__ rank3,
                                     const int* __restrict__ voff, const int64_t* __restrict__ doff, int nb, int nv,
                                     int ct, int nsplit, int dsplit, const double* __restrict__ C,
                                     const double* __restrict__ D,
                                     int64_t csize, int64_t dsize, double divisor, const double* __restrict__ diag,
-                                    double zpe, double* __restrict__ M, int64_t ld)
+                                    double zpe, double* __restrict__ M, int64_t ld,
+                                    const int* __restrict__ tile_of, const int* __restrict__ red3,
+                                    const int* __restrict__ wb_off)
 {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (int64_t)nb * nb) return;
@@ -513,7 +560,7 @@ __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int
     const int r = min(i, j), c = max(i, j);
     auto cidx = [&](int vr, int col) -> int64_t {
         if (N256)
-            return ((int64_t)(col >> 8) * ct + (vr >> 7)) * (128 * 256) +
+            return (int64_t)tile_of[(vr >> 7) * ct + (col >> 8)] * (128 * 256) +
                    (int64_t)(((col >> 7) & 1) * 128 + (col & 127)) * 128 + (vr & 127);
         return ((int64_t)(vr >> 7) * ct + (col >> 7)) * (128 * 128) + (int64_t)(vr & 127) * 128 + (col & 127);
     };
@@ -533,6 +580,10 @@ __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int
             double t = 0.0;
             if (b < 0) {
                 const int64_t x = cidx(voff[m] + rank3[3 * r + a], c);
+                for (int s = 0; s < nsplit; s++) t += C[s * csize + x];
+            } else if (wb_off) {
+                // W_b row (m, rank of r, level of c in m) against Phi of c without m
+                const int64_t x = cidx(wb_off[m * 4 + lc[b]] + rank3[3 * r + a], red3[3 * c + b]);
                 for (int s = 0; s < nsplit; s++) t += C[s * csize + x];
             } else {
                 // D holds the upper triangle of ranks (functions ordered by level in m)
@@ -684,14 +735,105 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         // ranges per tile minimising waves per range, at most 16, partials under ~4 GB.
         p.split = true;
         p.bpairs = (p.ct + 1) / 2;
-        p.ntiles2 = p.rt * p.bpairs;
-        const int64_t rows = (int64_t)p.nv_pad + p.nb_pad;
+        // The same-mode pair sums as products too, when every function j exciting m
+        // is, without its mode-m factor, again a basis function (red3) and the
+        // expansion's table holds the weights of the level pairs present:
+        // T^m_ij = sum_s [R_i^m K^m_{a_i b_j}] Phi_{red(j, m)}.
+        std::map<std::array<int, 6>, int> index_of;     // sorted (mode, level) factors -> basis index
+        auto key_of = [](const int* mm, const int* ll, int k, int skip) {
+            std::array<int, 6> key{-1, -1, -1, -1, -1, -1};
+            std::vector<std::pair<int, int>> f;
+            for (int a = 0; a < k; a++)
+                if (a != skip) f.push_back({mm[a], ll[a]});
+            std::sort(f.begin(), f.end());
+            for (size_t u = 0; u < f.size(); u++) key[2 * u] = f[u].first, key[2 * u + 1] = f[u].second;
+            return key;
+        };
+        for (int j = 0; j < p.nb; j++) {
+            int mm[3], ll[3];
+            const int k = decode(desc[j], mm, ll);
+            index_of[key_of(mm, ll, k, -1)] = j;
+        }
+        std::vector<int> red3((size_t)p.nb * 3, -1);
+        bool closed = true;
+        for (int j = 0; j < p.nb; j++) {
+            int mm[3], ll[3];
+            const int k = decode(desc[j], mm, ll);
+            for (int a = 0; a < k; a++) {
+                const auto it = index_of.find(key_of(mm, ll, k, a));
+                if (it == index_of.end()) closed = false;
+                else red3[(size_t)3 * j + a] = it->second;
+            }
+        }
+        std::vector<int> levmask(nm, 0);
+        for (int m = 0; m < nm; m++)
+            for (int l : lev[m]) levmask[m] |= 1 << l;
+        int pmask = 0;
+        for (int m = 0; m < nm; m++)
+            for (int a = 1; a <= 3; a++)
+                for (int b = a; b <= 3; b++)
+                    if (((levmask[m] >> a) & 1) && ((levmask[m] >> b) & 1)) pmask |= 1 << level_pair(a, b);
+        const int trows_pairs = 2 + 6 * nm + __builtin_popcount(pmask) * nm;
+        p.tcpairs = closed && trows_pairs <= 1024 && sizeof(float) * trows_pairs * kSxSlots <= 227 * 1024;
+        p.pmask = p.tcpairs ? pmask : 0;
+        const int trows = 2 + 6 * nm + __builtin_popcount(p.pmask) * nm;
+        auto kidx = [&](int m, int a, int b) {   // table row of K^m_ab
+            const int k = level_pair(a, b);
+            return (uint32_t)(2 + 6 * nm + __builtin_popcount(p.pmask & ((1 << k) - 1)) * nm + m);
+        };
+        // W_b blocks (m, b), one per level b present in mode m, e_m rows each
+        std::vector<int> wb_off((size_t)nm * 4, -1);
+        int nwb = 0;
+        if (p.tcpairs)
+            for (int m = 0; m < nm; m++)
+                for (int b = 1; b <= 3; b++)
+                    if ((levmask[m] >> b) & 1) {
+                        wb_off[(size_t)m * 4 + b] = p.nv_pad + nwb;
+                        nwb += (int)E[m].size();
+                    }
+        p.nwb_pad = (int)round_up(nwb, 128);
+        const int wpanels = (p.nv_pad + p.nwb_pad) / 128;
+        const int phi0 = p.nv_pad + p.nwb_pad;     // first Phi row
+        const int64_t rows = (int64_t)phi0 + p.nb_pad;
         auto slots_of = [](int64_t k) { return k / tc::kFlush * tc::kSlotsPerFlush; };
         int64_t chunk = chunk_cfg > 0 ? chunk_cfg : 65536;
         while (chunk > tc::kFlush && rows * slots_of(chunk) * 4 > (4ll << 30)) chunk /= 2;
         chunk = std::max<int64_t>(chunk / tc::kFlush * tc::kFlush, tc::kFlush);
         p.chunk = chunk;
         p.slots = slots_of(chunk);
+        // tiles: every W panel of the direct terms against every Phi pair (pair-major,
+        // so a wave's tiles share their pairs), then every W_b panel against the pairs
+        // that hold its rows' reduced functions
+        std::vector<int4> tl;
+        std::vector<int> tile_of((size_t)wpanels * p.bpairs, -1);
+        auto add_tile = [&](int r, int q) {
+            const int b0 = phi0 + 2 * q * 128, b1 = 2 * q + 1 < p.ct ? b0 + 128 : b0;
+            tile_of[(size_t)r * p.bpairs + q] = (int)tl.size();
+            tl.push_back(make_int4(r * 128, b0, 0, b1));
+        };
+        for (int q = 0; q < p.bpairs; q++)
+            for (int r = 0; r < p.rt; r++) add_tile(r, q);
+        if (p.tcpairs) {
+            std::vector<std::vector<char>> need((size_t)wpanels, std::vector<char>((size_t)p.bpairs, 0));
+            for (int m = 0; m < nm; m++)
+                for (int b = 1; b <= 3; b++) {
+                    const int o = wb_off[(size_t)m * 4 + b], en = (int)E[m].size();
+                    if (o < 0) continue;
+                    for (int r = 0; r < en; r++) {
+                        if (lev[m][r] != b) continue;
+                        int mm[3], ll[3];
+                        const int k = decode(desc[E[m][r]], mm, ll);
+                        for (int a = 0; a < k; a++)
+                            if (mm[a] == m)
+                                for (int pr = o / 128; pr <= (o + en - 1) / 128; pr++)
+                                    need[pr][red3[(size_t)3 * E[m][r] + a] / 256] = 1;
+                    }
+                }
+            for (int r = p.rt; r < wpanels; r++)
+                for (int q = 0; q < p.bpairs; q++)
+                    if (need[r][q]) add_tile(r, q);
+        }
+        p.ntiles2 = (int)tl.size();
         double best = 1e300;
         p.nsplit = 1;
         for (int m = 1; m <= 16; m++) {
@@ -701,14 +843,7 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
             if (cost < best - 1e-12) best = cost, p.nsplit = m;
         }
         p.dsplit = 1;
-        while (p.dsplit < 64 && p.dsplit * 2 * p.dsize * 8 <= (256ll << 20)) p.dsplit *= 2;
-        std::vector<int4> tl;
-        for (int q = 0; q < p.bpairs; q++)          // pair-major: a wave's tiles share their Phi pairs
-            for (int r = 0; r < p.rt; r++) {
-                const int b0 = p.nv_pad + 2 * q * 128;
-                const int b1 = 2 * q + 1 < p.ct ? b0 + 128 : b0;
-                tl.push_back(make_int4(r * 128, b0, 0, b1));
-            }
+        while (!p.tcpairs && p.dsplit < 64 && p.dsplit * 2 * p.dsize * 8 <= (256ll << 20)) p.dsplit *= 2;
         const std::vector<int> nosign((size_t)(chunk / tc::kFlush), tc::kSlotsPerFlush / 16);
         const size_t xop_elems = (size_t)2 * rows * p.slots;
         // per operand row, three indices into the expansion's table (0 = the constant 1)
@@ -724,12 +859,25 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
             xd[r] = (uint32_t)(1 + (2 + a) * nm + m) | hidx((vd >> 10) & 255, (vd >> 18) & 3) << 10 |
                     hidx((vd >> 20) & 255, (vd >> 28) & 3) << 20;
         }
+        for (int m = 0; m < nm; m++)        // W_b(m, r) = R^m_{E_m[r]} K^m_{a_r b}
+            for (int b = 1; b <= 3; b++) {
+                const int o = wb_off[(size_t)m * 4 + b];
+                if (o < 0) continue;
+                for (size_t r = 0; r < E[m].size(); r++) {
+                    const uint32_t vd = vrdesc[voff[m] + r];
+                    xd[(size_t)o + r] = kidx(m, lev[m][r], b) | hidx((vd >> 10) & 255, (vd >> 18) & 3) << 10 |
+                                        hidx((vd >> 20) & 255, (vd >> 28) & 3) << 20;
+                }
+            }
         for (int j = 0; j < p.nb; j++) {
             int mm[3] = {0, 0, 0}, ll[3] = {0, 0, 0};
             decode(desc[j], mm, ll);
-            xd[(size_t)p.nv_pad + j] = hidx(mm[0], ll[0]) | hidx(mm[1], ll[1]) << 10 | hidx(mm[2], ll[2]) << 20;
+            xd[(size_t)phi0 + j] = hidx(mm[0], ll[0]) | hidx(mm[1], ll[1]) << 10 | hidx(mm[2], ll[2]) << 20;
         }
         if ((rc = upload(&p.xdesc, xd.data(), xd.size())) || (rc = upload(&p.tiles2, tl.data(), tl.size())) ||
+            (rc = upload(&p.tile_of, tile_of.data(), tile_of.size())) ||
+            (p.tcpairs && ((rc = upload(&p.red3, red3.data(), red3.size())) ||
+                           (rc = upload(&p.wb_off, wb_off.data(), wb_off.size())))) ||
             (rc = upload(&p.nosign, nosign.data(), nosign.size())) ||
             (rc = dalloc(&p.xop, xop_elems)) || (rc = dalloc(&p.P, (size_t)p.nsplit * p.ntiles2 * 128 * 256)) ||
             (rc = dalloc(&p.err, (size_t)1))) {
@@ -739,7 +887,7 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         // padding rows and the slots closing each 4096-sample block are never written
         SCP3_CUDA(cudaMemset(p.xop, 0, sizeof(uint16_t) * xop_elems));
         SCP3_CUDA(cudaMemset(p.err, 0, sizeof(int)));
-        const size_t es = sizeof(float) * (6 * (size_t)nm + 2) * kSxSlots;
+        const size_t es = sizeof(float) * (size_t)trows * kSxSlots;
         if (es > 48 * 1024)
             SCP3_CUDA(cudaFuncSetAttribute(stein_expand_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)es));
@@ -748,7 +896,7 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         (rc = upload(&p.voff, voff.data(), voff.size())) || (rc = upload(&p.doff, doff.data(), doff.size())) ||
         (p.ndtasks && (rc = upload(&p.dtasks, tasks.data(), tasks.size()))) ||
         (p.nftasks && (rc = upload(&p.ftasks, ftasks.data(), ftasks.size()))) ||
-        (rc = dalloc(&p.D, (size_t)p.dsize * p.dsplit))) {
+        (!p.tcpairs && (rc = dalloc(&p.D, (size_t)p.dsize * p.dsplit)))) {
         stein_destroy(p);
         return rc;
     }
@@ -765,6 +913,7 @@ void stein_destroy(SteinPlan& p)
     cudaFree(p.vrdesc), cudaFree(p.rank3), cudaFree(p.voff), cudaFree(p.doff), cudaFree(p.dtasks), cudaFree(p.ftasks);
     cudaFree(p.W), cudaFree(p.Phi), cudaFree(p.C), cudaFree(p.D);
     cudaFree(p.xop), cudaFree(p.xdesc), cudaFree(p.tiles2), cudaFree(p.nosign), cudaFree(p.P), cudaFree(p.err);
+    cudaFree(p.tile_of), cudaFree(p.red3), cudaFree(p.wb_off);
     p = SteinPlan{};
 }
 
@@ -776,7 +925,7 @@ int stein_zero(const SteinPlan& p, cudaStream_t s)
     } else {
         SCP3_CUDA(cudaMemsetAsync(p.C, 0, sizeof(double) * (size_t)p.rt * p.ct * 128 * 128 * p.nsplit, s));
     }
-    SCP3_CUDA(cudaMemsetAsync(p.D, 0, sizeof(double) * (size_t)p.dsize * p.dsplit, s));
+    if (p.D) SCP3_CUDA(cudaMemsetAsync(p.D, 0, sizeof(double) * (size_t)p.dsize * p.dsplit, s));
     return SCP3GPU_OK;
 }
 
@@ -788,11 +937,12 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
     int rc;
     if (p.split) {
         const int nflush = (int)(k / tc::kFlush);
-        const int rows = p.nv_pad + p.nb_pad;
-        const size_t es = sizeof(float) * (6 * (size_t)p.nm + 2) * kSxSlots;
+        const int rows = p.nv_pad + p.nwb_pad + p.nb_pad;
+        const size_t es = sizeof(float) * (6 * (size_t)p.nm + 2 + (size_t)__builtin_popcount(p.pmask) * p.nm) *
+                          kSxSlots;
         dim3 eg((unsigned)(nflush * kSxBlocksPerFlush), (unsigned)((rows + kSxRowsPerCta - 1) / kSxRowsPerCta));
-        stein_expand_split_kernel<<<eg, kSxThreads, es, s>>>(p.xdesc, rows, p.nm, q, v, vq, k, p.slots / tc::kKBlock2,
-                                                             p.xop);
+        stein_expand_split_kernel<<<eg, kSxThreads, es, s>>>(p.xdesc, rows, p.nm, p.pmask, q, v, vq, k,
+                                                             p.slots / tc::kKBlock2, p.xop);
         SCP3_CUDA(cudaGetLastError());
         const int units = p.ntiles2 * p.nsplit;
         int sms = 148, dev = 0;
@@ -812,6 +962,7 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
         rc = launch_gemm_fp64_rect(p.W, p.nv_pad, p.Phi, p.nb_pad, k, p.rt, p.ct, p.nsplit, p.C, s);
     }
     if (rc) return rc;
+    if (p.tcpairs) return SCP3GPU_OK;      // the pair sums were part of the products
     if (p.ndtasks) {
         const size_t ps = sizeof(double) * ((size_t)kPS * p.nm + 2 * kPS + 2 * kPS * kPT + 16 * kPS);
         if (ps > 48 * 1024)
@@ -844,13 +995,14 @@ int stein_unpack(const SteinPlan& p, const uint32_t* desc, double divisor, const
         SCP3_CUDA(cudaMemcpyAsync(&err, p.err, sizeof(int), cudaMemcpyDeviceToHost, s));
         SCP3_CUDA(cudaStreamSynchronize(s));
         if (err) return fail(SCP3GPU_ERR_TIMEOUT, "tensor-core contraction: a bounded pipeline wait expired");
-        stein_unpack_kernel<true><<<grid, 256, 0, s>>>(desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.rt, p.nsplit,
+        stein_unpack_kernel<true><<<grid, 256, 0, s>>>(desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.bpairs, p.nsplit,
                                                        p.dsplit, p.P, p.D, (int64_t)p.ntiles2 * 128 * 256, p.dsize,
-                                                       divisor, diag, zpe, M, ld);
+                                                       divisor, diag, zpe, M, ld, p.tile_of, p.red3,
+                                                       p.tcpairs ? p.wb_off : nullptr);
     } else {
         stein_unpack_kernel<false><<<grid, 256, 0, s>>>(desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.ct, p.nsplit,
                                                         p.dsplit, p.C, p.D, (int64_t)p.rt * p.ct * 128 * 128, p.dsize,
-                                                        divisor, diag, zpe, M, ld);
+                                                        divisor, diag, zpe, M, ld, nullptr, nullptr, nullptr);
     }
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
