@@ -187,7 +187,8 @@ struct SteinPlan {
     // b present in m), against the Phi columns of the reduced functions.
     bool tcpairs = false;
     int nwb_pad = 0;                 // W_b rows, padded to 128; Phi rows start at nv_pad + nwb_pad
-    int pmask = 0;                   // level pairs (a <= b) whose weights K_ab the table holds
+    int trows = 0;                   // rows of the expansion's table (1, h_l(q_m), K^m_a0, V, K^m_ab)
+    uint32_t* tspec = nullptr;       // [trows] kind | a << 4 | b << 6 | mode << 8 of each table row
     int* tile_of = nullptr;          // [row panels][bpairs] tile of (W panel, Phi pair), -1 = none
     int* red3 = nullptr;             // [nb * 3] function i without its k-th factor (basis index)
     int* wb_off = nullptr;           // [nm * 4] first operand row of block (m, b)

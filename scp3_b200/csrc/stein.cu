@@ -174,10 +174,13 @@ __device__ __forceinline__ void split_bf16x2(float x0, float x1, uint32_t& hi, u
     lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
-constexpr int kSxSlots = 64, kSxThreads = 256;
-constexpr int kSxRowsPerCta = 2048;                                 // rows of the operand one CTA writes
-constexpr int kSxBlocksPerFlush = tc::kSlotsPerFlush / kSxSlots;   // 65: the last holds only padding slots
+constexpr int kSxSlots = 32, kSxThreads = 256, kSxLd = 33;
+constexpr int kSxBlocksPerFlush = tc::kSlotsPerFlush / kSxSlots;   // 130: the last two hold only padding slots
 constexpr uint32_t kSxZeroRow = 0xffffffffu;                        // padding row: never written
+constexpr int kSxMaxTable = 1024;                                   // table rows (10-bit indices)
+
+// Kinds of table rows (TableSpec: kind | a << 4 | b << 6 | mode << 8)
+enum : uint32_t { kTOne = 0, kTHo = 1, kTKa0 = 2, kTV = 3, kTKab = 4 };
 
 // h_a(q), h_a(0), h_a'(q), d_a(q), d_a'(q) in FP32 (as ho_parts)
 __device__ __forceinline__ void ho_parts_f(int a, float q, float& h, float& h0, float& dh, float& d, float& dd)
@@ -213,84 +216,102 @@ __host__ __device__ __forceinline__ int level_pair(int a, int b)
     return lo == 1 ? hi - 1 : lo == 2 ? hi + 1 : 5;
 }
 
-// Table column of slot l (0..63): slots 8g..8g+3 at columns 4g..4g+3 and
-// 8g+4..8g+7 at 32+4g..32+4g+3, so the 8 threads of a row (thread g taking
-// slots 8g..8g+7) read two contiguous 128-byte spans (no bank conflict).
-__device__ __forceinline__ int sx_col(int l) { return ((l >> 3) << 2) | (l & 3) | ((l & 4) << 3); }
+// Table entry of row r for slot l (0..31): slots 8g..8g+3 at 4g..4g+3 and
+// 8g+4..8g+7 at 16+4g..16+4g+3, the two halves swapped on odd rows, so that the
+// 4 threads of an operand row read 64 contiguous bytes per load and rows of
+// different parity fall in different banks.
+__device__ __forceinline__ int sx_col(int r, int l)
+{
+    return ((((l >> 2) & 1) << 4) ^ ((r & 1) << 4)) | ((l >> 3) << 2) | (l & 3);
+}
 
 // The split operand of a pass: the W rows (reduced function x Stein weight K^m_a0,
-// and the ground row V) from row 0 and the Phi rows from row nv_pad, as BF16
-// hi + lo in the 32-slot, 64-byte-swizzled boxes the tensor-core contraction
-// reads ([row block][k-block][hi, lo][128 x 32], 16-byte chunk c of row r at
-// c ^ ((r >> 1) & 3)).  K slot l of 4096-sample block f holds sample 4096 f + l
-// (l < 4096); the block's last 64 slots and the padding rows are never written
-// (zero since creation).
+// and the ground row V) from row 0, the W_b rows (R_i^m K^m_ab) after them and the
+// Phi rows last, as BF16 hi + lo in the 32-slot, 64-byte-swizzled boxes the
+// tensor-core contraction reads ([row block][k-block][hi, lo][128 x 32], 16-byte
+// chunk c of row r at c ^ ((r >> 1) & 3)).  K slot l of 4096-sample block f holds
+// sample 4096 f + l (l < 4096); the block's last 64 slots and the padding rows
+// are never written (zero since creation).
 //
-// Per 64-slot block the CTA tabulates, in FP32, T = [1, h1(q_m), h2(q_m), h3(q_m),
-// K^m_10, K^m_20, K^m_30, V] (6 nm + 2 rows x 64 slots; with b = 0 the Stein
-// weights of stein_weight reduce to K_10 = Vm / sqrt2, K_20 = q Vm / sqrt2,
-// K_30 = (2 q / sqrt3) V + (2 q^2 - 3) / (2 sqrt3) Vm), followed, when the pair
-// sums run on the tensor cores, by K^m_ab for each level pair a <= b in pmask
-// (in the order 11, 12, 13, 22, 23, 33); every operand row is the product of
-// three table entries (xdesc: three 10-bit indices, 0 = the constant 1).  The
-// values are rounded to FP32 before the BF16 split in any case.
-// CTA: one 64-slot block x kSxRowsPerCta rows; thread (g, r) writes slots
-// 8g..8g+7 of rows r, r + 32, ...: one 16-byte chunk of the hi box and one of
-// the lo box each.
+// Per 32-slot block the CTA tabulates in FP32 the entries the operand's rows use
+// (tspec: 1, h_l(q_m), K^m_a0, V, K^m_ab; with b = 0 the Stein weights of
+// stein_weight reduce to K_10 = Vm / sqrt2, K_20 = q Vm / sqrt2, K_30 = (2 q /
+// sqrt3) V + (2 q^2 - 3) / (2 sqrt3) Vm); a warp fills one table row at a time, so
+// its kind is uniform.  Every operand row is the product of three table entries
+// (xdesc: three 10-bit indices, 0 = the constant 1).  The values are rounded to
+// FP32 before the BF16 split in any case.  CTA: one 32-slot block x `per` rows;
+// thread (g, r) writes slots 8g..8g+7 of rows r, r + 64, ...: one 16-byte chunk of
+// the hi box and one of the lo box each.
 __global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
-    const uint32_t* __restrict__ xdesc, int rows, int nm, int pmask, const double* __restrict__ q,
-    const double* __restrict__ v, const double* __restrict__ vq, int64_t n, int64_t nkb_alloc,
-    uint16_t* __restrict__ xop)
+    const uint32_t* __restrict__ tspec, int trows, const uint32_t* __restrict__ xdesc, int rows, int per, int nm,
+    const double* __restrict__ q, const double* __restrict__ v, const double* __restrict__ vq, int64_t n,
+    int64_t nkb_alloc, uint16_t* __restrict__ xop)
 {
-    extern __shared__ __align__(16) float tx[];   // [6 nm + 2 + pairs nm][64]
+    extern __shared__ __align__(16) float tx[];   // table [trows][32]; q, Vm [nm][33]; V [32]
     const int kb = blockIdx.x;
     const int f = kb / kSxBlocksPerFlush, lb = kb - f * kSxBlocksPerFlush;
     if (lb * kSxSlots >= tc::kFlush) return;
     const int t = threadIdx.x;
     const int64_t s0 = (int64_t)f * tc::kFlush + (int64_t)lb * kSxSlots;
-    float* Vt = tx + (size_t)(1 + 6 * nm) * kSxSlots;
-    for (int l = t; l < kSxSlots; l += kSxThreads) {
-        tx[sx_col(l)] = 1.0f;
-        Vt[sx_col(l)] = s0 + l < n ? (float)v[s0 + l] : 0.0f;
-    }
+    float* qs = tx + (size_t)trows * kSxSlots;
+    float* vms = qs + (size_t)nm * kSxLd;
+    float* vs = vms + (size_t)nm * kSxLd;
     for (int e = t; e < nm * kSxSlots; e += kSxThreads) {
         const int l = e / nm, m = e - l * nm;      // coalesced reads of sample s0 + l
         const bool ok = s0 + l < n;
-        const float x = ok ? (float)q[(s0 + l) * nm + m] : 0.0f;
-        const float vm = ok ? (float)vq[(s0 + l) * nm + m] : 0.0f;
-        const float V = ok ? (float)v[s0 + l] : 0.0f;
-        const float x2 = 2.0f * x * x;
-        const int c = sx_col(l);
-        tx[(1 + m) * kSxSlots + c] = 1.41421356f * x;                                  // h1
-        tx[(1 + nm + m) * kSxSlots + c] = (x2 - 1.0f) * 0.70710678f;                   // h2
-        tx[(1 + 2 * nm + m) * kSxSlots + c] = (x2 - 3.0f) * x * 0.57735027f;           // h3
-        tx[(1 + 3 * nm + m) * kSxSlots + c] = 0.70710678f * vm;                        // K_10
-        tx[(1 + 4 * nm + m) * kSxSlots + c] = 0.70710678f * x * vm;                    // K_20
-        tx[(1 + 5 * nm + m) * kSxSlots + c] = 1.15470054f * x * V + (x2 - 3.0f) * 0.28867513f * vm;   // K_30
-        int k = 0;
-        for (int a = 1; a <= 3; a++)
-            for (int b = a; b <= 3; b++)
-                if ((pmask >> level_pair(a, b)) & 1)
-                    tx[(2 + 6 * nm + (k++) * nm + m) * kSxSlots + c] = stein_weight_f(a, b, x, V, vm);
+        qs[m * kSxLd + l] = ok ? (float)q[(s0 + l) * nm + m] : 0.0f;
+        vms[m * kSxLd + l] = ok ? (float)vq[(s0 + l) * nm + m] : 0.0f;
+    }
+    for (int l = t; l < kSxSlots; l += kSxThreads) vs[l] = s0 + l < n ? (float)v[s0 + l] : 0.0f;
+    __syncthreads();
+    for (int e = t; e < trows * kSxSlots; e += kSxThreads) {
+        const int r = e / kSxSlots, l = e - r * kSxSlots;
+        const uint32_t sp = __ldg(tspec + r);
+        const int kind = sp & 15, a = (sp >> 4) & 3, b = (sp >> 6) & 3, m = sp >> 8;
+        float val = 1.0f;
+        if (kind == kTV) {
+            val = vs[l];
+        } else if (kind != kTOne) {
+            const float x = qs[m * kSxLd + l];
+            if (kind == kTHo) {
+                const float x2 = 2.0f * x * x;
+                val = a == 1 ? 1.41421356f * x : a == 2 ? (x2 - 1.0f) * 0.70710678f : (x2 - 3.0f) * x * 0.57735027f;
+            } else if (kind == kTKa0) {
+                const float vm = vms[m * kSxLd + l];
+                val = a == 1 ? 0.70710678f * vm
+                             : a == 2 ? 0.70710678f * x * vm
+                                      : 1.15470054f * x * vs[l] + (2.0f * x * x - 3.0f) * 0.28867513f * vm;
+            } else {
+                val = stein_weight_f(a, b, x, vs[l], vms[m * kSxLd + l]);
+            }
+        }
+        tx[r * kSxSlots + sx_col(r, l)] = val;
     }
     __syncthreads();
-    const int g = t & 7, rl = t >> 3;
+    const int g = t & 3, rl = t >> 2;
     const float4* tab4 = reinterpret_cast<const float4*>(tx);
-    const int64_t box_k = (int64_t)kb * 2 + (g >> 2);          // the thread's 32-slot box
-    const int c = g & 3;                                       // its 16-byte chunk of a box row
-    const int r1 = min(rows, (int)(blockIdx.y + 1) * kSxRowsPerCta);
-    for (int row = blockIdx.y * kSxRowsPerCta + rl; row < r1; row += kSxThreads / 8) {
+    const int64_t box_k = kb;                                  // the block's 32-slot box
+    auto rd = [&](uint32_t i, float4& lo4, float4& hi4) {
+        const uint32_t sw = (i & 1u) << 2;                      // swapped halves (in float4 units)
+        lo4 = tab4[i * (kSxSlots / 4) + (sw ^ 0u) + g];
+        hi4 = tab4[i * (kSxSlots / 4) + (sw ^ 4u) + g];
+    };
+    const int r0 = blockIdx.y * per, r1 = min(rows, r0 + per);
+    for (int row = r0 + rl; row < r1; row += kSxThreads / 4) {
         const uint32_t d = __ldg(xdesc + row);
         if (d == kSxZeroRow) continue;
         const uint32_t ia = d & 1023u, ib = (d >> 10) & 1023u, ic = d >> 20;
-        float4 a0 = tab4[ia * (kSxSlots / 4) + g], a1 = tab4[ia * (kSxSlots / 4) + g + 8];
+        float4 a0, a1;
+        rd(ia, a0, a1);
         if (ib) {
-            const float4 b0 = tab4[ib * (kSxSlots / 4) + g], b1 = tab4[ib * (kSxSlots / 4) + g + 8];
+            float4 b0, b1;
+            rd(ib, b0, b1);
             a0.x *= b0.x, a0.y *= b0.y, a0.z *= b0.z, a0.w *= b0.w;
             a1.x *= b1.x, a1.y *= b1.y, a1.z *= b1.z, a1.w *= b1.w;
         }
         if (ic) {
-            const float4 c0 = tab4[ic * (kSxSlots / 4) + g], c1 = tab4[ic * (kSxSlots / 4) + g + 8];
+            float4 c0, c1;
+            rd(ic, c0, c1);
             a0.x *= c0.x, a0.y *= c0.y, a0.z *= c0.z, a0.w *= c0.w;
             a1.x *= c1.x, a1.y *= c1.y, a1.z *= c1.z, a1.w *= c1.w;
         }
@@ -301,7 +322,7 @@ __global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
         split_bf16x2(a1.z, a1.w, hi.w, lo.w);
         const int rin = row & (tc::kTile - 1);
         uint16_t* box = xop + ((size_t)(row / tc::kTile) * nkb_alloc + box_k) * (2 * tc::kTile * tc::kKBlock2);
-        const int off = rin * tc::kKBlock2 + ((c ^ ((rin >> 1) & 3)) << 3);
+        const int off = rin * tc::kKBlock2 + ((g ^ ((rin >> 1) & 3)) << 3);
         *reinterpret_cast<uint4*>(box + off) = hi;
         *reinterpret_cast<uint4*>(box + tc::kTile * tc::kKBlock2 + off) = lo;
     }
@@ -624,8 +645,8 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
     p.nb_pad = (int)round_up(p.nb, 128);
     if (sizeof(double) * (2 * (size_t)nm * kExpLd + kExpS) > 227 * 1024)
         return fail(SCP3GPU_ERR_ARG, "stein: too many modes for the expansion's shared memory (at most 220)");
-    if (split && sizeof(float) * (6 * (size_t)nm + 2) * kSxSlots > 227 * 1024)
-        return fail(SCP3GPU_ERR_ARG, "stein: too many modes for the split expansion's table (at most 147)");
+    if (split && 6 * nm + 2 > kSxMaxTable)
+        return fail(SCP3GPU_ERR_ARG, "stein: too many modes for the split expansion's table (at most 170)");
     // functions exciting each mode, in basis order; rank of each in its mode's list
     std::vector<std::vector<int>> E(nm);
     std::vector<std::vector<int>> lev(nm);
@@ -768,19 +789,9 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         std::vector<int> levmask(nm, 0);
         for (int m = 0; m < nm; m++)
             for (int l : lev[m]) levmask[m] |= 1 << l;
-        int pmask = 0;
-        for (int m = 0; m < nm; m++)
-            for (int a = 1; a <= 3; a++)
-                for (int b = a; b <= 3; b++)
-                    if (((levmask[m] >> a) & 1) && ((levmask[m] >> b) & 1)) pmask |= 1 << level_pair(a, b);
-        const int trows_pairs = 2 + 6 * nm + __builtin_popcount(pmask) * nm;
-        p.tcpairs = closed && trows_pairs <= 1024 && sizeof(float) * trows_pairs * kSxSlots <= 227 * 1024;
-        p.pmask = p.tcpairs ? pmask : 0;
-        const int trows = 2 + 6 * nm + __builtin_popcount(p.pmask) * nm;
-        auto kidx = [&](int m, int a, int b) {   // table row of K^m_ab
-            const int k = level_pair(a, b);
-            return (uint32_t)(2 + 6 * nm + __builtin_popcount(p.pmask & ((1 << k) - 1)) * nm + m);
-        };
+        // the expansion's table holds at most 1 + 3 nm Hermite values, 3 nm weights
+        // K_a0, V and 6 nm weights K_ab: 10-bit indices
+        p.tcpairs = closed && 12 * nm + 2 <= kSxMaxTable;
         // W_b blocks (m, b), one per level b present in mode m, e_m rows each
         std::vector<int> wb_off((size_t)nm * 4, -1);
         int nwb = 0;
@@ -846,17 +857,29 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         while (!p.tcpairs && p.dsplit < 64 && p.dsplit * 2 * p.dsize * 8 <= (256ll << 20)) p.dsplit *= 2;
         const std::vector<int> nosign((size_t)(chunk / tc::kFlush), tc::kSlotsPerFlush / 16);
         const size_t xop_elems = (size_t)2 * rows * p.slots;
-        // per operand row, three indices into the expansion's table (0 = the constant 1)
-        auto hidx = [&](int m, int l) { return l ? (uint32_t)(1 + (l - 1) * nm + m) : 0u; };
+        // per operand row, three indices into the expansion's table (0 = the constant 1);
+        // the table holds the entries the rows use, numbered as they are first needed
+        std::map<uint32_t, uint32_t> tslot;
+        std::vector<uint32_t> tspec{kTOne};
+        auto tab = [&](uint32_t kind, int a, int b, int m) -> uint32_t {
+            const uint32_t key = kind | (uint32_t)a << 4 | (uint32_t)b << 6 | (uint32_t)m << 8;
+            const auto it = tslot.find(key);
+            if (it != tslot.end()) return it->second;
+            const uint32_t i = (uint32_t)tspec.size();
+            tspec.push_back(key);
+            tslot[key] = i;
+            return i;
+        };
+        auto hidx = [&](int m, int l) { return l ? tab(kTHo, l, 0, m) : 0u; };
         std::vector<uint32_t> xd((size_t)rows, kSxZeroRow);
         for (int r = 0; r < p.nv; r++) {
             const uint32_t vd = vrdesc[r];
             if (vd & kGroundRow) {
-                xd[r] = (uint32_t)(1 + 6 * nm);
+                xd[r] = tab(kTV, 0, 0, 0);
                 continue;
             }
             const int m = vd & 255, a = (vd >> 8) & 3;
-            xd[r] = (uint32_t)(1 + (2 + a) * nm + m) | hidx((vd >> 10) & 255, (vd >> 18) & 3) << 10 |
+            xd[r] = tab(kTKa0, a, 0, m) | hidx((vd >> 10) & 255, (vd >> 18) & 3) << 10 |
                     hidx((vd >> 20) & 255, (vd >> 28) & 3) << 20;
         }
         for (int m = 0; m < nm; m++)        // W_b(m, r) = R^m_{E_m[r]} K^m_{a_r b}
@@ -865,7 +888,9 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
                 if (o < 0) continue;
                 for (size_t r = 0; r < E[m].size(); r++) {
                     const uint32_t vd = vrdesc[voff[m] + r];
-                    xd[(size_t)o + r] = kidx(m, lev[m][r], b) | hidx((vd >> 10) & 255, (vd >> 18) & 3) << 10 |
+                    const int a = lev[m][r];
+                    xd[(size_t)o + r] = tab(kTKab, std::min(a, b), std::max(a, b), m) |
+                                        hidx((vd >> 10) & 255, (vd >> 18) & 3) << 10 |
                                         hidx((vd >> 20) & 255, (vd >> 28) & 3) << 20;
                 }
             }
@@ -874,7 +899,13 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
             decode(desc[j], mm, ll);
             xd[(size_t)phi0 + j] = hidx(mm[0], ll[0]) | hidx(mm[1], ll[1]) << 10 | hidx(mm[2], ll[2]) << 20;
         }
-        if ((rc = upload(&p.xdesc, xd.data(), xd.size())) || (rc = upload(&p.tiles2, tl.data(), tl.size())) ||
+        p.trows = (int)tspec.size();
+        if (p.trows > kSxMaxTable) {
+            stein_destroy(p);
+            return fail(SCP3GPU_ERR_ARG, "stein: the split expansion's table exceeds 1024 rows");
+        }
+        if ((rc = upload(&p.xdesc, xd.data(), xd.size())) || (rc = upload(&p.tspec, tspec.data(), tspec.size())) ||
+            (rc = upload(&p.tiles2, tl.data(), tl.size())) ||
             (rc = upload(&p.tile_of, tile_of.data(), tile_of.size())) ||
             (p.tcpairs && ((rc = upload(&p.red3, red3.data(), red3.size())) ||
                            (rc = upload(&p.wb_off, wb_off.data(), wb_off.size())))) ||
@@ -887,7 +918,7 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         // padding rows and the slots closing each 4096-sample block are never written
         SCP3_CUDA(cudaMemset(p.xop, 0, sizeof(uint16_t) * xop_elems));
         SCP3_CUDA(cudaMemset(p.err, 0, sizeof(int)));
-        const size_t es = sizeof(float) * (size_t)trows * kSxSlots;
+        const size_t es = sizeof(float) * ((size_t)p.trows * kSxSlots + 2 * (size_t)nm * kSxLd + kSxSlots);
         if (es > 48 * 1024)
             SCP3_CUDA(cudaFuncSetAttribute(stein_expand_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)es));
@@ -913,7 +944,7 @@ void stein_destroy(SteinPlan& p)
     cudaFree(p.vrdesc), cudaFree(p.rank3), cudaFree(p.voff), cudaFree(p.doff), cudaFree(p.dtasks), cudaFree(p.ftasks);
     cudaFree(p.W), cudaFree(p.Phi), cudaFree(p.C), cudaFree(p.D);
     cudaFree(p.xop), cudaFree(p.xdesc), cudaFree(p.tiles2), cudaFree(p.nosign), cudaFree(p.P), cudaFree(p.err);
-    cudaFree(p.tile_of), cudaFree(p.red3), cudaFree(p.wb_off);
+    cudaFree(p.tile_of), cudaFree(p.red3), cudaFree(p.wb_off), cudaFree(p.tspec);
     p = SteinPlan{};
 }
 
@@ -938,10 +969,11 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
     if (p.split) {
         const int nflush = (int)(k / tc::kFlush);
         const int rows = p.nv_pad + p.nwb_pad + p.nb_pad;
-        const size_t es = sizeof(float) * (6 * (size_t)p.nm + 2 + (size_t)__builtin_popcount(p.pmask) * p.nm) *
-                          kSxSlots;
-        dim3 eg((unsigned)(nflush * kSxBlocksPerFlush), (unsigned)((rows + kSxRowsPerCta - 1) / kSxRowsPerCta));
-        stein_expand_split_kernel<<<eg, kSxThreads, es, s>>>(p.xdesc, rows, p.nm, p.pmask, q, v, vq, k,
+        const size_t es = sizeof(float) * ((size_t)p.trows * kSxSlots + 2 * (size_t)p.nm * kSxLd + kSxSlots);
+        // rows in chunks of at most 4096 per CTA (whole 64-row trips)
+        const int ny = (rows + 4095) / 4096, per = (int)round_up((rows + ny - 1) / ny, 64);
+        dim3 eg((unsigned)(nflush * kSxBlocksPerFlush), (unsigned)ny);
+        stein_expand_split_kernel<<<eg, kSxThreads, es, s>>>(p.tspec, p.trows, p.xdesc, rows, per, p.nm, q, v, vq, k,
                                                              p.slots / tc::kKBlock2, p.xop);
         SCP3_CUDA(cudaGetLastError());
         const int units = p.ntiles2 * p.nsplit;
