@@ -89,6 +89,16 @@ __device__ inline double potential(const T* crd, const WarpSlot<T>& w, int nw, c
 constexpr size_t kMuaSmemMax = 64 * 1024;
 
 __host__ __device__ inline int mua_groups(int nw) { return (9 * nw + 63) / 64; }
+
+// On the gradient path MUa of the selected modes is also staged transposed,
+// [coordinate][selected mode] in FP64, when it fits this many bytes: the lane of
+// mode m then reads row c at m (consecutive lanes, consecutive words) where a
+// read of MUa[k][c] from global memory touched one cache line per lane.
+constexpr size_t kMuaTSmemMax = 48 * 1024;
+__host__ __device__ inline size_t muat_smem_bytes(int nw, int nm)
+{
+    return (sizeof(double) * 9 * (size_t)nw * nm + 15) / 16 * 16;   // the warp slots follow, 16-byte aligned
+}
 template <typename T>
 __host__ __device__ inline size_t mua_smem_bytes(int nw, int nm0)
 {
@@ -150,8 +160,17 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
         }
         __syncthreads();
     }
-    char* slots = smem + (mua_in_smem ? mua_b : 0);
     const bool grad = a.vq != nullptr;
+    const bool muat_in_smem = grad && muat_smem_bytes(nw, a.nm) <= kMuaTSmemMax;
+    double* muat = reinterpret_cast<double*>(smem + (mua_in_smem ? mua_b : 0));   // [N3][nm]
+    if (muat_in_smem) {
+        for (int e = threadIdx.x; e < N3 * a.nm; e += blockDim.x) {
+            const int c = e / a.nm, m = e - c * a.nm;
+            muat[e] = a.MUa[(size_t)__ldg(a.modes + m) * N3 + c];
+        }
+        __syncthreads();
+    }
+    char* slots = smem + (mua_in_smem ? mua_b : 0) + (muat_in_smem ? muat_smem_bytes(nw, a.nm) : 0);
     WarpSlot<T> w = warp_slot<T>(slots + wib * slot_bytes<T>(PES, nm0, nw, grad, kGroup), PES, nm0, nw, grad, kGroup);
     // Each warp takes one contiguous range of samples, the ranges balanced to
     // within one sample (the grid is sized to the SMs, so there is no tail wave):
@@ -369,7 +388,10 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
                     for (int m = lane; m < a.nm; m += 32) {
                         const int k = __ldg(a.modes + m);
                         double acc = 0.0;
-                        for (int c = 0; c < N3; c++) acc += MUa[(size_t)k * N3 + c] * w.g[c];
+                        if (muat_in_smem)
+                            for (int c = 0; c < N3; c++) acc += muat[(size_t)c * a.nm + m] * w.g[c];
+                        else
+                            for (int c = 0; c < N3; c++) acc += MUa[(size_t)k * N3 + c] * w.g[c];
                         a.vq[s * a.nm + m] = acc * (kBohr / kAuToKcalPerMol) - __ldg(a.omega + k) * (double)q[k];
                     }
                 }
@@ -563,8 +585,9 @@ template <int PES, typename T>
 int launch_samples_t(const SampleArgs& a, cudaStream_t s)
 {
     const size_t mua_b = mua_smem_bytes<T>(a.nw, a.nm0);
+    const size_t muat_b = muat_smem_bytes(a.nw, a.nm);
     const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw, a.vq != nullptr, kGroup) +
-                      (mua_b <= kMuaSmemMax ? mua_b : 0);
+                      (mua_b <= kMuaSmemMax ? mua_b : 0) + (a.vq && muat_b <= kMuaTSmemMax ? muat_b : 0);
     if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_kernel<PES, T>,
                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     samples_kernel<PES, T><<<sample_grid(samples_kernel<PES, T>, sm, a.n), kWarpsPerBlock * 32, sm, s>>>(a);
