@@ -390,8 +390,9 @@ __global__ void __launch_bounds__(1024) partition_kernel(const double* __restric
 // Per k-block the CTA tabulates, per slot, [1, h1(q_m), h2(q_m), h3(q_m)] for
 // all modes in shared memory; every basis value is then the product of three
 // table entries (basis_factor_table).  Thread (g, r) handles slots 8g..8g+7 of
-// rows r, r+32, ...: two 16-byte table reads per factor (the table's columns
-// are permuted so these are conflict-free) and one 16-byte store per half, so
+// rows 4r..4r+3, 4r+128..4r+131, ...: two 16-byte table reads per factor (the
+// table's columns are permuted so these are conflict-free; a first factor shared
+// with the previous row is not read again) and one 16-byte store per half, so
 // the 8 threads of a row write its 128 contiguous bytes.  While a
 // k-block's rows are written, its successor's q rows and V values are already
 // in flight into a staging area (cp.async), so the table build that follows
@@ -452,7 +453,7 @@ __host__ __device__ inline size_t expand_smem(int nm, bool staged)
 // The operand is written as 32-slot boxes in the 64-byte swizzle (nkb counts
 // 32-slot k-blocks per row block).
 template <bool F16>
-__global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandDesc* __restrict__ descs, int ncl,
+__global__ void __launch_bounds__(kExpThreads, 3) expand_split_kernel(const ExpandDesc* __restrict__ descs, int ncl,
                                                                     int64_t nkbp, int64_t nkb, int staged,
                                                                     uint16_t* __restrict__ xop)
 {
@@ -590,23 +591,27 @@ __global__ void __launch_bounds__(kExpThreads) expand_split_kernel(const ExpandD
             const float4 w1 = reinterpret_cast<const float4*>(sv)[g8 + 8];
             // rows past nb stay as the operand's allocation zeroed them
             const int rend = min(cur.r1, nb);
-            for (int r = cur.r0 + rl; r < rend; r += 4 * kStep) {
+            // thread rl takes 4 consecutive rows per trip: consecutive rows mostly share
+            // their first factor (pairs (m, n), (m, n + 1), ...), read once
+            for (int r = cur.r0 + 4 * rl; r < rend; r += 4 * kStep) {
                 uint32_t f[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int rr = r + u * kStep;
-                    f[u] = rr < rend ? __ldg(factors + rr) : kNone;
-                }
+                for (int u = 0; u < 4; u++) f[u] = r + u < rend ? __ldg(factors + r + u) : kNone;
+                uint32_t pia = 0xffffffffu;
+                float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
-                    const int rr = r + u * kStep;
+                    const int rr = r + u;
                     if (rr >= rend) break;
                     uint4 hi = make_uint4(0, 0, 0, 0), lo = hi;
                     if (f[u] != kNone) {
                         // factor 0 is the constant 1: not read (most rows have one or two)
-                        const uint32_t ib = (f[u] >> 10) & 1023u, ic = f[u] >> 20;
-                        const float4* A = tab4 + (f[u] & 1023u) * (kExpSlots / 4) + g8;
-                        const float4 a0 = A[0], a1 = A[8];
+                        const uint32_t ia = f[u] & 1023u, ib = (f[u] >> 10) & 1023u, ic = f[u] >> 20;
+                        if (ia != pia) {
+                            a0 = tab4[ia * (kExpSlots / 4) + g8];
+                            a1 = tab4[ia * (kExpSlots / 4) + g8 + 8];
+                            pia = ia;
+                        }
                         const float4 one = make_float4(1.f, 1.f, 1.f, 1.f);
                         float4 b0 = one, b1 = one, c0 = one, c1 = one;
                         if (ib) b0 = tab4[ib * (kExpSlots / 4) + g8], b1 = tab4[ib * (kExpSlots / 4) + g8 + 8];
