@@ -44,9 +44,9 @@ WORKLOAD = "hexamer prism qTIP4P/f, 48 modes, doubles basis Nb=1225, 2^20 scramb
 METRIC = "Sobol samples/s (hexamer H-build) at <=0.1 cm^-1 on 10 lowest levels vs FP64"
 FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (vector and tensor) nominal; no measured FP64 peak on this pool
 # DRAM bytes (read + write) of the BF16x3 contraction on the hexamer doubles basis, from an ncu
-# capture of one 2^18-sample pass (its two launches: dram__bytes_read.sum + dram__bytes_write.sum =
-# 1071.7 + 42.9 MB and 461.5 + 0.9 MB); per launch it grows with the samples the launch covers
-CONTRACT_DRAM_BYTES_PER_SAMPLE = (1071.655936e6 + 42.878208e6 + 461.541376e6 + 0.873216e6) / 262144
+# capture of one 2^18-sample pass (one launch of 140 CTAs: dram__bytes_read.sum +
+# dram__bytes_write.sum = 1447.6 + 42.2 MB); per launch it grows with the samples the launch covers
+CONTRACT_DRAM_BYTES_PER_SAMPLE = (1447.607808e6 + 42.220288e6) / 262144
 
 
 def load_peaks():
