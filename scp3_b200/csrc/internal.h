@@ -191,7 +191,14 @@ struct SteinPlan {
     uint32_t* tspec = nullptr;       // [trows] kind | a << 4 | b << 6 | mode << 8 of each table row
     int* tile_of = nullptr;          // [row panels][bpairs] tile of (W panel, Phi pair), -1 = none
     int* red3 = nullptr;             // [nb * 3] function i without its k-th factor (basis index)
-    int* wb_off = nullptr;           // [nm * 4] first operand row of block (m, b)
+    int* wb_off = nullptr;           // [nm * 4] first operand row of block (m, b), -1 = none
+    // Blocks (m, b) whose functions all reduce to the constant (red = the ground
+    // function: for the doubles basis, level 2 = h2(q_m) alone) need only sum_s of
+    // each row: they are summed in the expansion instead of multiplied.
+    int nsum = 0;                    // rows summed
+    int* sum_off = nullptr;          // [nm * 4] first summed row of block (m, b), -1 = none
+    float* spart = nullptr;          // [chunk / 4096 * 130][nsum] per-32-slot-block sums of a pass
+    double* sums = nullptr;          // [nsum] sum over the samples so far
     int4* tiles2 = nullptr;          // (W row, Phi row, 0, second Phi row)
     int* nosign = nullptr;           // [chunk / 4096] first negative 16-group: never
     double* P = nullptr;             // [nsplit][ntiles2][128 x 256] tile-local column-major

@@ -243,9 +243,9 @@ __device__ __forceinline__ int sx_col(int r, int l)
 // thread (g, r) writes slots 8g..8g+7 of rows r, r + 64, ...: one 16-byte chunk of
 // the hi box and one of the lo box each.
 __global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
-    const uint32_t* __restrict__ tspec, int trows, const uint32_t* __restrict__ xdesc, int rows, int per, int nm,
-    const double* __restrict__ q, const double* __restrict__ v, const double* __restrict__ vq, int64_t n,
-    int64_t nkb_alloc, uint16_t* __restrict__ xop)
+    const uint32_t* __restrict__ tspec, int trows, const uint32_t* __restrict__ xdesc, int rows, int nsum, int per,
+    int nm, const double* __restrict__ q, const double* __restrict__ v, const double* __restrict__ vq, int64_t n,
+    int64_t nkb_alloc, uint16_t* __restrict__ xop, float* __restrict__ spart)
 {
     extern __shared__ __align__(16) float tx[];   // table [trows][32]; q, Vm [nm][33]; V [32]
     const int kb = blockIdx.x;
@@ -296,10 +296,38 @@ __global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
         lo4 = tab4[i * (kSxSlots / 4) + (sw ^ 0u) + g];
         hi4 = tab4[i * (kSxSlots / 4) + (sw ^ 4u) + g];
     };
-    const int r0 = blockIdx.y * per, r1 = min(rows, r0 + per);
-    for (int row = r0 + rl; row < r1; row += kSxThreads / 4) {
-        const uint32_t d = __ldg(xdesc + row);
-        if (d == kSxZeroRow) continue;
+    const int r0 = blockIdx.y * per, r1 = min(rows + nsum, r0 + per);
+    for (int rb = r0; rb < r1; rb += kSxThreads / 4) {
+        const int row = rb + rl;
+        const uint32_t d = row < r1 ? __ldg(xdesc + row) : kSxZeroRow;
+        if (row >= rows && row < r1) {
+            // a summed row: its 32 values added, in FP32, into this block's partial
+            float x = 0.0f;
+            if (d != kSxZeroRow) {
+                const uint32_t ia = d & 1023u, ib = (d >> 10) & 1023u, ic = d >> 20;
+                float4 a0, a1;
+                rd(ia, a0, a1);
+                if (ib) {
+                    float4 b0, b1;
+                    rd(ib, b0, b1);
+                    a0.x *= b0.x, a0.y *= b0.y, a0.z *= b0.z, a0.w *= b0.w;
+                    a1.x *= b1.x, a1.y *= b1.y, a1.z *= b1.z, a1.w *= b1.w;
+                }
+                if (ic) {
+                    float4 c0, c1;
+                    rd(ic, c0, c1);
+                    a0.x *= c0.x, a0.y *= c0.y, a0.z *= c0.z, a0.w *= c0.w;
+                    a1.x *= c1.x, a1.y *= c1.y, a1.z *= c1.z, a1.w *= c1.w;
+                }
+                x = ((a0.x + a0.y) + (a0.z + a0.w)) + ((a1.x + a1.y) + (a1.z + a1.w));
+            }
+            const unsigned grp = 0xfu << (threadIdx.x & 28);     // the 4 lanes of this row
+            x += __shfl_xor_sync(grp, x, 1);
+            x += __shfl_xor_sync(grp, x, 2);
+            if (g == 0) spart[(size_t)kb * nsum + (row - rows)] = x;
+            continue;
+        }
+        if (row >= r1 || d == kSxZeroRow) continue;
         const uint32_t ia = d & 1023u, ib = (d >> 10) & 1023u, ic = d >> 20;
         float4 a0, a1;
         rd(ia, a0, a1);
@@ -555,6 +583,36 @@ __global__ void __launch_bounds__(kTriThreads) stein_pairs_tri_kernel(const int*
         }
 }
 
+// sums[i] += the summed rows' partials of a pass (the last two blocks of every
+// 4096-sample block hold only padding slots and are skipped).  CTA: 32 rows;
+// warp w adds the blocks b = w mod 8 (a coalesced 128-byte read per block), the
+// eight warp sums are then added in warp order, so the result does not depend
+// on scheduling.
+__global__ void __launch_bounds__(256) stein_rowsum_kernel(const float* __restrict__ spart, int nsum, int nblocks,
+                                                           double* __restrict__ sums)
+{
+    __shared__ double ws[8][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + lane;
+    constexpr int kValid = tc::kFlush / kSxSlots;     // 128 sample blocks per 130
+    const int nvalid = nblocks / kSxBlocksPerFlush * kValid;
+    double acc = 0.0;
+    if (i < nsum) {
+#pragma unroll 8
+        for (int vb = w; vb < nvalid; vb += 8) {
+            const int b = vb / kValid * kSxBlocksPerFlush + vb % kValid;
+            acc += (double)__ldg(spart + (size_t)b * nsum + i);
+        }
+    }
+    ws[w][lane] = acc;
+    __syncthreads();
+    if (w == 0 && i < nsum) {
+        double t = 0.0;
+        for (int k = 0; k < 8; k++) t += ws[k][lane];
+        sums[i] += t;
+    }
+}
+
 // Element (i, j) of the dense matrix from its terms: for each mode m that r =
 // min(i, j) or c = max(i, j) excites, C at virtual row (m, r) column c, or at
 // (m, c) column r, or the pair sum D^m when both excite m; the mean over those
@@ -573,7 +631,8 @@ __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int
                                     int64_t csize, int64_t dsize, double divisor, const double* __restrict__ diag,
                                     double zpe, double* __restrict__ M, int64_t ld,
                                     const int* __restrict__ tile_of, const int* __restrict__ red3,
-                                    const int* __restrict__ wb_off)
+                                    const int* __restrict__ wb_off, const int* __restrict__ sum_off,
+                                    const double* __restrict__ sums)
 {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (int64_t)nb * nb) return;
@@ -602,6 +661,9 @@ __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int
             if (b < 0) {
                 const int64_t x = cidx(voff[m] + rank3[3 * r + a], c);
                 for (int s = 0; s < nsplit; s++) t += C[s * csize + x];
+            } else if (sum_off && sum_off[m * 4 + lc[b]] >= 0) {
+                // summed row (m, rank of r, level of c in m): c without m is the constant
+                t = sums[sum_off[m * 4 + lc[b]] + rank3[3 * r + a]];
             } else if (wb_off) {
                 // W_b row (m, rank of r, level of c in m) against Phi of c without m
                 const int64_t x = cidx(wb_off[m * 4 + lc[b]] + rank3[3 * r + a], red3[3 * c + b]);
@@ -792,16 +854,34 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         // the expansion's table holds at most 1 + 3 nm Hermite values, 3 nm weights
         // K_a0, V and 6 nm weights K_ab: 10-bit indices
         p.tcpairs = closed && 12 * nm + 2 <= kSxMaxTable;
-        // W_b blocks (m, b), one per level b present in mode m, e_m rows each
-        std::vector<int> wb_off((size_t)nm * 4, -1);
+        // W_b blocks (m, b), one per level b present in mode m, e_m rows each: in the
+        // operand, or summed when every function of level b in m reduces to the
+        // constant (its only Phi column would be the ground function's)
+        std::vector<int> wb_off((size_t)nm * 4, -1), sum_off((size_t)nm * 4, -1);
+        auto reduces_to_ground = [&](int m, int b) {
+            for (size_t r = 0; r < E[m].size(); r++) {
+                if (lev[m][r] != b) continue;
+                int mm[3], ll[3];
+                const int k = decode(desc[E[m][r]], mm, ll);
+                for (int a = 0; a < k; a++)
+                    if (mm[a] == m && red3[(size_t)3 * E[m][r] + a] != 0) return false;
+            }
+            return true;
+        };
         int nwb = 0;
+        p.nsum = 0;
         if (p.tcpairs)
             for (int m = 0; m < nm; m++)
-                for (int b = 1; b <= 3; b++)
-                    if ((levmask[m] >> b) & 1) {
+                for (int b = 1; b <= 3; b++) {
+                    if (!((levmask[m] >> b) & 1)) continue;
+                    if (reduces_to_ground(m, b)) {
+                        sum_off[(size_t)m * 4 + b] = p.nsum;
+                        p.nsum += (int)E[m].size();
+                    } else {
                         wb_off[(size_t)m * 4 + b] = p.nv_pad + nwb;
                         nwb += (int)E[m].size();
                     }
+                }
         p.nwb_pad = (int)round_up(nwb, 128);
         const int wpanels = (p.nv_pad + p.nwb_pad) / 128;
         const int phi0 = p.nv_pad + p.nwb_pad;     // first Phi row
@@ -871,7 +951,7 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
             return i;
         };
         auto hidx = [&](int m, int l) { return l ? tab(kTHo, l, 0, m) : 0u; };
-        std::vector<uint32_t> xd((size_t)rows, kSxZeroRow);
+        std::vector<uint32_t> xd((size_t)rows + p.nsum, kSxZeroRow);   // operand rows, then summed rows
         for (int r = 0; r < p.nv; r++) {
             const uint32_t vd = vrdesc[r];
             if (vd & kGroundRow) {
@@ -884,7 +964,9 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         }
         for (int m = 0; m < nm; m++)        // W_b(m, r) = R^m_{E_m[r]} K^m_{a_r b}
             for (int b = 1; b <= 3; b++) {
-                const int o = wb_off[(size_t)m * 4 + b];
+                const int o = wb_off[(size_t)m * 4 + b] >= 0 ? wb_off[(size_t)m * 4 + b]
+                              : sum_off[(size_t)m * 4 + b] >= 0 ? (int)rows + sum_off[(size_t)m * 4 + b]
+                                                                 : -1;
                 if (o < 0) continue;
                 for (size_t r = 0; r < E[m].size(); r++) {
                     const uint32_t vd = vrdesc[voff[m] + r];
@@ -908,7 +990,10 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
             (rc = upload(&p.tiles2, tl.data(), tl.size())) ||
             (rc = upload(&p.tile_of, tile_of.data(), tile_of.size())) ||
             (p.tcpairs && ((rc = upload(&p.red3, red3.data(), red3.size())) ||
-                           (rc = upload(&p.wb_off, wb_off.data(), wb_off.size())))) ||
+                           (rc = upload(&p.wb_off, wb_off.data(), wb_off.size())) ||
+                           (rc = upload(&p.sum_off, sum_off.data(), sum_off.size())))) ||
+            (p.nsum && ((rc = dalloc(&p.spart, (size_t)(chunk / tc::kFlush) * kSxBlocksPerFlush * p.nsum)) ||
+                        (rc = dalloc(&p.sums, (size_t)p.nsum)))) ||
             (rc = upload(&p.nosign, nosign.data(), nosign.size())) ||
             (rc = dalloc(&p.xop, xop_elems)) || (rc = dalloc(&p.P, (size_t)p.nsplit * p.ntiles2 * 128 * 256)) ||
             (rc = dalloc(&p.err, (size_t)1))) {
@@ -917,6 +1002,9 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         }
         // padding rows and the slots closing each 4096-sample block are never written
         SCP3_CUDA(cudaMemset(p.xop, 0, sizeof(uint16_t) * xop_elems));
+        if (p.spart)   // the blocks of padding slots are never written
+            SCP3_CUDA(cudaMemset(p.spart, 0,
+                                 sizeof(float) * (size_t)(chunk / tc::kFlush) * kSxBlocksPerFlush * p.nsum));
         SCP3_CUDA(cudaMemset(p.err, 0, sizeof(int)));
         const size_t es = sizeof(float) * ((size_t)p.trows * kSxSlots + 2 * (size_t)nm * kSxLd + kSxSlots);
         if (es > 48 * 1024)
@@ -945,6 +1033,7 @@ void stein_destroy(SteinPlan& p)
     cudaFree(p.W), cudaFree(p.Phi), cudaFree(p.C), cudaFree(p.D);
     cudaFree(p.xop), cudaFree(p.xdesc), cudaFree(p.tiles2), cudaFree(p.nosign), cudaFree(p.P), cudaFree(p.err);
     cudaFree(p.tile_of), cudaFree(p.red3), cudaFree(p.wb_off), cudaFree(p.tspec);
+    cudaFree(p.sum_off), cudaFree(p.spart), cudaFree(p.sums);
     p = SteinPlan{};
 }
 
@@ -957,6 +1046,7 @@ int stein_zero(const SteinPlan& p, cudaStream_t s)
         SCP3_CUDA(cudaMemsetAsync(p.C, 0, sizeof(double) * (size_t)p.rt * p.ct * 128 * 128 * p.nsplit, s));
     }
     if (p.D) SCP3_CUDA(cudaMemsetAsync(p.D, 0, sizeof(double) * (size_t)p.dsize * p.dsplit, s));
+    if (p.sums) SCP3_CUDA(cudaMemsetAsync(p.sums, 0, sizeof(double) * (size_t)p.nsum, s));
     return SCP3GPU_OK;
 }
 
@@ -971,10 +1061,15 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
         const int rows = p.nv_pad + p.nwb_pad + p.nb_pad;
         const size_t es = sizeof(float) * ((size_t)p.trows * kSxSlots + 2 * (size_t)p.nm * kSxLd + kSxSlots);
         // rows in chunks of at most 4096 per CTA (whole 64-row trips)
-        const int ny = (rows + 4095) / 4096, per = (int)round_up((rows + ny - 1) / ny, 64);
+        const int vrows = rows + p.nsum;   // operand rows, then summed rows
+        const int ny = (vrows + 4095) / 4096, per = (int)round_up((vrows + ny - 1) / ny, 64);
         dim3 eg((unsigned)(nflush * kSxBlocksPerFlush), (unsigned)ny);
-        stein_expand_split_kernel<<<eg, kSxThreads, es, s>>>(p.tspec, p.trows, p.xdesc, rows, per, p.nm, q, v, vq, k,
-                                                             p.slots / tc::kKBlock2, p.xop);
+        stein_expand_split_kernel<<<eg, kSxThreads, es, s>>>(p.tspec, p.trows, p.xdesc, rows, p.nsum, per, p.nm, q,
+                                                             v, vq, k, p.slots / tc::kKBlock2, p.xop, p.spart);
+        SCP3_CUDA(cudaGetLastError());
+        if (p.nsum)
+            stein_rowsum_kernel<<<(p.nsum + 31) / 32, 256, 0, s>>>(p.spart, p.nsum, nflush * kSxBlocksPerFlush,
+                                                                   p.sums);
         SCP3_CUDA(cudaGetLastError());
         const int units = p.ntiles2 * p.nsplit;
         int sms = 148, dev = 0;
@@ -1030,11 +1125,13 @@ int stein_unpack(const SteinPlan& p, const uint32_t* desc, double divisor, const
         stein_unpack_kernel<true><<<grid, 256, 0, s>>>(desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.bpairs, p.nsplit,
                                                        p.dsplit, p.P, p.D, (int64_t)p.ntiles2 * 128 * 256, p.dsize,
                                                        divisor, diag, zpe, M, ld, p.tile_of, p.red3,
-                                                       p.tcpairs ? p.wb_off : nullptr);
+                                                       p.tcpairs ? p.wb_off : nullptr,
+                                                       p.nsum ? p.sum_off : nullptr, p.sums);
     } else {
         stein_unpack_kernel<false><<<grid, 256, 0, s>>>(desc, p.rank3, p.voff, p.doff, p.nb, p.nv, p.ct, p.nsplit,
                                                         p.dsplit, p.C, p.D, (int64_t)p.rt * p.ct * 128 * 128, p.dsize,
-                                                        divisor, diag, zpe, M, ld, nullptr, nullptr, nullptr);
+                                                        divisor, diag, zpe, M, ld, nullptr, nullptr, nullptr,
+                                                        nullptr, nullptr);
     }
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
