@@ -57,6 +57,24 @@ def test_dimer_gradient_build_matches_reference(scp3, z, tag, pes):
     assert np.allclose(diag_g, diag_d, rtol=0, atol=1e-12)
 
 
+@pytest.mark.parametrize("tag,pes", [("dimer", "qtip4pf"), ("dimer_ttm3f", "ttm3f")])
+def test_dimer_split_gradient_build_matches_reference(scp3, z, tag, pes):
+    """The BF16x3 form of the gradient build (device Sobol, the potential's FP64
+    gradient, products and pair sums on the tensor cores) against the same
+    reference matrices: every upper element within 2e-5 of the largest."""
+    n2, n3, ns = int(z[tag + "_n2"]), int(z[tag + "_n3"]), int(z[tag + "_nsamples"])
+    hb = scp3.HBuild(2, z[tag + "_x0"], z[tag + "_MUa"], z[tag + "_omega"], n2=n2, n3=n3, pes=pes,
+                     scramble_seed=int(z[tag + "_scramble_seed"]), estimator="gradient", precision="bf16x3")
+    hb.accumulate(0, ns)
+    M = hb.read(0)
+    assert hb.status()[0] == 0
+    got = M.T[np.tril_indices(M.shape[0])]
+    ref = z[tag + "_M_upper"]
+    err = np.abs(got - ref) / np.abs(ref).max()
+    print("\nsplit gradient, %s: max %.2e median %.2e of max|M|" % (tag, err.max(), np.median(err)))
+    assert err.max() <= 2e-5, err.max()
+
+
 def test_add_epot_grad_matches_oracle(scp3, oracle_mod):
     c = np.load(os.path.join(GOLDEN, "hbuild_ref.npz"))
     omega = c["hexamer_qtip4pf__omega"]
