@@ -124,11 +124,12 @@ typedef struct scp3gpu_config {
 /* matrix-element estimator (SCP3.cpp:226-231) */
 #define SCP3GPU_ESTIMATOR_DIRECT 0   /* -G: sum_s Phi V Phi^T (ScaledMatrixElements.cpp:951-971)         */
 #define SCP3GPU_ESTIMATOR_GRADIENT 1 /* the default: Stein estimator from V and dV/dq
-                                        (ScaledMatrixElements.cpp:102-725, TripleExcitations.h); the
-                                        potential and its gradient in FP64 (qtip4pf.cpp:252-397,
-                                        ttm3f.cpp:325-720); its products W Phi^T in FP64
-                                        (SCP3GPU_PREC_FP64) or BF16x3 on tcgen05 (SCP3GPU_PREC_BF16X3,
-                                        _BF16X3_PES64); FP16 forms are SCP3GPU_ERR_UNSUPPORTED       */
+                                        (ScaledMatrixElements.cpp:102-725, TripleExcitations.h); its
+                                        products in FP64 (SCP3GPU_PREC_FP64) or BF16x3 on tcgen05
+                                        (SCP3GPU_PREC_BF16X3, _BF16X3_PES64); the potential and its
+                                        gradient (qtip4pf.cpp:252-397, ttm3f.cpp:325-720) in FP64, or
+                                        FP32 for qTIP4P/f with SCP3GPU_PREC_BF16X3; FP16 forms are
+                                        SCP3GPU_ERR_UNSUPPORTED                                      */
 
 /* Replaces ScaledMatrixElements(omega(modes), N2, N3) + M.zeros (SCP3.cpp:164-169). */
 int scp3gpu_hbuild_create(const scp3gpu_config* cfg, scp3gpu_hbuild** out);

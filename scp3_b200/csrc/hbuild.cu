@@ -543,11 +543,13 @@ int scp3gpu_hbuild_create(const scp3gpu_config* c, scp3gpu_hbuild** out)
     h->cfg.x0 = h->cfg.MUa = h->cfg.omega = nullptr;
     h->cfg.modes = nullptr;
     h->dev = c->device;
-    // The gradient estimator keeps its own pass structure in every form: the
-    // potential and its gradient in FP64, its products in FP64 or BF16x3 (stein.cu).
+    // The gradient estimator keeps its own pass structure in every form (stein.cu):
+    // its products in FP64 or BF16x3; the potential and its gradient in FP64, or in
+    // FP32 for qTIP4P/f with SCP3GPU_PREC_BF16X3.
     const bool gradient = c->estimator == SCP3GPU_ESTIMATOR_GRADIENT;
     h->split_form = c->precision != SCP3GPU_PREC_FP64 && !gradient;
-    h->pes_fp32 = !gradient && (c->precision == SCP3GPU_PREC_BF16X3 || c->precision == SCP3GPU_PREC_F16X3);
+    h->pes_fp32 = (c->precision == SCP3GPU_PREC_BF16X3 || c->precision == SCP3GPU_PREC_F16X3) &&
+                  (!gradient || c->pes == SCP3GPU_PES_QTIP4PF);
     const int nm0 = c->nmodes0, N3 = 9 * c->nw;
     h->nb = (int)scp3gpu_basis_size(c->nmodes, c->n2, c->n3);
     // HO diagonal of the selected modes and the inactive-mode zero point (SCP3.cpp:239)

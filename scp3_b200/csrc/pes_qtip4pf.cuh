@@ -112,11 +112,14 @@ __device__ double energy_warp(const T* crd, T* ms, int nw, const uint32_t* __res
 // ---------------------------------------------------------------- energy + gradient
 // qtip4pf.cpp:252-397 (the E+g operator of the gradient path): the same terms,
 // their derivatives in kcal/mol/A.  The M site is gammaM O + gamma1 (H1 + H2), so
-// the force on it is spread over the three atoms with those weights.  FP64.
+// the force on it is spread over the three atoms with those weights.  In the
+// precision T (FP64 for the parity form; FP32 for the split form's products),
+// each term's energy returned in FP64 and summed in FP64.
 
-__device__ __forceinline__ double monomer_grad(const double* w, double* g)
+template <typename T>
+__device__ __forceinline__ double monomer_grad(const T* w, T* g)
 {
-    double d1[3], d2[3], r1 = 0, r2 = 0, c = 0;
+    T d1[3], d2[3], r1 = 0, r2 = 0, c = 0;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         d1[k] = w[3 + k] - w[k];
@@ -127,80 +130,83 @@ __device__ __forceinline__ double monomer_grad(const double* w, double* g)
     }
     r1 = sqrt(r1);
     r2 = sqrt(r2);
-    const double x1 = kAlphaR * (r1 - kROHeq), x2 = kAlphaR * (r2 - kROHeq);
-    const double v1 = x1 * x1 * (1.0 - x1 * (1.0 - (7.0 / 12.0) * x1)) * kDR;
-    const double v2 = x2 * x2 * (1.0 - x2 * (1.0 - (7.0 / 12.0) * x2)) * kDR;
-    const double dv1 = kDR * kAlphaR * x1 * (2.0 - x1 * (3.0 - (7.0 / 3.0) * x1));   // dv/dr
-    const double dv2 = kDR * kAlphaR * x2 * (2.0 - x2 * (3.0 - (7.0 / 3.0) * x2));
-    const double cs = c / (r1 * r2);
-    const double dth = acos(cs) - kAHOHeqRad;
-    const double de_dc = -kKTheta * dth / sqrt(1.0 - cs * cs);                       // dE/dcos(theta)
+    const T x1 = T(kAlphaR) * (r1 - T(kROHeq)), x2 = T(kAlphaR) * (r2 - T(kROHeq));
+    const T v1 = x1 * x1 * (T(1.0) - x1 * (T(1.0) - T(7.0 / 12.0) * x1)) * T(kDR);
+    const T v2 = x2 * x2 * (T(1.0) - x2 * (T(1.0) - T(7.0 / 12.0) * x2)) * T(kDR);
+    const T dv1 = T(kDR) * T(kAlphaR) * x1 * (T(2.0) - x1 * (T(3.0) - T(7.0 / 3.0) * x1));   // dv/dr
+    const T dv2 = T(kDR) * T(kAlphaR) * x2 * (T(2.0) - x2 * (T(3.0) - T(7.0 / 3.0) * x2));
+    const T cs = c / (r1 * r2);
+    const T dth = acos(cs) - T(kAHOHeqRad);
+    const T de_dc = -T(kKTheta) * dth / sqrt(T(1.0) - cs * cs);                           // dE/dcos(theta)
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        const double u1 = d1[k] / r1, u2 = d2[k] / r2;
-        const double gh1 = dv1 * u1 + de_dc * (u2 - cs * u1) / r1;
-        const double gh2 = dv2 * u2 + de_dc * (u1 - cs * u2) / r2;
+        const T u1 = d1[k] / r1, u2 = d2[k] / r2;
+        const T gh1 = dv1 * u1 + de_dc * (u2 - cs * u1) / r1;
+        const T gh2 = dv2 * u2 + de_dc * (u1 - cs * u2) / r2;
         atomicAdd(g + 3 + k, gh1);
         atomicAdd(g + 6 + k, gh2);
         atomicAdd(g + k, -(gh1 + gh2));
     }
-    return v1 + v2 + 0.5 * kKTheta * dth * dth;
+    return (double)(v1 + v2 + T(0.5) * T(kKTheta) * dth * dth);
 }
 
 // q q' / |a - b|: energy; gradient into ga (at a) and gb (at b)
-__device__ __forceinline__ double coulomb_grad(double qq, const double* a, const double* b, double* ga, double* gb)
+template <typename T>
+__device__ __forceinline__ double coulomb_grad(double qq, const T* a, const T* b, T* ga, T* gb)
 {
-    const double d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
-    const double ir = 1.0 / sqrt(d0 * d0 + d1 * d1 + d2 * d2), e = qq * ir, f = -e * ir * ir;
+    const T d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
+    const T ir = T(1.0) / sqrt(d0 * d0 + d1 * d1 + d2 * d2), e = T(qq) * ir, f = -e * ir * ir;
     atomicAdd(ga + 0, f * d0), atomicAdd(ga + 1, f * d1), atomicAdd(ga + 2, f * d2);
     atomicAdd(gb + 0, -f * d0), atomicAdd(gb + 1, -f * d1), atomicAdd(gb + 2, -f * d2);
-    return e;
+    return (double)e;
 }
 
-__device__ __forceinline__ double pair_grad(uint32_t task, const double* crd, const double* ms, double* g, double* gm)
+template <typename T>
+__device__ __forceinline__ double pair_grad(uint32_t task, const T* crd, const T* ms, T* g, T* gm)
 {
     const uint32_t type = task & 3u, a = (task >> 2) & 0x7fffu, b = task >> 17;
     switch (type) {
-        case 0: return coulomb_grad(kQH * kQM, ms + 3 * a, crd + 3 * b, gm + 3 * a, g + 3 * b);
-        case 1: return coulomb_grad(kQH * kQH, crd + 3 * a, crd + 3 * b, g + 3 * a, g + 3 * b);
+        case 0: return coulomb_grad<T>(kQH * kQM, ms + 3 * a, crd + 3 * b, gm + 3 * a, g + 3 * b);
+        case 1: return coulomb_grad<T>(kQH * kQH, crd + 3 * a, crd + 3 * b, g + 3 * a, g + 3 * b);
         case 2: {
-            const double d0 = crd[3 * a] - crd[3 * b], d1 = crd[3 * a + 1] - crd[3 * b + 1];
-            const double d2 = crd[3 * a + 2] - crd[3 * b + 2];
-            const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
-            const double s2 = kSigma * kSigma / r2, s6 = s2 * s2 * s2;
-            const double f = 2.0 * 4 * kEpsilon * (3.0 * s6 - 6.0 * s6 * s6) / r2;   // 2 dE/d(r^2)
+            const T d0 = crd[3 * a] - crd[3 * b], d1 = crd[3 * a + 1] - crd[3 * b + 1];
+            const T d2 = crd[3 * a + 2] - crd[3 * b + 2];
+            const T r2 = d0 * d0 + d1 * d1 + d2 * d2;
+            const T s2 = T(kSigma * kSigma) / r2, s6 = s2 * s2 * s2;
+            const T f = T(2.0 * 4 * kEpsilon) * (T(3.0) * s6 - T(6.0) * s6 * s6) / r2;   // 2 dE/d(r^2)
             atomicAdd(g + 3 * a, f * d0), atomicAdd(g + 3 * a + 1, f * d1), atomicAdd(g + 3 * a + 2, f * d2);
             atomicAdd(g + 3 * b, -f * d0), atomicAdd(g + 3 * b + 1, -f * d1), atomicAdd(g + 3 * b + 2, -f * d2);
-            return 4 * kEpsilon * s6 * (s6 - 1.0);
+            return (double)(T(4 * kEpsilon) * s6 * (s6 - T(1.0)));
         }
-        default: return coulomb_grad(kQM * kQM, ms + 3 * a, ms + 3 * b, gm + 3 * a, gm + 3 * b);
+        default: return coulomb_grad<T>(kQM * kQM, ms + 3 * a, ms + 3 * b, gm + 3 * a, gm + 3 * b);
     }
 }
 
 // Energy (all lanes) and gradient g[9nw] (shared, complete after the call) of
 // the geometry crd; ms[3nw] and gm[3nw] are shared scratch (M sites, their forces).
-__device__ inline double energy_grad_warp(const double* crd, double* ms, double* g, double* gm, int nw,
-                                   const uint32_t* __restrict__ tasks, int ntasks, int lane)
+template <typename T>
+__device__ inline double energy_grad_warp(const T* crd, T* ms, T* g, T* gm, int nw,
+                                          const uint32_t* __restrict__ tasks, int ntasks, int lane)
 {
-    for (int c = lane; c < 9 * nw; c += 32) g[c] = 0.0;
-    for (int c = lane; c < 3 * nw; c += 32) gm[c] = 0.0;
+    for (int c = lane; c < 9 * nw; c += 32) g[c] = T(0);
+    for (int c = lane; c < 3 * nw; c += 32) gm[c] = T(0);
     for (int i = lane; i < nw; i += 32) {
-        const double* w = crd + 9 * i;
+        const T* w = crd + 9 * i;
 #pragma unroll
-        for (int k = 0; k < 3; k++) ms[3 * i + k] = kGammaM * w[k] + kGamma1 * (w[3 + k] + w[6 + k]);
+        for (int k = 0; k < 3; k++) ms[3 * i + k] = T(kGammaM) * w[k] + T(kGamma1) * (w[3 + k] + w[6 + k]);
     }
     __syncwarp();
     double part = 0;
-    for (int i = lane; i < nw; i += 32) part += monomer_grad(crd + 9 * i, g + 9 * i);
-    for (int t = lane; t < ntasks; t += 32) part += pair_grad(__ldg(tasks + t), crd, ms, g, gm);
+    for (int i = lane; i < nw; i += 32) part += monomer_grad<T>(crd + 9 * i, g + 9 * i);
+    for (int t = lane; t < ntasks; t += 32) part += pair_grad<T>(__ldg(tasks + t), crd, ms, g, gm);
     __syncwarp();
     for (int i = lane; i < nw; i += 32)
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            const double f = gm[3 * i + k];
-            g[9 * i + k] += kGammaM * f;
-            g[9 * i + 3 + k] += kGamma1 * f;
-            g[9 * i + 6 + k] += kGamma1 * f;
+            const T f = gm[3 * i + k];
+            g[9 * i + k] += T(kGammaM) * f;
+            g[9 * i + 3 + k] += T(kGamma1) * f;
+            g[9 * i + 6 + k] += T(kGamma1) * f;
         }
     __syncwarp();
     return warp_sum(part);

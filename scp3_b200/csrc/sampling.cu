@@ -116,14 +116,20 @@ struct Pair<float> {
     using type = float2;
 };
 
-template <int PES, typename T>
+// G: the gradient path (dV/dq) is compiled in; the energy-only instances keep
+// their registers for the energy path.
+template <int PES, typename T, bool G = false>
 __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem);
 
-template <int PES, typename T>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_kernel(SampleArgs a)
+template <int PES, typename T, bool G>
+// Blocks per SM the registers must allow: 4 for the FP32 energy path (64
+// registers), 3 for the FP32 gradient path (85: a few spills, 1.3x faster than
+// at 2), 2 for FP64.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, sizeof(T) == 4 ? (G ? 3 : 4) : 2)
+    samples_kernel(SampleArgs a)
 {
     extern __shared__ __align__(16) char smem[];
-    samples_body<PES, T>(a, smem);
+    samples_body<PES, T, G>(a, smem);
 }
 
 // Several clusters of a batch: cluster blockIdx.y takes args[blockIdx.y].
@@ -139,7 +145,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) samples_batch_kernel(cons
     samples_body<PES, T>(a, smem);
 }
 
-template <int PES, typename T>
+template <int PES, typename T, bool G>
 __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
 {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -160,7 +166,7 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
         }
         __syncthreads();
     }
-    const bool grad = a.vq != nullptr;
+    const bool grad = G && a.vq != nullptr;
     const bool muat_in_smem = grad && muat_smem_bytes(nw, a.nm) <= kMuaTSmemMax;
     double* muat = reinterpret_cast<double*>(smem + (mua_in_smem ? mua_b : 0));   // [N3][nm]
     if (muat_in_smem) {
@@ -395,6 +401,28 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
                         a.vq[s * a.nm + m] = acc * (kBohr / kAuToKcalPerMol) - __ldg(a.omega + k) * (double)q[k];
                     }
                 }
+            } else if constexpr (PES == SCP3GPU_PES_QTIP4PF) {
+                if (grad) {
+                    // the same in FP32 (the split form's products): the gradient in FP32
+                    // shared memory (the slot's FP64 gradient storage holds it), the energy
+                    // terms and the projection onto the modes summed in FP64
+                    float* gf = reinterpret_cast<float*>(w.g);
+                    float* gmf = gf + 9 * nw;
+                    const double e = qt::energy_grad_warp<float>(crd, w.ms, gf, gmf, nw, a.tasks, a.ntasks, lane);
+                    double h = 0.0;
+                    for (int d = lane; d < nm0; d += 32) h += (double)q[d] * (__ldg(a.omega + d) * (double)q[d]);
+                    h = warp_sum(h);
+                    V = e / kAuToKcalPerMol - 0.5 * h;
+                    for (int m = lane; m < a.nm; m += 32) {
+                        const int k = __ldg(a.modes + m);
+                        double acc = 0.0;
+                        if (muat_in_smem)
+                            for (int c = 0; c < N3; c++) acc += muat[(size_t)c * a.nm + m] * (double)gf[c];
+                        else
+                            for (int c = 0; c < N3; c++) acc += MUa[(size_t)k * N3 + c] * (double)gf[c];
+                        a.vq[s * a.nm + m] = acc * (kBohr / kAuToKcalPerMol) - __ldg(a.omega + k) * (double)q[k];
+                    }
+                }
             }
             if (!a.skip_pes && !grad) {
                 const double e = PES == SCP3GPU_PES_QTIP4PF ? e4j
@@ -588,9 +616,9 @@ int launch_samples_t(const SampleArgs& a, cudaStream_t s)
     const size_t muat_b = muat_smem_bytes(a.nw, a.nm);
     const size_t sm = kWarpsPerBlock * slot_bytes<T>(PES, a.nm0, a.nw, a.vq != nullptr, kGroup) +
                       (mua_b <= kMuaSmemMax ? mua_b : 0) + (a.vq && muat_b <= kMuaTSmemMax ? muat_b : 0);
-    if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(samples_kernel<PES, T>,
-                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    samples_kernel<PES, T><<<sample_grid(samples_kernel<PES, T>, sm, a.n), kWarpsPerBlock * 32, sm, s>>>(a);
+    auto kern = a.vq ? samples_kernel<PES, T, true> : samples_kernel<PES, T, false>;
+    if (sm > 48 * 1024) SCP3_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<sample_grid(kern, sm, a.n), kWarpsPerBlock * 32, sm, s>>>(a);
     SCP3_CUDA(cudaGetLastError());
     return SCP3GPU_OK;
 }
@@ -670,7 +698,8 @@ int ttm_init_device()
 int launch_samples(int pes, bool fp32, const SampleArgs& a, cudaStream_t s)
 {
     if (a.n <= 0) return SCP3GPU_OK;
-    if (a.vq && fp32) return fail(SCP3GPU_ERR_UNSUPPORTED, "gradient path: FP64 potential only");
+    if (a.vq && fp32 && pes != SCP3GPU_PES_QTIP4PF)
+        return fail(SCP3GPU_ERR_UNSUPPORTED, "gradient path: FP32 potential for qTIP4P/f only");
     if (pes == SCP3GPU_PES_QTIP4PF)
         return fp32 ? launch_samples_t<SCP3GPU_PES_QTIP4PF, float>(a, s)
                     : launch_samples_t<SCP3GPU_PES_QTIP4PF, double>(a, s);
