@@ -868,6 +868,29 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
             }
             return true;
         };
+        // The products of the W_b blocks pay whole tiles for the few columns each
+        // needs: worth it while they add no more tiles than the direct terms have
+        // (hexamer doubles basis: 19 against 95); otherwise (triples bases, where
+        // each block reaches Phi pairs all over the basis) the pair sums stay FP64.
+        if (p.tcpairs) {
+            int64_t est = 0;
+            for (int m = 0; m < nm; m++)
+                for (int b = 1; b <= 3; b++) {
+                    if (!((levmask[m] >> b) & 1) || reduces_to_ground(m, b)) continue;
+                    std::vector<char> pairs((size_t)p.bpairs, 0);
+                    for (size_t r = 0; r < E[m].size(); r++) {
+                        if (lev[m][r] != b) continue;
+                        int mm[3], ll[3];
+                        const int k = decode(desc[E[m][r]], mm, ll);
+                        for (int a = 0; a < k; a++)
+                            if (mm[a] == m) pairs[red3[(size_t)3 * E[m][r] + a] / 256] = 1;
+                    }
+                    int np = 0;
+                    for (char c : pairs) np += c;
+                    est += (int64_t)np * (int64_t)E[m].size();     // tile rows: 128 per tile
+                }
+            if (est > (int64_t)128 * p.rt * p.bpairs) p.tcpairs = false;
+        }
         int nwb = 0;
         p.nsum = 0;
         if (p.tcpairs)
