@@ -699,6 +699,40 @@ int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 
 }  // namespace
 
+// red3[3 j + a]: the basis index of function j without its a-th factor (decode
+// order), -1 where that function is not in the basis; *closed: none is missing.
+std::vector<int> reduced_functions(const std::vector<uint32_t>& desc, bool* closed)
+{
+    const int nb = (int)desc.size();
+    std::map<std::array<int, 6>, int> index_of;     // sorted (mode, level) factors -> basis index
+    auto key_of = [](const int* mm, const int* ll, int k, int skip) {
+        std::array<int, 6> key{-1, -1, -1, -1, -1, -1};
+        std::vector<std::pair<int, int>> f;
+        for (int a = 0; a < k; a++)
+            if (a != skip) f.push_back({mm[a], ll[a]});
+        std::sort(f.begin(), f.end());
+        for (size_t u = 0; u < f.size(); u++) key[2 * u] = f[u].first, key[2 * u + 1] = f[u].second;
+        return key;
+    };
+    for (int j = 0; j < nb; j++) {
+        int mm[3], ll[3];
+        const int k = decode(desc[j], mm, ll);
+        index_of[key_of(mm, ll, k, -1)] = j;
+    }
+    std::vector<int> red3((size_t)nb * 3, -1);
+    *closed = true;
+    for (int j = 0; j < nb; j++) {
+        int mm[3], ll[3];
+        const int k = decode(desc[j], mm, ll);
+        for (int a = 0; a < k; a++) {
+            const auto it = index_of.find(key_of(mm, ll, k, a));
+            if (it == index_of.end()) *closed = false;
+            else red3[(size_t)3 * j + a] = it->second;
+        }
+    }
+    return red3;
+}
+
 int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_t chunk_cfg, int sms, bool split)
 {
     p = SteinPlan{};
@@ -822,32 +856,8 @@ int stein_create(SteinPlan& p, const std::vector<uint32_t>& desc, int nm, int64_
         // is, without its mode-m factor, again a basis function (red3) and the
         // expansion's table holds the weights of the level pairs present:
         // T^m_ij = sum_s [R_i^m K^m_{a_i b_j}] Phi_{red(j, m)}.
-        std::map<std::array<int, 6>, int> index_of;     // sorted (mode, level) factors -> basis index
-        auto key_of = [](const int* mm, const int* ll, int k, int skip) {
-            std::array<int, 6> key{-1, -1, -1, -1, -1, -1};
-            std::vector<std::pair<int, int>> f;
-            for (int a = 0; a < k; a++)
-                if (a != skip) f.push_back({mm[a], ll[a]});
-            std::sort(f.begin(), f.end());
-            for (size_t u = 0; u < f.size(); u++) key[2 * u] = f[u].first, key[2 * u + 1] = f[u].second;
-            return key;
-        };
-        for (int j = 0; j < p.nb; j++) {
-            int mm[3], ll[3];
-            const int k = decode(desc[j], mm, ll);
-            index_of[key_of(mm, ll, k, -1)] = j;
-        }
-        std::vector<int> red3((size_t)p.nb * 3, -1);
         bool closed = true;
-        for (int j = 0; j < p.nb; j++) {
-            int mm[3], ll[3];
-            const int k = decode(desc[j], mm, ll);
-            for (int a = 0; a < k; a++) {
-                const auto it = index_of.find(key_of(mm, ll, k, a));
-                if (it == index_of.end()) closed = false;
-                else red3[(size_t)3 * j + a] = it->second;
-            }
-        }
+        const std::vector<int> red3 = reduced_functions(desc, &closed);
         std::vector<int> levmask(nm, 0);
         for (int m = 0; m < nm; m++)
             for (int l : lev[m]) levmask[m] |= 1 << l;
@@ -1161,3 +1171,16 @@ int stein_unpack(const SteinPlan& p, const uint32_t* desc, double divisor, const
 }
 
 }  // namespace scp3
+
+// Host-only view of the split gradient estimator's reduced functions, for tests:
+// red3 (nb * 3 ints, may be null) as reduced_functions gives it for the basis of
+// (nmodes, n2, n3); returns 1 when the basis is closed under removing a factor,
+// 0 when it is not, negative on bad arguments.
+extern "C" int scp3gpu_internal_reduced(int nmodes, int n2, int n3, int* red3)
+{
+    if (scp3gpu_basis_size(nmodes, n2, n3) < 0) return -1;
+    bool closed = true;
+    const std::vector<int> r = scp3::reduced_functions(scp3::basis_descriptors(nmodes, n2, n3), &closed);
+    if (red3) std::copy(r.begin(), r.end(), red3);
+    return closed ? 1 : 0;
+}
