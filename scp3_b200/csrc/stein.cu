@@ -638,18 +638,28 @@ __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int
     if (e >= (int64_t)nb * nb) return;
     const int j = (int)(e / nb), i = (int)(e - (int64_t)j * nb);
     const int r = min(i, j), c = max(i, j);
+    // a term whose tile the plan did not make reads NaN into the element (never,
+    // by construction; a visible result rather than an out-of-range read)
     auto cidx = [&](int vr, int col) -> int64_t {
-        if (N256)
-            return (int64_t)tile_of[(vr >> 7) * ct + (col >> 8)] * (128 * 256) +
-                   (int64_t)(((col >> 7) & 1) * 128 + (col & 127)) * 128 + (vr & 127);
+        if (N256) {
+            const int t = tile_of[(vr >> 7) * ct + (col >> 8)];
+            if (t < 0) return -1;
+            return (int64_t)t * (128 * 256) + (int64_t)(((col >> 7) & 1) * 128 + (col & 127)) * 128 + (vr & 127);
+        }
         return ((int64_t)(vr >> 7) * ct + (col >> 7)) * (128 * 128) + (int64_t)(vr & 127) * 128 + (col & 127);
+    };
+    auto csum = [&](int64_t x) {
+        if (x < 0) return __longlong_as_double(0x7ff8000000000000ll);
+        double t = 0.0;
+        for (int s = 0; s < nsplit; s++) t += C[s * csize + x];
+        return t;
     };
     int mr[3], lr[3], mc[3], lc[3];
     const int nr = decode(desc[r], mr, lr), ncn = decode(desc[c], mc, lc);
     double val = 0.0;
     if (nr + ncn == 0) {   // <0|V|0>
         const int64_t x = cidx(nv - 1, 0);
-        for (int s = 0; s < nsplit; s++) val += C[s * csize + x];
+        val += csum(x);
     } else {
         int ns = 0;
         for (int a = 0; a < nr; a++) {
@@ -660,14 +670,14 @@ __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int
             double t = 0.0;
             if (b < 0) {
                 const int64_t x = cidx(voff[m] + rank3[3 * r + a], c);
-                for (int s = 0; s < nsplit; s++) t += C[s * csize + x];
+                t += csum(x);
             } else if (sum_off && sum_off[m * 4 + lc[b]] >= 0) {
                 // summed row (m, rank of r, level of c in m): c without m is the constant
                 t = sums[sum_off[m * 4 + lc[b]] + rank3[3 * r + a]];
             } else if (wb_off) {
                 // W_b row (m, rank of r, level of c in m) against Phi of c without m
                 const int64_t x = cidx(wb_off[m * 4 + lc[b]] + rank3[3 * r + a], red3[3 * c + b]);
-                for (int s = 0; s < nsplit; s++) t += C[s * csize + x];
+                t += csum(x);
             } else {
                 // D holds the upper triangle of ranks (functions ordered by level in m)
                 const int en = voff[m + 1] - voff[m];
@@ -684,7 +694,7 @@ __global__ void stein_unpack_kernel(const uint32_t* __restrict__ desc, const int
             if (shared) continue;
             const int64_t x = cidx(voff[mc[b]] + rank3[3 * c + b], r);
             double t = 0.0;
-            for (int s = 0; s < nsplit; s++) t += C[s * csize + x];
+            t += csum(x);
             val += t;
             ns++;
         }
