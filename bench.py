@@ -637,6 +637,20 @@ def gradient_form(prec, nw, x0, MUa, omega, n, steps, warmup):
             "status": {"rc": rc, "nonfinite": nonfinite, "not_converged": notconv}, "levels": levels}
 
 
+def gradient_record(nw, x0, MUa, omega, n, steps):
+    """The gradient (Stein) estimator on the hexamer doubles basis: the BF16x3 form
+    against the FP64 form on the same points (samples/s, ratio, level error)."""
+    split = gradient_form("bf16x3", nw, x0, MUa, omega, n, steps, 1)
+    ref = gradient_form("fp64", nw, x0, MUa, omega, n, steps, 1)
+    return {"workload": "hexamer prism qTIP4P/f, doubles basis Nb=%d, %d scrambled Sobol points per step, Stein "
+                        "estimator (SCP3's default path)" % (split["nb"], n),
+            "bf16x3": {"value": split["value"], "unit": "samples/s", "kernel_ms": split["kernel_ms"]},
+            "fp64": {"value": ref["value"], "unit": "samples/s", "kernel_ms": ref["kernel_ms"]},
+            "speedup_vs_fp64": split["value"] / ref["value"],
+            "max_abs_err_cm1_vs_fp64": float(np.abs(split["levels"] - ref["levels"]).max()),
+            "status": split["status"]}
+
+
 def run_gradient(args):
     """The reference's default estimator (no -G): the Stein estimator of every
     upper element from V and dV/dq (ScaledMatrixElements.cpp:102-725,
@@ -951,6 +965,8 @@ def main():
         bt = guarded(batch_record, args.precision, 1 << 18, 3, 1)
         line["batch"] = bt if "error" in bt else {k: v for k, v in bt.items() if k != "clusters"}
         line["cv"] = guarded(cv_record, args.precision, 100)
+        # the reference's default estimator (no -G) in compact form (full line: --config gradient)
+        line["gradient"] = guarded(gradient_record, nw, x0, MUa, omega, 1 << 18, 3)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         normals = scp3_b200.std_normals(nm0, 0, 1 << 17, scramble_seed=SCRAMBLE_SEED)
         line["cpu_baseline"] = cpu_reference(nw, x0, MUa, omega, np.arange(nm0, dtype=np.int32), 48, 0, normals)
