@@ -240,8 +240,8 @@ __device__ __forceinline__ int sx_col(int r, int l)
 // its kind is uniform.  Every operand row is the product of three table entries
 // (xdesc: three 10-bit indices, 0 = the constant 1).  The values are rounded to
 // FP32 before the BF16 split in any case.  CTA: one 32-slot block x `per` rows;
-// thread (g, r) writes slots 8g..8g+7 of rows r, r + 64, ...: one 16-byte chunk of
-// the hi box and one of the lo box each.
+// thread (g, r) writes slots 8g..8g+7 of rows 4r..4r+3, 4r+256..4r+259, ...: one
+// 16-byte chunk of the hi box and one of the lo box each.
 __global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
     const uint32_t* __restrict__ tspec, int trows, const uint32_t* __restrict__ xdesc, int rows, int nsum, int per,
     int nm, const double* __restrict__ q, const double* __restrict__ v, const double* __restrict__ vq, int64_t n,
@@ -297,16 +297,26 @@ __global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
         hi4 = tab4[i * (kSxSlots / 4) + (sw ^ 4u) + g];
     };
     const int r0 = blockIdx.y * per, r1 = min(rows + nsum, r0 + per);
-    for (int rb = r0; rb < r1; rb += kSxThreads / 4) {
-        const int row = rb + rl;
-        const uint32_t d = row < r1 ? __ldg(xdesc + row) : kSxZeroRow;
-        if (row >= rows && row < r1) {
-            // a summed row: its 32 values added, in FP32, into this block's partial
-            float x = 0.0f;
-            if (d != kSxZeroRow) {
+    // four consecutive rows per thread: consecutive rows mostly share their first
+    // factor (the weight K^m of one mode and level, or the first Hermite factor of
+    // a pair), read once
+    for (int rb = r0 + 4 * rl; rb < r1; rb += kSxThreads) {
+        uint32_t pia = 0xffffffffu;
+        float4 f0 = make_float4(0.f, 0.f, 0.f, 0.f), f1 = f0;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int row = rb + u;
+            if (row >= r1) break;
+            const uint32_t d = __ldg(xdesc + row);
+            const bool has = d != kSxZeroRow;
+            float4 a0 = f0, a1 = f1;
+            if (has) {
                 const uint32_t ia = d & 1023u, ib = (d >> 10) & 1023u, ic = d >> 20;
-                float4 a0, a1;
-                rd(ia, a0, a1);
+                if (ia != pia) {
+                    rd(ia, f0, f1);
+                    pia = ia;
+                }
+                a0 = f0, a1 = f1;
                 if (ib) {
                     float4 b0, b1;
                     rd(ib, b0, b1);
@@ -319,40 +329,28 @@ __global__ void __launch_bounds__(kSxThreads) stein_expand_split_kernel(
                     a0.x *= c0.x, a0.y *= c0.y, a0.z *= c0.z, a0.w *= c0.w;
                     a1.x *= c1.x, a1.y *= c1.y, a1.z *= c1.z, a1.w *= c1.w;
                 }
-                x = ((a0.x + a0.y) + (a0.z + a0.w)) + ((a1.x + a1.y) + (a1.z + a1.w));
             }
-            const unsigned grp = 0xfu << (threadIdx.x & 28);     // the 4 lanes of this row
-            x += __shfl_xor_sync(grp, x, 1);
-            x += __shfl_xor_sync(grp, x, 2);
-            if (g == 0) spart[(size_t)kb * nsum + (row - rows)] = x;
-            continue;
+            if (row >= rows) {
+                // a summed row: its 32 values added, in FP32, into this block's partial
+                float x = has ? ((a0.x + a0.y) + (a0.z + a0.w)) + ((a1.x + a1.y) + (a1.z + a1.w)) : 0.0f;
+                const unsigned grp = 0xfu << (threadIdx.x & 28);     // the 4 lanes of this row
+                x += __shfl_xor_sync(grp, x, 1);
+                x += __shfl_xor_sync(grp, x, 2);
+                if (g == 0) spart[(size_t)kb * nsum + (row - rows)] = x;
+                continue;
+            }
+            if (!has) continue;
+            uint4 hi, lo;
+            split_bf16x2(a0.x, a0.y, hi.x, lo.x);
+            split_bf16x2(a0.z, a0.w, hi.y, lo.y);
+            split_bf16x2(a1.x, a1.y, hi.z, lo.z);
+            split_bf16x2(a1.z, a1.w, hi.w, lo.w);
+            const int rin = row & (tc::kTile - 1);
+            uint16_t* box = xop + ((size_t)(row / tc::kTile) * nkb_alloc + box_k) * (2 * tc::kTile * tc::kKBlock2);
+            const int off = rin * tc::kKBlock2 + ((g ^ ((rin >> 1) & 3)) << 3);
+            *reinterpret_cast<uint4*>(box + off) = hi;
+            *reinterpret_cast<uint4*>(box + tc::kTile * tc::kKBlock2 + off) = lo;
         }
-        if (row >= r1 || d == kSxZeroRow) continue;
-        const uint32_t ia = d & 1023u, ib = (d >> 10) & 1023u, ic = d >> 20;
-        float4 a0, a1;
-        rd(ia, a0, a1);
-        if (ib) {
-            float4 b0, b1;
-            rd(ib, b0, b1);
-            a0.x *= b0.x, a0.y *= b0.y, a0.z *= b0.z, a0.w *= b0.w;
-            a1.x *= b1.x, a1.y *= b1.y, a1.z *= b1.z, a1.w *= b1.w;
-        }
-        if (ic) {
-            float4 c0, c1;
-            rd(ic, c0, c1);
-            a0.x *= c0.x, a0.y *= c0.y, a0.z *= c0.z, a0.w *= c0.w;
-            a1.x *= c1.x, a1.y *= c1.y, a1.z *= c1.z, a1.w *= c1.w;
-        }
-        uint4 hi, lo;
-        split_bf16x2(a0.x, a0.y, hi.x, lo.x);
-        split_bf16x2(a0.z, a0.w, hi.y, lo.y);
-        split_bf16x2(a1.x, a1.y, hi.z, lo.z);
-        split_bf16x2(a1.z, a1.w, hi.w, lo.w);
-        const int rin = row & (tc::kTile - 1);
-        uint16_t* box = xop + ((size_t)(row / tc::kTile) * nkb_alloc + box_k) * (2 * tc::kTile * tc::kKBlock2);
-        const int off = rin * tc::kKBlock2 + ((g ^ ((rin >> 1) & 3)) << 3);
-        *reinterpret_cast<uint4*>(box + off) = hi;
-        *reinterpret_cast<uint4*>(box + tc::kTile * tc::kKBlock2 + off) = lo;
     }
 }
 
