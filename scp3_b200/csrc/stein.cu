@@ -1101,9 +1101,12 @@ int stein_pass(const SteinPlan& p, const uint32_t* desc, const double* q, const 
         const int nflush = (int)(k / tc::kFlush);
         const int rows = p.nv_pad + p.nwb_pad + p.nb_pad;
         const size_t es = sizeof(float) * ((size_t)p.trows * kSxSlots + 2 * (size_t)p.nm * kSxLd + kSxSlots);
-        // rows in chunks of at most 4096 per CTA (whole 64-row trips)
+        // rows in chunks of at most 16384 per CTA: each chunk builds the block's table
+        // again, and the table build is a third of a 2816-row chunk's time (measured:
+        // 8496 rows in one chunk instead of three took the split pass from 31.2 to
+        // 32.8 M samples/s)
         const int vrows = rows + p.nsum;   // operand rows, then summed rows
-        const int ny = (vrows + 4095) / 4096, per = (int)round_up((vrows + ny - 1) / ny, 64);
+        const int ny = (vrows + 16383) / 16384, per = (int)round_up((vrows + ny - 1) / ny, 64);
         dim3 eg((unsigned)(nflush * kSxBlocksPerFlush), (unsigned)ny);
         stein_expand_split_kernel<<<eg, kSxThreads, es, s>>>(p.tspec, p.trows, p.xdesc, rows, p.nsum, per, p.nm, q,
                                                              v, vq, k, p.slots / tc::kKBlock2, p.xop, p.spart);
