@@ -212,5 +212,50 @@ __device__ inline double energy_grad_warp(const T* crd, T* ms, T* g, T* gm, int 
     return warp_sum(part);
 }
 
+// Energies and gradients of ng <= 4 geometries crd + j * stride at once (the
+// FP32 gradient path): lane l works for geometry l % 4 only, as energy_warp4;
+// ms [4][3nw], g [4][9nw] and gm [4][3nw] are shared scratch, g complete after
+// the call; lane l returns the energy of geometry l % 4.
+template <typename T>
+__device__ double energy_grad_warp4(const T* crd, int stride, T* ms, T* g, T* gm, int nw, int ng,
+                                    const uint32_t* __restrict__ tasks, int ntasks, int lane)
+{
+    const int j = lane & 3;
+    const bool on = j < ng;
+    const T* cj = crd + j * stride;
+    T* mj = ms + j * 3 * nw;
+    T* gj = g + j * 9 * nw;
+    T* gmj = gm + j * 3 * nw;
+    for (int c = lane; c < 4 * 9 * nw; c += 32) g[c] = T(0);
+    for (int c = lane; c < 4 * 3 * nw; c += 32) gm[c] = T(0);
+    if (on)
+        for (int i = lane >> 2; i < nw; i += 8) {
+            const T* w = cj + 9 * i;
+#pragma unroll
+            for (int k = 0; k < 3; k++) mj[3 * i + k] = T(kGammaM) * w[k] + T(kGamma1) * (w[3 + k] + w[6 + k]);
+        }
+    __syncwarp();
+    double part = 0;
+    if (on) {
+        for (int i = lane >> 2; i < nw; i += 8) part += monomer_grad<T>(cj + 9 * i, gj + 9 * i);
+        for (int t = lane >> 2; t < ntasks; t += 8) part += pair_grad<T>(__ldg(tasks + t), cj, mj, gj, gmj);
+    }
+    __syncwarp();
+    if (on)
+        for (int i = lane >> 2; i < nw; i += 8)
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const T f = gmj[3 * i + k];
+                gj[9 * i + k] += T(kGammaM) * f;
+                gj[9 * i + 3 + k] += T(kGamma1) * f;
+                gj[9 * i + 6 + k] += T(kGamma1) * f;
+            }
+    __syncwarp();
+    part += __shfl_xor_sync(0xffffffffu, part, 4);
+    part += __shfl_xor_sync(0xffffffffu, part, 8);
+    part += __shfl_xor_sync(0xffffffffu, part, 16);
+    return part;
+}
+
 }  // namespace qt
 }  // namespace scp3

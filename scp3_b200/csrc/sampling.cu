@@ -40,13 +40,21 @@ struct WarpSlot {
     int qs;         // q stride: nm0 rounded up to even (16-byte aligned rows)
 };
 
+// Gradient storage of a warp slot: [9nw] + [3nw] in FP64, or in the FP32 form
+// the four geometries' [4][9nw] + [4][3nw].
+template <typename T>
+__host__ __device__ inline size_t grad_bytes(int nw, int group)
+{
+    return sizeof(T) == 4 ? sizeof(float) * (size_t)(12 * nw * group) : sizeof(double) * (size_t)(12 * nw);
+}
+
 template <typename T>
 __host__ __device__ inline size_t slot_bytes(int pes, int nm0, int nw, bool grad = false, int group = 1)
 {
     size_t b = sizeof(T) * ((size_t)group * ((nm0 + 1) & ~1) + (size_t)(12 * nw * group));
     if (pes == SCP3GPU_PES_TTM3F) b += sizeof(T) * ttm::scratch_elems(nw, grad);
     b = (b + 7) & ~(size_t)7;
-    if (grad) b += sizeof(double) * (size_t)(12 * nw);
+    if (grad) b += grad_bytes<T>(nw, group);
     if (sizeof(T) == 4) b += (size_t)group * nm0 * (sizeof(uint64_t) + sizeof(uint16_t));
     return (b + 15) & ~(size_t)15;
 }
@@ -65,7 +73,7 @@ __device__ inline WarpSlot<T> warp_slot(char* base, int pes, int nm0, int nw, bo
     off = (off + 7) & ~(size_t)7;
     s.g = grad ? reinterpret_cast<double*>(base + off) : nullptr;
     s.gm = grad ? s.g + 9 * nw : nullptr;
-    if (grad) off += sizeof(double) * (size_t)(12 * nw);
+    if (grad) off += grad_bytes<T>(nw, group);
     s.xs = sizeof(T) == 4 ? reinterpret_cast<uint64_t*>(base + off) : nullptr;
     s.tl = sizeof(T) == 4 ? reinterpret_cast<uint16_t*>(base + off + sizeof(uint64_t) * (size_t)group * nm0) : nullptr;
     return s;
@@ -357,6 +365,29 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
         if constexpr (PES == SCP3GPU_PES_QTIP4PF) {
             if (!a.skip_pes && !grad) e4 = qt::energy_warp4<T>(w.crd, N3, w.ms, nw, gn, a.tasks, a.ntasks, lane);
         }
+        if constexpr (PES == SCP3GPU_PES_QTIP4PF && sizeof(T) == 4) {
+            if (grad) {
+                // FP32 gradient path (the split form's products): energies and
+                // gradients of the group in one warp pass, then dV_anh/dq of the
+                // group's (sample, mode) items over the lanes, summed in FP64
+                T* g4 = reinterpret_cast<T*>(w.g);
+                T* gm4 = g4 + 4 * 9 * nw;
+                e4 = qt::energy_grad_warp4<T>(w.crd, N3, w.ms, g4, gm4, nw, gn, a.tasks, a.ntasks, lane);
+                for (int it = lane; it < gn * a.nm; it += 32) {
+                    const int j = it / a.nm, m = it - j * a.nm;
+                    const int k = __ldg(a.modes + m);
+                    const T* gj = g4 + j * 9 * nw;
+                    double acc = 0.0;
+                    if (muat_in_smem)
+                        for (int c = 0; c < N3; c++) acc += muat[(size_t)c * a.nm + m] * (double)gj[c];
+                    else
+                        for (int c = 0; c < N3; c++) acc += MUa[(size_t)k * N3 + c] * (double)gj[c];
+                    a.vq[(s0 + j) * a.nm + m] =
+                        acc * (kBohr / kAuToKcalPerMol) - __ldg(a.omega + k) * (double)w.q[j * w.qs + k];
+                }
+                __syncwarp();
+            }
+        }
         for (int j = 0; j < gn; j++) {
             const int64_t s = s0 + j;
             const T* q = w.q + j * w.qs;
@@ -403,25 +434,12 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
                 }
             } else if constexpr (PES == SCP3GPU_PES_QTIP4PF) {
                 if (grad) {
-                    // the same in FP32 (the split form's products): the gradient in FP32
-                    // shared memory (the slot's FP64 gradient storage holds it), the energy
-                    // terms and the projection onto the modes summed in FP64
-                    float* gf = reinterpret_cast<float*>(w.g);
-                    float* gmf = gf + 9 * nw;
-                    const double e = qt::energy_grad_warp<float>(crd, w.ms, gf, gmf, nw, a.tasks, a.ntasks, lane);
+                    // the FP32 form: the group's energies and dV/dq came from the
+                    // group pass above
                     double h = 0.0;
                     for (int d = lane; d < nm0; d += 32) h += (double)q[d] * (__ldg(a.omega + d) * (double)q[d]);
                     h = warp_sum(h);
-                    V = e / kAuToKcalPerMol - 0.5 * h;
-                    for (int m = lane; m < a.nm; m += 32) {
-                        const int k = __ldg(a.modes + m);
-                        double acc = 0.0;
-                        if (muat_in_smem)
-                            for (int c = 0; c < N3; c++) acc += muat[(size_t)c * a.nm + m] * (double)gf[c];
-                        else
-                            for (int c = 0; c < N3; c++) acc += MUa[(size_t)k * N3 + c] * (double)gf[c];
-                        a.vq[s * a.nm + m] = acc * (kBohr / kAuToKcalPerMol) - __ldg(a.omega + k) * (double)q[k];
-                    }
+                    V = e4j / kAuToKcalPerMol - 0.5 * h;
                 }
             }
             if (!a.skip_pes && !grad) {
