@@ -70,3 +70,26 @@ def test_cli_readout_loop_matches_reference(tmp_path):
     assert np.all(np.tril(D, -1) == 0.0)                           # upper triangle, as the reference's file
     ulp = np.abs(np.spacing(Mout.astype(np.float32))).astype(np.float64)
     assert np.all(np.abs(D - ref32) <= ulp), np.abs(D - ref32).max()
+
+
+def test_cli_default_estimator_split_form_matches_fp64(tmp_path):
+    """scp3 without -G runs the reference's default (gradient) estimator; with
+    --precision bf16x3 its products run on the tensor cores.  Its periodic
+    readout (E0_sd.dat, SCP3.cpp:234-250) matches the FP64 form's on the same
+    points within 0.1 cm^-1."""
+    import torch
+    assert torch.cuda.is_available()
+    inp = os.path.join(ROOT, "scp3_b200", "data", "prism_qtip4pf.dat")
+    rows = {}
+    for prec in ("fp64", "bf16x3"):
+        d = tmp_path / prec
+        d.mkdir()
+        r = subprocess.run([CLI, "-N", "15", "-m", "0-7", "-2", "6", "-3", "3", "--precision", prec, inp],
+                           cwd=d, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+        rows[prec] = np.loadtxt(d / "E0_sd.dat")
+    assert rows["fp64"].shape == (2, 4)
+    assert np.array_equal(rows["fp64"][:, 0], rows["bf16x3"][:, 0])
+    err = np.abs(rows["fp64"][:, 1:3] - rows["bf16x3"][:, 1:3]).max()
+    print("\nCLI gradient estimator, bf16x3 vs fp64 E0_sd levels: max %.4f cm^-1" % err)
+    assert err <= 0.1, err
