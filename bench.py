@@ -203,7 +203,31 @@ def cpu_reference(nw, x0, MUa, omega, modes, n2, n3, normals, target_s=12.0, max
             "sample": "%d of the %d samples (blocks of %d, -r normals path: PES + get_bra + dsyr2k, OpenMP/OpenBLAS on "
                       "all host threads); Sobol skip walk excluded" % (n, SAMPLES, block),
             "split_s": {"pes": float(t[0]), "bra": float(t[1]), "dsyr2k": float(t[2])},
-            "threads": oracle.ref_thread_env()}
+            "threads": oracle.ref_thread_env(), "_M": M, "_n": n}
+
+
+def levels_vs_reference(ref, nw, x0, MUa, omega, normals, precision, device):
+    """The 10 lowest levels of Mout = M/n + HO diagonal from the reference's own
+    build (cpu_reference's matrix, dsyr2k 'U') against the GPU build of the same
+    normals through the -r path, in the benchmark's precision: the level gate
+    of the metric pinned to the reference itself."""
+    import oracle
+    import scp3_b200
+    M, n = ref.pop("_M"), ref.pop("_n")
+    Mref = np.asfortranarray(np.triu(M) + np.triu(M, 1).T) / n
+    oracle.add_ho_diagonal(Mref, omega, 48, 0, 0.0)
+    e_ref = np.linalg.eigvalsh(Mref)[:10]
+    hb = scp3_b200.HBuild(nw, x0, MUa, omega, n2=48, n3=0, pes="qtip4pf", precision=precision,
+                          scramble_seed=SCRAMBLE_SEED, device=device)
+    hb.accumulate_normals(np.ascontiguousarray(normals[:n]))
+    e_gpu = np.linalg.eigvalsh(hb.read(1))[:10]
+    hb.close()
+    autocm = scp3_b200.constants.autocm
+    return {"samples": int(n), "precision": precision,
+            "max_abs_err_cm1": float(np.abs(e_gpu - e_ref).max() * autocm),
+            "lowest10_cm1_reference": [float(x * autocm) for x in e_ref],
+            "note": "the reference's build (oracle/_ref) and the GPU build on the same normals; levels of a "
+                    "2^17-point build are dominated by Monte Carlo noise, so this compares arithmetic, not physics"}
 
 
 def run_standin(args, world, rank):
@@ -969,7 +993,13 @@ def main():
         line["gradient"] = guarded(gradient_record, nw, x0, MUa, omega, 1 << 18, 3)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         normals = scp3_b200.std_normals(nm0, 0, 1 << 17, scramble_seed=SCRAMBLE_SEED)
-        line["cpu_baseline"] = cpu_reference(nw, x0, MUa, omega, np.arange(nm0, dtype=np.int32), 48, 0, normals)
+        cb = cpu_reference(nw, x0, MUa, omega, np.arange(nm0, dtype=np.int32), 48, 0, normals)
+        if cb is not None:
+            line["levels_vs_reference"] = guarded(levels_vs_reference, cb, nw, x0, MUa, omega, normals,
+                                                  args.precision, local)
+            cb.pop("_M", None)
+            cb.pop("_n", None)
+        line["cpu_baseline"] = cb
     if rank == 0:
         print(json.dumps(line))
     hb.close()
