@@ -196,6 +196,7 @@ def cpu_reference(nw, x0, MUa, omega, modes, n2, n3, normals, target_s=12.0, max
     per = max(t.sum(), 1e-6) / n
     n = int(min(max(block * 4, target_s / per), normals.shape[0] if max_samples is None else max_samples))
     n -= n % block
+    M.fill(0.0)          # the timed run's matrix holds its own n samples only
     t0 = time.perf_counter()
     M, t, _ = oracle.ref_hbuild(0, nw, x0, MUa, omega, modes, n2, n3, n, block, normals=normals[:n], fast=fast, M=M)
     wall = time.perf_counter() - t0
