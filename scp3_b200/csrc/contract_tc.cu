@@ -77,10 +77,12 @@ constexpr double kF16Unscale = 1.0 / 4096.0;
 //
 // Accumulation.  One FP32 TMEM accumulator per tile takes all three products
 // (256 columns; two alternate, so a drain overlaps the next run's MMAs).  It is
-// drained every 4 k-blocks (128 K slots, 24 MMAs) into FP32 registers of the
+// drained every 12 k-blocks (384 K slots, 72 MMAs) into FP32 registers of the
 // epilogue threads (one row and 128 columns each), which are added into the
-// unit's own FP64 partial at the unit's end, and every 256 drains (32768 K slots)
-// within longer units.  Each write-back is a read-modify-write of the unit's
+// unit's own FP64 partial at the unit's end, and every 256 drains (98304 K slots)
+// within longer units.  Longer TMEM runs cost accuracy (the hexamer's 10 lowest
+// levels against FP64: 0.049 cm^-1 at 4 k-blocks, 0.054 at 8, 0.063 at 12, 0.073
+// at 16) and save drain hand-offs (contraction time -6 % at 8, -9 % at 12).  Each write-back is a read-modify-write of the unit's
 // 256 KB partial in HBM, so the fewer the better: at one per unit the hexamer
 // pass moves ~0.2 GB of partials per 2^17 samples instead of ~0.5 GB at one per
 // 32 drains, with no measurable change in the levels (the FP32 register sums
@@ -91,7 +93,7 @@ constexpr int kStages2 = 4;
 constexpr int kBox2 = kTile * kBK2 * 2;            // 8 KB: one half of one panel
 constexpr int kStageBytes2 = 6 * kBox2;            // A hi, A lo, B hi x2, B lo x2
 constexpr int kKB2PerFlush = kSlotsPerFlush / kBK2;   // 130
-constexpr int kDrain2 = 4;                          // k-blocks per FP32 TMEM run
+constexpr int kDrain2 = 12;                         // k-blocks per FP32 TMEM run
 constexpr int kL2Drains = 256;                      // runs per FP64 flush (at most)
 constexpr int kSmemBytes2 = kStages2 * kStageBytes2 + 1024 + 256;
 constexpr int kN2 = 2 * kTile;
