@@ -59,14 +59,56 @@ __device__ __forceinline__ T pair(uint32_t task, const T* crd, const T* ms)
     }
 }
 
+// Water pair p of the row-major upper triangle of nw waters: a < b.
+__device__ __forceinline__ void water_pair_of(int p, int nw, int& a, int& b)
+{
+    a = 0;
+    while (p >= nw - 1 - a) {
+        p -= nw - 1 - a;
+        a++;
+    }
+    b = a + 1 + p;
+}
+
+// The ten site pairs of waters a < b that the reference's pair loops visit
+// (qtip4pf.cpp:213-283): the M site of each water against the two H of the
+// other, the four H/H pairs, O/O (Lennard-Jones) and M/M.  The eight sites are
+// read once; each term is formed in T exactly as pair() forms it and summed in
+// FP64.
+template <typename T>
+__device__ __forceinline__ double water_pair(int a, int b, const T* crd, const T* ms)
+{
+    T s[2][4][3];   // [water][O, H1, H2, M][x, y, z]
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+#pragma unroll
+        for (int l = 0; l < 3; l++) s[0][l][k] = crd[9 * a + 3 * l + k], s[1][l][k] = crd[9 * b + 3 * l + k];
+        s[0][3][k] = ms[3 * a + k];
+        s[1][3][k] = ms[3 * b + k];
+    }
+    double e = 0.0;
+#pragma unroll
+    for (int w = 0; w < 2; w++)
+#pragma unroll
+        for (int l = 1; l < 3; l++) e += (double)(T(kQH * kQM) * inv_sqrt(dist2(s[w][3], s[1 - w][l])));
+#pragma unroll
+    for (int l = 1; l < 3; l++)
+#pragma unroll
+        for (int m = 1; m < 3; m++) e += (double)(T(kQH * kQH) * inv_sqrt(dist2(s[0][l], s[1][m])));
+    const T s2 = T(kSigma * kSigma) / dist2(s[0][0], s[1][0]);
+    const T s6 = s2 * s2 * s2;
+    e += (double)(T(4 * kEpsilon) * s6 * (s6 - T(1)));
+    e += (double)(T(kQM * kQM) * inv_sqrt(dist2(s[0][3], s[1][3])));
+    return e;
+}
+
 // Energies of ng <= 4 geometries crd + j * stride (shared memory, T) at once,
 // ms a [4][3nw] shared scratch: lane l works for geometry l % 4 only (M sites and
-// monomers as items (water, geometry), pair terms as items (task, geometry)), so
-// a warp keeps all lanes busy on the per-water terms and the pair tasks of one
-// type run together; lane l returns the sum of geometry l % 4.
+// monomers as items (water, geometry), pair terms as items (water pair,
+// geometry)), so a warp keeps its lanes busy on the per-water and per-pair
+// terms; lane l returns the sum of geometry l % 4.
 template <typename T>
-__device__ double energy_warp4(const T* crd, int stride, T* ms, int nw, int ng, const uint32_t* __restrict__ tasks,
-                               int ntasks, int lane)
+__device__ double energy_warp4(const T* crd, int stride, T* ms, int nw, int ng, int lane)
 {
     const int j = lane & 3;
     const bool on = j < ng;
@@ -82,7 +124,12 @@ __device__ double energy_warp4(const T* crd, int stride, T* ms, int nw, int ng, 
     double part = 0;    // terms in T, their sums in FP64
     if (on) {
         for (int i = lane >> 2; i < nw; i += 8) part += (double)monomer(cj + 9 * i);
-        for (int t = lane >> 2; t < ntasks; t += 8) part += (double)pair(__ldg(tasks + t), cj, mj);
+        const int np = nw * (nw - 1) / 2;
+        for (int p = lane >> 2; p < np; p += 8) {
+            int a, b;
+            water_pair_of(p, nw, a, b);
+            part += water_pair<T>(a, b, cj, mj);
+        }
     }
     part += __shfl_xor_sync(0xffffffffu, part, 4);
     part += __shfl_xor_sync(0xffffffffu, part, 8);
@@ -212,13 +259,65 @@ __device__ inline double energy_grad_warp(const T* crd, T* ms, T* g, T* gm, int 
     return warp_sum(part);
 }
 
+// The ten site pairs of waters a < b with their gradients, as water_pair:
+// each term formed in T as pair_grad() forms it, the forces on the eight sites
+// gathered in registers and added to g (O, H1, H2) and gm (M) once per site.
+template <typename T>
+__device__ __forceinline__ double water_pair_grad(int a, int b, const T* crd, const T* ms, T* g, T* gm)
+{
+    T s[2][4][3], f[2][4][3];   // [water][O, H1, H2, M][x, y, z]: positions, forces
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+#pragma unroll
+        for (int l = 0; l < 3; l++) s[0][l][k] = crd[9 * a + 3 * l + k], s[1][l][k] = crd[9 * b + 3 * l + k];
+        s[0][3][k] = ms[3 * a + k];
+        s[1][3][k] = ms[3 * b + k];
+#pragma unroll
+        for (int l = 0; l < 4; l++) f[0][l][k] = f[1][l][k] = T(0);
+    }
+    double e = 0.0;
+    // q q' / |u - v| with its forces, u = site x of water w, v = site y of water 1 - w
+    auto coulomb = [&](T qq, int w, int x, int y) {
+        const T d0 = s[w][x][0] - s[1 - w][y][0], d1 = s[w][x][1] - s[1 - w][y][1], d2 = s[w][x][2] - s[1 - w][y][2];
+        const T ir = T(1.0) / sqrt(d0 * d0 + d1 * d1 + d2 * d2), eu = qq * ir, fu = -eu * ir * ir;
+        f[w][x][0] += fu * d0, f[w][x][1] += fu * d1, f[w][x][2] += fu * d2;
+        f[1 - w][y][0] -= fu * d0, f[1 - w][y][1] -= fu * d1, f[1 - w][y][2] -= fu * d2;
+        e += (double)eu;
+    };
+#pragma unroll
+    for (int w = 0; w < 2; w++)
+#pragma unroll
+        for (int l = 1; l < 3; l++) coulomb(T(kQH * kQM), w, 3, l);
+#pragma unroll
+    for (int l = 1; l < 3; l++)
+#pragma unroll
+        for (int m = 1; m < 3; m++) coulomb(T(kQH * kQH), 0, l, m);
+    {
+        const T d0 = s[0][0][0] - s[1][0][0], d1 = s[0][0][1] - s[1][0][1], d2 = s[0][0][2] - s[1][0][2];
+        const T r2 = d0 * d0 + d1 * d1 + d2 * d2;
+        const T s2 = T(kSigma * kSigma) / r2, s6 = s2 * s2 * s2;
+        const T fo = T(2.0 * 4 * kEpsilon) * (T(3.0) * s6 - T(6.0) * s6 * s6) / r2;   // 2 dE/d(r^2)
+        f[0][0][0] += fo * d0, f[0][0][1] += fo * d1, f[0][0][2] += fo * d2;
+        f[1][0][0] -= fo * d0, f[1][0][1] -= fo * d1, f[1][0][2] -= fo * d2;
+        e += (double)(T(4 * kEpsilon) * s6 * (s6 - T(1.0)));
+    }
+    coulomb(T(kQM * kQM), 0, 3, 3);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+#pragma unroll
+        for (int l = 0; l < 3; l++) atomicAdd(g + 9 * a + 3 * l + k, f[0][l][k]), atomicAdd(g + 9 * b + 3 * l + k, f[1][l][k]);
+        atomicAdd(gm + 3 * a + k, f[0][3][k]);
+        atomicAdd(gm + 3 * b + k, f[1][3][k]);
+    }
+    return e;
+}
+
 // Energies and gradients of ng <= 4 geometries crd + j * stride at once (the
 // FP32 gradient path): lane l works for geometry l % 4 only, as energy_warp4;
 // ms [4][3nw], g [4][9nw] and gm [4][3nw] are shared scratch, g complete after
 // the call; lane l returns the energy of geometry l % 4.
 template <typename T>
-__device__ double energy_grad_warp4(const T* crd, int stride, T* ms, T* g, T* gm, int nw, int ng,
-                                    const uint32_t* __restrict__ tasks, int ntasks, int lane)
+__device__ double energy_grad_warp4(const T* crd, int stride, T* ms, T* g, T* gm, int nw, int ng, int lane)
 {
     const int j = lane & 3;
     const bool on = j < ng;
@@ -238,7 +337,12 @@ __device__ double energy_grad_warp4(const T* crd, int stride, T* ms, T* g, T* gm
     double part = 0;
     if (on) {
         for (int i = lane >> 2; i < nw; i += 8) part += monomer_grad<T>(cj + 9 * i, gj + 9 * i);
-        for (int t = lane >> 2; t < ntasks; t += 8) part += pair_grad<T>(__ldg(tasks + t), cj, mj, gj, gmj);
+        const int np = nw * (nw - 1) / 2;
+        for (int p = lane >> 2; p < np; p += 8) {
+            int a, b;
+            water_pair_of(p, nw, a, b);
+            part += water_pair_grad<T>(a, b, cj, mj, gj, gmj);
+        }
     }
     __syncwarp();
     if (on)

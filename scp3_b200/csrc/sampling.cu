@@ -363,7 +363,7 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
         // qTIP4P/f energies of the whole group in one warp pass
         double e4 = 0.0;
         if constexpr (PES == SCP3GPU_PES_QTIP4PF) {
-            if (!a.skip_pes && !grad) e4 = qt::energy_warp4<T>(w.crd, N3, w.ms, nw, gn, a.tasks, a.ntasks, lane);
+            if (!a.skip_pes && !grad) e4 = qt::energy_warp4<T>(w.crd, N3, w.ms, nw, gn, lane);
         }
         if constexpr (PES == SCP3GPU_PES_QTIP4PF && sizeof(T) == 4) {
             if (grad) {
@@ -372,7 +372,7 @@ __device__ __forceinline__ void samples_body(const SampleArgs& a, char* smem)
                 // group's (sample, mode) items over the lanes, summed in FP64
                 T* g4 = reinterpret_cast<T*>(w.g);
                 T* gm4 = g4 + 4 * 9 * nw;
-                e4 = qt::energy_grad_warp4<T>(w.crd, N3, w.ms, g4, gm4, nw, gn, a.tasks, a.ntasks, lane);
+                e4 = qt::energy_grad_warp4<T>(w.crd, N3, w.ms, g4, gm4, nw, gn, lane);
                 for (int it = lane; it < gn * a.nm; it += 32) {
                     const int j = it / a.nm, m = it - j * a.nm;
                     const int k = __ldg(a.modes + m);
