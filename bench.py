@@ -45,8 +45,8 @@ METRIC = "Sobol samples/s (hexamer H-build) at <=0.1 cm^-1 on 10 lowest levels v
 FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (vector and tensor) nominal; no measured FP64 peak on this pool
 # DRAM bytes (read + write) of the BF16x3 contraction on the hexamer doubles basis, from an ncu
 # capture of one 2^18-sample pass (one launch of 140 CTAs: dram__bytes_read.sum +
-# dram__bytes_write.sum = 1447.6 + 42.2 MB); per launch it grows with the samples the launch covers
-CONTRACT_DRAM_BYTES_PER_SAMPLE = (1447.607808e6 + 42.220288e6) / 262144
+# dram__bytes_write.sum = 1522.6 + 11.8 MB); per launch it grows with the samples the launch covers
+CONTRACT_DRAM_BYTES_PER_SAMPLE = (1522.616320e6 + 11.786240e6) / 262144
 
 
 def load_peaks():
