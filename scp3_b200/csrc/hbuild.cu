@@ -287,10 +287,11 @@ int zero_sums(scp3gpu_hbuild* h)
 // The -r path for normals of type T (double, or float for the FP32 entry): the
 // host buffer goes in piece by piece into two device buffers (FP64-sized, so
 // either type fits), each copy on the copy stream overlapped with the previous
-// piece's pass.  The first copy overlaps nothing, so the pieces ramp up from
-// 2^15 samples, doubling after the second piece, to 2^17 samples (at ~50 GB/s
-// a piece's FP32 normals then copy in about half its pass, and the last pass,
-// which follows its copy, stays short).
+// piece's pass.  The first copy overlaps nothing, so the pieces ramp up: 2^15,
+// 2^15, 2^16, 2^17, 2^17, then 2^18 samples (at ~50 GB/s a piece's FP32
+// normals copy in about 0.7 of its pass; the second 2^17 piece lets the copies
+// get ahead before they double again, and the longer pieces after it make
+// fewer passes).
 template <typename T>
 int accumulate_host_normals(scp3gpu_hbuild* h, const T* normals, int64_t n, const char* who)
 {
@@ -318,7 +319,8 @@ int accumulate_host_normals(scp3gpu_hbuild* h, const T* normals, int64_t n, cons
     };
     int k = 0;
     for (int64_t off = 0, c = 0; off < n && rc == SCP3GPU_OK; off += c, k++) {
-        const int64_t part = (int64_t)1 << std::min(17, 15 + (k > 0 ? k - 1 : 0));
+        static const int kRamp[] = {15, 15, 16, 17, 17};
+        const int64_t part = (int64_t)1 << (k < 5 ? kRamp[k] : 18);
         c = std::min(std::min(h->chunk, part), n - off);
         if ((rc = step(off, c, k & 1)) == SCP3GPU_OK) h->count += c;
     }
