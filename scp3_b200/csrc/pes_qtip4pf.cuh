@@ -60,7 +60,7 @@ __device__ __forceinline__ T pair(uint32_t task, const T* crd, const T* ms)
 }
 
 // Water pair p of the row-major upper triangle of nw waters: a < b.
-__device__ __forceinline__ void water_pair_of(int p, int nw, int& a, int& b)
+__host__ __device__ __forceinline__ void water_pair_of(int p, int nw, int& a, int& b)
 {
     a = 0;
     while (p >= nw - 1 - a) {

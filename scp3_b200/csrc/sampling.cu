@@ -792,3 +792,13 @@ int launch_std_normal(int dims, int64_t index0, int64_t n, const int64_t* vdir, 
 }
 
 }  // namespace scp3
+
+// Host-only view of the water-pair items of the four-sample qTIP4P/f kernels, for
+// tests: ab[2 p], ab[2 p + 1] = the waters a < b of pair p, p < nw (nw - 1) / 2.
+extern "C" int scp3gpu_internal_water_pairs(int nw, int* ab)
+{
+    if (nw < 1 || nw > 64 || !ab) return SCP3GPU_ERR_ARG;
+    const int np = nw * (nw - 1) / 2;
+    for (int p = 0; p < np; p++) scp3::qt::water_pair_of(p, nw, ab[2 * p], ab[2 * p + 1]);
+    return SCP3GPU_OK;
+}
